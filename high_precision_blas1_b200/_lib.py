@@ -1,0 +1,123 @@
+"""ctypes binding of libhpblas1.so (the C ABI declared in include/hpblas1.h).
+
+The library is built in-tree by ``high_precision_blas1_b200.build``.  There
+is no fallback: if the shared object is missing or fails to load, importing
+this module raises, so no caller can silently run without the CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libhpblas1.so"
+
+TYPES = ("f32", "f64", "c64", "c128")
+
+
+class hpb_c64(C.Structure):
+    _fields_ = [("re", C.c_float), ("im", C.c_float)]
+
+
+class hpb_c128(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+SCALAR = {"f32": C.c_float, "f64": C.c_double, "c64": hpb_c64, "c128": hpb_c128}
+
+STATUS = {
+    0: "HPB_SUCCESS",
+    -1: "HPB_ERROR_INVALID_VALUE",
+    -2: "HPB_ERROR_CUDA",
+    -3: "HPB_ERROR_OUT_OF_MEMORY",
+    -4: "HPB_ERROR_NOT_SUPPORTED",
+    -5: "HPB_ERROR_BREAKDOWN",
+    -6: "HPB_ERROR_NOT_FINITE",
+    -7: "HPB_ERROR_NOT_CONVERGED",
+}
+
+
+class HpbError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python -m high_precision_blas1_b200.build` "
+            "(there is no CPU fallback)")
+    return C.CDLL(str(LIB_PATH))
+
+
+lib = _load()
+
+P = C.c_void_p
+I64 = C.c_int64
+I32 = C.c_int32
+
+
+def _sig(name, res, args):
+    f = getattr(lib, name)
+    f.restype = res
+    f.argtypes = args
+    return f
+
+
+# context / errors
+_sig("hpb_create", C.c_int, [C.POINTER(P), C.c_int, P])
+_sig("hpb_destroy", C.c_int, [P])
+_sig("hpb_set_stream", C.c_int, [P, P])
+_sig("hpb_get_stream", P, [P])
+_sig("hpb_synchronize", C.c_int, [P])
+_sig("hpb_status_string", C.c_char_p, [C.c_int])
+_sig("hpb_last_error", C.c_char_p, [P])
+_sig("hpb_version", C.c_int, [C.POINTER(C.c_int)] * 3)
+_sig("hpb_launch_count", C.c_uint64, [])
+
+# reductions
+for t in TYPES:
+    for op in ("dot2", "dot"):
+        _sig(f"hpb_{op}_{t}", C.c_int, [P, I64, P, P, P])
+        _sig(f"hpb_{op}_{t}_host", C.c_int, [P, I64, P, P, P])
+    for op in ("sum2", "asum2", "nrm2", "asum", "nrm2plain"):
+        _sig(f"hpb_{op}_{t}", C.c_int, [P, I64, P, P])
+        _sig(f"hpb_{op}_{t}_host", C.c_int, [P, I64, P, P])
+
+# elementwise
+for t in TYPES:
+    S = SCALAR[t]
+    _sig(f"hpb_axpy_{t}", C.c_int, [P, I64, S, P, P])
+    _sig(f"hpb_axpby_{t}", C.c_int, [P, I64, S, P, S, P])
+    _sig(f"hpb_lincomb2_{t}", C.c_int, [P, I64, S, P, S, P, P])
+    _sig(f"hpb_axpbypcz_{t}", C.c_int, [P, I64, S, P, S, P, S, P])
+    _sig(f"hpb_axpbypcwpdz_{t}", C.c_int, [P, I64, S, P, S, P, S, P, S, P])
+    _sig(f"hpb_lincomb4_{t}", C.c_int, [P, I64, S, P, S, P, S, P, S, P, P])
+    _sig(f"hpb_scal_{t}", C.c_int, [P, I64, S, P, P])
+    _sig(f"hpb_add_scalar_{t}", C.c_int, [P, I64, S, S, P])
+    _sig(f"hpb_fill_{t}", C.c_int, [P, I64, S, P])
+    _sig(f"hpb_mul_pointwise_{t}", C.c_int, [P, I64, S, P, S, P, P])
+    _sig(f"hpb_div_pointwise_{t}", C.c_int, [P, I64, S, P, S, P, P])
+    _sig(f"hpb_abs_{t}", C.c_int, [P, I64, P, P])
+    _sig(f"hpb_isfinite_{t}", C.c_int, [P, I64, P, C.POINTER(C.c_int)])
+    _sig(f"hpb_csr_spmv_{t}", C.c_int, [P, I32, I32, I64, P, P, P, S, P, S, P])
+_sig("hpb_gendot_f64", C.c_int, [C.c_uint64, I64, C.c_double, P, P, C.POINTER(C.c_int64)])
+_sig("hpb_gendot_c128", C.c_int, [C.c_uint64, I64, C.c_double, P, P])
+_sig("hpb_copy", C.c_int, [P, I64, C.c_size_t, P, P])
+_sig("hpb_swap", C.c_int, [P, I64, C.c_size_t, P, P])
+
+
+def scalar(t: str, v):
+    """Convert a Python number to the C scalar type of element type t."""
+    if t in ("c64", "c128"):
+        v = complex(v)
+        return SCALAR[t](v.real, v.imag)
+    return SCALAR[t](float(v))
+
+
+def exported_symbols() -> list[str]:
+    """Names declared in include/hpblas1.h (parsed from the header)."""
+    import re
+    hdr = Path(__file__).resolve().parent.parent / "include" / "hpblas1.h"
+    txt = hdr.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|void\*|const char\*|uint64_t)\s+(hpb_\w+)\s*\(", txt, re.M)))

@@ -1,0 +1,109 @@
+"""Build libhpblas1.so in-tree for sm_100a.
+
+Usage: python -m high_precision_blas1_b200.build [--force] [-j N]
+
+Every .cu/.cpp file under csrc/ is compiled to an object in _build/ and the
+objects are linked into high_precision_blas1_b200/lib/libhpblas1.so.  nvcc
+cross-compiles for sm_100a without a GPU, so this runs on CPU-only hosts.
+A file is recompiled when it, or any header under csrc/ or include/, is
+newer than its object.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+BUILD = ROOT / "_build" / "hpblas1"
+LIBDIR = PKG / "lib"
+LIB = LIBDIR / "libhpblas1.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + [
+    "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
+    "-Xcompiler", "-fPIC,-O2,-fno-fast-math,-ffp-contract=off",
+    "-I", str(INCLUDE), "-I", str(CSRC),
+]
+
+
+def nvcc() -> str:
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build libhpblas1")
+    return cand
+
+
+def _headers() -> list[Path]:
+    hs = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.rglob("*.h"))
+    return hs
+
+
+def _stale(obj: Path, src: Path, headers: list[Path]) -> bool:
+    if not obj.exists():
+        return True
+    t = obj.stat().st_mtime
+    if src.stat().st_mtime > t:
+        return True
+    return any(h.stat().st_mtime > t for h in headers)
+
+
+def _compile(src: Path, obj: Path) -> None:
+    cmd = [nvcc()] + NVCC_FLAGS + ["-c", str(src), "-o", str(obj)]
+    if src.suffix == ".cpp":
+        cmd = [nvcc(), "-x", "cu"] + NVCC_FLAGS + ["-c", str(src), "-o", str(obj)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+
+
+def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> Path:
+    BUILD.mkdir(parents=True, exist_ok=True)
+    LIBDIR.mkdir(parents=True, exist_ok=True)
+    headers = _headers()
+    srcs = sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
+    objs = []
+    todo = []
+    for s in srcs:
+        o = BUILD / (s.stem + ".o")
+        objs.append(o)
+        if force or _stale(o, s, headers):
+            todo.append((s, o))
+    if todo:
+        n = jobs or min(len(todo), os.cpu_count() or 4)
+        with cf.ThreadPoolExecutor(max_workers=n) as ex:
+            futs = {ex.submit(_compile, s, o): s for s, o in todo}
+            for f in cf.as_completed(futs):
+                f.result()
+                if verbose:
+                    print("compiled", futs[f].name)
+    if todo or force or not LIB.exists() or any(o.stat().st_mtime > LIB.stat().st_mtime for o in objs):
+        tmp = LIB.with_suffix(".so.tmp")
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + [str(o) for o in objs] + ["-lcudart"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, LIB)
+        if verbose:
+            print("linked", LIB)
+    return LIB
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("-j", type=int, default=None)
+    a = ap.parse_args(argv)
+    build(force=a.force, jobs=a.j, verbose=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

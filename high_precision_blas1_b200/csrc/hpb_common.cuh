@@ -1,0 +1,143 @@
+// Shared definitions of libhpblas1: context, status plumbing, scalar types
+// and the error-free transformations (TwoSum, TwoProd) of the
+// Ogita-Rump-Oishi algorithms.
+//
+// Every floating-point operation inside the error-free transformations uses
+// the explicit round-to-nearest intrinsics (__dadd_rn, __dmul_rn, __fma_rn,
+// ...).  nvcc contracts a*b+c into an FMA by default; such a contraction of
+// "s + a*b" would make the TwoSum error term describe a different rounding
+// than the one that produced s and silently lose the compensation.  The
+// intrinsics are never contracted.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <atomic>
+
+#include "../../include/hpblas1.h"
+
+struct hpb_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    int max_blocks = 0;          // partials capacity (blocks of a reduction)
+    void* partials = nullptr;    // device: max_blocks * 32 bytes
+    unsigned int* ticket = nullptr;  // device: last-block-done counters
+    double* result_slot = nullptr;   // device: 16 doubles for blocking calls
+    double* host_slot = nullptr;     // pinned host: 16 doubles
+    int* flag_dev = nullptr;         // device: flags for isfinite
+    char last_error[512] = {0};
+};
+
+namespace hpb {
+
+extern std::atomic<uint64_t> g_launches;
+
+inline void count_launch(uint64_t k = 1) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+
+int set_error(hpb_context* ctx, int status, const char* fmt, ...);
+int check_launch(hpb_context* ctx, const char* what);
+
+#define HPB_CHECK_CTX(ctx)                                                      \
+    do {                                                                        \
+        if ((ctx) == nullptr) return HPB_ERROR_INVALID_VALUE;                   \
+    } while (0)
+
+#define HPB_CUDA_TRY(ctx, call)                                                 \
+    do {                                                                        \
+        cudaError_t e__ = (call);                                               \
+        if (e__ != cudaSuccess)                                                 \
+            return hpb::set_error((ctx), HPB_ERROR_CUDA, "%s: %s (%s:%d)", #call, \
+                                  cudaGetErrorString(e__), __FILE__, __LINE__); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Element types.  Complex values are stored interleaved (re, im) with the
+// natural 8/16-byte alignment of float2/double2.
+// ---------------------------------------------------------------------------
+struct cf { float re, im; };
+struct __align__(16) cd { double re, im; };
+
+// Element load/store for the unaligned (scalar) paths: a complex<double>
+// that is only 8-byte aligned is moved as two doubles, never as one 16-byte
+// access.
+template <class E>
+__device__ __forceinline__ E ldE(const E* p, int64_t i) { return p[i]; }
+template <>
+__device__ __forceinline__ cd ldE<cd>(const cd* p, int64_t i) {
+    const double* q = reinterpret_cast<const double*>(p) + 2 * i;
+    return cd{q[0], q[1]};
+}
+template <class E>
+__device__ __forceinline__ void stE(E* p, int64_t i, E v) { p[i] = v; }
+template <>
+__device__ __forceinline__ void stE<cd>(cd* p, int64_t i, cd v) {
+    double* q = reinterpret_cast<double*>(p) + 2 * i;
+    q[0] = v.re;
+    q[1] = v.im;
+}
+
+template <class T> struct real_of { using type = T; };
+template <> struct real_of<cf> { using type = float; };
+template <> struct real_of<cd> { using type = double; };
+
+template <class T> struct is_cplx { static constexpr bool value = false; };
+template <> struct is_cplx<cf> { static constexpr bool value = true; };
+template <> struct is_cplx<cd> { static constexpr bool value = true; };
+
+// ---------------------------------------------------------------------------
+// Round-to-nearest arithmetic that the compiler may not contract.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// Knuth's TwoSum: s = fl(a+b) and the exact error e with a + b = s + e
+// (6 flops, no branch, valid for any ordering of |a|, |b|).
+template <class R>
+__device__ __forceinline__ R two_sum(R a, R b, R& e) {
+    R s = add_rn(a, b);
+    R bv = sub_rn(s, a);
+    R av = sub_rn(s, bv);
+    e = add_rn(sub_rn(b, bv), sub_rn(a, av));
+    return s;
+}
+
+// TwoProd with FMA: p = fl(a*b), e = a*b - p exactly.
+template <class R>
+__device__ __forceinline__ R two_prod(R a, R b, R& e) {
+    R p = mul_rn(a, b);
+    e = fma_rn(a, b, -p);
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// Complex helpers (plain arithmetic; used by elementwise kernels)
+// ---------------------------------------------------------------------------
+template <class T> __host__ __device__ __forceinline__ T cmul(T a, T b) {
+    return T{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <class T> __host__ __device__ __forceinline__ T cadd(T a, T b) { return T{a.re + b.re, a.im + b.im}; }
+template <class T> __host__ __device__ __forceinline__ T cdiv(T a, T b) {
+    using R = decltype(a.re);
+    R d = b.re * b.re + b.im * b.im;
+    return T{(a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d};
+}
+
+// Grid sizing shared by all kernels.
+inline int grid_for(const hpb_context* ctx, int64_t work_items, int threads, int per_sm) {
+    int64_t blocks = (work_items + threads - 1) / threads;
+    int64_t cap = int64_t(ctx->num_sms) * per_sm;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    return int(blocks);
+}
+
+}  // namespace hpb

@@ -1,0 +1,275 @@
+/*
+ * hpblas1.h -- C ABI of the B200 compensated BLAS-1 library (libhpblas1.so).
+ *
+ * Every entry point takes plain pointers and sizes.  Device pointers are
+ * CUDA device addresses on the context's device; "host" in a name means the
+ * result is written to host memory and the call blocks until it is there.
+ * All calls return 0 (HPB_SUCCESS) or a negative hpb_status; the message of
+ * the last failure on a context is available from hpb_last_error().
+ *
+ * Layouts:
+ *   f32/f64   : float / double arrays.
+ *   c64/c128  : interleaved complex arrays (re, im), the layout of
+ *               thrust::complex<float|double>, cuComplex and std::complex.
+ *   reduction results (device or host buffers of doubles):
+ *     real    : out[0] = hi, out[1] = lo            (2 doubles)
+ *     complex : out[0..1] = hi (re, im), out[2..3] = lo (re, im)  (4 doubles)
+ *   hi is the rounded result, lo the rounding error of hi, so hi + lo is the
+ *   unevaluated double-double value of the compensated reduction.  Float and
+ *   complex<float> reductions combine their per-block (sum, error) pairs in
+ *   binary64, so their hi/lo are doubles too.
+ *
+ * Context: one hpb_context per (device, stream, host thread).  It owns the
+ * O(#SM) partials buffer, the ticket counter of the single-pass cross-block
+ * combine and a pinned result slot; calls on one context are stream-ordered
+ * and must not be issued concurrently from several host threads.
+ *
+ * Each function names the reference interface it replaces (paths relative to
+ * the reference's source/ directory).
+ */
+#ifndef HPBLAS1_H
+#define HPBLAS1_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HPB_VERSION_MAJOR 0
+#define HPB_VERSION_MINOR 1
+#define HPB_VERSION_PATCH 0
+
+typedef enum hpb_status {
+    HPB_SUCCESS = 0,
+    HPB_ERROR_INVALID_VALUE = -1,   /* bad size, null pointer, bad argument */
+    HPB_ERROR_CUDA = -2,            /* a CUDA runtime call failed */
+    HPB_ERROR_OUT_OF_MEMORY = -3,   /* device or pinned allocation failed */
+    HPB_ERROR_NOT_SUPPORTED = -4,   /* option the library does not provide */
+    HPB_ERROR_BREAKDOWN = -5,       /* solver breakdown (rho == 0, ...) */
+    HPB_ERROR_NOT_FINITE = -6,      /* NaN/Inf met where a finite value is required */
+    HPB_ERROR_NOT_CONVERGED = -7    /* solver stopped at max_iters above tolerance */
+} hpb_status;
+
+typedef struct hpb_context hpb_context;
+
+typedef struct hpb_c64 { float re, im; } hpb_c64;
+typedef struct hpb_c128 { double re, im; } hpb_c128;
+
+/* ---------------------------------------------------------------------- */
+/* Context, errors, version                                                */
+/* ---------------------------------------------------------------------- */
+
+/* Creates a context on `device` bound to `stream` (a cudaStream_t, NULL for
+ * the legacy default stream).  Replaces the per-object helper buffers that
+ * common/ogita/gpu_reduction_ogita.h:44-52 allocates (4 n-sized arrays). */
+int hpb_create(hpb_context** ctx, int device, void* stream);
+int hpb_destroy(hpb_context* ctx);
+int hpb_set_stream(hpb_context* ctx, void* stream);
+void* hpb_get_stream(const hpb_context* ctx);
+int hpb_synchronize(hpb_context* ctx);
+const char* hpb_status_string(int status);
+const char* hpb_last_error(const hpb_context* ctx);
+int hpb_version(int* major, int* minor, int* patch);
+/* Number of kernels this library has launched in this process (all
+ * contexts); used by harnesses to count launches in a timed region. */
+uint64_t hpb_launch_count(void);
+
+/* ---------------------------------------------------------------------- */
+/* Compensated reductions (Ogita-Rump-Oishi Sum2 / Dot2), device results   */
+/* ---------------------------------------------------------------------- */
+/* Dot2: sum_i conj(x_i) * y_i with TwoProd (FMA) + TwoSum, (sum, error)
+ * pairs carried through every tree level, one launch, deterministic.
+ * Replaces gpu_reduction_ogita<T>::dot (common/ogita/gpu_reduction_ogita.h:85-89,
+ * kernel common/ogita/gpu_reduction_ogita_impl.cuh:471-676, host combine
+ * :1227-1282).  `out` is a device buffer (layout above). */
+int hpb_dot2_f32(hpb_context* ctx, int64_t n, const float* x, const float* y, double* out);
+int hpb_dot2_f64(hpb_context* ctx, int64_t n, const double* x, const double* y, double* out);
+int hpb_dot2_c64(hpb_context* ctx, int64_t n, const void* x, const void* y, double* out);
+int hpb_dot2_c128(hpb_context* ctx, int64_t n, const void* x, const void* y, double* out);
+
+/* Sum2: sum_i x_i (gpu_reduction_ogita<T>::sum, gpu_reduction_ogita.h:74-78,
+ * kernel gpu_reduction_ogita_impl.cuh:248-468). */
+int hpb_sum2_f32(hpb_context* ctx, int64_t n, const float* x, double* out);
+int hpb_sum2_f64(hpb_context* ctx, int64_t n, const double* x, double* out);
+int hpb_sum2_c64(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_sum2_c128(hpb_context* ctx, int64_t n, const void* x, double* out);
+
+/* asum2: sum_i |x_i| for real, sum_i (|re_i| + |im_i|) for complex, with
+ * TwoSum on every addition; real result (2 doubles).  Replaces
+ * gpu_reduction_ogita<T>::asum (gpu_reduction_ogita.h:79-84, kernel
+ * gpu_reduction_ogita_impl.cuh:35-246, complex |re|+|im| at
+ * gpu_reduction_ogita_impl_functions.cuh:224-243). */
+int hpb_asum2_f32(hpb_context* ctx, int64_t n, const float* x, double* out);
+int hpb_asum2_f64(hpb_context* ctx, int64_t n, const double* x, double* out);
+int hpb_asum2_c64(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_asum2_c128(hpb_context* ctx, int64_t n, const void* x, double* out);
+
+/* nrm2 = sqrt(Re Dot2(x, x)), reading x once.  out[0] = the norm,
+ * out[1] = hi of the compensated sum of squares, out[2] = its lo.
+ * Replaces gpu_reduction_ogita<T>::norm (gpu_reduction_ogita.h:91-96). */
+int hpb_nrm2_f32(hpb_context* ctx, int64_t n, const float* x, double* out);
+int hpb_nrm2_f64(hpb_context* ctx, int64_t n, const double* x, double* out);
+int hpb_nrm2_c64(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_nrm2_c128(hpb_context* ctx, int64_t n, const void* x, double* out);
+
+/* Plain ("standard precision") reductions: one FMA per term, plain tree,
+ * same output layout with lo = 0.  Replace the cuBLAS ?dot/?dotc, ?asum and
+ * ?nrm2 calls of the standard path (external_libraries/cublas_wrap.h:520-590). */
+int hpb_dot_f32(hpb_context* ctx, int64_t n, const float* x, const float* y, double* out);
+int hpb_dot_f64(hpb_context* ctx, int64_t n, const double* x, const double* y, double* out);
+int hpb_dot_c64(hpb_context* ctx, int64_t n, const void* x, const void* y, double* out);
+int hpb_dot_c128(hpb_context* ctx, int64_t n, const void* x, const void* y, double* out);
+int hpb_asum_f32(hpb_context* ctx, int64_t n, const float* x, double* out);
+int hpb_asum_f64(hpb_context* ctx, int64_t n, const double* x, double* out);
+int hpb_asum_c64(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_asum_c128(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_nrm2plain_f32(hpb_context* ctx, int64_t n, const float* x, double* out);
+int hpb_nrm2plain_f64(hpb_context* ctx, int64_t n, const double* x, double* out);
+int hpb_nrm2plain_c64(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_nrm2plain_c128(hpb_context* ctx, int64_t n, const void* x, double* out);
+
+/* Blocking variants: same computation, result copied to the HOST buffer
+ * `out` (through the context's pinned slot) before returning.  These are
+ * what the by-value C++ drop-in calls (gpu_vector_operations.h:257-340). */
+int hpb_dot2_f32_host(hpb_context* ctx, int64_t n, const float* x, const float* y, double* out);
+int hpb_dot2_f64_host(hpb_context* ctx, int64_t n, const double* x, const double* y, double* out);
+int hpb_dot2_c64_host(hpb_context* ctx, int64_t n, const void* x, const void* y, double* out);
+int hpb_dot2_c128_host(hpb_context* ctx, int64_t n, const void* x, const void* y, double* out);
+int hpb_sum2_f32_host(hpb_context* ctx, int64_t n, const float* x, double* out);
+int hpb_sum2_f64_host(hpb_context* ctx, int64_t n, const double* x, double* out);
+int hpb_sum2_c64_host(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_sum2_c128_host(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_asum2_f32_host(hpb_context* ctx, int64_t n, const float* x, double* out);
+int hpb_asum2_f64_host(hpb_context* ctx, int64_t n, const double* x, double* out);
+int hpb_asum2_c64_host(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_asum2_c128_host(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_nrm2_f32_host(hpb_context* ctx, int64_t n, const float* x, double* out);
+int hpb_nrm2_f64_host(hpb_context* ctx, int64_t n, const double* x, double* out);
+int hpb_nrm2_c64_host(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_nrm2_c128_host(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_dot_f32_host(hpb_context* ctx, int64_t n, const float* x, const float* y, double* out);
+int hpb_dot_f64_host(hpb_context* ctx, int64_t n, const double* x, const double* y, double* out);
+int hpb_dot_c64_host(hpb_context* ctx, int64_t n, const void* x, const void* y, double* out);
+int hpb_dot_c128_host(hpb_context* ctx, int64_t n, const void* x, const void* y, double* out);
+int hpb_asum_f32_host(hpb_context* ctx, int64_t n, const float* x, double* out);
+int hpb_asum_f64_host(hpb_context* ctx, int64_t n, const double* x, double* out);
+int hpb_asum_c64_host(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_asum_c128_host(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_nrm2plain_f32_host(hpb_context* ctx, int64_t n, const float* x, double* out);
+int hpb_nrm2plain_f64_host(hpb_context* ctx, int64_t n, const double* x, double* out);
+int hpb_nrm2plain_c64_host(hpb_context* ctx, int64_t n, const void* x, double* out);
+int hpb_nrm2plain_c128_host(hpb_context* ctx, int64_t n, const void* x, double* out);
+
+/* ---------------------------------------------------------------------- */
+/* Elementwise BLAS-1 (common/gpu_vector_operations_impl.cuh:35-528 and    */
+/* the cuBLAS axpy/scal/copy/swap of common/gpu_vector_operations.h:433-462)*/
+/* ---------------------------------------------------------------------- */
+/* y := a*x + y                      (add_mul(a,x,y), cuBLAS axpy) */
+int hpb_axpy_f32(hpb_context* ctx, int64_t n, float a, const float* x, float* y);
+int hpb_axpy_f64(hpb_context* ctx, int64_t n, double a, const double* x, double* y);
+int hpb_axpy_c64(hpb_context* ctx, int64_t n, hpb_c64 a, const void* x, void* y);
+int hpb_axpy_c128(hpb_context* ctx, int64_t n, hpb_c128 a, const void* x, void* y);
+/* y := a*x + b*y                    (add_mul(a,x,b,y), impl.cuh add_mul_kernel) */
+int hpb_axpby_f32(hpb_context* ctx, int64_t n, float a, const float* x, float b, float* y);
+int hpb_axpby_f64(hpb_context* ctx, int64_t n, double a, const double* x, double b, double* y);
+int hpb_axpby_c64(hpb_context* ctx, int64_t n, hpb_c64 a, const void* x, hpb_c64 b, void* y);
+int hpb_axpby_c128(hpb_context* ctx, int64_t n, hpb_c128 a, const void* x, hpb_c128 b, void* y);
+/* z := a*x + b*y                    (assign_mul(a,x,b,y,z)) */
+int hpb_lincomb2_f32(hpb_context* ctx, int64_t n, float a, const float* x, float b, const float* y, float* z);
+int hpb_lincomb2_f64(hpb_context* ctx, int64_t n, double a, const double* x, double b, const double* y, double* z);
+int hpb_lincomb2_c64(hpb_context* ctx, int64_t n, hpb_c64 a, const void* x, hpb_c64 b, const void* y, void* z);
+int hpb_lincomb2_c128(hpb_context* ctx, int64_t n, hpb_c128 a, const void* x, hpb_c128 b, const void* y, void* z);
+/* z := a*x + b*y + c*z              (add_mul 3-term) */
+int hpb_axpbypcz_f32(hpb_context* ctx, int64_t n, float a, const float* x, float b, const float* y, float c, float* z);
+int hpb_axpbypcz_f64(hpb_context* ctx, int64_t n, double a, const double* x, double b, const double* y, double c, double* z);
+int hpb_axpbypcz_c64(hpb_context* ctx, int64_t n, hpb_c64 a, const void* x, hpb_c64 b, const void* y, hpb_c64 c, void* z);
+int hpb_axpbypcz_c128(hpb_context* ctx, int64_t n, hpb_c128 a, const void* x, hpb_c128 b, const void* y, hpb_c128 c, void* z);
+/* z := a*x + b*y + c*w + d*z        (add_mul 4-term) */
+int hpb_axpbypcwpdz_f32(hpb_context* ctx, int64_t n, float a, const float* x, float b, const float* y, float c, const float* w, float d, float* z);
+int hpb_axpbypcwpdz_f64(hpb_context* ctx, int64_t n, double a, const double* x, double b, const double* y, double c, const double* w, double d, double* z);
+int hpb_axpbypcwpdz_c64(hpb_context* ctx, int64_t n, hpb_c64 a, const void* x, hpb_c64 b, const void* y, hpb_c64 c, const void* w, hpb_c64 d, void* z);
+int hpb_axpbypcwpdz_c128(hpb_context* ctx, int64_t n, hpb_c128 a, const void* x, hpb_c128 b, const void* y, hpb_c128 c, const void* w, hpb_c128 d, void* z);
+/* z := a*x + b*y + c*v + d*w        (assign_mul 4-term) */
+int hpb_lincomb4_f32(hpb_context* ctx, int64_t n, float a, const float* x, float b, const float* y, float c, const float* v, float d, const float* w, float* z);
+int hpb_lincomb4_f64(hpb_context* ctx, int64_t n, double a, const double* x, double b, const double* y, double c, const double* v, double d, const double* w, double* z);
+int hpb_lincomb4_c64(hpb_context* ctx, int64_t n, hpb_c64 a, const void* x, hpb_c64 b, const void* y, hpb_c64 c, const void* v, hpb_c64 d, const void* w, void* z);
+int hpb_lincomb4_c128(hpb_context* ctx, int64_t n, hpb_c128 a, const void* x, hpb_c128 b, const void* y, hpb_c128 c, const void* v, hpb_c128 d, const void* w, void* z);
+/* y := a*x  (assign_mul(a,x,y)); y may alias x, giving x := a*x (scale) */
+int hpb_scal_f32(hpb_context* ctx, int64_t n, float a, const float* x, float* y);
+int hpb_scal_f64(hpb_context* ctx, int64_t n, double a, const double* x, double* y);
+int hpb_scal_c64(hpb_context* ctx, int64_t n, hpb_c64 a, const void* x, void* y);
+int hpb_scal_c128(hpb_context* ctx, int64_t n, hpb_c128 a, const void* x, void* y);
+/* x := a*x + s                      (add_mul_scalar(s, a, x)) */
+int hpb_add_scalar_f32(hpb_context* ctx, int64_t n, float s, float a, float* x);
+int hpb_add_scalar_f64(hpb_context* ctx, int64_t n, double s, double a, double* x);
+int hpb_add_scalar_c64(hpb_context* ctx, int64_t n, hpb_c64 s, hpb_c64 a, void* x);
+int hpb_add_scalar_c128(hpb_context* ctx, int64_t n, hpb_c128 s, hpb_c128 a, void* x);
+/* x := s                            (assign_scalar) */
+int hpb_fill_f32(hpb_context* ctx, int64_t n, float s, float* x);
+int hpb_fill_f64(hpb_context* ctx, int64_t n, double s, double* x);
+int hpb_fill_c64(hpb_context* ctx, int64_t n, hpb_c64 s, void* x);
+int hpb_fill_c128(hpb_context* ctx, int64_t n, hpb_c128 s, void* x);
+/* y := x (assign, cuBLAS copy) ; x <-> y (swap); `elem_bytes` 4, 8 or 16 */
+int hpb_copy(hpb_context* ctx, int64_t n, size_t elem_bytes, const void* x, void* y);
+int hpb_swap(hpb_context* ctx, int64_t n, size_t elem_bytes, void* x, void* y);
+/* z := (a*x) .* (b*y) ; x := x .* (b*y)      (mul_pointwise, 2 overloads) */
+int hpb_mul_pointwise_f32(hpb_context* ctx, int64_t n, float a, const float* x, float b, const float* y, float* z);
+int hpb_mul_pointwise_f64(hpb_context* ctx, int64_t n, double a, const double* x, double b, const double* y, double* z);
+int hpb_mul_pointwise_c64(hpb_context* ctx, int64_t n, hpb_c64 a, const void* x, hpb_c64 b, const void* y, void* z);
+int hpb_mul_pointwise_c128(hpb_context* ctx, int64_t n, hpb_c128 a, const void* x, hpb_c128 b, const void* y, void* z);
+/* z := (a*x) ./ (b*y)                        (div_pointwise) */
+int hpb_div_pointwise_f32(hpb_context* ctx, int64_t n, float a, const float* x, float b, const float* y, float* z);
+int hpb_div_pointwise_f64(hpb_context* ctx, int64_t n, double a, const double* x, double b, const double* y, double* z);
+int hpb_div_pointwise_c64(hpb_context* ctx, int64_t n, hpb_c64 a, const void* x, hpb_c64 b, const void* y, void* z);
+int hpb_div_pointwise_c128(hpb_context* ctx, int64_t n, hpb_c128 a, const void* x, hpb_c128 b, const void* y, void* z);
+/* y := |x|; complex: y = (|re| + |im|, 0)     (make_abs_copy / make_abs) */
+int hpb_abs_f32(hpb_context* ctx, int64_t n, const float* x, float* y);
+int hpb_abs_f64(hpb_context* ctx, int64_t n, const double* x, double* y);
+int hpb_abs_c64(hpb_context* ctx, int64_t n, const void* x, void* y);
+int hpb_abs_c128(hpb_context* ctx, int64_t n, const void* x, void* y);
+/* All entries finite?  Complex: isfinite(re + im), the reference's test
+ * (check_is_valid_number, gpu_vector_operations_impl.cuh:151-224).
+ * *result_host = 1 if all finite else 0.  Blocking; no allocation. */
+int hpb_isfinite_f32(hpb_context* ctx, int64_t n, const float* x, int* result_host);
+int hpb_isfinite_f64(hpb_context* ctx, int64_t n, const double* x, int* result_host);
+int hpb_isfinite_c64(hpb_context* ctx, int64_t n, const void* x, int* result_host);
+int hpb_isfinite_c128(hpb_context* ctx, int64_t n, const void* x, int* result_host);
+
+/* ---------------------------------------------------------------------- */
+/* CSR SpMV:  y := alpha*A*x + beta*y   (replaces csr::gpu_matrix::axpy,    */
+/* common/csr/gpu_matrix.h:322-375, i.e. cusparseSpMV with a per-call       */
+/* cudaMalloc'd buffer).  0-based int32 row_ptr[rows+1], col_ind[nnz].      */
+/* When beta == 0, y is not read (NaN in y does not propagate).             */
+/* ---------------------------------------------------------------------- */
+int hpb_csr_spmv_f32(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
+                     const int32_t* row_ptr, const int32_t* col_ind, const float* val,
+                     float alpha, const float* x, float beta, float* y);
+int hpb_csr_spmv_f64(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
+                     const int32_t* row_ptr, const int32_t* col_ind, const double* val,
+                     double alpha, const double* x, double beta, double* y);
+int hpb_csr_spmv_c64(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
+                     const int32_t* row_ptr, const int32_t* col_ind, const void* val,
+                     hpb_c64 alpha, const void* x, hpb_c64 beta, void* y);
+int hpb_csr_spmv_c128(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
+                      const int32_t* row_ptr, const int32_t* col_ind, const void* val,
+                      hpb_c128 alpha, const void* x, hpb_c128 beta, void* y);
+
+/* ---------------------------------------------------------------------- */
+/* Seeded input generators (host memory; no GPU needed)                    */
+/* ---------------------------------------------------------------------- */
+/* Ill-conditioned pair x, y of length n with condition number about
+ * `cond` (the GenDot scheme of generate_vector_pair::generate,
+ * generate_vector_pair.hpp:119-182, seeded).  *n_fixed_out (may be NULL)
+ * receives the number of tail entries fixed to cancel the running sum. */
+int hpb_gendot_f64(uint64_t seed, int64_t n, double cond, double* x, double* y, int64_t* n_fixed_out);
+/* Complex pair (interleaved): Re conj(x).y is ill-conditioned
+ * (generate_vector_pair_complex.hpp:142-460 generates complex pairs). */
+int hpb_gendot_c128(uint64_t seed, int64_t n, double cond, double* x, double* y);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPBLAS1_H */

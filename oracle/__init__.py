@@ -1,0 +1,193 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes loaders for the oracle.
+
+* ``oro()``  -- liboro.so, the CPU restatement of the reference's Dot2/Sum2
+  and the exact (fixed-point) accumulator, built from oro.c.
+* ``ref()``  -- _ref/libhpb_ref.so, the reference's own CPU code compiled
+  from the reference sources (None when it was not built on this host).
+
+Only tests/, the smoke check and the benchmark's CPU-baseline leg use these.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+_ORO = None
+_REF = None
+
+D = C.c_double
+I64 = C.c_int64
+PD = C.POINTER(C.c_double)
+P = C.c_void_p
+
+
+def build() -> None:
+    """Build liboro.so (and _ref/ when the reference sources exist)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True, capture_output=True)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(P)
+
+
+def oro():
+    global _ORO
+    if _ORO is None:
+        so = HERE / "liboro.so"
+        if not so.exists():
+            build()
+        lib = C.CDLL(str(so))
+        for name in ("oro_dot2_seq_f64", "oro_dot2_seq_f32", "oro_dot2_seq_c128", "oro_dot2_seq_c64",
+                     "oro_dot_naive_f64", "oro_exact_dot_f64", "oro_exact_dot_f32", "oro_exact_dot_c128",
+                     "oro_exact_dot_c64", "oro_exact_absdot_f64"):
+            getattr(lib, name).argtypes = [I64, P, P, P]
+            getattr(lib, name).restype = None
+        for name in ("oro_sum2_seq_f64", "oro_sum2_seq_f32"):
+            getattr(lib, name).argtypes = [I64, P, C.c_int, P]
+            getattr(lib, name).restype = None
+        lib.oro_dot2_threaded_f64.argtypes = [I64, P, P, C.c_int, P]
+        for name in ("oro_exact_sum_f64", "oro_exact_sum_f32"):
+            getattr(lib, name).argtypes = [I64, P, C.c_int, C.c_int, P]
+        lib.oro_exact_sumsq_f64.argtypes = [I64, P, C.c_int, P]
+        lib.oro_abs_err_dot_f64.argtypes = [I64, P, P, D, D, P]
+        for name in ("oro_bound_dot2_real", "oro_bound_dot2_complex", "oro_bound_sum2", "oro_bound_dot_naive_real"):
+            getattr(lib, name).argtypes = [D, D, D]
+            getattr(lib, name).restype = D
+        lib.oro_bound_dot2_block_real.argtypes = [D, D, D, D]
+        lib.oro_bound_dot2_block_real.restype = D
+        _ORO = lib
+    return _ORO
+
+
+def ref():
+    """The reference's own CPU reductions, or None if _ref was not built."""
+    global _REF
+    if _REF is None:
+        so = HERE / "_ref" / "libhpb_ref.so"
+        if not so.exists():
+            return None
+        lib = C.CDLL(str(so))
+        lib.ref_dot_ogita_f64.argtypes = [I64, P, P]
+        lib.ref_dot_ogita_f64.restype = D
+        lib.ref_dot_naive_f64.argtypes = [I64, P, P]
+        lib.ref_dot_naive_f64.restype = D
+        lib.ref_dot_ogita_f32.argtypes = [I64, P, P]
+        lib.ref_dot_ogita_f32.restype = C.c_float
+        for name in ("ref_dot_ogita_c128", "ref_dot_ogita_c64", "ref_dot_naive_c128"):
+            getattr(lib, name).argtypes = [I64, P, P, P]
+        lib.ref_threaded_dot_f64.argtypes = [I64, P, P, C.c_int, C.c_int]
+        lib.ref_threaded_dot_f64.restype = D
+        lib.ref_threaded_dot_f32.argtypes = [I64, P, P, C.c_int, C.c_int]
+        lib.ref_threaded_dot_f32.restype = C.c_float
+        lib.ref_threaded_sum_f64.argtypes = [I64, P, C.c_int, C.c_int, C.c_int]
+        lib.ref_threaded_sum_f64.restype = D
+        lib.ref_threaded_dot_f64_loop.argtypes = [I64, P, P, C.c_int, C.c_int]
+        lib.ref_threaded_dot_f64_loop.restype = D
+        for name in ("ref_bounds_dot_real_f64", "ref_bounds_dot_complex_f64", "ref_bounds_sum_real_f64"):
+            getattr(lib, name).argtypes = [I64, D, I64, P]
+        _REF = lib
+    return _REF
+
+
+# ----------------------------------------------------------------- helpers
+def exact_dot(x: np.ndarray, y: np.ndarray) -> tuple:
+    """Exact sum conj(x_i) y_i as (hi, lo) (real) or (hi, lo) complex pairs."""
+    lib = oro()
+    n = x.shape[0]
+    if x.dtype == np.float64:
+        out = np.zeros(2)
+        lib.oro_exact_dot_f64(n, _ptr(x), _ptr(y), _ptr(out))
+        return out[0], out[1]
+    if x.dtype == np.float32:
+        out = np.zeros(2)
+        lib.oro_exact_dot_f32(n, _ptr(x), _ptr(y), _ptr(out))
+        return out[0], out[1]
+    out = np.zeros(4)
+    if x.dtype == np.complex128:
+        lib.oro_exact_dot_c128(n, _ptr(x), _ptr(y), _ptr(out))
+    else:
+        lib.oro_exact_dot_c64(n, _ptr(x), _ptr(y), _ptr(out))
+    return complex(out[0], out[1]), complex(out[2], out[3])
+
+
+def exact_sum(x: np.ndarray, absolute: bool = False) -> tuple:
+    lib = oro()
+    n = x.shape[0]
+    ncomp = 2 if np.iscomplexobj(x) else 1
+    out = np.zeros(4)
+    if x.dtype in (np.float64, np.complex128):
+        lib.oro_exact_sum_f64(n, _ptr(x), ncomp, 1 if absolute else 0, _ptr(out))
+    else:
+        lib.oro_exact_sum_f32(n, _ptr(x), ncomp, 1 if absolute else 0, _ptr(out))
+    if ncomp == 2 and not absolute:
+        return complex(out[0], out[1]), complex(out[2], out[3])
+    return out[0], out[1]
+
+
+def exact_sumsq(x: np.ndarray) -> tuple:
+    lib = oro()
+    xd = np.ascontiguousarray(x.astype(np.complex128 if np.iscomplexobj(x) else np.float64))
+    out = np.zeros(2)
+    lib.oro_exact_sumsq_f64(x.shape[0], _ptr(xd), 2 if np.iscomplexobj(x) else 1, _ptr(out))
+    return out[0], out[1]
+
+
+def condition_dot(x: np.ndarray, y: np.ndarray) -> float:
+    """cond = sum|x_i y_i| / |sum x_i y_i| (real float64 inputs), exactly."""
+    lib = oro()
+    a = np.zeros(2)
+    lib.oro_exact_absdot_f64(x.shape[0], _ptr(x), _ptr(y), _ptr(a))
+    hi, _ = exact_dot(x, y)
+    return float("inf") if hi == 0 else a[0] / abs(hi)
+
+
+def dot2_seq(x: np.ndarray, y: np.ndarray):
+    """The reference's sequential Dot2 restated (dot_product<T>::dot_ogita)."""
+    lib = oro()
+    n = x.shape[0]
+    if x.dtype == np.float64:
+        out = np.zeros(3)
+        lib.oro_dot2_seq_f64(n, _ptr(x), _ptr(y), _ptr(out))
+        return out[0]
+    if x.dtype == np.float32:
+        out = np.zeros(3)
+        lib.oro_dot2_seq_f32(n, _ptr(x), _ptr(y), _ptr(out))
+        return np.float32(out[0])
+    out = np.zeros(6)
+    if x.dtype == np.complex128:
+        lib.oro_dot2_seq_c128(n, _ptr(x), _ptr(y), _ptr(out))
+        return complex(out[0], out[1])
+    lib.oro_dot2_seq_c64(n, _ptr(x), _ptr(y), _ptr(out))
+    return np.complex64(complex(out[0], out[1]))
+
+
+def dot2_threaded(x: np.ndarray, y: np.ndarray, parts: int) -> float:
+    out = np.zeros(1)
+    oro().oro_dot2_threaded_f64(x.shape[0], _ptr(x), _ptr(y), parts, _ptr(out))
+    return out[0]
+
+
+def sum2_seq(x: np.ndarray, absolute: bool = False):
+    lib = oro()
+    out = np.zeros(3)
+    if x.dtype == np.float64:
+        lib.oro_sum2_seq_f64(x.shape[0], _ptr(x), 1 if absolute else 0, _ptr(out))
+        return out[0]
+    lib.oro_sum2_seq_f32(x.shape[0], _ptr(x), 1 if absolute else 0, _ptr(out))
+    return np.float32(out[0])
+
+
+def bound_dot2(n: int, cond: float, complex_: bool = False, eps: float = 2.0 ** -52) -> float:
+    """Relative a priori bound of compensated Dot2 (error_bounds.hpp)."""
+    lib = oro()
+    if complex_:
+        return lib.oro_bound_dot2_complex(float(n), float(cond), eps)
+    return lib.oro_bound_dot2_real(float(n), float(cond), eps)
+
+
+def bound_sum2(n: int, cond: float, eps: float = 2.0 ** -52) -> float:
+    return oro().oro_bound_sum2(float(max(n, 2)), float(cond), eps)
