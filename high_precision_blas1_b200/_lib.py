@@ -101,10 +101,51 @@ for t in TYPES:
     _sig(f"hpb_abs_{t}", C.c_int, [P, I64, P, P])
     _sig(f"hpb_isfinite_{t}", C.c_int, [P, I64, P, C.POINTER(C.c_int)])
     _sig(f"hpb_csr_spmv_{t}", C.c_int, [P, I32, I32, I64, P, P, P, S, P, S, P])
+    _sig(f"hpb_csr_diag_{t}", C.c_int, [P, I32, P, P, P, P])
+    _sig(f"hpb_random_{t}", C.c_int, [P, I64, C.c_uint64, S, S, P])
 _sig("hpb_gendot_f64", C.c_int, [C.c_uint64, I64, C.c_double, P, P, C.POINTER(C.c_int64)])
 _sig("hpb_gendot_c128", C.c_int, [C.c_uint64, I64, C.c_double, P, P])
 _sig("hpb_copy", C.c_int, [P, I64, C.c_size_t, P, P])
 _sig("hpb_swap", C.c_int, [P, I64, C.c_size_t, P, P])
+
+
+class hpb_solver_params(C.Structure):
+    _fields_ = [("method", C.c_int), ("basis", C.c_int), ("rel_tol", C.c_double), ("abs_tol", C.c_double),
+                ("max_iters", C.c_int), ("precond", C.c_int), ("high_precision", C.c_int),
+                ("resid_recalc_freq", C.c_int), ("early_exit", C.c_int), ("reorthogonalize", C.c_int)]
+
+
+class hpb_solver_report(C.Structure):
+    _fields_ = [("converged", C.c_int), ("iters", C.c_int), ("breakdown", C.c_int), ("history_len", C.c_int),
+                ("rhs_norm", C.c_double), ("resid_norm", C.c_double), ("true_resid_norm", C.c_double),
+                ("true_rhs_norm", C.c_double), ("seconds", C.c_double)]
+
+
+SOLVER = {"bicgstabl": 0, "gmres": 1, "bicgstab": 2}
+PRECOND = {"none": 0, "jacobi": 1}
+
+_sig("hpb_solver_params_default", C.c_int, [C.POINTER(hpb_solver_params)])
+for t in TYPES:
+    for suf in ("", "_host"):
+        _sig(f"hpb_csr_solve_{t}{suf}", C.c_int,
+             [C.POINTER(hpb_solver_params), I32, I64, P, P, P, P, P, C.POINTER(hpb_solver_report), P, C.c_int])
+
+
+def solver_params(method="bicgstabl", basis=2, rel_tol=1e-10, abs_tol=0.0, max_iters=10000, precond="none",
+                  high_precision=True, resid_recalc_freq=0, early_exit=False, reorthogonalize=False):
+    p = hpb_solver_params()
+    lib.hpb_solver_params_default(C.byref(p))
+    p.method = SOLVER[method]
+    p.basis = basis
+    p.rel_tol = rel_tol
+    p.abs_tol = abs_tol
+    p.max_iters = max_iters
+    p.precond = PRECOND[precond]
+    p.high_precision = 1 if high_precision else 0
+    p.resid_recalc_freq = resid_recalc_freq
+    p.early_exit = 1 if early_exit else 0
+    p.reorthogonalize = 1 if reorthogonalize else 0
+    return p
 
 
 def scalar(t: str, v):

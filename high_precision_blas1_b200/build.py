@@ -30,7 +30,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
     "-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr",
     "-Xcompiler", "-fPIC,-O2,-fno-fast-math,-ffp-contract=off",
-    "-I", str(INCLUDE), "-I", str(CSRC),
+    "-I", str(INCLUDE), "-I", str(INCLUDE / "hpblas1_dropin"), "-I", str(CSRC),
 ]
 
 

@@ -93,6 +93,30 @@ int spmv_impl(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz, const i
     return check_launch(ctx, name);
 }
 
+// diag[r] = A(r, r) (0 where the row stores no diagonal entry)
+template <class E>
+__global__ void csr_diag_kernel(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                                const E* __restrict__ val, E* __restrict__ diag) {
+    const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    E d{};
+    for (int32_t k = rp[r]; k < rp[r + 1]; ++k)
+        if (ci[k] == r) d = ldE(val, k);
+    stE(diag, r, d);
+}
+
+template <class E>
+int diag_impl(hpb_context* ctx, int32_t rows, const int32_t* rp, const int32_t* ci, const E* val, E* diag,
+              const char* name) {
+    HPB_CHECK_CTX(ctx);
+    if (rows < 0) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: invalid dimensions", name);
+    if (rows == 0) return HPB_SUCCESS;
+    if (!rp || !ci || !val || !diag) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null pointer", name);
+    csr_diag_kernel<E><<<(rows + 255) / 256, 256, 0, ctx->stream>>>(rows, rp, ci, val, diag);
+    count_launch();
+    return check_launch(ctx, name);
+}
+
 }  // namespace hpb
 
 using hpb::cd;
@@ -121,6 +145,25 @@ int hpb_csr_spmv_c128(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
     return hpb::spmv_impl<cd>(ctx, rows, cols, nnz, row_ptr, col_ind, static_cast<const cd*>(val),
                               cd{alpha.re, alpha.im}, static_cast<const cd*>(x), cd{beta.re, beta.im},
                               static_cast<cd*>(y), "hpb_csr_spmv_c128");
+}
+
+int hpb_csr_diag_f32(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,
+                     const float* val, float* diag) {
+    return hpb::diag_impl<float>(ctx, rows, row_ptr, col_ind, val, diag, "hpb_csr_diag_f32");
+}
+int hpb_csr_diag_f64(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,
+                     const double* val, double* diag) {
+    return hpb::diag_impl<double>(ctx, rows, row_ptr, col_ind, val, diag, "hpb_csr_diag_f64");
+}
+int hpb_csr_diag_c64(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,
+                     const void* val, void* diag) {
+    return hpb::diag_impl<cf>(ctx, rows, row_ptr, col_ind, static_cast<const cf*>(val), static_cast<cf*>(diag),
+                              "hpb_csr_diag_c64");
+}
+int hpb_csr_diag_c128(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,
+                      const void* val, void* diag) {
+    return hpb::diag_impl<cd>(ctx, rows, row_ptr, col_ind, static_cast<const cd*>(val), static_cast<cd*>(diag),
+                              "hpb_csr_diag_c128");
 }
 
 }  // extern "C"

@@ -222,6 +222,55 @@ int isfinite_impl(hpb_context* ctx, int64_t n, const E* x, int* result_host, con
     return HPB_SUCCESS;
 }
 
+// ------------------------------------------------------------ random fill
+// x_i = a + (b - a) * u_i with u_i in [0, 1) from a counter-based hash of
+// (seed, i): reproducible, independent of the launch shape.  Complex:
+// re and im drawn independently in the square [a.re, b.re) x [a.im, b.im)
+// (the reference's scale_complex_vector adapter, gpu_vector_operations_impl.cuh:148-160).
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ double u01(uint64_t seed, uint64_t i) {
+    return double(mix64(seed ^ mix64(i)) >> 11) * 0x1.0p-53;
+}
+template <class E> struct RandGen;
+template <> struct RandGen<float> {
+    __device__ static float gen(uint64_t s, int64_t i, float a, float b) { return float(a + (b - a) * u01(s, 2 * i)); }
+};
+template <> struct RandGen<double> {
+    __device__ static double gen(uint64_t s, int64_t i, double a, double b) { return a + (b - a) * u01(s, 2 * i); }
+};
+template <> struct RandGen<cf> {
+    __device__ static cf gen(uint64_t s, int64_t i, cf a, cf b) {
+        return cf{float(a.re + (b.re - a.re) * u01(s, 2 * i)), float(a.im + (b.im - a.im) * u01(s, 2 * i + 1))};
+    }
+};
+template <> struct RandGen<cd> {
+    __device__ static cd gen(uint64_t s, int64_t i, cd a, cd b) {
+        return cd{a.re + (b.re - a.re) * u01(s, 2 * i), a.im + (b.im - a.im) * u01(s, 2 * i + 1)};
+    }
+};
+template <class E>
+__global__ void random_kernel(int64_t n, uint64_t seed, E a, E b, E* x) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+        stE(x, i, RandGen<E>::gen(seed, i, a, b));
+}
+template <class E>
+int random_impl(hpb_context* ctx, int64_t n, uint64_t seed, E a, E b, E* x, const char* name) {
+    HPB_CHECK_CTX(ctx);
+    if (n < 0 || (n > 0 && x == nullptr)) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: invalid argument", name);
+    if (reinterpret_cast<uintptr_t>(x) % sizeof(typename real_of<E>::type) != 0)
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: pointer not aligned to its element type", name);
+    if (n == 0) return HPB_SUCCESS;
+    random_kernel<E><<<grid_for(ctx, n, kMapThreads, 8), kMapThreads, 0, ctx->stream>>>(n, seed, a, b, x);
+    count_launch();
+    return check_launch(ctx, name);
+}
+
 inline float sc(float v) { return v; }
 inline double sc(double v) { return v; }
 inline cf sc(hpb_c64 v) { return cf{v.re, v.im}; }
@@ -311,6 +360,10 @@ using hpb::sc;
     int hpb_isfinite_##SUF(hpb_context* ctx, int64_t n, const PT* x, int* result_host) {                  \
         using E = E_;                                                                                      \
         return hpb::isfinite_impl<E>(ctx, n, CE(x), result_host, "hpb_isfinite_" #SUF);                    \
+    }                                                                                                      \
+    int hpb_random_##SUF(hpb_context* ctx, int64_t n, uint64_t seed, ST a, ST b, PT* x) {                  \
+        using E = E_;                                                                                      \
+        return hpb::random_impl<E>(ctx, n, seed, sc(a), sc(b), ME(x), "hpb_random_" #SUF);                 \
     }
 
 extern "C" {

@@ -237,6 +237,14 @@ int hpb_isfinite_f64(hpb_context* ctx, int64_t n, const double* x, int* result_h
 int hpb_isfinite_c64(hpb_context* ctx, int64_t n, const void* x, int* result_host);
 int hpb_isfinite_c128(hpb_context* ctx, int64_t n, const void* x, int* result_host);
 
+/* x_i := a + (b - a) u_i, u_i in [0,1) from a counter-based hash of
+ * (seed, i); complex: re and im independently (assign_random,
+ * gpu_vector_operations.h:498-523, there with an unseeded cuRAND). */
+int hpb_random_f32(hpb_context* ctx, int64_t n, uint64_t seed, float a, float b, float* x);
+int hpb_random_f64(hpb_context* ctx, int64_t n, uint64_t seed, double a, double b, double* x);
+int hpb_random_c64(hpb_context* ctx, int64_t n, uint64_t seed, hpb_c64 a, hpb_c64 b, void* x);
+int hpb_random_c128(hpb_context* ctx, int64_t n, uint64_t seed, hpb_c128 a, hpb_c128 b, void* x);
+
 /* ---------------------------------------------------------------------- */
 /* CSR SpMV:  y := alpha*A*x + beta*y   (replaces csr::gpu_matrix::axpy,    */
 /* common/csr/gpu_matrix.h:322-375, i.e. cusparseSpMV with a per-call       */
@@ -255,6 +263,90 @@ int hpb_csr_spmv_c64(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
 int hpb_csr_spmv_c128(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
                       const int32_t* row_ptr, const int32_t* col_ind, const void* val,
                       hpb_c128 alpha, const void* x, hpb_c128 beta, void* y);
+
+/* diag[r] := A(r, r) (0 if row r stores no diagonal entry); used by the
+ * Jacobi preconditioner (the diagonal scaling of linear_operator.hpp:59-91). */
+int hpb_csr_diag_f32(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,
+                     const float* val, float* diag);
+int hpb_csr_diag_f64(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,
+                     const double* val, double* diag);
+int hpb_csr_diag_c64(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,
+                     const void* val, void* diag);
+int hpb_csr_diag_c128(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,
+                      const void* val, void* diag);
+
+/* ---------------------------------------------------------------------- */
+/* Krylov solvers on a CSR matrix (the reference's bicgstabl.h, gmres.h,   */
+/* bicgstab.h over gpu_vector_operations + csr::gpu_matrix, as driven by   */
+/* test_csr_linear_solver.cpp:101-353), plain drop-in path: every          */
+/* reduction result returns to the host.                                    */
+/* ---------------------------------------------------------------------- */
+typedef enum hpb_solver_method {
+    HPB_SOLVER_BICGSTABL = 0,   /* BiCGStab(l), basis = l (bicgstabl.h) */
+    HPB_SOLVER_GMRES = 1,       /* restarted GMRES(m), basis = m (gmres.h) */
+    HPB_SOLVER_BICGSTAB = 2     /* BiCGStab (bicgstab.h) */
+} hpb_solver_method;
+
+typedef enum hpb_precond_kind {
+    HPB_PRECOND_NONE = 0,
+    HPB_PRECOND_JACOBI = 1      /* x := D^{-1} x (left) */
+} hpb_precond_kind;
+
+typedef struct hpb_solver_params {
+    int method;             /* hpb_solver_method */
+    int basis;              /* l of BiCGStab(l) / m of GMRES(m) */
+    double rel_tol;         /* stop when ||r|| <= abs_tol + rel_tol * ||b|| (default_monitor.h) */
+    double abs_tol;
+    int max_iters;          /* iteration cap (BiCGStab(l) counts l per cycle) */
+    int precond;            /* hpb_precond_kind */
+    int high_precision;     /* 1: Dot2/Sum2 reductions; 0: plain reductions */
+    int resid_recalc_freq;  /* recompute the true residual every k cycles (0: never) */
+    int early_exit;         /* GMRES: end a cycle when the rotated estimate meets tol */
+    int reorthogonalize;    /* GMRES: second Gram-Schmidt pass */
+} hpb_solver_params;
+
+typedef struct hpb_solver_report {
+    int converged;
+    int iters;
+    int breakdown;
+    int history_len;        /* entries written to history (pairs iter, ||r||) */
+    double rhs_norm;        /* monitor's ||b|| (||P b|| when preconditioned) */
+    double resid_norm;      /* monitor's last residual norm */
+    double true_resid_norm; /* ||b - A x||, compensated, after the solve */
+    double true_rhs_norm;   /* ||b||, compensated */
+    double seconds;         /* wall time of the iteration (device synchronised) */
+} hpb_solver_report;
+
+int hpb_solver_params_default(hpb_solver_params* p);
+/* Device arrays (resident in HBM).  x holds the initial guess on entry.
+ * history (optional, host) receives up to history_cap (iter, ||r||) pairs.
+ * Returns HPB_SUCCESS, HPB_ERROR_NOT_CONVERGED or HPB_ERROR_BREAKDOWN with
+ * the report filled, or another error. */
+int hpb_csr_solve_f32(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                      const int32_t* col_ind, const float* val, const float* b, float* x,
+                      hpb_solver_report* rep, double* history, int history_cap);
+int hpb_csr_solve_f64(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                      const int32_t* col_ind, const double* val, const double* b, double* x,
+                      hpb_solver_report* rep, double* history, int history_cap);
+int hpb_csr_solve_c64(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                      const int32_t* col_ind, const void* val, const void* b, void* x,
+                      hpb_solver_report* rep, double* history, int history_cap);
+int hpb_csr_solve_c128(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                       const int32_t* col_ind, const void* val, const void* b, void* x,
+                       hpb_solver_report* rep, double* history, int history_cap);
+/* Same with every array in HOST memory: copies in, solves, copies x out. */
+int hpb_csr_solve_f32_host(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                           const int32_t* col_ind, const float* val, const float* b, float* x,
+                           hpb_solver_report* rep, double* history, int history_cap);
+int hpb_csr_solve_f64_host(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                           const int32_t* col_ind, const double* val, const double* b, double* x,
+                           hpb_solver_report* rep, double* history, int history_cap);
+int hpb_csr_solve_c64_host(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                           const int32_t* col_ind, const void* val, const void* b, void* x,
+                           hpb_solver_report* rep, double* history, int history_cap);
+int hpb_csr_solve_c128_host(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                            const int32_t* col_ind, const void* val, const void* b, void* x,
+                            hpb_solver_report* rep, double* history, int history_cap);
 
 /* ---------------------------------------------------------------------- */
 /* Seeded input generators (host memory; no GPU needed)                    */

@@ -1,0 +1,179 @@
+// Drop-in replacement of the reference's common/csr/gpu_matrix.h.
+//
+// csr::gpu_matrix<VectorOperations, CudaBlas, Ordinal> keeps the
+// reference's constructors, init / set_dim / set / init_set / get_dim and
+// axpy(alpha, x, beta, y, transpose) (csr/gpu_matrix.h:93-375 with the base
+// class csr/matrix.h:33-158), but axpy runs the library's CSR kernel
+// (hpb_csr_spmv_*) instead of cusparseSpMV with a cudaMalloc'd work buffer
+// per call.
+//
+// Shape contract: the reference hands cuSPARSE size_row = rows+1 and
+// size_col = nnz as the matrix dimensions (csr/gpu_matrix.h:389-396), an
+// off-by-one.  Here the operator is rows x columns from set_dim(); without
+// set_dim the matrix is taken square with rows = size_row - 1.
+// Only 0-based int32 indices are supported (the configs' matrices).
+// Triangular solves (the csrsv2 path, removed from CUDA 12) and the
+// transposed product report "not supported".
+#ifndef __CSR__GPU_MATRIX_H__
+#define __CSR__GPU_MATRIX_H__
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <type_traits>
+
+#include <common/gpu_vector_operations.h>
+
+namespace csr {
+
+template <class VectorOperations, class CudaBlas, class Ordinal = int>
+class gpu_matrix {
+    static_assert(std::is_same<Ordinal, int>::value || std::is_same<Ordinal, std::int32_t>::value,
+                  "csr::gpu_matrix: the drop-in supports int32 indices");
+
+public:
+    using T = typename VectorOperations::scalar_type;
+    using T_vec = typename VectorOperations::vector_type;
+    using I = Ordinal;
+    using I_vec = Ordinal*;
+    struct dimensions_t {
+        int columns = 0;
+        int rows = 0;
+    };
+
+    explicit gpu_matrix(CudaBlas* cublas_ = nullptr) : cublas(cublas_) { ctx = hpb_dropin::make_context(); }
+    gpu_matrix(int nnz_, int size_col_, int size_row_, CudaBlas* cublas_) : cublas(cublas_) {
+        ctx = hpb_dropin::make_context();
+        init(nnz_, size_col_, size_row_);
+    }
+    gpu_matrix(const gpu_matrix& m) : cublas(m.cublas), dim(m.dim) {
+        ctx = hpb_dropin::make_context();
+        if (m.initialized) {
+            init(m.nnz, m.size_col, m.size_row);
+            copy_d2d(data, m.data, size_t(nnz) * sizeof(T));
+            copy_d2d(col_ind, m.col_ind, size_t(size_col) * sizeof(I));
+            copy_d2d(row_ptr, m.row_ptr, size_t(size_row) * sizeof(I));
+        }
+    }
+    gpu_matrix& operator=(const gpu_matrix&) = delete;
+    ~gpu_matrix() {
+        if (owns_) {
+            cudaFree(data);
+            cudaFree(col_ind);
+            cudaFree(row_ptr);
+        }
+        hpb_destroy(ctx);
+    }
+
+    void set_dim(int matrix_columns_, int matrix_rows_) {
+        dim.columns = matrix_columns_;
+        dim.rows = matrix_rows_;
+    }
+    // allocate nnz values, size_col column indices and size_row row pointers
+    void init(int nnz_, int size_col_, int size_row_) {
+        if (initialized) return;
+        if (nnz_ < 0 || size_col_ < 0 || size_row_ < 1) throw std::runtime_error("csr::gpu_matrix: invalid sizes");
+        nnz = nnz_;
+        size_col = size_col_;
+        size_row = size_row_;
+        data = static_cast<T*>(dalloc(size_t(nnz) * sizeof(T)));
+        col_ind = static_cast<I*>(dalloc(size_t(size_col) * sizeof(I)));
+        row_ptr = static_cast<I*>(dalloc(size_t(size_row) * sizeof(I)));
+        initialized = true;
+    }
+    dimensions_t get_dim() const {
+        dimensions_t d = dim;
+        if (d.rows == 0 && initialized) {
+            d.rows = size_row - 1;
+            d.columns = d.rows;
+        }
+        return d;
+    }
+    // upload host arrays (values, column indices, row pointers)
+    void set(const T_vec data_, const I_vec col_ind_, const I_vec row_ptr_) {
+        if (!initialized) throw std::runtime_error("csr::gpu_matrix: trying to set an uninitialized matrix.");
+        h2d(data, data_, size_t(nnz) * sizeof(T));
+        h2d(col_ind, col_ind_, size_t(size_col) * sizeof(I));
+        h2d(row_ptr, row_ptr_, size_t(size_row) * sizeof(I));
+    }
+    void init_set(int nnz_, int size_col_, int size_row_, const T_vec data_, const I_vec col_ind_,
+                  const I_vec row_ptr_, int matrix_columns_, int matrix_rows_) {
+        init(nnz_, size_col_, size_row_);
+        set_dim(matrix_columns_, matrix_rows_);
+        set(data_, col_ind_, row_ptr_);
+    }
+
+    // y := alpha*A*x + beta*y
+    void axpy(const T& alpha_, const T_vec& x_, const T& beta_, T_vec& y_, bool transpose_ = false) const {
+        if (transpose_) throw std::logic_error("csr::gpu_matrix::axpy: transposed product is not supported");
+        if (!initialized) throw std::runtime_error("csr::gpu_matrix::axpy: matrix not set");
+        dimensions_t d = get_dim();
+        using A = hpb_dropin::abi<T>;
+        hpb_dropin::check(A::spmv(ctx, d.rows, d.columns, nnz, row_ptr, col_ind, data, A::s(alpha_), x_, A::s(beta_),
+                                  y_),
+                          ctx, "csr::gpu_matrix::axpy");
+    }
+    void triangular_solve_lower(const T_vec&, T_vec&, const T& = T(1.0), bool = false) const {
+        throw std::logic_error("csr::gpu_matrix: triangular solves are not supported by this library");
+    }
+    void triangular_solve_upper(const T_vec&, T_vec&, const T& = T(1.0), bool = false) const {
+        throw std::logic_error("csr::gpu_matrix: triangular solves are not supported by this library");
+    }
+
+    // ------------------------------------------------------------ extensions
+    // Use CSR arrays already resident on the device (not copied, not freed).
+    void attach(int rows, int cols, int nnz_, const I* row_ptr_dev, const I* col_ind_dev, const T* val_dev) {
+        if (initialized) throw std::runtime_error("csr::gpu_matrix::attach: matrix already initialised");
+        nnz = nnz_;
+        size_col = nnz_;
+        size_row = rows + 1;
+        data = const_cast<T*>(val_dev);
+        col_ind = const_cast<I*>(col_ind_dev);
+        row_ptr = const_cast<I*>(row_ptr_dev);
+        set_dim(cols, rows);
+        owns_ = false;
+        initialized = true;
+    }
+    const T* values() const { return data; }
+    const I* columns() const { return col_ind; }
+    const I* row_pointers() const { return row_ptr; }
+    int nonzeros() const { return nnz; }
+    hpb_context* context() const { return ctx; }
+    // diagonal of A into the device vector d (d_i = A_ii)
+    void diagonal(T_vec& d) const {
+        using A = hpb_dropin::abi<T>;
+        hpb_dropin::check(A::diag(ctx, get_dim().rows, row_ptr, col_ind, data, d), ctx, "csr::gpu_matrix::diagonal");
+    }
+
+protected:
+    T_vec data = nullptr;
+    I_vec col_ind = nullptr;
+    I_vec row_ptr = nullptr;
+    int size_row = 0, size_col = 0, nnz = 0;
+    bool initialized = false;
+    dimensions_t dim;
+
+private:
+    CudaBlas* cublas;
+    hpb_context* ctx = nullptr;
+    bool owns_ = true;
+
+    static void* dalloc(size_t b) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, b ? b : 4) != cudaSuccess) throw std::runtime_error("csr::gpu_matrix: cudaMalloc failed");
+        return p;
+    }
+    static void h2d(void* d, const void* h, size_t b) {
+        if (b && cudaMemcpy(d, h, b, cudaMemcpyHostToDevice) != cudaSuccess)
+            throw std::runtime_error("csr::gpu_matrix: failed to set the gpu_matrix.");
+    }
+    static void copy_d2d(void* d, const void* s, size_t b) {
+        if (b && cudaMemcpy(d, s, b, cudaMemcpyDeviceToDevice) != cudaSuccess)
+            throw std::runtime_error("csr::gpu_matrix: copy failed");
+    }
+};
+
+}  // namespace csr
+
+#endif

@@ -1,0 +1,413 @@
+// Drop-in replacement of the reference's common/gpu_vector_operations.h.
+//
+// Same include path, class name, template signature, typedefs, method
+// names, argument meaning and ownership rules as the reference's
+// gpu_vector_operations<T, BLOCK_SIZE> (common/gpu_vector_operations.h:86-538),
+// so the reference's Krylov solvers (numerical_algos/lin_solvers/*.h) and
+// monitor compile against it unchanged: put include/hpblas1_dropin/ ahead
+// of the reference's source/ directory on the include path and link
+// libhpblas1.so.
+//
+// Every operation runs in libhpblas1 (include/hpblas1.h); nothing here
+// calls cuBLAS, cuRAND or a CPU fallback.  Differences, all deliberate:
+//   * "standard precision" uses the library's plain FMA reductions instead
+//     of cuBLAS ?dot/?nrm2/?asum, and no call synchronises the device except
+//     those that return a value to the host (reductions, isfinite, get);
+//   * high-precision reductions are single-launch Dot2/Sum2 kernels; the
+//     object holds an O(#SM) context instead of 4 n-sized helper arrays;
+//   * absolute_sum of REAL vectors in high precision sums |x_i| (the
+//     reference's real Ogita asum kernel sums x_i without the absolute
+//     value, gpu_reduction_ogita_impl_functions.cuh:208-215, which is a bug;
+//     for complex vectors both sum |re| + |im|);
+//   * assign_random is seeded (set_random_seed) instead of std::random_device.
+// Errors raise std::runtime_error with the library's message, as the
+// reference's *_SAFE_CALL macros do (utils/cuda_safe_call.h:51).
+#ifndef __gpu_vector_operations_H__
+#define __gpu_vector_operations_H__
+
+#include <cuda_runtime.h>
+#include <thrust/complex.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <external_libraries/cublas_wrap.h>
+#include <hpblas1.h>
+
+namespace gpu_vector_operations_type {
+template <typename T> struct vec_ops_cuComplex_type_hlp {};
+template <> struct vec_ops_cuComplex_type_hlp<float> { typedef float norm_type; };
+template <> struct vec_ops_cuComplex_type_hlp<double> { typedef double norm_type; };
+template <> struct vec_ops_cuComplex_type_hlp<thrust::complex<float> > { typedef float norm_type; };
+template <> struct vec_ops_cuComplex_type_hlp<thrust::complex<double> > { typedef double norm_type; };
+}  // namespace gpu_vector_operations_type
+
+namespace cublas_real_types {
+template <typename T> struct cublas_real_type_hlp { typedef T type; };
+template <> struct cublas_real_type_hlp<thrust::complex<float> > { typedef float type; };
+template <> struct cublas_real_type_hlp<thrust::complex<double> > { typedef double type; };
+}  // namespace cublas_real_types
+
+namespace hpb_dropin {
+
+inline void check(int st, hpb_context* ctx, const char* what) {
+    if (st != HPB_SUCCESS) {
+        std::string msg = std::string(what) + ": " + hpb_status_string(st);
+        if (ctx) msg += std::string(" (") + hpb_last_error(ctx) + ")";
+        throw std::runtime_error(msg);
+    }
+}
+
+// Type dispatch onto the C ABI.
+template <class T> struct abi;
+
+#define HPB_DROPIN_ABI(T, SUF, ST, MKS)                                                                   \
+    template <> struct abi<T> {                                                                           \
+        using S = ST;                                                                                     \
+        static S s(const T& v) { return MKS; }                                                            \
+        static constexpr size_t bytes = sizeof(T);                                                        \
+        static int dot2(hpb_context* c, int64_t n, const T* x, const T* y, double* o) {                   \
+            return hpb_dot2_##SUF##_host(c, n, x, y, o);                                                  \
+        }                                                                                                 \
+        static int dot(hpb_context* c, int64_t n, const T* x, const T* y, double* o) {                    \
+            return hpb_dot_##SUF##_host(c, n, x, y, o);                                                   \
+        }                                                                                                 \
+        static int nrm2(hpb_context* c, int64_t n, const T* x, double* o) { return hpb_nrm2_##SUF##_host(c, n, x, o); } \
+        static int nrm2plain(hpb_context* c, int64_t n, const T* x, double* o) {                          \
+            return hpb_nrm2plain_##SUF##_host(c, n, x, o);                                                \
+        }                                                                                                 \
+        static int asum2(hpb_context* c, int64_t n, const T* x, double* o) { return hpb_asum2_##SUF##_host(c, n, x, o); } \
+        static int asum(hpb_context* c, int64_t n, const T* x, double* o) { return hpb_asum_##SUF##_host(c, n, x, o); } \
+        static int sum2(hpb_context* c, int64_t n, const T* x, double* o) { return hpb_sum2_##SUF##_host(c, n, x, o); } \
+        static int axpy(hpb_context* c, int64_t n, S a, const T* x, T* y) { return hpb_axpy_##SUF(c, n, a, x, y); } \
+        static int axpby(hpb_context* c, int64_t n, S a, const T* x, S b, T* y) {                         \
+            return hpb_axpby_##SUF(c, n, a, x, b, y);                                                     \
+        }                                                                                                 \
+        static int lincomb2(hpb_context* c, int64_t n, S a, const T* x, S b, const T* y, T* z) {          \
+            return hpb_lincomb2_##SUF(c, n, a, x, b, y, z);                                               \
+        }                                                                                                 \
+        static int axpbypcz(hpb_context* c, int64_t n, S a, const T* x, S b, const T* y, S g, T* z) {     \
+            return hpb_axpbypcz_##SUF(c, n, a, x, b, y, g, z);                                            \
+        }                                                                                                 \
+        static int axpbypcwpdz(hpb_context* c, int64_t n, S a, const T* x, S b, const T* y, S g,          \
+                               const T* w, S d, T* z) {                                                   \
+            return hpb_axpbypcwpdz_##SUF(c, n, a, x, b, y, g, w, d, z);                                   \
+        }                                                                                                 \
+        static int lincomb4(hpb_context* c, int64_t n, S a, const T* x, S b, const T* y, S g, const T* v, \
+                            S d, const T* w, T* z) {                                                      \
+            return hpb_lincomb4_##SUF(c, n, a, x, b, y, g, v, d, w, z);                                   \
+        }                                                                                                 \
+        static int scal(hpb_context* c, int64_t n, S a, const T* x, T* y) { return hpb_scal_##SUF(c, n, a, x, y); } \
+        static int add_scalar(hpb_context* c, int64_t n, S s_, S a, T* x) {                               \
+            return hpb_add_scalar_##SUF(c, n, s_, a, x);                                                  \
+        }                                                                                                 \
+        static int fill(hpb_context* c, int64_t n, S s_, T* x) { return hpb_fill_##SUF(c, n, s_, x); }   \
+        static int mulpw(hpb_context* c, int64_t n, S a, const T* x, S b, const T* y, T* z) {             \
+            return hpb_mul_pointwise_##SUF(c, n, a, x, b, y, z);                                          \
+        }                                                                                                 \
+        static int divpw(hpb_context* c, int64_t n, S a, const T* x, S b, const T* y, T* z) {             \
+            return hpb_div_pointwise_##SUF(c, n, a, x, b, y, z);                                          \
+        }                                                                                                 \
+        static int abs(hpb_context* c, int64_t n, const T* x, T* y) { return hpb_abs_##SUF(c, n, x, y); } \
+        static int isfinite(hpb_context* c, int64_t n, const T* x, int* r) {                              \
+            return hpb_isfinite_##SUF(c, n, x, r);                                                        \
+        }                                                                                                 \
+        static int random(hpb_context* c, int64_t n, uint64_t seed, S a, S b, T* x) {                     \
+            return hpb_random_##SUF(c, n, seed, a, b, x);                                                 \
+        }                                                                                                 \
+        static int spmv(hpb_context* c, int32_t rows, int32_t cols, int64_t nnz, const int32_t* rp,       \
+                        const int32_t* ci, const T* v, S a, const T* x, S b, T* y) {                      \
+            return hpb_csr_spmv_##SUF(c, rows, cols, nnz, rp, ci, v, a, x, b, y);                         \
+        }                                                                                                 \
+        static int diag(hpb_context* c, int32_t rows, const int32_t* rp, const int32_t* ci, const T* v,   \
+                        T* d) {                                                                           \
+            return hpb_csr_diag_##SUF(c, rows, rp, ci, v, d);                                             \
+        }                                                                                                 \
+    };
+
+HPB_DROPIN_ABI(float, f32, float, v)
+HPB_DROPIN_ABI(double, f64, double, v)
+HPB_DROPIN_ABI(thrust::complex<float>, c64, hpb_c64, (hpb_c64{v.real(), v.imag()}))
+HPB_DROPIN_ABI(thrust::complex<double>, c128, hpb_c128, (hpb_c128{v.real(), v.imag()}))
+#undef HPB_DROPIN_ABI
+
+template <class T> struct value_of {
+    static T from(const double* o) { return T(o[0]); }
+};
+template <> struct value_of<thrust::complex<float> > {
+    static thrust::complex<float> from(const double* o) { return thrust::complex<float>(float(o[0]), float(o[1])); }
+};
+template <> struct value_of<thrust::complex<double> > {
+    static thrust::complex<double> from(const double* o) { return thrust::complex<double>(o[0], o[1]); }
+};
+
+// A context per vector-operations object, on the device that is current when
+// the object is built and the legacy default stream (the reference's stream).
+inline hpb_context* make_context() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+    hpb_context* c = nullptr;
+    check(hpb_create(&c, dev, nullptr), nullptr, "gpu_vector_operations: hpb_create");
+    return c;
+}
+
+}  // namespace hpb_dropin
+
+template <typename T, int BLOCK_SIZE = 1024>
+struct gpu_vector_operations {
+    typedef T scalar_type;
+    typedef T* vector_type;
+    typedef typename gpu_vector_operations_type::vec_ops_cuComplex_type_hlp<T>::norm_type norm_type;
+    typedef norm_type Tsc;
+    typedef typename cublas_real_types::cublas_real_type_hlp<T>::type redef_type;
+    bool location;
+
+    gpu_vector_operations(size_t sz_, cublas_wrap* cuBLAS_ = NULL) : sz(sz_), cuBLAS(cuBLAS_) {
+        location = true;
+        ctx = hpb_dropin::make_context();
+        x_host.resize(sz);
+    }
+    gpu_vector_operations(size_t sz_, dim3, dim3) : sz(sz_), cuBLAS(NULL) {
+        location = true;
+        ctx = hpb_dropin::make_context();
+        x_host.resize(sz);
+    }
+    gpu_vector_operations(const gpu_vector_operations&) = delete;
+    gpu_vector_operations& operator=(const gpu_vector_operations&) = delete;
+    ~gpu_vector_operations() { hpb_destroy(ctx); }
+
+    // ------------------------------------------------------------ precision
+    void use_high_precision() const { use_high_precision_dot = true; }
+    void use_standard_precision() const { use_high_precision_dot = false; }
+    bool get_current_precision() const { return use_high_precision_dot; }
+
+    // ------------------------------------------------------------ lifecycle
+    void init_vector(vector_type& x) const { x = NULL; }
+    void init_vector_rank1(vector_type& x) const { x = NULL; }
+    void free_vector(vector_type& x) const {
+        if (x != NULL) cudaFree(x);
+    }
+    void start_use_vector(vector_type& x) const {
+        if (x == NULL) x = alloc(sz);
+    }
+    void start_use_vector_rank1(vector_type& x) const {
+        if (x == NULL) x = alloc(sz + 1);
+    }
+    void stop_use_vector(vector_type&) const {}
+    size_t get_vector_size() const { return sz; }
+    size_t get_l2_size() const { return size_t(std::sqrt(Tsc(sz))); }
+    bool device_location() const { return location; }
+
+    // ------------------------------------------------------------ host views
+    vector_type view(const vector_type& x) const {
+        if (x == nullptr) return nullptr;
+        d2h(x_host.data(), x, sz);
+        return x_host.data();
+    }
+    void set(vector_type& x) const {
+        if (x != nullptr) h2d(x, x_host.data(), sz);
+    }
+    void set(const vector_type& x_host_, vector_type& x_) {
+        if (x_ != nullptr) h2d(x_, x_host_, sz);
+    }
+    void get(vector_type& x_, vector_type& x_host_) {
+        if (x_ != nullptr) d2h(x_host_, x_, sz);
+    }
+    vector_type get_buffer() { return x_host.data(); }
+    void debug_view(const vector_type& vec, const std::string& f_name) const {
+        vector_type h = view(vec);
+        std::ofstream f(f_name);
+        for (size_t j = 0; j < sz; j++) f << std::scientific << std::setprecision(16) << h[j] << (j + 1 < sz ? "\n" : "");
+    }
+
+    // ------------------------------------------------------------ reductions
+    bool check_is_valid_number(const vector_type& x) const {
+        int ok = 1;
+        hpb_dropin::check(A::isfinite(ctx, int64_t(sz), x, &ok), ctx, "check_is_valid_number");
+        return ok != 0;
+    }
+    scalar_type scalar_prod(const vector_type& x, const vector_type& y) const {
+        double o[4];
+        if (use_high_precision_dot)
+            hpb_dropin::check(A::dot2(ctx, int64_t(sz), x, y, o), ctx, "scalar_prod");
+        else
+            hpb_dropin::check(A::dot(ctx, int64_t(sz), x, y, o), ctx, "scalar_prod");
+        return hpb_dropin::value_of<T>::from(o);
+    }
+    void scalar_prod(const vector_type& x, const vector_type& y, scalar_type* result) {
+        result[0] = scalar_prod(x, y);
+    }
+    redef_type absolute_sum(const vector_type& x) const {
+        double o[4];
+        if (use_high_precision_dot)
+            hpb_dropin::check(A::asum2(ctx, int64_t(sz), x, o), ctx, "absolute_sum");
+        else
+            hpb_dropin::check(A::asum(ctx, int64_t(sz), x, o), ctx, "absolute_sum");
+        return redef_type(o[0]);
+    }
+    void absolute_sum(const vector_type& x, redef_type* result) { result[0] = absolute_sum(x); }
+    Tsc norm(const vector_type& x) const { return Tsc(norm_n(x, sz)); }
+    Tsc norm_l2(const vector_type& x) const { return norm(x) / std::sqrt(Tsc(sz)); }
+    // norm of [x; val_x] (the reference builds an (sz+1)-vector,
+    // gpu_vector_operations.h:343-366); here the extra square is merged into
+    // the compensated sum of squares on the host.
+    Tsc norm_rank1(const vector_type& x, const scalar_type val_x) { return Tsc(norm_ext(x, val_x)); }
+    Tsc norm_rank1_(const vector_type& x, const scalar_type val_x) {
+        return Tsc(norm_ext(x, scalar_type(Tsc(sz)) * val_x));
+    }
+    Tsc norm_rank1_l2(const vector_type& x, const scalar_type val_x) { return norm_rank1_(x, val_x) / std::sqrt(Tsc(sz)); }
+    void norm(const vector_type& x, Tsc* result) { result[0] = norm(x); }
+    Tsc normalize(vector_type& x) {
+        Tsc nr = norm(x);
+        scale(scalar_type(Tsc(1) / nr), x);
+        return nr;
+    }
+    void normalize(vector_type& x, Tsc* nr) { nr[0] = normalize(x); }
+
+    // ------------------------------------------------------------ elementwise
+    void assign_scalar(const scalar_type scalar, vector_type& x) const {
+        hpb_dropin::check(A::fill(ctx, int64_t(sz), A::s(scalar), x), ctx, "assign_scalar");
+    }
+    void add_mul_scalar(const scalar_type scalar, const scalar_type mul_x, vector_type& x) const {
+        hpb_dropin::check(A::add_scalar(ctx, int64_t(sz), A::s(scalar), A::s(mul_x), x), ctx, "add_mul_scalar");
+    }
+    void scale(const T alpha, vector_type& x) const {
+        hpb_dropin::check(A::scal(ctx, int64_t(sz), A::s(alpha), x, x), ctx, "scale");
+    }
+    void assign(const vector_type& x, vector_type& y) const {
+        hpb_dropin::check(hpb_copy(ctx, int64_t(sz), sizeof(T), x, y), ctx, "assign");
+    }
+    void swap(vector_type& x, vector_type& y) const {
+        hpb_dropin::check(hpb_swap(ctx, int64_t(sz), sizeof(T), x, y), ctx, "swap");
+    }
+    void make_abs_copy(const vector_type& x, vector_type& y) const {
+        hpb_dropin::check(A::abs(ctx, int64_t(sz), x, y), ctx, "make_abs_copy");
+    }
+    void make_abs(vector_type& x) const { hpb_dropin::check(A::abs(ctx, int64_t(sz), x, x), ctx, "make_abs"); }
+    // y := mul_x*x
+    void assign_mul(const scalar_type mul_x, const vector_type& x, vector_type& y) const {
+        hpb_dropin::check(A::scal(ctx, int64_t(sz), A::s(mul_x), x, y), ctx, "assign_mul");
+    }
+    // y := y + mul_x*x
+    void add_mul(scalar_type mul_x, const vector_type& x, vector_type& y) const {
+        hpb_dropin::check(A::axpy(ctx, int64_t(sz), A::s(mul_x), x, y), ctx, "add_mul");
+    }
+    // z := mul_x*x + mul_y*y
+    void assign_mul(const scalar_type mul_x, const vector_type& x, const scalar_type mul_y, const vector_type& y,
+                    vector_type& z) const {
+        hpb_dropin::check(A::lincomb2(ctx, int64_t(sz), A::s(mul_x), x, A::s(mul_y), y, z), ctx, "assign_mul");
+    }
+    // y := mul_x*x + mul_y*y
+    void add_mul(const scalar_type mul_x, const vector_type& x, const scalar_type mul_y, vector_type& y) const {
+        hpb_dropin::check(A::axpby(ctx, int64_t(sz), A::s(mul_x), x, A::s(mul_y), y), ctx, "add_mul");
+    }
+    // z := mul_x*x + mul_y*y + mul_z*z
+    void add_mul(const scalar_type mul_x, const vector_type& x, const scalar_type mul_y, const vector_type& y,
+                 const scalar_type mul_z, vector_type& z) const {
+        hpb_dropin::check(A::axpbypcz(ctx, int64_t(sz), A::s(mul_x), x, A::s(mul_y), y, A::s(mul_z), z), ctx,
+                          "add_mul");
+    }
+    // z := (mul_x*x).*(mul_y*y)
+    void mul_pointwise(const scalar_type mul_x, const vector_type& x, const scalar_type mul_y, const vector_type& y,
+                       vector_type& z) const {
+        hpb_dropin::check(A::mulpw(ctx, int64_t(sz), A::s(mul_x), x, A::s(mul_y), y, z), ctx, "mul_pointwise");
+    }
+    // x := x.*(mul_y*y)
+    void mul_pointwise(vector_type& x, const scalar_type mul_y, const vector_type& y) const {
+        hpb_dropin::check(A::mulpw(ctx, int64_t(sz), A::s(scalar_type(1)), x, A::s(mul_y), y, x), ctx, "mul_pointwise");
+    }
+    // z := (mul_x*x)./(mul_y*y)
+    void div_pointwise(const scalar_type mul_x, const vector_type& x, const scalar_type mul_y, const vector_type& y,
+                       vector_type& z) const {
+        hpb_dropin::check(A::divpw(ctx, int64_t(sz), A::s(mul_x), x, A::s(mul_y), y, z), ctx, "div_pointwise");
+    }
+    // x := x./(mul_y*y)
+    void div_pointwise(vector_type& x, const scalar_type mul_y, const vector_type& y) const {
+        hpb_dropin::check(A::divpw(ctx, int64_t(sz), A::s(scalar_type(1)), x, A::s(mul_y), y, x), ctx, "div_pointwise");
+    }
+    // z := mul_x*x + mul_y*y + mul_w*w + mul_z*z
+    void add_mul(const scalar_type mul_x, const vector_type& x, const scalar_type mul_y, const vector_type& y,
+                 const scalar_type mul_w, const vector_type& w, const scalar_type mul_z, vector_type& z) const {
+        hpb_dropin::check(A::axpbypcwpdz(ctx, int64_t(sz), A::s(mul_x), x, A::s(mul_y), y, A::s(mul_w), w,
+                                         A::s(mul_z), z), ctx, "add_mul");
+    }
+    // z := mul_x*x + mul_y*y + mul_v*v + mul_w*w
+    void assign_mul(scalar_type mul_x, const vector_type& x, const scalar_type mul_y, const vector_type& y,
+                    scalar_type mul_v, const vector_type& v, const scalar_type mul_w, const vector_type& w,
+                    vector_type& z) const {
+        hpb_dropin::check(A::lincomb4(ctx, int64_t(sz), A::s(mul_x), x, A::s(mul_y), y, A::s(mul_v), v, A::s(mul_w),
+                                      w, z), ctx, "assign_mul");
+    }
+    void set_value_at_point(scalar_type val_x, size_t at, vector_type& x) { set_value_at_point(val_x, at, x, sz); }
+    void set_value_at_point(scalar_type val_x, size_t at, vector_type& x, size_t sz_l) {
+        if (at >= sz_l) return;  // the reference kernel ignores out-of-range positions
+        sync();
+        h2d(x + at, &val_x, 1);
+    }
+    T get_value_at_point(size_t at, vector_type& x) {
+        if (at >= sz) throw std::runtime_error("get_value_at_point: position out of range");
+        T v;
+        sync();
+        d2h(&v, x + at, 1);
+        return v;
+    }
+    // x := U(0,1] per entry (complex: re and im independently)
+    void assign_random(vector_type& vec) { assign_random(vec, scalar_type(0), scalar_type(1)); }
+    void assign_random(vector_type& vec, scalar_type a, scalar_type b) {
+        hpb_dropin::check(A::random(ctx, int64_t(sz), seed_++, A::s(a), A::s(b), vec), ctx, "assign_random");
+    }
+    void set_random_seed(uint64_t s) { seed_ = s; }
+
+    // ------------------------------------------------------------ extensions
+    hpb_context* context() const { return ctx; }
+    void sync() const { hpb_dropin::check(hpb_synchronize(ctx), ctx, "synchronize"); }
+
+private:
+    using A = hpb_dropin::abi<T>;
+    mutable std::vector<T> x_host;
+    cublas_wrap* cuBLAS;
+    size_t sz;
+    hpb_context* ctx = nullptr;
+    mutable bool use_high_precision_dot = false;
+    uint64_t seed_ = 0x5eed;
+
+    static T* alloc(size_t n) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess)
+            throw std::runtime_error("gpu_vector_operations: cudaMalloc failed");
+        return static_cast<T*>(p);
+    }
+    void h2d(T* d, const T* h, size_t n) const {
+        if (cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+            throw std::runtime_error("gpu_vector_operations: host to device copy failed");
+    }
+    void d2h(T* h, const T* d, size_t n) const {
+        if (cudaMemcpy(h, d, n * sizeof(T), cudaMemcpyDeviceToHost) != cudaSuccess)
+            throw std::runtime_error("gpu_vector_operations: device to host copy failed");
+    }
+    double norm_n(const T* x, size_t n) const {
+        double o[4];
+        if (use_high_precision_dot)
+            hpb_dropin::check(A::nrm2(ctx, int64_t(n), x, o), ctx, "norm");
+        else
+            hpb_dropin::check(A::nrm2plain(ctx, int64_t(n), x, o), ctx, "norm");
+        return o[0];
+    }
+    double norm_ext(const T* x, scalar_type v) const {
+        double o[4];
+        if (use_high_precision_dot)
+            hpb_dropin::check(A::nrm2(ctx, int64_t(sz), x, o), ctx, "norm_rank1");
+        else
+            hpb_dropin::check(A::nrm2plain(ctx, int64_t(sz), x, o), ctx, "norm_rank1");
+        double a = double(std::abs(v));
+        return std::sqrt(o[1] + (o[2] + a * a));
+    }
+};
+
+#endif

@@ -93,6 +93,41 @@ def ref():
     return _REF
 
 
+_REF_SOLVER = None
+
+
+def ref_solver():
+    """The reference's own CPU Krylov solvers (oracle/_ref), or None."""
+    global _REF_SOLVER
+    if _REF_SOLVER is None:
+        so = HERE / "_ref" / "libhpb_ref_solver.so"
+        if not so.exists():
+            return None
+        lib = C.CDLL(str(so))
+        lib.ref_cpu_solve_f64.argtypes = [C.c_int, C.c_int, P, P, P, P, P, C.c_int, D, C.c_int, C.c_int, C.c_int,
+                                          C.POINTER(C.c_int), PD, PD]
+        lib.ref_cpu_solve_f64.restype = C.c_int
+        _REF_SOLVER = lib
+    return _REF_SOLVER
+
+
+def ref_cpu_solve(method: int, A, b: np.ndarray, x0: np.ndarray, basis: int, rel_tol: float, max_iters: int,
+                  high_prec: int = 1, threads: int = -1):
+    """Run the reference's bicgstabl (method 0) / gmres (method 1) on the CPU.
+    Returns (converged, iters, monitor residual norm, seconds, x)."""
+    lib = ref_solver()
+    if lib is None:
+        return None
+    x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+    bb = np.ascontiguousarray(b, dtype=np.float64).copy()
+    it = C.c_int()
+    res = C.c_double()
+    sec = C.c_double()
+    ok = lib.ref_cpu_solve_f64(method, A.n, _ptr(A.row_ptr), _ptr(A.col_ind), _ptr(A.val), _ptr(bb), _ptr(x), basis,
+                               rel_tol, max_iters, high_prec, threads, C.byref(it), C.byref(res), C.byref(sec))
+    return bool(ok), it.value, res.value, sec.value, x
+
+
 # ----------------------------------------------------------------- helpers
 def exact_dot(x: np.ndarray, y: np.ndarray) -> tuple:
     """Exact sum conj(x_i) y_i as (hi, lo) (real) or (hi, lo) complex pairs."""

@@ -1,0 +1,115 @@
+"""GPU parity of the CSR SpMV (through the C ABI) against a numpy
+float64/complex128 restatement.  Tolerance per row:
+|gpu - ref| <= 4 (nnz_row + 2) eps(type) (|alpha| sum_k |a_k||x_k| + |beta||y|)."""
+import numpy as np
+import pytest
+
+from gpu_utils import EPS, dev, host
+from high_precision_blas1_b200 import _lib, problems
+
+pytestmark = pytest.mark.gpu
+
+DT = {"f32": np.float32, "f64": np.float64, "c64": np.complex64, "c128": np.complex128}
+WIDE = {"f32": np.float64, "f64": np.float64, "c64": np.complex128, "c128": np.complex128}
+
+
+def random_csr(rng, rows, cols, density, long_rows=(), empty_rows=()):
+    rp = [0]
+    ci = []
+    for r in range(rows):
+        if r in empty_rows:
+            k = 0
+        elif r in long_rows:
+            k = cols
+        else:
+            k = rng.binomial(cols, density)
+        c = np.sort(rng.choice(cols, size=k, replace=False)) if k else np.zeros(0, dtype=np.int64)
+        ci.extend(c.tolist())
+        rp.append(len(ci))
+    return problems.CSR(rows, np.array(rp, dtype=np.int32), np.array(ci, dtype=np.int32),
+                        rng.standard_normal(len(ci)))
+
+
+def spmv(ctx, torch, t, A, alpha, x, beta, y):
+    d = [dev(torch, a) for a in (A.row_ptr, A.col_ind, A.val.astype(DT[t]), x.astype(DT[t]), y.astype(DT[t]))]
+    st = getattr(_lib.lib, f"hpb_csr_spmv_{t}")(ctx.h, A.n, x.shape[0], A.nnz, d[0].data_ptr(), d[1].data_ptr(),
+                                               d[2].data_ptr(), _lib.scalar(t, alpha), d[3].data_ptr(),
+                                               _lib.scalar(t, beta), d[4].data_ptr())
+    ctx.check(st, "spmv")
+    torch.cuda.synchronize()
+    return host(d[4])
+
+
+def check(A, t, alpha, x, beta, y, got):
+    W = WIDE[t]
+    v = A.val.astype(DT[t]).astype(W)
+    xs = x.astype(DT[t]).astype(W)
+    ys = y.astype(DT[t]).astype(W)
+    want = alpha * problems.CSR(A.n, A.row_ptr, A.col_ind, v).matvec(xs) + (beta * ys if beta != 0 else 0)
+    absA = problems.CSR(A.n, A.row_ptr, A.col_ind, np.abs(v)).matvec(np.abs(xs))
+    rowlen = np.diff(A.row_ptr)
+    tol = 4 * (rowlen + 2) * EPS[t] * (abs(alpha) * absA + (abs(beta) * np.abs(ys) if beta != 0 else 0)) + 1e-300
+    err = np.abs(got.astype(W) - want)
+    assert np.all(err <= tol), (t, float(np.max(err / tol)))
+
+
+@pytest.mark.parametrize("t", ["f32", "f64", "c64", "c128"])
+def test_spmv_stencils(gpu, t):
+    ctx, torch = gpu
+    rng = np.random.default_rng(1)
+    for A in (problems.convdiff2d(37), problems.poisson3d_aniso(11), problems.diffusion3d_lognormal(12, seed=3)):
+        cplx = t.startswith("c")
+        if cplx:
+            A = problems.CSR(A.n, A.row_ptr, A.col_ind, A.val * (1 + 0.3j))
+        x = rng.standard_normal(A.n) + (1j * rng.standard_normal(A.n) if cplx else 0)
+        y = rng.standard_normal(A.n) + (1j * rng.standard_normal(A.n) if cplx else 0)
+        for alpha, beta in ((1.0, 0.0), (2.5, -0.75), (-1.0, 1.0)):
+            if cplx:
+                alpha, beta = complex(alpha, 0.5), complex(beta, -0.25) if beta else 0.0
+            got = spmv(ctx, torch, t, A, alpha, x, beta, y)
+            check(A, t, alpha, x, beta, y, got)
+
+
+@pytest.mark.parametrize("t", ["f64", "c128", "f32"])
+def test_spmv_ragged_empty_and_long_rows(gpu, t):
+    """Empty rows, rows longer than the shared-memory staging capacity, and
+    a row count that is not a multiple of the block's 256 rows."""
+    ctx, torch = gpu
+    rng = np.random.default_rng(5)
+    A = random_csr(rng, 1000, 3000, 0.002, long_rows=(3, 700), empty_rows=(0, 1, 999))
+    if t.startswith("c"):
+        A = problems.CSR(A.n, A.row_ptr, A.col_ind, A.val + 1j * rng.standard_normal(A.nnz))
+    x = rng.standard_normal(3000) + (1j * rng.standard_normal(3000) if t.startswith("c") else 0)
+    y = rng.standard_normal(1000) + (1j * rng.standard_normal(1000) if t.startswith("c") else 0)
+    got = spmv(ctx, torch, t, A, 1.5, x, -0.5, y)
+    check(A, t, 1.5, x, -0.5, y, got)
+
+
+def test_spmv_beta_zero_ignores_y(gpu):
+    ctx, torch = gpu
+    A = problems.convdiff2d(20)
+    x = np.ones(A.n)
+    y = np.full(A.n, np.nan)
+    got = spmv(ctx, torch, "f64", A, 1.0, x, 0.0, y)
+    assert np.all(np.isfinite(got))
+    assert np.allclose(got, A.matvec(x))
+
+
+def test_spmv_zero_rows_and_bad_args(gpu):
+    ctx, torch = gpu
+    L = _lib.lib
+    assert L.hpb_csr_spmv_f64(ctx.h, 0, 0, 0, None, None, None, 1.0, None, 0.0, None) == 0
+    assert L.hpb_csr_spmv_f64(ctx.h, -1, 0, 0, None, None, None, 1.0, None, 0.0, None) == -1
+    assert L.hpb_csr_spmv_f64(ctx.h, 4, 4, 4, None, None, None, 1.0, None, 0.0, None) == -1
+
+
+def test_csr_diagonal(gpu):
+    ctx, torch = gpu
+    A = problems.convdiff2d(16)
+    d = dev(torch, np.zeros(A.n))
+    rp, ci, va = dev(torch, A.row_ptr), dev(torch, A.col_ind), dev(torch, A.val)
+    ctx.check(_lib.lib.hpb_csr_diag_f64(ctx.h, A.n, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), d.data_ptr()))
+    torch.cuda.synchronize()
+    want = np.array([A.val[A.row_ptr[r]:A.row_ptr[r + 1]][A.col_ind[A.row_ptr[r]:A.row_ptr[r + 1]] == r][0]
+                     for r in range(A.n)])
+    assert np.array_equal(host(d), want)
