@@ -67,7 +67,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.proc = None
         time.sleep(0.15)
@@ -149,8 +149,86 @@ def ref_dot2(ref, args, cores):
     }
 
 
+SOLVER_N = 1024
+SOLVER_L = 4
+SOLVER_TOL = 1e-10
+REF_CAL = ROOT / "tests" / "golden" / "ref_solver_calibration.json"
+
+
+def solver_problem(rank=0):
+    from high_precision_blas1_b200 import problems
+    A = problems.convdiff2d(SOLVER_N, peclet=50.0)
+    b = problems.rhs_uniform(A.n, 2024 + rank)
+    return A, b
+
+
+class quiet_stdout:
+    """Silence fd 1 (the reference's logger prints its 'failed to converge'
+    line there when a bounded sample stops at its iteration cap)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        self.null = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(self.null, 1)
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+        os.close(self.null)
+
+
+def ref_cpu_cycles_sample(A, b, cycles, threads=-1):
+    """Time `cycles` BiCGStab(4) cycles of the reference's own CPU solver."""
+    import oracle
+    with quiet_stdout():
+        r = oracle.ref_cpu_solve(0, A, b, np.zeros(A.n), SOLVER_L, 1e-300, SOLVER_L * cycles, 1, threads)
+    ok, it, res, sec, x = r
+    return sec / (it / SOLVER_L), it
+
+
+def ref_full_iters():
+    """Iterations the reference CPU BiCGStab(4) needs on this system (measured
+    once to convergence by tests/golden/make_solver_calibration.py)."""
+    try:
+        return int(json.loads(REF_CAL.read_text())["iters"])
+    except Exception:
+        return None
+
+
 def ref_solver(args, cores):
-    raise SystemExit("solver workload not built yet")
+    A, b = solver_problem(0)
+    iters = ref_full_iters()
+    per_step_cycles = 4
+    ref_cpu_cycles_sample(A, b, 1)  # warm-up
+    t = []
+    for _ in range(args.steps):
+        sec_per_cycle, _ = ref_cpu_cycles_sample(A, b, per_step_cycles)
+        t.append(sec_per_cycle)
+    sec_per_cycle = float(np.median(t))
+    full = iters if iters else 0
+    value = sec_per_cycle * (full / SOLVER_L) if full else None
+    return {
+        "impl": "reference", "metric": "time_to_1e-10_residual", "value": value, "unit": "s",
+        "higher_is_better": False, "n_gpus": 0, "steps": args.steps, "warmup": 1,
+        "ms_per_step": sec_per_cycle * per_step_cycles * 1e3, "dtype": "f64", "data": "synthetic",
+        "config": solver_config(),
+        "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "reference",
+                         "sample": f"{per_step_cycles} BiCGStab(4) cycles per step of the reference's "
+                                   f"bicgstabl.h over cpu_vector_operations<double> (Dot2, threaded_reduction "
+                                   f"with {cores} threads, OpenMP CSR product); time per cycle x "
+                                   f"{full // SOLVER_L if full else '?'} cycles to converge"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "sec_per_cycle": sec_per_cycle, "full_iters": full,
+    }
+
+
+def solver_config():
+    return {"workload": "BiCGStab(4) f64 + Dot2, 2-D convection-diffusion 5-point 1024x1024 "
+                        "(n=1048576, nnz=5238784), Peclet 50, RHS U[-1,1], tol 1e-10",
+            "n": SOLVER_N * SOLVER_N, "nnz": 5238784, "basis": SOLVER_L, "rel_tol": SOLVER_TOL,
+            "l2": "working set (matrix 84 MB + 13 vectors of 8 MB) > 126 MB L2",
+            "parallelism": "replicas"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -243,6 +321,157 @@ def bench_dot2(args, ws, rank, local, torch, dist):
     }
 
 
+def spmv_roofline(torch, L, ctx, A, reps=40):
+    """Live per-launch time of the CSR SpMV on the solver's matrix, two
+    matrix copies rotated (2 x 84 MB > L2)."""
+    mats = []
+    for _ in range(2):
+        mats.append([torch.from_numpy(a).cuda() for a in (A.row_ptr, A.col_ind, A.val)])
+    xs = [torch.rand(A.n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    ys = [torch.empty(A.n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    stream = torch.cuda.current_stream()
+
+    def launch(i):
+        rp, ci, va = mats[i % 2]
+        ctx.check(L.hpb_csr_spmv_f64(ctx.h, A.n, A.n, A.nnz, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), 1.0,
+                                     xs[i % 2].data_ptr(), 0.0, ys[i % 2].data_ptr()))
+    for i in range(4):
+        launch(i)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(reps):
+        launch(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    us = e0.elapsed_time(e1) * 1e3 / reps
+    alg = 12.0 * A.nnz + 4.0 * (A.n + 1) + 8.0 * A.n + 8.0 * A.n
+    hbm, src = peaks()
+    ach = alg / (us * 1e-6) / 1e9
+    return {"kernel": "csr_stream_kernel<double>", "bound": "hbm", "achieved": ach, "peak": hbm, "peak_source": src,
+            "unit": "GB/s", "frac": ach / hbm, "traffic": None, "algorithmic_bytes_per_launch": alg,
+            "avg_launch_us": us}
+
+
+def bench_solver(args, ws, rank, local, torch, dist):
+    import ctypes as C
+    from high_precision_blas1_b200 import Context, _lib
+    L = _lib.lib
+    A, b = solver_problem(rank)
+    dA = [torch.from_numpy(a).cuda() for a in (A.row_ptr, A.col_ind, A.val)]
+    db = torch.from_numpy(b).cuda()
+    dx = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    p = _lib.solver_params("bicgstabl", basis=SOLVER_L, rel_tol=SOLVER_TOL, max_iters=200000, high_precision=True)
+    rep = _lib.hpb_solver_report()
+    stream = torch.cuda.current_stream()
+
+    def one():
+        dx.zero_()
+        st = L.hpb_csr_solve_f64(C.byref(p), A.n, A.nnz, dA[0].data_ptr(), dA[1].data_ptr(), dA[2].data_ptr(),
+                                 db.data_ptr(), dx.data_ptr(), C.byref(rep), None, 0)
+        if st != 0:
+            raise RuntimeError(f"solve failed: status {st}, iters {rep.iters}")
+    for _ in range(args.warmup):
+        one()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    launches0 = L.hpb_launch_count()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    iters, rel = [], []
+    for i in range(args.steps):
+        evs[i][0].record(stream)
+        one()
+        evs[i][1].record(stream)
+        iters.append(rep.iters)
+        rel.append(rep.true_resid_norm / rep.true_rhs_norm)
+    torch.cuda.synchronize()
+    launches = L.hpb_launch_count() - launches0
+    clocks = clk.stop()
+    times = [a.elapsed_time(bb) * 1e-3 for a, bb in evs]
+    t_step = float(np.mean(times))
+    if dist:
+        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step = tt.item()
+    with Context(local, stream.cuda_stream) as ctx:
+        roof = spmv_roofline(torch, L, ctx, A)
+        dot2 = dot2_probe(torch, L, ctx)
+
+    # e2e: host CSR + host b -> C ABI (copies in, solves, copies x out)
+    hx = np.zeros(A.n)
+    e2e = []
+    for _ in range(max(1, min(args.steps, 2))):
+        hx[:] = 0
+        t0 = time.perf_counter()
+        st = L.hpb_csr_solve_f64_host(C.byref(p), A.n, A.nnz, A.row_ptr.ctypes.data, A.col_ind.ctypes.data,
+                                      A.val.ctypes.data, b.ctypes.data, hx.ctypes.data, C.byref(rep), None, 0)
+        e2e.append(time.perf_counter() - t0)
+        assert st == 0
+    h2d = A.row_ptr.nbytes + A.col_ind.nbytes + A.val.nbytes + b.nbytes + hx.nbytes
+    return {
+        "metric": "time_to_1e-10_residual", "value": t_step, "unit": "s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": solver_config(),
+        "solver": {"path": "plain drop-in (host-synchronised reductions)", "iters": iters,
+                   "true_rel_residual": rel, "cycles": [i // SOLVER_L for i in iters]},
+        "roofline": roof,
+        "e2e": {"value": float(np.mean(e2e)), "unit": "s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(hx.nbytes)},
+        "gpu_launches": int(launches // max(1, args.steps)),
+        "gpu_launches_note": "library kernel launches per solve",
+        "clocks": clocks,
+        "dot2": dot2,
+    }
+
+
+def dot2_probe(torch, L, ctx, reps=200):
+    """Config-1 Dot2 (n = 2^20 f64 GenDot) throughput, 16 pairs rotated."""
+    n = 1 << 20
+    x = np.zeros(n)
+    y = np.zeros(n)
+    L.hpb_gendot_f64(1, n, 1e20, x.ctypes.data, y.ctypes.data, None)
+    R = 16
+    xs = [torch.from_numpy(x).cuda() for _ in range(R)]
+    ys = [torch.from_numpy(y).cuda() for _ in range(R)]
+    out = torch.zeros(64, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream()
+    for i in range(10):
+        ctx.check(L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(), out.data_ptr()))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(reps):
+        ctx.check(L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(), out.data_ptr()))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    us = e0.elapsed_time(e1) * 1e3 / reps
+    hbm, src = peaks()
+    gbs = 16.0 * n / (us * 1e-6) / 1e9
+    return {"workload": "dot2 f64 GenDot n=1048576 cond~1e20, 16 pairs rotated (268 MB > L2)",
+            "value": gbs, "unit": "GB/s", "us_per_call": us, "frac_of_hbm": gbs / hbm, "peak_source": src}
+
+
+def cpu_baseline_solver(t_gpu_iters):
+    import oracle
+    if oracle.ref_solver() is None:
+        return None
+    A, b = solver_problem(0)
+    cores = os.cpu_count() or 1
+    cycles = 4
+    sec_per_cycle, _ = ref_cpu_cycles_sample(A, b, cycles)
+    full = ref_full_iters() or t_gpu_iters
+    return {"value": sec_per_cycle * full / SOLVER_L, "unit": "s", "cores": cores, "kind": "reference",
+            "sample": f"{cycles} BiCGStab(4) cycles of the reference's bicgstabl.h over "
+                      f"cpu_vector_operations<double> (Dot2, {cores} threads) timed, x {full // SOLVER_L} cycles "
+                      f"to converge ({'reference run to convergence' if ref_full_iters() else 'GPU iteration count'})"}
+
+
 def cpu_baseline_dot2():
     import oracle
     ref = oracle.ref()
@@ -278,7 +507,7 @@ def main():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["solver", "dot2"], default="dot2")
+    ap.add_argument("--workload", choices=["solver", "dot2"], default="solver")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.steps is None:
@@ -306,10 +535,13 @@ def main():
         if args.workload == "dot2":
             res = bench_dot2(args, ws, rank, local, torch, dist)
         else:
-            raise SystemExit("solver workload not built yet")
+            res = bench_solver(args, ws, rank, local, torch, dist)
         if rank == 0:
             if not args.no_cpu_baseline:
-                res["cpu_baseline"] = cpu_baseline_dot2()
+                if args.workload == "dot2":
+                    res["cpu_baseline"] = cpu_baseline_dot2()
+                else:
+                    res["cpu_baseline"] = cpu_baseline_solver(int(np.max(res["solver"]["iters"])))
             print(json.dumps(res))
     finally:
         if dist is not None:

@@ -46,7 +46,11 @@ class CSR:
     def matvec(self, x: np.ndarray) -> np.ndarray:
         """Reference product for tests (numpy, float64/complex128)."""
         prod = self.val * x[self.col_ind]
-        return np.add.reduceat(prod, self.row_ptr[:-1]) if self.n else prod[:0]
+        rows = np.repeat(np.arange(self.n), np.diff(self.row_ptr))
+        if np.iscomplexobj(prod):
+            return (np.bincount(rows, weights=prod.real, minlength=self.n)
+                    + 1j * np.bincount(rows, weights=prod.imag, minlength=self.n))
+        return np.bincount(rows, weights=prod, minlength=self.n)
 
 
 def _assemble(n: int, cols: np.ndarray, vals: np.ndarray) -> CSR:
