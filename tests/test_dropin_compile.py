@@ -1,0 +1,60 @@
+"""CPU test: the reference's own solver headers compile unchanged against the
+C++ drop-in (include/hpblas1_dropin), for real and complex scalar types.
+Skipped where the reference sources are not present."""
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+REF = Path("/root/reference/source")
+
+SRC = r'''
+#include <common/gpu_vector_operations.h>
+#include <common/csr/gpu_matrix.h>
+#include <common/csr/linear_operator.h>
+#include <common/csr/preconditioner.h>
+#include <numerical_algos/lin_solvers/default_monitor.h>
+#include <numerical_algos/lin_solvers/bicgstabl.h>
+#include <numerical_algos/lin_solvers/bicgstab.h>
+#include <numerical_algos/lin_solvers/gmres.h>
+#include <utils/log.h>
+#include <thrust/complex.h>
+template <class T> int run(int n) {
+    using vec_ops_t = gpu_vector_operations<T>;
+    using mat_t = csr::gpu_matrix<vec_ops_t, cublas_wrap>;
+    using lin_op_t = csr::linear_operator<vec_ops_t, mat_t>;
+    using prec_t = csr::preconditioner<vec_ops_t, lin_op_t, mat_t>;
+    using log_t = utils::log_std;
+    using mon_t = numerical_algos::lin_solvers::default_monitor<vec_ops_t, log_t>;
+    cublas_wrap cublas(true);
+    vec_ops_t vec_ops(n, &cublas);
+    mat_t mat(&cublas);
+    lin_op_t lin_op(&vec_ops, &mat);
+    prec_t prec(&vec_ops);
+    log_t log;
+    numerical_algos::lin_solvers::bicgstabl<lin_op_t, prec_t, vec_ops_t, mon_t, log_t> s1(&vec_ops, &log);
+    numerical_algos::lin_solvers::gmres<lin_op_t, prec_t, vec_ops_t, mon_t, log_t, 300> s2(&vec_ops, &log);
+    numerical_algos::lin_solvers::bicgstab<lin_op_t, prec_t, vec_ops_t, mon_t, log_t> s3(&vec_ops, &log);
+    s1.set_preconditioner(&prec); s1.set_basis_size(4); s1.monitor().init(1e-10, 0, 100);
+    s2.set_preconditioner(&prec); s2.set_restarts(30); s2.monitor().init(1e-10, 0, 100);
+    s3.set_preconditioner(&prec); s3.monitor().init(1e-10, 0, 100);
+    T *x, *b; vec_ops.init_vector(x); vec_ops.start_use_vector(x); vec_ops.init_vector(b); vec_ops.start_use_vector(b);
+    vec_ops.use_high_precision();
+    bool ok = s1.solve(lin_op, b, x) && s2.solve(lin_op, b, x) && s3.solve(lin_op, b, x);
+    vec_ops.free_vector(x); vec_ops.free_vector(b);
+    return ok;
+}
+int main() { return run<double>(10) + run<float>(10) + run<thrust::complex<double> >(10) + run<thrust::complex<float> >(10); }
+'''
+
+
+@pytest.mark.skipif(not REF.exists(), reason="reference sources not present")
+def test_reference_solvers_compile_against_dropin(tmp_path):
+    src = tmp_path / "dropin_driver.cu"
+    src.write_text(SRC)
+    cmd = ["nvcc", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-w", "-c",
+           "-I", str(ROOT / "include" / "hpblas1_dropin"), "-I", str(ROOT / "include"), "-I", str(REF),
+           str(src), "-o", str(tmp_path / "d.o")]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-3000:]

@@ -1,0 +1,57 @@
+"""The reference's own bicgstabl.h / gmres.h / default_monitor.h, compiled
+unchanged against the C++ drop-in (oracle/_ref/libhpb_ref_dropin.so), run
+beside the library's solvers on the same device arrays.  Real data: the
+inner products are symmetric, so both run the same recurrences on the same
+kernels and must agree bit for bit (iteration count and iterate)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from gpu_utils import dev, host
+from high_precision_blas1_b200 import _lib, problems
+
+pytestmark = pytest.mark.gpu
+
+
+def ref_dropin():
+    so = oracle.HERE / "_ref" / "libhpb_ref_dropin.so"
+    if not so.exists():
+        pytest.skip("oracle/_ref/libhpb_ref_dropin.so not built")
+    lib = C.CDLL(str(so))
+    lib.ref_dropin_solve_f64.argtypes = [C.c_int, C.c_int, C.c_int64] + [C.c_void_p] * 5 + [
+        C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    return lib
+
+
+@pytest.mark.parametrize("method,basis,N", [(0, 4, 64), (0, 2, 40), (1, 30, 24)])
+def test_reference_solver_over_dropin_matches_library_solver(gpu, method, basis, N):
+    ctx, torch = gpu
+    lib = ref_dropin()
+    A = problems.convdiff2d(N)
+    b = problems.rhs_uniform(A.n, 11)
+    tol = 1e-10 if method == 0 else 1e-8
+    d = [dev(torch, a) for a in (A.row_ptr, A.col_ind, A.val, b)]
+    x_ref = dev(torch, np.zeros(A.n))
+    it = C.c_int()
+    res = C.c_double()
+    ok = lib.ref_dropin_solve_f64(method, A.n, A.nnz, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                  d[3].data_ptr(), x_ref.data_ptr(), basis, tol, 100000, 1, C.byref(it),
+                                  C.byref(res))
+    assert ok == 1
+    x = dev(torch, np.zeros(A.n))
+    rep = _lib.hpb_solver_report()
+    p = _lib.solver_params("bicgstabl" if method == 0 else "gmres", basis=basis, rel_tol=tol, max_iters=100000)
+    st = _lib.lib.hpb_csr_solve_f64(C.byref(p), A.n, A.nnz, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                    d[3].data_ptr(), x.data_ptr(), C.byref(rep), None, 0)
+    torch.cuda.synchronize()
+    assert st == 0
+    assert rep.iters == it.value
+    if method == 0:
+        assert np.array_equal(host(x), host(x_ref))
+    else:
+        # GMRES: host-side Givens/triangular solve in the reference runs in T,
+        # here in binary64 for every T -- identical for T = double
+        assert np.allclose(host(x), host(x_ref), rtol=1e-12, atol=1e-14)
+    assert rep.resid_norm == pytest.approx(res.value, rel=1e-12)
