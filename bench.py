@@ -362,13 +362,14 @@ def bench_solver(args, ws, rank, local, torch, dist):
     dA = [torch.from_numpy(a).cuda() for a in (A.row_ptr, A.col_ind, A.val)]
     db = torch.from_numpy(b).cuda()
     dx = torch.zeros(A.n, dtype=torch.float64, device="cuda")
-    p = _lib.solver_params("bicgstabl", basis=SOLVER_L, rel_tol=SOLVER_TOL, max_iters=200000, high_precision=True)
+    p = _lib.solver_params("bicgstabl", basis=SOLVER_L, rel_tol=SOLVER_TOL, max_iters=200000, high_precision=True,
+                           fused=not args.plain)
     rep = _lib.hpb_solver_report()
     stream = torch.cuda.current_stream()
 
-    def one():
+    def one(params=p):
         dx.zero_()
-        st = L.hpb_csr_solve_f64(C.byref(p), A.n, A.nnz, dA[0].data_ptr(), dA[1].data_ptr(), dA[2].data_ptr(),
+        st = L.hpb_csr_solve_f64(C.byref(params), A.n, A.nnz, dA[0].data_ptr(), dA[1].data_ptr(), dA[2].data_ptr(),
                                  db.data_ptr(), dx.data_ptr(), C.byref(rep), None, 0)
         if st != 0:
             raise RuntimeError(f"solve failed: status {st}, iters {rep.iters}")
@@ -398,6 +399,18 @@ def bench_solver(args, ws, rank, local, torch, dist):
         tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t_step = tt.item()
+    # the plain drop-in path (host-synchronised reductions) on the same system, for comparison
+    plain = None
+    if not args.plain:
+        pp = _lib.solver_params("bicgstabl", basis=SOLVER_L, rel_tol=SOLVER_TOL, max_iters=200000)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        one(pp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain = {"s": e0.elapsed_time(e1) * 1e-3, "iters": rep.iters,
+                 "true_rel_residual": rep.true_resid_norm / rep.true_rhs_norm}
     with Context(local, stream.cuda_stream) as ctx:
         roof = spmv_roofline(torch, L, ctx, A)
         dot2 = dot2_probe(torch, L, ctx)
@@ -417,8 +430,10 @@ def bench_solver(args, ws, rank, local, torch, dist):
         "metric": "time_to_1e-10_residual", "value": t_step, "unit": "s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": solver_config(),
-        "solver": {"path": "plain drop-in (host-synchronised reductions)", "iters": iters,
-                   "true_rel_residual": rel, "cycles": [i // SOLVER_L for i in iters]},
+        "solver": {"path": "plain drop-in (host-synchronised reductions)" if args.plain else
+                   "fused device-resident BiCGStab(4): scalars on the GPU, SpMV+Dot2 fused, one CUDA graph per cycle",
+                   "iters": iters, "true_rel_residual": rel, "cycles": [i // SOLVER_L for i in iters],
+                   "plain_dropin": plain},
         "roofline": roof,
         "e2e": {"value": float(np.mean(e2e)), "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(hx.nbytes)},
@@ -427,6 +442,121 @@ def bench_solver(args, ws, rank, local, torch, dist):
         "clocks": clocks,
         "dot2": dot2,
     }
+
+
+# ------------------------------------------------ precision / complex / learned forms
+def _timed(torch, fn):
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    out = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) * 1e-3, out
+
+
+def fused_solve(torch, A, b, method, basis, tol, precond="none", complex_=False, max_iters=20000):
+    from high_precision_blas1_b200 import _lib
+    dt = np.complex128 if complex_ else np.float64
+    d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (A.row_ptr, A.col_ind, A.val.astype(dt),
+                                                                    b.astype(dt), np.zeros(A.n, dtype=dt))]
+    p = _lib.solver_params(method, basis=basis, rel_tol=tol, max_iters=max_iters, precond=precond, fused=True)
+    rep = _lib.hpb_solver_report()
+    f = _lib.lib.hpb_csr_solve_c128 if complex_ else _lib.lib.hpb_csr_solve_f64
+    t, st = _timed(torch, lambda: f(C.byref(p), A.n, A.nnz, *[a.data_ptr() for a in d], C.byref(rep), None, 0))
+    x = d[4].cpu().numpy()
+    return t, st, rep, x
+
+
+def ir_solve(torch, A, b, inner, basis, precond="none", M=None, complex_=False, inner_tol=1e-5, max_iters=5000):
+    from high_precision_blas1_b200 import _lib
+    dt = np.complex128 if complex_ else np.float64
+    d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (A.row_ptr, A.col_ind, A.val.astype(dt),
+                                                                    b.astype(dt), np.zeros(A.n, dtype=dt))]
+    p = _lib.ir_params(inner, basis=basis, inner_rel_tol=inner_tol, inner_max_iters=max_iters, precond=precond,
+                       rel_tol=SOLVER_TOL, max_refinements=40)
+    rep = _lib.hpb_ir_report()
+    mp = [None, None, None, 0] if M is None else [d[0].data_ptr(), d[1].data_ptr(), M.data_ptr(), A.nnz]
+    f = _lib.lib.hpb_ir_solve_c128 if complex_ else _lib.lib.hpb_ir_solve_f64
+    t, st = _timed(torch, lambda: f(C.byref(p), A.n, A.nnz, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), None,
+                                    mp[0], mp[1], mp[2], mp[3], d[3].data_ptr(), d[4].data_ptr(), C.byref(rep),
+                                    None, 0))
+    x = d[4].cpu().numpy()
+    return t, st, rep, x
+
+
+def _rel(A, b, x):
+    return float(np.linalg.norm(b - A.matvec(x)) / np.linalg.norm(b))
+
+
+def bench_forms(torch, log=lambda *a: None):
+    """Configs 3-5 of the reference's benchmark family, one run each."""
+    from high_precision_blas1_b200 import problems, spai
+    out = {}
+    # ---- config 3: precision form, GMRES(50), 3-D anisotropic Poisson 128^3
+    try:
+        A = problems.poisson3d_aniso(128, eps=(1.0, 1e-2, 1e-4))
+        b = problems.rhs_uniform(A.n, 303)
+        t64, st64, r64, x64 = fused_solve(torch, A, b, "gmres", 50, SOLVER_TOL)
+        _, sto, ro, xo = fused_solve(torch, A, b, "gmres", 50, 1e-13, max_iters=40000)
+        tir, stir, rir, xir = ir_solve(torch, A, b, "gmres", 50)
+        nx = np.linalg.norm(xo)
+        out["precision_gmres50_poisson3d_aniso128"] = {
+            "n": A.n, "nnz": A.nnz,
+            "fp64_gmres50": {"s": t64, "status": st64, "iters": r64.iters, "true_rel_residual": _rel(A, b, x64),
+                             "rel_err_vs_fp64_oracle": float(np.linalg.norm(x64 - xo) / nx)},
+            "fp32_dot2_gmres50_in_fp64_refinement": {
+                "s": tir, "status": stir, "refinements": rir.refinements, "inner_iters": rir.inner_iters,
+                "true_rel_residual": _rel(A, b, xir), "rel_err_vs_fp64_oracle": float(np.linalg.norm(xir - xo) / nx)},
+            "fp64_oracle": {"tol": 1e-13, "status": sto, "iters": ro.iters},
+            "speedup": t64 / tir if stir == 0 else None}
+    except Exception as e:  # a failure here must not lose the headline line
+        out["precision_gmres50_poisson3d_aniso128"] = {"error": repr(e)}
+    # ---- config 4: complex form, BiCGStab(2), Helmholtz 2048^2
+    try:
+        A = problems.helmholtz2d(2048, ppw=10.0, damping=0.5)
+        b = problems.rhs_uniform(A.n, 404, complex_=True)
+        t128, st128, r128, x128 = fused_solve(torch, A, b, "bicgstabl", 2, SOLVER_TOL, complex_=True)
+        tir, stir, rir, xir = ir_solve(torch, A, b, "bicgstabl", 2, complex_=True, inner_tol=1e-4)
+        out["complex_bicgstab2_helmholtz2048"] = {
+            "n": A.n, "nnz": A.nnz,
+            "c128_bicgstab2": {"s": t128, "status": st128, "iters": r128.iters, "true_rel_residual": _rel(A, b, x128)},
+            "c64_dot2_bicgstab2_in_c128_refinement": {
+                "s": tir, "status": stir, "refinements": rir.refinements, "inner_iters": rir.inner_iters,
+                "true_rel_residual": _rel(A, b, xir),
+                "rel_diff_vs_c128": float(np.linalg.norm(xir - x128) / np.linalg.norm(x128))},
+            "speedup": t128 / tir if stir == 0 else None}
+    except Exception as e:
+        out["complex_bicgstab2_helmholtz2048"] = {"error": repr(e)}
+    # ---- config 5: learned preconditioner, GMRES(30), lognormal diffusion 96^3
+    try:
+        A = spai.family(96, seed=424242)  # outside the training seeds
+        b = problems.rhs_uniform(A.n, 505)
+        res = {"n": A.n, "nnz": A.nnz}
+        t64, st64, r64, x64 = fused_solve(torch, A, b, "gmres", 30, SOLVER_TOL, max_iters=30000)
+        res["plain_fp64_gmres30"] = {"s": t64, "status": st64, "iters": r64.iters, "true_rel_residual": _rel(A, b, x64)}
+        for pc in ("none", "jacobi"):
+            t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond=pc, max_iters=30000)
+            res[f"fp32_dot2_gmres30_refined_{pc}"] = {"s": t, "status": st, "inner_iters": r.inner_iters,
+                                                      "refinements": r.refinements, "true_rel_residual": _rel(A, b, x)}
+        wfile = spai.WEIGHTS_FILE
+        if wfile.exists():
+            offs, dslot = spai.stencil7(96)
+            net = spai.SpaiNet(offs, dslot)
+            net.set_weights(np.load(wfile))
+            tb, M = _timed(torch, lambda: net.assemble(torch, spai.DeviceCSR(torch, A)))
+            t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond="matrix", M=M, max_iters=30000)
+            res["fp32_dot2_gmres30_refined_learned_spai"] = {
+                "s": t, "build_s": tb, "status": st, "inner_iters": r.inner_iters, "refinements": r.refinements,
+                "true_rel_residual": _rel(A, b, x)}
+            net.close()
+            if st == 0:
+                res["speedup_learned_vs_plain_fp64"] = t64 / (t + tb) if st64 == 0 else None
+        out["learned_pc_gmres30_lognormal96"] = res
+    except Exception as e:
+        out["learned_pc_gmres30_lognormal96"] = {"error": repr(e)}
+    return out
 
 
 def dot2_probe(torch, L, ctx, reps=200):
@@ -509,6 +639,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["solver", "dot2"], default="solver")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain", action="store_true", help="time the plain drop-in solver path instead of the fused one")
+    ap.add_argument("--no-forms", action="store_true", help="skip the precision / complex / learned-preconditioner runs")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 200 if args.workload == "dot2" else 3
@@ -542,6 +674,8 @@ def main():
                     res["cpu_baseline"] = cpu_baseline_dot2()
                 else:
                     res["cpu_baseline"] = cpu_baseline_solver(int(np.max(res["solver"]["iters"])))
+            if args.workload == "solver" and not args.no_forms and ws == 1:
+                res["forms"] = bench_forms(torch)
             print(json.dumps(res))
     finally:
         if dist is not None:

@@ -42,12 +42,27 @@ class HpbError(RuntimeError):
         self.status = status
 
 
+class _TypedCDLL(C.CDLL):
+    """CDLL that only hands out the functions declared below (with their
+    argtypes).  A plain CDLL creates a fresh, untyped function object when
+    __getattr__ is called directly, which would pass 64-bit device pointers
+    as 32-bit ints; here an undeclared name raises instead."""
+
+    def __getattr__(self, name):
+        d = self.__dict__
+        if name in d:  # a direct __getattr__ call returns the typed function too
+            return d[name]
+        if name.startswith("hpb_") and "_declared" in d:
+            raise AttributeError(f"{name} is not declared in high_precision_blas1_b200/_lib.py")
+        return super().__getattr__(name)
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(
             f"{LIB_PATH} is missing: build it with `python -m high_precision_blas1_b200.build` "
             "(there is no CPU fallback)")
-    return C.CDLL(str(LIB_PATH))
+    return _TypedCDLL(str(LIB_PATH))
 
 
 lib = _load()
@@ -58,9 +73,11 @@ I32 = C.c_int32
 
 
 def _sig(name, res, args):
-    f = getattr(lib, name)
+    f = C.CDLL.__getattr__(lib, name)
     f.restype = res
     f.argtypes = args
+    lib.__dict__.setdefault("_declared", set()).add(name)
+    lib.__dict__[name] = f
     return f
 
 
@@ -112,7 +129,8 @@ _sig("hpb_swap", C.c_int, [P, I64, C.c_size_t, P, P])
 class hpb_solver_params(C.Structure):
     _fields_ = [("method", C.c_int), ("basis", C.c_int), ("rel_tol", C.c_double), ("abs_tol", C.c_double),
                 ("max_iters", C.c_int), ("precond", C.c_int), ("high_precision", C.c_int),
-                ("resid_recalc_freq", C.c_int), ("early_exit", C.c_int), ("reorthogonalize", C.c_int)]
+                ("resid_recalc_freq", C.c_int), ("early_exit", C.c_int), ("reorthogonalize", C.c_int),
+                ("fused", C.c_int)]
 
 
 class hpb_solver_report(C.Structure):
@@ -122,7 +140,19 @@ class hpb_solver_report(C.Structure):
 
 
 SOLVER = {"bicgstabl": 0, "gmres": 1, "bicgstab": 2}
-PRECOND = {"none": 0, "jacobi": 1}
+PRECOND = {"none": 0, "jacobi": 1, "matrix": 2}
+
+
+class hpb_ir_params(C.Structure):
+    _fields_ = [("inner_method", C.c_int), ("inner_basis", C.c_int), ("inner_rel_tol", C.c_double),
+                ("inner_max_iters", C.c_int), ("precond", C.c_int), ("rel_tol", C.c_double),
+                ("max_refinements", C.c_int)]
+
+
+class hpb_ir_report(C.Structure):
+    _fields_ = [("converged", C.c_int), ("refinements", C.c_int), ("inner_iters", C.c_int),
+                ("history_len", C.c_int), ("rhs_norm", C.c_double), ("true_resid_norm", C.c_double),
+                ("seconds", C.c_double)]
 
 _sig("hpb_solver_params_default", C.c_int, [C.POINTER(hpb_solver_params)])
 for t in TYPES:
@@ -131,8 +161,43 @@ for t in TYPES:
              [C.POINTER(hpb_solver_params), I32, I64, P, P, P, P, P, C.POINTER(hpb_solver_report), P, C.c_int])
 
 
+_sig("hpb_ir_params_default", C.c_int, [C.POINTER(hpb_ir_params)])
+for _n in ("hpb_ir_solve_f64", "hpb_ir_solve_c128"):
+    _sig(_n, C.c_int, [C.POINTER(hpb_ir_params), I32, I64, P, P, P, P, P, P, P, I64, P, P,
+                       C.POINTER(hpb_ir_report), P, C.c_int])
+
+
+class hpb_spai_system(C.Structure):
+    _fields_ = [("rows", C.c_int32), ("nnz", C.c_int64), ("row_ptr", P), ("col_ind", P), ("val", P),
+                ("nres", C.c_int), ("residuals", P)]
+
+
+_sig("hpb_spai_create", C.c_int, [C.POINTER(P), C.c_int, C.c_int, C.POINTER(C.c_int), C.c_uint64])
+_sig("hpb_spai_destroy", C.c_int, [P])
+_sig("hpb_spai_num_params", C.c_int, [])
+_sig("hpb_spai_set_weights", C.c_int, [P, P])
+_sig("hpb_spai_get_weights", C.c_int, [P, P])
+_sig("hpb_spai_assemble", C.c_int, [P, C.POINTER(hpb_spai_system), P])
+_sig("hpb_spai_loss_grad", C.c_int, [P, C.POINTER(hpb_spai_system), C.c_float, C.c_float, P, P])
+_sig("hpb_spai_adam", C.c_int, [P, C.c_float, C.c_float])
+
+
+def ir_params(inner="gmres", basis=50, inner_rel_tol=1e-5, inner_max_iters=5000, precond="none", rel_tol=1e-10,
+              max_refinements=30):
+    p = hpb_ir_params()
+    lib.hpb_ir_params_default(C.byref(p))
+    p.inner_method = SOLVER[inner]
+    p.inner_basis = basis
+    p.inner_rel_tol = inner_rel_tol
+    p.inner_max_iters = inner_max_iters
+    p.precond = PRECOND[precond]
+    p.rel_tol = rel_tol
+    p.max_refinements = max_refinements
+    return p
+
+
 def solver_params(method="bicgstabl", basis=2, rel_tol=1e-10, abs_tol=0.0, max_iters=10000, precond="none",
-                  high_precision=True, resid_recalc_freq=0, early_exit=False, reorthogonalize=False):
+                  high_precision=True, resid_recalc_freq=0, early_exit=False, reorthogonalize=False, fused=False):
     p = hpb_solver_params()
     lib.hpb_solver_params_default(C.byref(p))
     p.method = SOLVER[method]
@@ -145,6 +210,7 @@ def solver_params(method="bicgstabl", basis=2, rel_tol=1e-10, abs_tol=0.0, max_i
     p.resid_recalc_freq = resid_recalc_freq
     p.early_exit = 1 if early_exit else 0
     p.reorthogonalize = 1 if reorthogonalize else 0
+    p.fused = 1 if fused else 0
     return p
 
 

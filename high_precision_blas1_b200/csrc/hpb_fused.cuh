@@ -1,0 +1,239 @@
+// Building blocks of the device-resident (fused) solvers: multi-dot Dot2
+// accumulation inside producer kernels, a single-pass cross-block combine
+// with a scalar epilogue run by the last block, and storage/scalar type
+// helpers.
+//
+// Storage type E (float, double, cf, cd) holds the vectors; scalar type S
+// (double, or cd for complex data) holds every solver scalar and every
+// reduction result on the device.  Elementwise updates compute in S and
+// round once to E, so float storage gets binary64 coefficients and
+// binary64 updates before the single rounding.
+#pragma once
+
+#include "hpb_common.cuh"
+
+namespace hpb {
+namespace fused {
+
+template <class E> struct scalar_of { using type = double; };
+template <> struct scalar_of<cf> { using type = cd; };
+template <> struct scalar_of<cd> { using type = cd; };
+
+// ---------------------------------------------------------------- S helpers
+__host__ __device__ __forceinline__ double s_zero(double) { return 0.0; }
+__host__ __device__ __forceinline__ cd s_zero(cd) { return cd{0.0, 0.0}; }
+__host__ __device__ __forceinline__ double s_one(double) { return 1.0; }
+__host__ __device__ __forceinline__ cd s_one(cd) { return cd{1.0, 0.0}; }
+__host__ __device__ __forceinline__ double s_add(double a, double b) { return a + b; }
+__host__ __device__ __forceinline__ cd s_add(cd a, cd b) { return cd{a.re + b.re, a.im + b.im}; }
+__host__ __device__ __forceinline__ double s_sub(double a, double b) { return a - b; }
+__host__ __device__ __forceinline__ cd s_sub(cd a, cd b) { return cd{a.re - b.re, a.im - b.im}; }
+__host__ __device__ __forceinline__ double s_mul(double a, double b) { return a * b; }
+__host__ __device__ __forceinline__ cd s_mul(cd a, cd b) { return cd{a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__host__ __device__ __forceinline__ double s_div(double a, double b) { return a / b; }
+__host__ __device__ __forceinline__ cd s_div(cd a, cd b) {
+    // Smith's algorithm (scaled, avoids overflow in |b|^2)
+    if (fabs(b.re) >= fabs(b.im)) {
+        double r = b.im / b.re, d = b.re + b.im * r;
+        return cd{(a.re + a.im * r) / d, (a.im - a.re * r) / d};
+    }
+    double r = b.re / b.im, d = b.re * r + b.im;
+    return cd{(a.re * r + a.im) / d, (a.im * r - a.re) / d};
+}
+template <class S> __host__ __device__ __forceinline__ S make_real(double v);
+template <> __host__ __device__ __forceinline__ double make_real<double>(double v) { return v; }
+template <> __host__ __device__ __forceinline__ cd make_real<cd>(double v) { return cd{v, 0.0}; }
+__host__ __device__ __forceinline__ double s_neg(double a) { return -a; }
+__host__ __device__ __forceinline__ cd s_neg(cd a) { return cd{-a.re, -a.im}; }
+__host__ __device__ __forceinline__ bool s_is_zero(double a) { return a == 0.0; }
+__host__ __device__ __forceinline__ bool s_is_zero(cd a) { return a.re == 0.0 && a.im == 0.0; }
+__host__ __device__ __forceinline__ double conj_s(double a) { return a; }
+__host__ __device__ __forceinline__ cd conj_s(cd a) { return cd{a.re, -a.im}; }
+__host__ __device__ __forceinline__ double s_real(double a) { return a; }
+__host__ __device__ __forceinline__ double s_real(cd a) { return a.re; }
+// a*x + y with one rounding per component where possible
+__device__ __forceinline__ double s_fma(double a, double x, double y) { return fma(a, x, y); }
+__device__ __forceinline__ cd s_fma(cd a, cd x, cd y) {
+    return cd{fma(a.re, x.re, fma(-a.im, x.im, y.re)), fma(a.re, x.im, fma(a.im, x.re, y.im))};
+}
+
+// ----------------------------------------------------- storage <-> scalar
+__device__ __forceinline__ double to_s(float v) { return double(v); }
+__device__ __forceinline__ double to_s(double v) { return v; }
+__device__ __forceinline__ cd to_s(cf v) { return cd{double(v.re), double(v.im)}; }
+__device__ __forceinline__ cd to_s(cd v) { return v; }
+template <class E> __device__ __forceinline__ E from_s(double v);
+template <> __device__ __forceinline__ float from_s<float>(double v) { return float(v); }
+template <> __device__ __forceinline__ double from_s<double>(double v) { return v; }
+template <class E> __device__ __forceinline__ E from_s(cd v);
+template <> __device__ __forceinline__ cf from_s<cf>(cd v) { return cf{float(v.re), float(v.im)}; }
+template <> __device__ __forceinline__ cd from_s<cd>(cd v) { return v; }
+__device__ __forceinline__ bool finite_e(float v) { return isfinite(v); }
+__device__ __forceinline__ bool finite_e(double v) { return isfinite(v); }
+__device__ __forceinline__ bool finite_e(cf v) { return isfinite(v.re + v.im); }
+__device__ __forceinline__ bool finite_e(cd v) { return isfinite(v.re + v.im); }
+
+// ------------------------------------------------------------ Dot2 pieces
+// (s, c) accumulator of conj(a)*b in binary64 (real) / complex binary64.
+struct Acc2 {
+    double s = 0.0, c = 0.0;
+};
+struct AccC {
+    cd s{0.0, 0.0}, c{0.0, 0.0};
+};
+template <class S> struct acc_of;
+template <> struct acc_of<double> { using type = Acc2; };
+template <> struct acc_of<cd> { using type = AccC; };
+
+__device__ __forceinline__ void acc_term(double& s, double& c, double p, double t) {
+    double e;
+    s = two_sum(s, p, e);
+    c = add_rn(c, add_rn(t, e));
+}
+// Dot2 term conj(a)*b, exact product split (TwoProd) then TwoSum.
+__device__ __forceinline__ void dot_add(Acc2& a, double x, double y) {
+    double t;
+    double p = two_prod(x, y, t);
+    acc_term(a.s, a.c, p, t);
+}
+__device__ __forceinline__ void dot_add(AccC& a, cd x, cd y) {
+    double tR1, tR2, tI1, tI2, t1, t2;
+    double pR1 = two_prod(x.re, y.re, tR1);
+    double pR2 = two_prod(x.im, y.im, tR2);
+    double pI1 = two_prod(x.re, y.im, tI1);
+    double pI2 = two_prod(-x.im, y.re, tI2);
+    double pR = two_sum(pR1, pR2, t1);
+    double pI = two_sum(pI1, pI2, t2);
+    acc_term(a.s.re, a.c.re, pR, add_rn(add_rn(tR1, tR2), t1));
+    acc_term(a.s.im, a.c.im, pI, add_rn(add_rn(tI1, tI2), t2));
+}
+
+__device__ __forceinline__ void merge2(double& s, double& c, double s2, double c2) {
+    double e;
+    s = two_sum(s, s2, e);
+    c = add_rn(c, add_rn(e, c2));
+}
+__device__ __forceinline__ void merge(Acc2& a, const Acc2& b) { merge2(a.s, a.c, b.s, b.c); }
+__device__ __forceinline__ void merge(AccC& a, const AccC& b) {
+    merge2(a.s.re, a.c.re, b.s.re, b.c.re);
+    merge2(a.s.im, a.c.im, b.s.im, b.c.im);
+}
+__device__ __forceinline__ Acc2 shfl_acc(const Acc2& a, int off) {
+    Acc2 r;
+    r.s = __shfl_xor_sync(0xffffffffu, a.s, off);
+    r.c = __shfl_xor_sync(0xffffffffu, a.c, off);
+    return r;
+}
+__device__ __forceinline__ AccC shfl_acc(const AccC& a, int off) {
+    AccC r;
+    r.s.re = __shfl_xor_sync(0xffffffffu, a.s.re, off);
+    r.s.im = __shfl_xor_sync(0xffffffffu, a.s.im, off);
+    r.c.re = __shfl_xor_sync(0xffffffffu, a.c.re, off);
+    r.c.im = __shfl_xor_sync(0xffffffffu, a.c.im, off);
+    return r;
+}
+__device__ __forceinline__ double acc_value(const Acc2& a) { return a.s + a.c; }
+__device__ __forceinline__ cd acc_value(const AccC& a) { return cd{a.s.re + a.c.re, a.s.im + a.c.im}; }
+
+__device__ __forceinline__ Acc2 ldcg_acc(const Acc2* p) {
+    const double* q = reinterpret_cast<const double*>(p);
+    Acc2 r;
+    r.s = __ldcg(q);
+    r.c = __ldcg(q + 1);
+    return r;
+}
+__device__ __forceinline__ AccC ldcg_acc(const AccC* p) {
+    const double* q = reinterpret_cast<const double*>(p);
+    AccC r;
+    r.s = cd{__ldcg(q), __ldcg(q + 1)};
+    r.c = cd{__ldcg(q + 2), __ldcg(q + 3)};
+    return r;
+}
+
+// Block-wide merge of ND accumulators (result valid in thread 0).
+template <int ND, class A>
+__device__ __forceinline__ void block_merge(A (&acc)[ND], A* sh /* [ND][32] */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int d = 0; d < ND; ++d)
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) merge(acc[d], shfl_acc(acc[d], off));
+    if (lane == 0)
+#pragma unroll
+        for (int d = 0; d < ND; ++d) sh[d * 32 + warp] = acc[d];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+            acc[d] = lane < nw ? sh[d * 32 + lane] : A{};
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) merge(acc[d], shfl_acc(acc[d], off));
+        }
+    }
+}
+
+// Cross-block finish: block partials -> ticket -> the last block merges all
+// partials in block order and runs `epi(values, bad)` on thread 0, where
+// values[d] = hi of dot d and bad = any block reported a non-finite entry.
+// Returns true in the last block's thread 0 only (after epi).
+template <int ND, class A, class Epi>
+__device__ __forceinline__ void grid_finish(A (&acc)[ND], bool bad, A* partials, unsigned int* ticket, int* badflag,
+                                            Epi epi) {
+    __shared__ A sh[ND * 32 > 0 ? ND * 32 : 1];
+    __shared__ bool am_last;
+    if (ND > 0) block_merge<ND>(acc, sh);
+    bool any_bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) partials[size_t(d) * gridDim.x + blockIdx.x] = acc[d];
+        if (any_bad) atomicOr(badflag, 1);
+        __threadfence();
+        am_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    A tot[ND > 0 ? ND : 1];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        tot[d] = A{};
+        for (int b = threadIdx.x; b < int(gridDim.x); b += blockDim.x) merge(tot[d], ldcg_acc(partials + size_t(d) * gridDim.x + b));
+    }
+    __syncthreads();
+    if (ND > 0) block_merge<ND>(tot, sh);
+    if (threadIdx.x == 0) {
+        using V = decltype(acc_value(tot[0]));
+        V vals[ND > 0 ? ND : 1];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) vals[d] = acc_value(tot[d]);
+        epi(vals, atomicExch(badflag, 0) != 0);
+        *ticket = 0;
+    }
+}
+
+// Right preconditioner of the fused GMRES: none, Jacobi (diagonal of A) or
+// a general CSR matrix M with the storage type of the iteration.
+template <class E>
+struct RightPrec {
+    int kind = 0;  // 0 none, 1 Jacobi, 2 CSR matrix
+    int32_t rows = 0;
+    int64_t nnz = 0;
+    const int32_t* rp = nullptr;
+    const int32_t* ci = nullptr;
+    const E* val = nullptr;
+};
+
+// Device-resident GMRES(m) (hpb_fused_gmres.cu); E in {float, double, cf, cd}.
+template <class E>
+int solve_gmres(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
+                const E* val, const RightPrec<E>& M, const E* b, E* x, hpb_solver_report* rep, double* hist, int cap,
+                int max_cycles);
+
+// Device-resident BiCGStab(l) (hpb_fused_bicgstabl.cu); E in {float,
+// double, cf, cd}.
+template <class E>
+int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
+                    const E* val, const E* b, E* x, hpb_solver_report* rep, double* hist, int cap);
+
+}  // namespace fused
+}  // namespace hpb

@@ -1,0 +1,558 @@
+// Device-resident BiCGStab(l) with Dot2 reductions (the fused solver path).
+//
+// Same algorithm, same recurrences and the same stopping test as the
+// drop-in path (include/hpblas1/solvers/bicgstabl.h, itself the published
+// Sleijpen-Fokkema BiCGStab(l) the reference runs in
+// numerical_algos/lin_solvers/bicgstabl.h:151-275), rebuilt for B200:
+//   * every solver scalar (rho, alpha, omega, beta, tau, sigma, gamma,
+//     gamma', gamma'') lives in device memory and is updated by the last
+//     block of the kernel that produced the reduction it depends on; no
+//     reduction result travels to the host inside a cycle;
+//   * each SpMV is fused with the Dot2 that consumes its output
+//     (u_{j+1} = A u_j with <rt, u_{j+1}>, r_{j+1} = A r_j with <rt, r_{j+1}>),
+//     and an optional Jacobi scaling (left preconditioning) is applied to
+//     the rows in the same kernel;
+//   * each modified-Gram-Schmidt pass of the MR part applies the previous
+//     projection and computes the next inner product(s) in one sweep;
+//   * the closing update of x, r_0, u_0 also produces ||r_0|| (the monitor's
+//     residual), <rt, r_0> (next cycle's rho) and the finiteness of x;
+//   * one cycle = 4l + l(l+1)/2 + 1 kernels, captured once into a CUDA graph
+//     and replayed; the host reads 16 bytes (||r_0||, breakdown, non-finite)
+//     per cycle to apply the monitor's test, as the reference does once per
+//     cycle (default_monitor.h:202-226).
+// Storage E in {float, double, complex<float>, complex<double>}; scalars and
+// reductions in binary64 (complex<binary64>).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+#include "hpb_fused.cuh"
+
+namespace hpb {
+namespace fused {
+
+constexpr int kMaxL = 8;
+constexpr int kThreads = 256;
+
+template <class S>
+struct BcgState {
+    S rho, alpha, omega, beta;
+    S tau[kMaxL + 1][kMaxL + 1];
+    S sigma[kMaxL + 1], gam[kMaxL + 1], gam1[kMaxL + 1], gam2[kMaxL + 1];
+    S last[2];
+};
+
+struct Report {
+    double rnorm;   // ||r_0|| (compensated)
+    int breakdown;  // rho == 0 met
+    int nonfinite;  // x held a non-finite entry
+};
+
+template <class E>
+struct Vecs {
+    E* r[kMaxL + 1];
+    E* u[kMaxL + 1];
+};
+
+enum Epi { EPI_NONE = 0, EPI_ALPHA, EPI_BETA, EPI_TAU, EPI_SIGMA, EPI_FINAL };
+
+template <class S>
+struct EpiArgs {
+    BcgState<S>* st;
+    Report* rep;
+    int kind, k, j, L;
+};
+
+template <class S>
+__device__ void run_epi(const EpiArgs<S>& a, const S* v, bool bad) {
+    BcgState<S>& st = *a.st;
+    switch (a.kind) {
+        case EPI_ALPHA:  // alpha = rho / <rt, u_{j+1}>
+            st.alpha = s_div(st.rho, v[0]);
+            break;
+        case EPI_BETA:  // rho1 = <rt, r_j>; beta = alpha rho1 / rho; rho = rho1
+            if (s_is_zero(st.rho)) a.rep->breakdown = 1;
+            st.beta = s_div(s_mul(st.alpha, v[0]), st.rho);
+            st.rho = v[0];
+            break;
+        case EPI_TAU:  // tau[k][j] = <r_k, r_j> / sigma[k]
+            st.tau[a.k][a.j] = s_div(v[0], st.sigma[a.k]);
+            break;
+        case EPI_SIGMA: {  // sigma[j] = <r_j, r_j>; gamma'_j = <r_j, r_0> / sigma[j]
+            st.sigma[a.j] = v[0];
+            st.gam1[a.j] = s_div(v[1], v[0]);
+            if (a.j == a.L) {
+                const int L = a.L;
+                st.gam[L] = st.gam1[L];
+                st.omega = st.gam[L];
+                for (int jj = L - 1; jj >= 1; --jj) {
+                    S g = st.gam1[jj];
+                    for (int i = jj + 1; i <= L; ++i) g = s_sub(g, s_mul(st.tau[jj][i], st.gam[i]));
+                    st.gam[jj] = g;
+                }
+                for (int jj = 1; jj < L; ++jj) {
+                    S g = st.gam[jj + 1];
+                    for (int i = jj + 1; i < L; ++i) g = s_add(g, s_mul(st.tau[jj][i], st.gam[i + 1]));
+                    st.gam2[jj] = g;
+                }
+            }
+            break;
+        }
+        case EPI_FINAL: {  // v[0] = <rt, r_0>, v[1] = <r_0, r_0>
+            a.rep->rnorm = sqrt(fmax(s_real(v[1]), 0.0));
+            a.rep->nonfinite = bad ? 1 : 0;
+            st.rho = s_neg(s_mul(st.omega, st.rho));  // next cycle: rho = -omega rho
+            if (s_is_zero(st.rho)) a.rep->breakdown = 1;
+            st.beta = s_div(s_mul(st.alpha, v[0]), st.rho);
+            st.rho = v[0];
+            break;
+        }
+        default:
+            break;
+    }
+    st.last[0] = v[0];
+}
+
+// ------------------------------------------------------------ SpMV (+ Dot2)
+// y = D^{-1} (A x) (diag = D, may be null: no scaling), and <w, y> when DOT.
+template <class E, bool DOT>
+__global__ void __launch_bounds__(kThreads)
+k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const E* __restrict__ val,
+           const E* __restrict__ diag, const E* __restrict__ x, E* __restrict__ y, const E* __restrict__ w,
+           typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
+           EpiArgs<typename scalar_of<E>::type> ea) {
+    using S = typename scalar_of<E>::type;
+    using A = typename acc_of<S>::type;
+    constexpr int kCap = 2048;
+    __shared__ E sv[kCap];
+    __shared__ int32_t sc[kCap];
+    const int32_t r0 = blockIdx.x * kThreads;
+    const int32_t r = r0 + threadIdx.x;
+    const int32_t rend = min(r0 + kThreads, rows);
+    const int32_t p0 = rp[r0];
+    const int32_t cnt = rp[rend] - p0;
+    int32_t b = 0, e = 0;
+    if (r < rows) {
+        b = rp[r];
+        e = rp[r + 1];
+    }
+    S acc = s_zero(S{});
+    if (cnt <= kCap) {
+#pragma unroll 4
+        for (int32_t k = threadIdx.x; k < cnt; k += kThreads) {
+            sv[k] = ldE(val, int64_t(p0) + k);
+            sc[k] = ci[p0 + k];
+        }
+        __syncthreads();
+        for (int32_t k = b - p0; k < e - p0; ++k) acc = s_fma(to_s(sv[k]), to_s(ldE(x, sc[k])), acc);
+    } else {
+        for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ldE(val, k)), to_s(ldE(x, ci[k])), acc);
+    }
+    A dacc[1];
+    if (r < rows) {
+        if (diag) acc = s_div(acc, to_s(ldE(diag, r)));
+        E out = from_s<E>(acc);
+        stE(y, r, out);
+        if (DOT) dot_add(dacc[0], to_s(ldE(w, r)), to_s(out));
+    }
+    if (DOT) grid_finish<1>(dacc, false, partials, ticket, badflag, [&](const S* v, bool bad) { run_epi(ea, v, bad); });
+}
+
+// ------------------------------------------------------------ BiCG updates
+// u_i = r_i - beta u_i, i = 0..j
+template <class E>
+__global__ void __launch_bounds__(kThreads) k_upd_u(int64_t n, int j, Vecs<E> V,
+                                                    const BcgState<typename scalar_of<E>::type>* st) {
+    using S = typename scalar_of<E>::type;
+    const S nb = s_neg(st->beta);
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+        for (int i = 0; i <= j; ++i) {
+            S ui = to_s(ldE(V.u[i], q));
+            stE(V.u[i], q, from_s<E>(s_fma(nb, ui, to_s(ldE(V.r[i], q)))));
+        }
+    }
+}
+
+// r_i = r_i - alpha u_{i+1}, i = 0..j ;  x = x + alpha u_0
+template <class E>
+__global__ void __launch_bounds__(kThreads) k_upd_rx(int64_t n, int j, Vecs<E> V, E* __restrict__ x,
+                                                     const BcgState<typename scalar_of<E>::type>* st) {
+    using S = typename scalar_of<E>::type;
+    const S al = st->alpha, nal = s_neg(st->alpha);
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+        for (int i = 0; i <= j; ++i)
+            stE(V.r[i], q, from_s<E>(s_fma(nal, to_s(ldE(V.u[i + 1], q)), to_s(ldE(V.r[i], q)))));
+        stE(x, q, from_s<E>(s_fma(al, to_s(ldE(V.u[0], q)), to_s(ldE(x, q)))));
+    }
+}
+
+// ------------------------------------------------------------ MR part
+// Pass k of the modified Gram-Schmidt sweep on r_j:
+//   if k > 1:  r_j -= tau[k-1][j] r_{k-1}
+//   if k < j:  tau[k][j] = <r_k, r_j> / sigma[k]
+//   if k == j: sigma[j] = <r_j, r_j>, gamma'_j = <r_j, r_0> / sigma[j]
+template <class E, int ND>
+__global__ void __launch_bounds__(kThreads)
+k_mgs(int64_t n, int k, int j, Vecs<E> V, BcgState<typename scalar_of<E>::type>* st,
+      typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
+      EpiArgs<typename scalar_of<E>::type> ea) {
+    using S = typename scalar_of<E>::type;
+    using A = typename acc_of<S>::type;
+    const bool upd = k > 1;
+    const S ntau = upd ? s_neg(st->tau[k - 1][j]) : s_zero(S{});
+    E* rj = V.r[j];
+    const E* rprev = upd ? V.r[k - 1] : nullptr;
+    const E* rk = V.r[k];
+    const E* r0 = V.r[0];
+    A acc[ND];
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+        S v = to_s(ldE(rj, q));
+        if (upd) {
+            E ve = from_s<E>(s_fma(ntau, to_s(ldE(rprev, q)), v));
+            stE(rj, q, ve);
+            v = to_s(ve);
+        }
+        if (ND == 1) {
+            dot_add(acc[0], to_s(ldE(rk, q)), v);
+        } else {
+            dot_add(acc[0], v, v);
+            dot_add(acc[ND - 1], v, to_s(ldE(r0, q)));
+        }
+    }
+    grid_finish<ND>(acc, false, partials, ticket, badflag, [&](const S* vals, bool bad) { run_epi(ea, vals, bad); });
+}
+
+// ------------------------------------------------------------ closing update
+// x += gamma_1 r_0 + sum_{j<L} gamma''_j r_j ; r_0 -= sum_j gamma'_j r_j ;
+// u_0 -= sum_j gamma_j u_j ; then <rt, r_0>, <r_0, r_0>, finiteness of x.
+template <class E>
+__global__ void __launch_bounds__(kThreads)
+k_final(int64_t n, int L, int update, Vecs<E> V, E* __restrict__ x, const E* __restrict__ rt,
+        BcgState<typename scalar_of<E>::type>* st, typename acc_of<typename scalar_of<E>::type>::type* partials,
+        unsigned int* ticket, int* badflag, EpiArgs<typename scalar_of<E>::type> ea) {
+    using S = typename scalar_of<E>::type;
+    using A = typename acc_of<S>::type;
+    S g[kMaxL + 1], g1[kMaxL + 1], g2[kMaxL + 1];
+    if (update)
+        for (int i = 1; i <= L; ++i) {
+            g[i] = s_neg(st->gam[i]);
+            g1[i] = s_neg(st->gam1[i]);
+            g2[i] = st->gam2[i];
+        }
+    A acc[2];
+    bool bad = false;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+        E r0e = ldE(V.r[0], q);
+        E xe = ldE(x, q);
+        if (update) {
+            S r0 = to_s(r0e);
+            S xs = s_fma(st->gam[1], r0, to_s(xe));
+            r0 = s_fma(g1[L], to_s(ldE(V.r[L], q)), r0);
+            S u0 = s_fma(g[L], to_s(ldE(V.u[L], q)), to_s(ldE(V.u[0], q)));
+            for (int jj = 1; jj < L; ++jj) {
+                S rj = to_s(ldE(V.r[jj], q));
+                xs = s_fma(g2[jj], rj, xs);
+                r0 = s_fma(g1[jj], rj, r0);
+                u0 = s_fma(g[jj], to_s(ldE(V.u[jj], q)), u0);
+            }
+            xe = from_s<E>(xs);
+            r0e = from_s<E>(r0);
+            stE(x, q, xe);
+            stE(V.r[0], q, r0e);
+            stE(V.u[0], q, from_s<E>(u0));
+        }
+        S rs = to_s(r0e);
+        dot_add(acc[0], to_s(ldE(rt, q)), rs);
+        dot_add(acc[1], rs, rs);
+        bad |= !finite_e(xe);
+    }
+    grid_finish<2>(acc, bad, partials, ticket, badflag, [&](const S* vals, bool b) { run_epi(ea, vals, b); });
+    (void)A{};
+}
+
+// ------------------------------------------------------------ small kernels
+template <class S>
+__global__ void k_init_state(BcgState<S>* st, Report* rep) {
+    st->rho = s_one(S{});
+    st->alpha = s_zero(S{});
+    st->omega = s_one(S{});
+    st->beta = s_zero(S{});
+    rep->rnorm = 0.0;
+    rep->breakdown = 0;
+    rep->nonfinite = 0;
+}
+__global__ void k_clear_flag(int* f) { *f = 0; }
+
+// r = D^{-1} (b - A x)   (diag may be null)
+template <class E>
+__global__ void k_residual_finish(int64_t n, const E* __restrict__ b, const E* __restrict__ ax,
+                                  const E* __restrict__ diag, E* __restrict__ r) {
+    using S = typename scalar_of<E>::type;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+        S v = s_sub(to_s(ldE(b, q)), to_s(ldE(ax, q)));
+        if (diag) v = s_div(v, to_s(ldE(diag, q)));
+        stE(r, q, from_s<E>(v));
+    }
+}
+// y = D^{-1} x
+template <class E>
+__global__ void k_scale_inv(int64_t n, const E* __restrict__ x, const E* __restrict__ diag, E* __restrict__ y) {
+    using S = typename scalar_of<E>::type;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride)
+        stE(y, q, from_s<E>(s_div(to_s(ldE(x, q)), to_s(ldE(diag, q)))));
+}
+// y = x * (1 / nrm[0])
+template <class E>
+__global__ void k_scale_by_inv_norm(int64_t n, const E* __restrict__ x, const double* nrm, E* __restrict__ y) {
+    using S = typename scalar_of<E>::type;
+    const double inv = 1.0 / nrm[0];
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+        stE(y, q, from_s<E>(s_mul(make_real<S>(inv), to_s(ldE(x, q)))));
+    }
+}
+
+}  // namespace fused
+}  // namespace hpb
+
+namespace hpb {
+namespace fused {
+
+// diag[r] = A(r, r)
+template <class E>
+__global__ void k_diag(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                       const E* __restrict__ val, E* __restrict__ diag) {
+    const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    E d{};
+    for (int32_t k = rp[r]; k < rp[r + 1]; ++k)
+        if (ci[k] == r) d = ldE(val, k);
+    stE(diag, r, d);
+}
+
+// out[slot] = sqrt(Re <v, v>) with Dot2
+template <class E>
+__global__ void __launch_bounds__(kThreads) k_norm(int64_t n, const E* __restrict__ v, double* out,
+                                                   typename acc_of<typename scalar_of<E>::type>::type* partials,
+                                                   unsigned int* ticket, int* badflag) {
+    using S = typename scalar_of<E>::type;
+    using A = typename acc_of<S>::type;
+    A acc[1];
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+        S s = to_s(ldE(v, q));
+        dot_add(acc[0], s, s);
+    }
+    grid_finish<1>(acc, false, partials, ticket, badflag,
+                   [&](const S* vals, bool) { out[0] = sqrt(fmax(s_real(vals[0]), 0.0)); });
+}
+
+namespace {
+struct Workspace {
+    std::vector<void*> dev;
+    void* pinned = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~Workspace() {
+        if (stream) cudaStreamSynchronize(stream);
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        for (void* p : dev) cudaFree(p);
+        if (pinned) cudaFreeHost(pinned);
+        if (ev) cudaEventDestroy(ev);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void* alloc(size_t bytes) {
+        void* p = nullptr;
+        if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return nullptr;
+        dev.push_back(p);
+        return p;
+    }
+};
+}  // namespace
+
+template <class E>
+int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
+                    const E* val, const E* b, E* x, hpb_solver_report* rep, double* hist, int cap) {
+    using S = typename scalar_of<E>::type;
+    using A = typename acc_of<S>::type;
+    const int L = p->basis > 0 ? p->basis : 2;
+    if (L > kMaxL) return HPB_ERROR_NOT_SUPPORTED;
+    const bool jac = p->precond == HPB_PRECOND_JACOBI;
+    if (!jac && p->precond != HPB_PRECOND_NONE) return HPB_ERROR_NOT_SUPPORTED;
+    if (!p->high_precision) return HPB_ERROR_NOT_SUPPORTED;  // the fused path carries Dot2 only
+    (void)nnz;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return HPB_ERROR_CUDA;
+    const int64_t n = rows;
+    const int g_ew = int(std::max<int64_t>(1, std::min<int64_t>((n + kThreads - 1) / kThreads, int64_t(sms) * 8)));
+    const int g_sp = (rows + kThreads - 1) / kThreads;
+
+    Workspace ws;
+    Vecs<E> V{};
+    const size_t vb = size_t(n) * sizeof(E);
+    for (int i = 0; i <= L; ++i) {
+        V.r[i] = static_cast<E*>(ws.alloc(vb));
+        V.u[i] = static_cast<E*>(ws.alloc(vb));
+        if (!V.r[i] || !V.u[i]) return HPB_ERROR_OUT_OF_MEMORY;
+    }
+    E* rt = static_cast<E*>(ws.alloc(vb));
+    E* tmp = static_cast<E*>(ws.alloc(vb));
+    E* diag = jac ? static_cast<E*>(ws.alloc(vb)) : nullptr;
+    auto* st = static_cast<BcgState<S>*>(ws.alloc(sizeof(BcgState<S>)));
+    auto* drep = static_cast<Report*>(ws.alloc(sizeof(Report)));
+    auto* partials = static_cast<A*>(ws.alloc(2 * size_t(std::max(g_ew, g_sp)) * sizeof(A)));
+    auto* ticket = static_cast<unsigned int*>(ws.alloc(64));
+    auto* badflag = static_cast<int*>(ws.alloc(64));
+    auto* dnorm = static_cast<double*>(ws.alloc(4 * sizeof(double)));
+    if (!rt || !tmp || (jac && !diag) || !st || !drep || !partials || !ticket || !badflag || !dnorm)
+        return HPB_ERROR_OUT_OF_MEMORY;
+    if (cudaMallocHost(&ws.pinned, sizeof(Report) + 8 * sizeof(double)) != cudaSuccess) return HPB_ERROR_OUT_OF_MEMORY;
+    Report* hrep = static_cast<Report*>(ws.pinned);
+    double* hnorm = reinterpret_cast<double*>(static_cast<char*>(ws.pinned) + sizeof(Report));
+    if (cudaStreamCreateWithFlags(&ws.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ws.ev, cudaEventDisableTiming) != cudaSuccess)
+        return HPB_ERROR_CUDA;
+    cudaStream_t s = ws.stream;
+    // run after the caller's work on the legacy default stream
+    if (cudaEventRecord(ws.ev, 0) != cudaSuccess || cudaStreamWaitEvent(s, ws.ev, 0) != cudaSuccess)
+        return HPB_ERROR_CUDA;
+    auto t0 = std::chrono::steady_clock::now();
+
+    cudaMemsetAsync(ticket, 0, 64, s);
+    cudaMemsetAsync(badflag, 0, 64, s);
+    cudaMemsetAsync(V.u[0], 0, vb, s);
+    k_init_state<S><<<1, 1, 0, s>>>(st, drep);
+    EpiArgs<S> none{st, drep, EPI_NONE, 0, 0, L};
+    if (jac) k_diag<E><<<(rows + 255) / 256, 256, 0, s>>>(rows, rp, ci, val, diag);
+    // monitor base ||P b||
+    const E* pb = b;
+    if (jac) {
+        k_scale_inv<E><<<g_ew, kThreads, 0, s>>>(n, b, diag, tmp);
+        pb = tmp;
+    }
+    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, pb, dnorm, partials, ticket, badflag);
+    // r0 = P (b - A x), rt = r0 / ||r0||
+    k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, nullptr, x, tmp, nullptr, partials, ticket,
+                                                   badflag, none);
+    k_residual_finish<E><<<g_ew, kThreads, 0, s>>>(n, b, tmp, diag, V.r[0]);
+    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[0], dnorm + 1, partials, ticket, badflag);
+    k_scale_by_inv_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[0], dnorm + 1, rt);
+    // ||r0||, <rt, r0>, finiteness of x, and the first cycle's beta / rho
+    k_final<E><<<g_ew, kThreads, 0, s>>>(n, L, 0, V, x, rt, st, partials, ticket, badflag,
+                                         EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L});
+    cudaMemcpyAsync(hrep, drep, sizeof(Report), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hnorm, dnorm, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HPB_ERROR_CUDA;
+    count_launch(jac ? 9 : 6);
+
+    // ---- one cycle as a CUDA graph
+    int kernels = 0;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HPB_ERROR_CUDA;
+    for (int j = 0; j < L; ++j) {
+        k_upd_u<E><<<g_ew, kThreads, 0, s>>>(n, j, V, st);
+        k_spmv_dot<E, true><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt, partials,
+                                                      ticket, badflag, EpiArgs<S>{st, drep, EPI_ALPHA, 0, j, L});
+        k_upd_rx<E><<<g_ew, kThreads, 0, s>>>(n, j, V, x, st);
+        if (j + 1 < L)
+            k_spmv_dot<E, true><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.r[j], V.r[j + 1], rt,
+                                                          partials, ticket, badflag,
+                                                          EpiArgs<S>{st, drep, EPI_BETA, 0, j, L});
+        else
+            k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.r[j], V.r[j + 1], nullptr,
+                                                           partials, ticket, badflag, none);
+        kernels += 4;
+    }
+    for (int j = 1; j <= L; ++j)
+        for (int k = 1; k <= j; ++k) {
+            if (k < j)
+                k_mgs<E, 1><<<g_ew, kThreads, 0, s>>>(n, k, j, V, st, partials, ticket, badflag,
+                                                      EpiArgs<S>{st, drep, EPI_TAU, k, j, L});
+            else
+                k_mgs<E, 2><<<g_ew, kThreads, 0, s>>>(n, k, j, V, st, partials, ticket, badflag,
+                                                      EpiArgs<S>{st, drep, EPI_SIGMA, k, j, L});
+            ++kernels;
+        }
+    k_final<E><<<g_ew, kThreads, 0, s>>>(n, L, 1, V, x, rt, st, partials, ticket, badflag,
+                                         EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L});
+    ++kernels;
+    cudaMemcpyAsync(hrep, drep, sizeof(Report), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamEndCapture(s, &ws.graph) != cudaSuccess) return HPB_ERROR_CUDA;
+    if (cudaGraphInstantiate(&ws.exec, ws.graph, 0) != cudaSuccess) return HPB_ERROR_CUDA;
+
+    // ---- monitor loop (default_monitor semantics, one test per cycle)
+    const double rhs = hnorm[0];
+    const double tol = p->abs_tol + p->rel_tol * rhs;
+    int iters = 0, hl = 0;
+    bool breakdown = false, valid = true, conv = false;
+    double rn = hrep->rnorm;
+    auto record = [&]() {
+        valid = !hrep->nonfinite && std::isfinite(hrep->rnorm);
+        rn = hrep->rnorm;
+        conv = valid && rn <= tol;
+        if (hl < cap) {
+            hist[2 * hl] = iters;
+            hist[2 * hl + 1] = rn;
+            ++hl;
+        }
+        return !valid || conv || iters >= p->max_iters;
+    };
+    bool finished = record();
+    while (!finished) {
+        if (cudaGraphLaunch(ws.exec, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+            return HPB_ERROR_CUDA;
+        count_launch(uint64_t(kernels));
+        iters += L;
+        if (hrep->breakdown) {
+            breakdown = true;
+            break;
+        }
+        finished = record();
+    }
+    auto t1 = std::chrono::steady_clock::now();
+
+    // true residual ||b - A x|| and ||b|| (compensated)
+    k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, nullptr, x, tmp, nullptr, partials, ticket,
+                                                   badflag, none);
+    k_residual_finish<E><<<g_ew, kThreads, 0, s>>>(n, b, tmp, nullptr, V.r[1]);
+    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[1], dnorm + 2, partials, ticket, badflag);
+    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, b, dnorm + 3, partials, ticket, badflag);
+    cudaMemcpyAsync(hnorm + 2, dnorm + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HPB_ERROR_CUDA;
+    count_launch(4);
+
+    rep->iters = iters;
+    rep->converged = conv ? 1 : 0;
+    rep->breakdown = breakdown ? 1 : 0;
+    rep->history_len = hl;
+    rep->rhs_norm = rhs;
+    rep->resid_norm = rn;
+    rep->true_resid_norm = hnorm[2];
+    rep->true_rhs_norm = hnorm[3];
+    rep->seconds = std::chrono::duration<double>(t1 - t0).count();
+    if (cudaGetLastError() != cudaSuccess) return HPB_ERROR_CUDA;
+    return conv ? HPB_SUCCESS : (breakdown ? HPB_ERROR_BREAKDOWN : HPB_ERROR_NOT_CONVERGED);
+}
+
+template int solve_bicgstabl<float>(const hpb_solver_params*, int32_t, int64_t, const int32_t*, const int32_t*,
+                                    const float*, const float*, float*, hpb_solver_report*, double*, int);
+template int solve_bicgstabl<double>(const hpb_solver_params*, int32_t, int64_t, const int32_t*, const int32_t*,
+                                     const double*, const double*, double*, hpb_solver_report*, double*, int);
+template int solve_bicgstabl<cf>(const hpb_solver_params*, int32_t, int64_t, const int32_t*, const int32_t*,
+                                 const cf*, const cf*, cf*, hpb_solver_report*, double*, int);
+template int solve_bicgstabl<cd>(const hpb_solver_params*, int32_t, int64_t, const int32_t*, const int32_t*,
+                                 const cd*, const cd*, cd*, hpb_solver_report*, double*, int);
+
+}  // namespace fused
+}  // namespace hpb

@@ -1,0 +1,256 @@
+// Mixed-precision iterative refinement (the precision form).
+//
+// Outer loop in binary64 (complex<binary64>): r = b - A x with a
+// compensated (Dot2) row sum and ||r|| in Dot2 -- the "true residual" that
+// decides convergence; inner correction solve A d = r / ||r|| in binary32
+// (complex<binary32>) storage with binary32 SpMV and Dot2 reductions,
+// GMRES(m) or BiCGStab(l) on the device-resident path, optionally right-
+// preconditioned by a binary32 CSR matrix M (the learned sparse approximate
+// inverse) or by Jacobi; x += ||r|| d in binary64.  The reference has no
+// refinement loop; its solvers run in one precision.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+#include "hpb_fused.cuh"
+
+namespace hpb {
+namespace fused {
+
+template <class E, class R>
+__global__ void k_ir_resid(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                           const E* __restrict__ val, const E* __restrict__ x, const E* __restrict__ b,
+                           E* __restrict__ r, double* out /* [0] ||r||, [1] nonfinite */,
+                           typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket,
+                           int* badflag) {
+    using S = typename scalar_of<E>::type;
+    using A = typename acc_of<S>::type;
+    const int32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+    A nacc[1];
+    bool bad = false;
+    if (row < rows) {
+        A ra;
+        ra.s = to_s(ldE(b, row));
+        for (int32_t k = rp[row]; k < rp[row + 1]; ++k) {
+            E xe = ldE(x, ci[k]);
+            bad |= !finite_e(xe);
+            dot_add(ra, s_neg(conj_s(to_s(ldE(val, k)))), to_s(xe));
+        }
+        S rv = acc_value(ra);
+        stE(r, row, from_s<E>(rv));
+        dot_add(nacc[0], rv, rv);
+    }
+    grid_finish<1>(nacc, bad, partials, ticket, badflag, [&](const S* v, bool anybad) {
+        out[0] = sqrt(fmax(s_real(v[0]), 0.0));
+        out[1] = anybad ? 1.0 : 0.0;
+    });
+}
+
+// lo = (r / rnorm) rounded to the inner storage type
+template <class E, class L>
+__global__ void k_ir_scale_down(int64_t n, const E* __restrict__ r, const double* rnorm, L* __restrict__ lo) {
+    using S = typename scalar_of<E>::type;
+    const double inv = 1.0 / rnorm[0];
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride)
+        stE(lo, q, from_s<L>(s_mul(make_real<S>(inv), to_s(ldE(r, q)))));
+}
+// x += rnorm * d
+template <class E, class L>
+__global__ void k_ir_update(int64_t n, E* __restrict__ x, const L* __restrict__ d, const double* rnorm) {
+    using S = typename scalar_of<E>::type;
+    const S f = make_real<S>(rnorm[0]);
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride)
+        stE(x, q, from_s<E>(s_fma(f, to_s(ldE(d, q)), to_s(ldE(x, q)))));
+}
+template <class E, class L>
+__global__ void k_ir_round(int64_t n, const E* __restrict__ a, L* __restrict__ b) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride)
+        stE(b, q, from_s<L>(to_s(ldE(a, q))));
+}
+template <class E>
+__global__ void k_ir_norm(int64_t n, const E* __restrict__ v, double* out,
+                          typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket,
+                          int* badflag) {
+    using S = typename scalar_of<E>::type;
+    using A = typename acc_of<S>::type;
+    A acc[1];
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+        S s = to_s(ldE(v, q));
+        dot_add(acc[0], s, s);
+    }
+    grid_finish<1>(acc, false, partials, ticket, badflag,
+                   [&](const S* vals, bool) { out[0] = sqrt(fmax(s_real(vals[0]), 0.0)); });
+}
+
+template <class E, class L>
+int ir_solve(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci, const E* val,
+             const L* val_lo_in, const int32_t* m_rp, const int32_t* m_ci, const L* m_val, int64_t m_nnz, const E* b,
+             E* x, hpb_ir_report* rep, double* hist, int cap) {
+    using S = typename scalar_of<E>::type;
+    using A = typename acc_of<S>::type;
+    if (!p || !rep || rows < 0 || nnz < 0 || (cap > 0 && !hist)) return HPB_ERROR_INVALID_VALUE;
+    *rep = hpb_ir_report{};
+    if (rows == 0) {
+        rep->converged = 1;
+        return HPB_SUCCESS;
+    }
+    if (p->precond == HPB_PRECOND_MATRIX && (!m_rp || !m_ci || !m_val)) return HPB_ERROR_INVALID_VALUE;
+    if (p->precond == HPB_PRECOND_MATRIX && p->inner_method != HPB_SOLVER_GMRES) return HPB_ERROR_NOT_SUPPORTED;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return HPB_ERROR_CUDA;
+    const int64_t n = rows;
+    const int g_ew = int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, int64_t(sms) * 8)));
+    const int g_row = (rows + 255) / 256;
+    std::vector<void*> allocs;
+    auto dalloc = [&](size_t bytes) -> void* {
+        void* q = nullptr;
+        if (cudaMalloc(&q, bytes ? bytes : 16) != cudaSuccess) return nullptr;
+        allocs.push_back(q);
+        return q;
+    };
+    struct Cleanup {
+        std::vector<void*>& a;
+        ~Cleanup() {
+            cudaDeviceSynchronize();
+            for (void* q : a) cudaFree(q);
+        }
+    } cleanup{allocs};
+    E* r = static_cast<E*>(dalloc(size_t(n) * sizeof(E)));
+    L* rlo = static_cast<L*>(dalloc(size_t(n) * sizeof(L)));
+    L* dlo = static_cast<L*>(dalloc(size_t(n) * sizeof(L)));
+    const L* vlo = val_lo_in;
+    if (!vlo) {
+        L* t = static_cast<L*>(dalloc(size_t(nnz) * sizeof(L)));
+        if (!t) return HPB_ERROR_OUT_OF_MEMORY;
+        k_ir_round<E, L><<<g_ew, 256>>>(nnz, val, t);
+        count_launch();
+        vlo = t;
+    }
+    A* partials = static_cast<A*>(dalloc(size_t(std::max(g_ew, g_row)) * sizeof(A)));
+    unsigned int* ticket = static_cast<unsigned int*>(dalloc(64));
+    int* badflag = static_cast<int*>(dalloc(64));
+    double* dn = static_cast<double*>(dalloc(8 * sizeof(double)));
+    if (!r || !rlo || !dlo || !partials || !ticket || !badflag || !dn) return HPB_ERROR_OUT_OF_MEMORY;
+    cudaMemset(ticket, 0, 64);
+    cudaMemset(badflag, 0, 64);
+    auto t0 = std::chrono::steady_clock::now();
+    double hn[2];
+    k_ir_norm<E><<<g_ew, 256>>>(n, b, dn + 2, partials, ticket, badflag);
+    count_launch();
+    if (cudaMemcpy(hn, dn + 2, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return HPB_ERROR_CUDA;
+    const double bnorm = hn[0];
+    const double tol = p->rel_tol * bnorm;
+
+    hpb_solver_params ip{};
+    hpb_solver_params_default(&ip);
+    ip.method = p->inner_method;
+    ip.basis = p->inner_basis;
+    ip.rel_tol = p->inner_rel_tol;
+    ip.abs_tol = 0.0;
+    ip.max_iters = p->inner_max_iters > 0 ? p->inner_max_iters : 10000;
+    ip.precond = p->precond == HPB_PRECOND_JACOBI ? HPB_PRECOND_JACOBI : HPB_PRECOND_NONE;
+    ip.high_precision = 1;
+    ip.fused = 1;
+    RightPrec<L> M;
+    if (p->precond == HPB_PRECOND_JACOBI) M.kind = 1;
+    if (p->precond == HPB_PRECOND_MATRIX) {
+        M.kind = 2;
+        M.rows = rows;
+        M.nnz = m_nnz;
+        M.rp = m_rp;
+        M.ci = m_ci;
+        M.val = m_val;
+    }
+
+    int refinements = 0, inner_iters = 0, hl = 0;
+    bool conv = false, valid = true;
+    double rn = 0.0;
+    for (;;) {
+        k_ir_resid<E, E><<<g_row, 256>>>(rows, rp, ci, val, x, b, r, dn, partials, ticket, badflag);
+        count_launch();
+        if (cudaMemcpy(hn, dn, 2 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return HPB_ERROR_CUDA;
+        rn = hn[0];
+        valid = hn[1] == 0.0 && std::isfinite(rn);
+        conv = valid && rn <= tol;
+        if (hl < cap) {
+            hist[2 * hl] = inner_iters;
+            hist[2 * hl + 1] = rn;
+            ++hl;
+        }
+        if (conv || !valid || refinements >= p->max_refinements) break;
+        k_ir_scale_down<E, L><<<g_ew, 256>>>(n, r, dn, rlo);
+        cudaMemset(dlo, 0, size_t(n) * sizeof(L));
+        count_launch();
+        hpb_solver_report irep{};
+        int st;
+        if (p->inner_method == HPB_SOLVER_GMRES)
+            st = solve_gmres<L>(&ip, rows, nnz, rp, ci, vlo, M, rlo, dlo, &irep, nullptr, 0, 0);
+        else if (p->inner_method == HPB_SOLVER_BICGSTABL)
+            st = solve_bicgstabl<L>(&ip, rows, nnz, rp, ci, vlo, rlo, dlo, &irep, nullptr, 0);
+        else
+            return HPB_ERROR_NOT_SUPPORTED;
+        if (st != HPB_SUCCESS && st != HPB_ERROR_NOT_CONVERGED && st != HPB_ERROR_BREAKDOWN) return st;
+        inner_iters += irep.iters;
+        k_ir_update<E, L><<<g_ew, 256>>>(n, x, dlo, dn);
+        count_launch();
+        ++refinements;
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess) return HPB_ERROR_CUDA;
+    auto t1 = std::chrono::steady_clock::now();
+    rep->converged = conv ? 1 : 0;
+    rep->refinements = refinements;
+    rep->inner_iters = inner_iters;
+    rep->rhs_norm = bnorm;
+    rep->true_resid_norm = rn;
+    rep->history_len = hl;
+    rep->seconds = std::chrono::duration<double>(t1 - t0).count();
+    return conv ? HPB_SUCCESS : HPB_ERROR_NOT_CONVERGED;
+}
+
+}  // namespace fused
+}  // namespace hpb
+
+using hpb::cd;
+using hpb::cf;
+
+extern "C" {
+
+int hpb_ir_params_default(hpb_ir_params* p) {
+    if (!p) return HPB_ERROR_INVALID_VALUE;
+    *p = hpb_ir_params{};
+    p->inner_method = HPB_SOLVER_GMRES;
+    p->inner_basis = 50;
+    p->inner_rel_tol = 1e-5;
+    p->inner_max_iters = 5000;
+    p->precond = HPB_PRECOND_NONE;
+    p->rel_tol = 1e-10;
+    p->max_refinements = 30;
+    return HPB_SUCCESS;
+}
+
+int hpb_ir_solve_f64(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr, const int32_t* col_ind,
+                     const double* val, const float* val_f32, const int32_t* m_row_ptr, const int32_t* m_col_ind,
+                     const float* m_val, int64_t m_nnz, const double* b, double* x, hpb_ir_report* rep,
+                     double* history, int history_cap) {
+    return hpb::fused::ir_solve<double, float>(p, rows, nnz, row_ptr, col_ind, val, val_f32, m_row_ptr, m_col_ind,
+                                               m_val, m_nnz, b, x, rep, history, history_cap);
+}
+
+int hpb_ir_solve_c128(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                      const int32_t* col_ind, const void* val, const void* val_c64, const int32_t* m_row_ptr,
+                      const int32_t* m_col_ind, const void* m_val, int64_t m_nnz, const void* b, void* x,
+                      hpb_ir_report* rep, double* history, int history_cap) {
+    return hpb::fused::ir_solve<cd, cf>(p, rows, nnz, row_ptr, col_ind, static_cast<const cd*>(val),
+                                        static_cast<const cf*>(val_c64), m_row_ptr, m_col_ind,
+                                        static_cast<const cf*>(m_val), m_nnz, static_cast<const cd*>(b),
+                                        static_cast<cd*>(x), rep, history, history_cap);
+}
+
+}  // extern "C"

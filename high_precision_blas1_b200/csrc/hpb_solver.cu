@@ -20,8 +20,13 @@
 #include <hpblas1/solvers/gmres.h>
 
 #include "hpb_common.cuh"
+#include "hpb_fused.cuh"
 
 namespace {
+
+template <class T> struct storage_of { using type = T; };
+template <> struct storage_of<thrust::complex<float> > { using type = hpb::cf; };
+template <> struct storage_of<thrust::complex<double> > { using type = hpb::cd; };
 
 template <class T>
 struct Stack {
@@ -57,6 +62,24 @@ int solve_device(const hpb_solver_params* p, int32_t rows, int64_t nnz, const in
     if (rows == 0) {
         rep->converged = 1;
         return HPB_SUCCESS;
+    }
+    if (p->fused) {
+        using E = typename storage_of<T>::type;
+        if (p->method == HPB_SOLVER_BICGSTABL)
+            return hpb::fused::solve_bicgstabl<E>(p, rows, nnz, rp, ci, reinterpret_cast<const E*>(val),
+                                                  reinterpret_cast<const E*>(b), reinterpret_cast<E*>(x), rep, hist,
+                                                  cap);
+        if (p->method == HPB_SOLVER_GMRES) {
+            hpb::fused::RightPrec<E> M;
+            if (p->precond == HPB_PRECOND_JACOBI)
+                M.kind = 1;
+            else if (p->precond != HPB_PRECOND_NONE)
+                return HPB_ERROR_NOT_SUPPORTED;
+            return hpb::fused::solve_gmres<E>(p, rows, nnz, rp, ci, reinterpret_cast<const E*>(val), M,
+                                              reinterpret_cast<const E*>(b), reinterpret_cast<E*>(x), rep, hist, cap,
+                                              0);
+        }
+        return HPB_ERROR_NOT_SUPPORTED;
     }
     T* bm = const_cast<T*>(b);  // the solver concept takes non-const vector references
     try {

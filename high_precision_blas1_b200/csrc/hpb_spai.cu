@@ -1,0 +1,679 @@
+// Learned sparse approximate inverse (SPAI) with A's sparsity pattern.
+//
+// A per-row MLP (16 -> 64 -> 64 -> 8, ReLU; weights held in bfloat16,
+// every product accumulated in binary32) reads local features of row i of
+// A and emits the entries of row i of M on A's pattern; M is used as a
+// right preconditioner (A M y = b, x = M y).  Training minimises
+//   w_F ||A M - I||_F^2 / n  +  w_R sum_s ||A M r_s - r_s||^2 / ||r_s||^2
+// over systems of the target family, the second term on residual vectors
+// r_s of the plain Jacobi iteration (the residual histories of a plain
+// solver).  Forward, backward, loss gradients and the Adam step are the
+// kernels below; nothing here calls a library.
+//
+// Stencil slots: a row's entries are addressed by their column offset
+// col - row, one of `nslot` offsets (7 for a 3-D 7-point stencil, 5 for a
+// 2-D 5-point one) given by the caller; slot `dslot` is the diagonal.
+// Features of row i (16, zero padded): a_{i,s}/a_ii for the off-diagonal
+// slots, a_{j,j}/a_ii of each neighbour j, log(a_ii / mean diag), 1.
+// Outputs: o_s, with M_{i,i+off_s} = o_s / a_ii (so o = e_dslot is Jacobi).
+// The matrices of this path are symmetric (diffusion); the Frobenius
+// gradient uses A^T = A.
+//
+// No counterpart in the reference (which has no learned component).
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+#include "hpb_common.cuh"
+
+namespace hpb {
+namespace spai {
+
+constexpr int kF = 16, kH = 64, kO = 8, kMaxSlot = 8, kMaxSq = 64;
+constexpr int kNumParams = kF * kH + kH + kH * kH + kH + kH * kO + kO;  // 5768
+constexpr int kTile = 64;                                                // rows per tile
+constexpr int kThreads = 256;
+
+struct Offsets {
+    int nslot, dslot;
+    int off[kMaxSlot];
+    // A^2 pattern: nsq distinct offsets; sq[p][q] = index of off[p] + off[q]
+    int nsq;
+    int sqoff[kMaxSq];
+    int sq[kMaxSlot][kMaxSlot];
+    // index of off[q] - off[p] in sqoff (-1 if absent)
+    int dq[kMaxSlot][kMaxSlot];
+};
+
+struct Params {  // offsets (in floats) of each tensor in the parameter vector
+    static constexpr int W1 = 0, B1 = W1 + kF * kH, W2 = B1 + kH, B2 = W2 + kH * kH, W3 = B2 + kH, B3 = W3 + kH * kO;
+};
+
+__device__ __forceinline__ int slot_of(const Offsets& o, int d) {
+    for (int s = 0; s < o.nslot; ++s)
+        if (o.off[s] == d) return s;
+    return -1;
+}
+
+// ---------------------------------------------------------------- features
+__global__ void k_features(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                           const float* __restrict__ val, const float* __restrict__ diag, float mean_log_diag,
+                           Offsets o, float* __restrict__ feat) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    float f[kF];
+#pragma unroll
+    for (int k = 0; k < kF; ++k) f[k] = 0.f;
+    const float dii = diag[i];
+    int nf = 0;
+    float a[kMaxSlot], dj[kMaxSlot];
+    for (int s = 0; s < kMaxSlot; ++s) {
+        a[s] = 0.f;
+        dj[s] = 0.f;
+    }
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+        int s = slot_of(o, ci[k] - i);
+        if (s < 0) continue;
+        a[s] = val[k] / dii;
+        dj[s] = diag[ci[k]] / dii;
+    }
+    for (int s = 0; s < o.nslot; ++s)
+        if (s != o.dslot) {
+            f[nf] = a[s];
+            f[nf + o.nslot - 1] = dj[s];
+            ++nf;
+        }
+    f[2 * (o.nslot - 1)] = logf(fabsf(dii)) - mean_log_diag;
+    f[2 * (o.nslot - 1) + 1] = 1.f;
+#pragma unroll
+    for (int k = 0; k < kF; ++k) feat[size_t(i) * kF + k] = f[k];
+}
+
+// ---------------------------------------------------------------- MLP
+// Stage the bf16 weights as binary32 in shared memory.
+__device__ __forceinline__ void load_weights(const __nv_bfloat16* __restrict__ w, float* sw) {
+    for (int k = threadIdx.x; k < kNumParams; k += blockDim.x) sw[k] = __bfloat162float(w[k]);
+}
+
+// out[i] = W3 relu(W2 relu(W1 x + b1) + b2) + b3 ; keeps h1, h2 (post-ReLU)
+__global__ void __launch_bounds__(kThreads)
+k_forward(int32_t rows, const float* __restrict__ feat, const __nv_bfloat16* __restrict__ w,
+          float* __restrict__ h1g, float* __restrict__ h2g, float* __restrict__ out) {
+    extern __shared__ float smem[];
+    float* sw = smem;                        // kNumParams
+    float* sx = sw + kNumParams;             // kTile * kF
+    float* sh1 = sx + kTile * kF;            // kTile * kH
+    float* sh2 = sh1 + kTile * kH;           // kTile * kH
+    load_weights(w, sw);
+    const int ntiles = (rows + kTile - 1) / kTile;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int32_t r0 = t * kTile;
+        const int nr = min(kTile, rows - r0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < kTile * kF; k += blockDim.x)
+            sx[k] = (k / kF) < nr ? feat[size_t(r0) * kF + k] : 0.f;
+        __syncthreads();
+        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x) {
+            const int r = k / kH, u = k % kH;
+            float z = sw[Params::B1 + u];
+#pragma unroll
+            for (int q = 0; q < kF; ++q) z = fmaf(sx[r * kF + q], sw[Params::W1 + q * kH + u], z);
+            sh1[k] = fmaxf(z, 0.f);
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x) {
+            const int r = k / kH, u = k % kH;
+            float z = sw[Params::B2 + u];
+#pragma unroll 16
+            for (int q = 0; q < kH; ++q) z = fmaf(sh1[r * kH + q], sw[Params::W2 + q * kH + u], z);
+            sh2[k] = fmaxf(z, 0.f);
+        }
+        __syncthreads();
+        for (int k = threadIdx.x; k < kTile * kO; k += blockDim.x) {
+            const int r = k / kO, u = k % kO;
+            float z = sw[Params::B3 + u];
+#pragma unroll 16
+            for (int q = 0; q < kH; ++q) z = fmaf(sh2[r * kH + q], sw[Params::W3 + q * kO + u], z);
+            if (r < nr) out[size_t(r0 + r) * kO + u] = z;
+        }
+        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x)
+            if (k / kH < nr) {
+                if (h1g) h1g[size_t(r0) * kH + k] = sh1[k];
+                if (h2g) h2g[size_t(r0) * kH + k] = sh2[k];
+            }
+    }
+}
+
+// Weight gradients of one block (summed over its tiles) into part[block][:].
+__global__ void __launch_bounds__(kThreads)
+k_backward(int32_t rows, const float* __restrict__ feat, const __nv_bfloat16* __restrict__ w,
+           const float* __restrict__ h1g, const float* __restrict__ h2g, const float* __restrict__ dout,
+           float* __restrict__ part) {
+    extern __shared__ float smem[];
+    float* sw = smem;                    // kNumParams
+    float* sx = sw + kNumParams;         // kTile * kF
+    float* sh1 = sx + kTile * kF;        // kTile * kH  (h1, then dh1 in place)
+    float* sh2 = sh1 + kTile * kH;       // kTile * kH  (h2)
+    float* sd2 = sh2 + kTile * kH;       // kTile * kH  (dh2)
+    float* sdo = sd2 + kTile * kH;       // kTile * kO
+    load_weights(w, sw);
+    float acc[(kNumParams + kThreads - 1) / kThreads];
+    constexpr int kPer = (kNumParams + kThreads - 1) / kThreads;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) acc[k] = 0.f;
+    const int ntiles = (rows + kTile - 1) / kTile;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int32_t r0 = t * kTile;
+        const int nr = min(kTile, rows - r0);
+        __syncthreads();
+        for (int k = threadIdx.x; k < kTile * kF; k += blockDim.x)
+            sx[k] = (k / kF) < nr ? feat[size_t(r0) * kF + k] : 0.f;
+        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x) {
+            const bool in = (k / kH) < nr;
+            sh1[k] = in ? h1g[size_t(r0) * kH + k] : 0.f;
+            sh2[k] = in ? h2g[size_t(r0) * kH + k] : 0.f;
+        }
+        for (int k = threadIdx.x; k < kTile * kO; k += blockDim.x)
+            sdo[k] = (k / kO) < nr ? dout[size_t(r0) * kO + k] : 0.f;
+        __syncthreads();
+        // dh2 = (dout W3^T) * [h2 > 0]
+        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x) {
+            const int r = k / kH, u = k % kH;
+            float g = 0.f;
+#pragma unroll
+            for (int q = 0; q < kO; ++q) g = fmaf(sdo[r * kO + q], sw[Params::W3 + u * kO + q], g);
+            sd2[k] = sh2[k] > 0.f ? g : 0.f;
+        }
+        __syncthreads();
+        // weight gradients that need h1/h2 before dh1 overwrites h1
+        for (int j = 0; j < kPer; ++j) {
+            const int pidx = threadIdx.x + j * kThreads;
+            if (pidx >= kNumParams) break;
+            float g = 0.f;
+            if (pidx >= Params::W3 && pidx < Params::B3) {  // dW3[q][u] = sum_r h2[r][q] dout[r][u]
+                const int q = (pidx - Params::W3) / kO, u = (pidx - Params::W3) % kO;
+                for (int r = 0; r < kTile; ++r) g = fmaf(sh2[r * kH + q], sdo[r * kO + u], g);
+            } else if (pidx >= Params::B3) {
+                const int u = pidx - Params::B3;
+                for (int r = 0; r < kTile; ++r) g += sdo[r * kO + u];
+            } else if (pidx >= Params::W2 && pidx < Params::B2) {  // dW2[q][u] = sum_r h1[r][q] dh2[r][u]
+                const int q = (pidx - Params::W2) / kH, u = (pidx - Params::W2) % kH;
+                for (int r = 0; r < kTile; ++r) g = fmaf(sh1[r * kH + q], sd2[r * kH + u], g);
+            } else if (pidx >= Params::B2 && pidx < Params::W3) {
+                const int u = pidx - Params::B2;
+                for (int r = 0; r < kTile; ++r) g += sd2[r * kH + u];
+            }
+            acc[j] += g;
+        }
+        __syncthreads();
+        // dh1 = (dh2 W2^T) * [h1 > 0], in place of h1
+        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x) {
+            const int r = k / kH, u = k % kH;
+            float g = 0.f;
+#pragma unroll 16
+            for (int q = 0; q < kH; ++q) g = fmaf(sd2[r * kH + q], sw[Params::W2 + u * kH + q], g);
+            sh2[k] = sh1[k] > 0.f ? g : 0.f;  // dh1 into sh2 (h2 no longer needed)
+        }
+        __syncthreads();
+        for (int j = 0; j < kPer; ++j) {
+            const int pidx = threadIdx.x + j * kThreads;
+            if (pidx >= Params::W2) break;
+            float g = 0.f;
+            if (pidx < Params::B1) {  // dW1[q][u] = sum_r x[r][q] dh1[r][u]
+                const int q = pidx / kH, u = pidx % kH;
+                for (int r = 0; r < kTile; ++r) g = fmaf(sx[r * kF + q], sh2[r * kH + u], g);
+            } else {
+                const int u = pidx - Params::B1;
+                for (int r = 0; r < kTile; ++r) g += sh2[r * kH + u];
+            }
+            acc[j] += g;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int pidx = threadIdx.x + j * kThreads;
+        if (pidx < kNumParams) part[size_t(blockIdx.x) * kNumParams + pidx] = acc[j];
+    }
+}
+
+// grad[p] = scale * sum_b part[b][p] (fixed order: deterministic)
+__global__ void k_reduce_grad(int nblocks, const float* __restrict__ part, float scale, float* __restrict__ grad) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kNumParams) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += part[size_t(b) * kNumParams + p];
+    grad[p] = float(s * scale);
+}
+
+// Adam on binary32 master weights, bf16 copy for the kernels
+__global__ void k_adam(int step, float lr, float b1, float b2, float eps, float* __restrict__ wm,
+                       float* __restrict__ m1, float* __restrict__ m2, const float* __restrict__ grad,
+                       __nv_bfloat16* __restrict__ wb) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= kNumParams) return;
+    const float g = grad[p];
+    m1[p] = b1 * m1[p] + (1.f - b1) * g;
+    m2[p] = b2 * m2[p] + (1.f - b2) * g * g;
+    const float mh = m1[p] / (1.f - powf(b1, float(step)));
+    const float vh = m2[p] / (1.f - powf(b2, float(step)));
+    wm[p] -= lr * mh / (sqrtf(vh) + eps);
+    wb[p] = __float2bfloat16(wm[p]);
+}
+
+// ---------------------------------------------------------------- SPAI
+// M_{i, i+off_s} = out[i][s] / a_ii on A's pattern
+__global__ void k_assemble(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                           const float* __restrict__ diag, const float* __restrict__ out, Offsets o,
+                           float* __restrict__ mval) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const float inv = 1.f / diag[i];
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+        const int s = slot_of(o, ci[k] - i);
+        mval[k] = s >= 0 ? out[size_t(i) * kO + s] * inv : 0.f;
+    }
+}
+
+// G = A M - I on the A^2 offsets (dense per row: nsq entries), and
+// per-block partial sums of ||G||^2 (binary64)
+__global__ void k_frob_g(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                         const float* __restrict__ aval, const float* __restrict__ mval, Offsets o,
+                         float* __restrict__ G, double* __restrict__ lpart) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float g[kMaxSq];
+    for (int t = 0; t < o.nsq; ++t) g[t] = 0.f;
+    double l = 0.0;
+    if (i < rows) {
+        for (int32_t ka = rp[i]; ka < rp[i + 1]; ++ka) {
+            const int k = ci[ka];
+            const int p = slot_of(o, k - i);
+            if (p < 0) continue;
+            const float aik = aval[ka];
+            for (int32_t km = rp[k]; km < rp[k + 1]; ++km) {
+                const int q = slot_of(o, ci[km] - k);
+                if (q < 0) continue;
+                g[o.sq[p][q]] = fmaf(aik, mval[km], g[o.sq[p][q]]);
+            }
+        }
+        for (int t = 0; t < o.nsq; ++t) {
+            if (o.sqoff[t] == 0) g[t] -= 1.f;
+            G[size_t(i) * o.nsq + t] = g[t];
+            l += double(g[t]) * double(g[t]);
+        }
+    }
+    // block sum (deterministic tree)
+    __shared__ double sh[kThreads];
+    sh[threadIdx.x] = l;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) lpart[blockIdx.x] = sh[0];
+}
+
+// dM_{k,q} += wf * 2 sum_p a_{k,p} G[k+off_p][idx(off_q - off_p)]   (A symmetric)
+__global__ void k_frob_grad(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                            const float* __restrict__ aval, const float* __restrict__ G, Offsets o, float wf,
+                            float* __restrict__ dm) {
+    const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= rows) return;
+    for (int32_t kq = rp[k]; kq < rp[k + 1]; ++kq) {
+        const int q = slot_of(o, ci[kq] - k);
+        float s = 0.f;
+        if (q >= 0)
+            for (int32_t kp = rp[k]; kp < rp[k + 1]; ++kp) {
+                const int p = slot_of(o, ci[kp] - k);
+                if (p < 0) continue;
+                const int t = o.dq[p][q];
+                if (t < 0) continue;
+                s = fmaf(aval[kp], G[size_t(ci[kp]) * o.nsq + t], s);
+            }
+        dm[kq] += wf * 2.f * s;
+    }
+}
+
+// residual term: y = M r, z = A y - r, g = A z; dM_{k,j} += wr * 2 g_k r_j
+// (the caller forms y, z, g with SpMVs); loss partial sum ||z||^2
+__global__ void k_resid_grad(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                             const float* __restrict__ g, const float* __restrict__ r, float wr,
+                             float* __restrict__ dm) {
+    const int32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= rows) return;
+    const float gk = g[k];
+    for (int32_t kq = rp[k]; kq < rp[k + 1]; ++kq) dm[kq] += wr * 2.f * gk * r[ci[kq]];
+}
+
+// dout[i][s] = dM_{i, i+off_s} / a_ii
+__global__ void k_dout(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                       const float* __restrict__ diag, const float* __restrict__ dm, Offsets o,
+                       float* __restrict__ dout) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    float d[kO];
+    for (int s = 0; s < kO; ++s) d[s] = 0.f;
+    const float inv = 1.f / diag[i];
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
+        const int s = slot_of(o, ci[k] - i);
+        if (s >= 0) d[s] = dm[k] * inv;
+    }
+    for (int s = 0; s < kO; ++s) dout[size_t(i) * kO + s] = d[s];
+}
+
+}  // namespace spai
+}  // namespace hpb
+
+// ===================================================================== host
+struct hpb_spai {
+    int device = 0;
+    hpb::spai::Offsets off{};
+    float* w = nullptr;            // binary32 master weights
+    __nv_bfloat16* wb = nullptr;   // bf16 copy used by the kernels
+    float* m1 = nullptr;
+    float* m2 = nullptr;
+    float* grad = nullptr;         // accumulated gradient
+    float* gtmp = nullptr;         // gradient of the current system
+    int step = 0;
+    hpb_context* ctx = nullptr;    // for the SpMVs of the residual term
+    // per-system workspace (grown on demand)
+    size_t cap_rows = 0, cap_nnz = 0;
+    float *feat = nullptr, *h1 = nullptr, *h2 = nullptr, *out = nullptr, *dout = nullptr, *diag = nullptr;
+    float *mval = nullptr, *dm = nullptr, *G = nullptr, *y = nullptr, *z = nullptr, *g = nullptr, *part = nullptr;
+    double* lpart = nullptr;
+    int part_blocks = 0;
+};
+
+namespace {
+using hpb::spai::kNumParams;
+constexpr int kGridMlp = 296;
+
+int grow(hpb_spai* net, int32_t rows, int64_t nnz) {
+    using namespace hpb::spai;
+    if (size_t(rows) <= net->cap_rows && size_t(nnz) <= net->cap_nnz) return HPB_SUCCESS;
+    float** fr[] = {&net->feat, &net->h1, &net->h2, &net->out, &net->dout, &net->diag, &net->y, &net->z, &net->g, &net->G};
+    for (auto f : fr) {
+        cudaFree(*f);
+        *f = nullptr;
+    }
+    cudaFree(net->mval);
+    cudaFree(net->dm);
+    cudaFree(net->lpart);
+    net->mval = net->dm = nullptr;
+    net->lpart = nullptr;
+    const size_t R = size_t(rows), Z = size_t(nnz ? nnz : 1);
+    if (cudaMalloc(&net->feat, R * kF * 4) || cudaMalloc(&net->h1, R * kH * 4) || cudaMalloc(&net->h2, R * kH * 4) ||
+        cudaMalloc(&net->out, R * kO * 4) || cudaMalloc(&net->dout, R * kO * 4) || cudaMalloc(&net->diag, R * 4) ||
+        cudaMalloc(&net->y, R * 4) || cudaMalloc(&net->z, R * 4) || cudaMalloc(&net->g, R * 4) ||
+        cudaMalloc(&net->G, R * kMaxSq * 4) || cudaMalloc(&net->mval, Z * 4) || cudaMalloc(&net->dm, Z * 4) ||
+        cudaMalloc(&net->lpart, ((R + kThreads - 1) / kThreads + 1) * 8)) {
+        net->cap_rows = net->cap_nnz = 0;
+        return HPB_ERROR_OUT_OF_MEMORY;
+    }
+    net->cap_rows = R;
+    net->cap_nnz = Z;
+    return HPB_SUCCESS;
+}
+
+size_t fwd_smem() {
+    using namespace hpb::spai;
+    return size_t(kNumParams + kTile * kF + 2 * kTile * kH) * sizeof(float);
+}
+size_t bwd_smem() {
+    using namespace hpb::spai;
+    return size_t(kNumParams + kTile * kF + 3 * kTile * kH + kTile * kO) * sizeof(float);
+}
+
+// diag of a binary32 CSR
+__global__ void k_fdiag(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                        const float* __restrict__ val, float* __restrict__ d) {
+    const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    float v = 0.f;
+    for (int32_t k = rp[r]; k < rp[r + 1]; ++k)
+        if (ci[k] == r) v = val[k];
+    d[r] = v;
+}
+__global__ void k_sub(int32_t n, float* __restrict__ z, const float* __restrict__ r) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) z[i] -= r[i];
+}
+__global__ void k_dot_partial(int32_t n, const float* __restrict__ a, const float* __restrict__ b,
+                              double* __restrict__ part) {
+    __shared__ double sh[256];
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    sh[threadIdx.x] = i < n ? double(a[i]) * double(b[i]) : 0.0;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+double host_sum(const double* dpart, int nb) {
+    std::vector<double> h(nb);
+    cudaMemcpy(h.data(), dpart, nb * sizeof(double), cudaMemcpyDeviceToHost);
+    double s = 0;
+    for (double v : h) s += v;
+    return s;
+}
+
+// forward + M for one system (binary32 CSR, device)
+int forward_system(hpb_spai* net, const hpb_spai_system& sys, bool keep) {
+    using namespace hpb::spai;
+    const int32_t n = sys.rows;
+    int st = grow(net, n, sys.nnz);
+    if (st) return st;
+    const int gb = (n + 255) / 256;
+    k_fdiag<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, net->diag);
+    // mean log|diag| (binary64 reduction via the partial-sum kernel)
+    std::vector<float> hd(n);
+    cudaMemcpy(hd.data(), net->diag, size_t(n) * 4, cudaMemcpyDeviceToHost);
+    double ml = 0;
+    for (float v : hd) ml += std::log(std::fabs(double(v)));
+    ml /= std::max(1, n);
+    k_features<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, net->diag, float(ml), net->off, net->feat);
+    k_forward<<<kGridMlp, kThreads, fwd_smem()>>>(n, net->feat, net->wb, keep ? net->h1 : nullptr,
+                                                 keep ? net->h2 : nullptr, net->out);
+    k_assemble<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, net->diag, net->out, net->off, net->mval);
+    hpb::count_launch(4);
+    return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
+}
+}  // namespace
+
+extern "C" {
+
+int hpb_spai_create(hpb_spai** out, int nslot, int dslot, const int* offsets, uint64_t seed) {
+    using namespace hpb::spai;
+    if (!out || nslot < 2 || nslot > kMaxSlot || dslot < 0 || dslot >= nslot || !offsets) return HPB_ERROR_INVALID_VALUE;
+    if (2 * (nslot - 1) + 2 > kF) return HPB_ERROR_NOT_SUPPORTED;
+    hpb_spai* net = new (std::nothrow) hpb_spai();
+    if (!net) return HPB_ERROR_OUT_OF_MEMORY;
+    Offsets& o = net->off;
+    o.nslot = nslot;
+    o.dslot = dslot;
+    for (int s = 0; s < nslot; ++s) o.off[s] = offsets[s];
+    o.nsq = 0;
+    for (int p = 0; p < nslot; ++p)
+        for (int q = 0; q < nslot; ++q) {
+            const int d = o.off[p] + o.off[q];
+            int t = 0;
+            while (t < o.nsq && o.sqoff[t] != d) ++t;
+            if (t == o.nsq) {
+                if (o.nsq == kMaxSq) {
+                    delete net;
+                    return HPB_ERROR_NOT_SUPPORTED;
+                }
+                o.sqoff[o.nsq++] = d;
+            }
+            o.sq[p][q] = t;
+        }
+    for (int p = 0; p < nslot; ++p)
+        for (int q = 0; q < nslot; ++q) {
+            const int d = o.off[q] - o.off[p];
+            int t = -1;
+            for (int u = 0; u < o.nsq; ++u)
+                if (o.sqoff[u] == d) t = u;
+            o.dq[p][q] = t;
+        }
+    cudaGetDevice(&net->device);
+    // He-style init for the hidden layers (seeded), zero output layer with
+    // bias e_dslot: the untrained network is exactly Jacobi.
+    std::vector<float> w(kNumParams, 0.f);
+    uint64_t sd = seed * 0x9E3779B97F4A7C15ull + 1;
+    auto rnd = [&]() {
+        sd ^= sd << 13;
+        sd ^= sd >> 7;
+        sd ^= sd << 17;
+        return double(sd >> 11) * 0x1.0p-53 * 2.0 - 1.0;
+    };
+    for (int i = 0; i < kF * kH; ++i) w[Params::W1 + i] = float(rnd() * std::sqrt(6.0 / kF));
+    for (int i = 0; i < kH * kH; ++i) w[Params::W2 + i] = float(rnd() * std::sqrt(6.0 / kH));
+    for (int i = 0; i < kH; ++i) {
+        w[Params::B1 + i] = 0.01f;
+        w[Params::B2 + i] = 0.01f;
+    }
+    w[Params::B3 + dslot] = 1.f;
+    if (cudaMalloc(&net->w, kNumParams * 4) || cudaMalloc(&net->wb, kNumParams * 2) ||
+        cudaMalloc(&net->m1, kNumParams * 4) || cudaMalloc(&net->m2, kNumParams * 4) ||
+        cudaMalloc(&net->grad, kNumParams * 4) || cudaMalloc(&net->gtmp, kNumParams * 4) ||
+        cudaMalloc(&net->part, size_t(kGridMlp) * kNumParams * 4)) {
+        hpb_spai_destroy(net);
+        return HPB_ERROR_OUT_OF_MEMORY;
+    }
+    cudaMemset(net->m1, 0, kNumParams * 4);
+    cudaMemset(net->m2, 0, kNumParams * 4);
+    cudaMemset(net->grad, 0, kNumParams * 4);
+    int st = hpb_spai_set_weights(net, w.data());
+    if (st) {
+        hpb_spai_destroy(net);
+        return st;
+    }
+    if (hpb_create(&net->ctx, net->device, nullptr) != HPB_SUCCESS) {
+        hpb_spai_destroy(net);
+        return HPB_ERROR_CUDA;
+    }
+    cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(fwd_smem()));
+    cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bwd_smem()));
+    *out = net;
+    return HPB_SUCCESS;
+}
+
+int hpb_spai_destroy(hpb_spai* net) {
+    if (!net) return HPB_SUCCESS;
+    cudaDeviceSynchronize();
+    void* ptrs[] = {net->w, net->wb, net->m1, net->m2, net->grad, net->gtmp, net->part, net->feat, net->h1, net->h2,
+                    net->out, net->dout, net->diag, net->mval, net->dm, net->G, net->y, net->z, net->g, net->lpart};
+    for (void* p : ptrs) cudaFree(p);
+    if (net->ctx) hpb_destroy(net->ctx);
+    delete net;
+    return HPB_SUCCESS;
+}
+
+int hpb_spai_num_params(void) { return kNumParams; }
+
+int hpb_spai_set_weights(hpb_spai* net, const float* w_host) {
+    if (!net || !w_host) return HPB_ERROR_INVALID_VALUE;
+    std::vector<__nv_bfloat16> b(kNumParams);
+    for (int i = 0; i < kNumParams; ++i) b[i] = __float2bfloat16(w_host[i]);
+    if (cudaMemcpy(net->w, w_host, kNumParams * 4, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(net->wb, b.data(), kNumParams * 2, cudaMemcpyHostToDevice))
+        return HPB_ERROR_CUDA;
+    return HPB_SUCCESS;
+}
+
+int hpb_spai_get_weights(hpb_spai* net, float* w_host) {
+    if (!net || !w_host) return HPB_ERROR_INVALID_VALUE;
+    return cudaMemcpy(w_host, net->w, kNumParams * 4, cudaMemcpyDeviceToHost) ? HPB_ERROR_CUDA : HPB_SUCCESS;
+}
+
+// M on A's pattern for one binary32 system: m_val[nnz] (device)
+int hpb_spai_assemble(hpb_spai* net, const hpb_spai_system* sys, float* m_val) {
+    if (!net || !sys || !m_val) return HPB_ERROR_INVALID_VALUE;
+    int st = forward_system(net, *sys, false);
+    if (st) return st;
+    return cudaMemcpy(m_val, net->mval, size_t(sys->nnz) * 4, cudaMemcpyDeviceToDevice) ? HPB_ERROR_CUDA
+                                                                                           : HPB_SUCCESS;
+}
+
+// Loss of one system and its parameter gradient, added to the network's
+// accumulated gradient.  loss[0] = total, [1] = Frobenius part, [2] =
+// residual part.  grad_host (optional) receives this system's gradient.
+int hpb_spai_loss_grad(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_resid, double* loss,
+                       float* grad_host) {
+    using namespace hpb::spai;
+    if (!net || !sys || sys->rows <= 0) return HPB_ERROR_INVALID_VALUE;
+    int st = forward_system(net, *sys, true);
+    if (st) return st;
+    const int32_t n = sys->rows;
+    const int gb = (n + 255) / 256;
+    cudaMemset(net->dm, 0, size_t(sys->nnz) * 4);
+    // Frobenius term (normalised by n)
+    k_frob_g<<<gb, kThreads>>>(n, sys->row_ptr, sys->col_ind, sys->val, net->mval, net->off, net->G, net->lpart);
+    const double lf = host_sum(net->lpart, gb) / n;
+    k_frob_grad<<<gb, 256>>>(n, sys->row_ptr, sys->col_ind, sys->val, net->G, net->off, w_frob / float(n), net->dm);
+    hpb::count_launch(2);
+    // residual-history term (normalised by the number of samples)
+    double lr = 0.0;
+    for (int sidx = 0; sidx < sys->nres; ++sidx) {
+        const float* r = sys->residuals + size_t(sidx) * n;
+        k_dot_partial<<<gb, 256>>>(n, r, r, net->lpart);
+        const double rr = host_sum(net->lpart, gb);
+        if (!(rr > 0)) continue;
+        // y = M r ; z = A y - r ; g = A z   (A symmetric)
+        st = hpb_csr_spmv_f32(net->ctx, n, n, sys->nnz, sys->row_ptr, sys->col_ind, net->mval, 1.f, r, 0.f, net->y);
+        if (!st) st = hpb_csr_spmv_f32(net->ctx, n, n, sys->nnz, sys->row_ptr, sys->col_ind, sys->val, 1.f, net->y, 0.f, net->z);
+        if (st) return st;
+        k_sub<<<gb, 256>>>(n, net->z, r);
+        k_dot_partial<<<gb, 256>>>(n, net->z, net->z, net->lpart);
+        lr += host_sum(net->lpart, gb) / rr / sys->nres;
+        st = hpb_csr_spmv_f32(net->ctx, n, n, sys->nnz, sys->row_ptr, sys->col_ind, sys->val, 1.f, net->z, 0.f, net->g);
+        if (st) return st;
+        k_resid_grad<<<gb, 256>>>(n, sys->row_ptr, sys->col_ind, net->g, r, float(w_resid / (rr * sys->nres)), net->dm);
+        hpb::count_launch(4);
+    }
+    k_dout<<<gb, 256>>>(n, sys->row_ptr, sys->col_ind, net->diag, net->dm, net->off, net->dout);
+    const int ntiles = (n + kTile - 1) / kTile;
+    const int grid = std::min(kGridMlp, ntiles);
+    k_backward<<<grid, kThreads, bwd_smem()>>>(n, net->feat, net->wb, net->h1, net->h2, net->dout, net->part);
+    k_reduce_grad<<<(kNumParams + 255) / 256, 256>>>(grid, net->part, 1.f, net->gtmp);
+    hpb::count_launch(3);
+    // grad += gtmp
+    {
+        std::vector<float> a(kNumParams), b(kNumParams);
+        cudaMemcpy(a.data(), net->gtmp, kNumParams * 4, cudaMemcpyDeviceToHost);
+        cudaMemcpy(b.data(), net->grad, kNumParams * 4, cudaMemcpyDeviceToHost);
+        for (int i = 0; i < kNumParams; ++i) b[i] += a[i];
+        cudaMemcpy(net->grad, b.data(), kNumParams * 4, cudaMemcpyHostToDevice);
+        if (grad_host) std::memcpy(grad_host, a.data(), kNumParams * 4);
+    }
+    if (loss) {
+        loss[0] = w_frob * lf + w_resid * lr;
+        loss[1] = lf;
+        loss[2] = lr;
+    }
+    return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
+}
+
+// One Adam step with the accumulated gradient scaled by `scale`; clears it.
+int hpb_spai_adam(hpb_spai* net, float lr, float scale) {
+    using namespace hpb::spai;
+    if (!net) return HPB_ERROR_INVALID_VALUE;
+    if (scale != 1.f) {
+        std::vector<float> g(kNumParams);
+        cudaMemcpy(g.data(), net->grad, kNumParams * 4, cudaMemcpyDeviceToHost);
+        for (float& v : g) v *= scale;
+        cudaMemcpy(net->grad, g.data(), kNumParams * 4, cudaMemcpyHostToDevice);
+    }
+    ++net->step;
+    k_adam<<<(kNumParams + 255) / 256, 256>>>(net->step, lr, 0.9f, 0.999f, 1e-8f, net->w, net->m1, net->m2, net->grad,
+                                              net->wb);
+    hpb::count_launch();
+    cudaMemset(net->grad, 0, kNumParams * 4);
+    return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
+}
+
+}  // extern "C"

@@ -289,7 +289,8 @@ typedef enum hpb_solver_method {
 
 typedef enum hpb_precond_kind {
     HPB_PRECOND_NONE = 0,
-    HPB_PRECOND_JACOBI = 1      /* x := D^{-1} x (left) */
+    HPB_PRECOND_JACOBI = 1,     /* D^{-1}: left for BiCGStab(l), right for the fused GMRES */
+    HPB_PRECOND_MATRIX = 2      /* a given CSR matrix M as right preconditioner (refinement, GMRES) */
 } hpb_precond_kind;
 
 typedef struct hpb_solver_params {
@@ -303,6 +304,13 @@ typedef struct hpb_solver_params {
     int resid_recalc_freq;  /* recompute the true residual every k cycles (0: never) */
     int early_exit;         /* GMRES: end a cycle when the rotated estimate meets tol */
     int reorthogonalize;    /* GMRES: second Gram-Schmidt pass */
+    int fused;              /* 1: device-resident path (scalars on the GPU, SpMV+Dot2
+                               fused, one CUDA graph per cycle), Dot2 reductions:
+                               BiCGStab(l) (l <= 8, left Jacobi or none) or GMRES(m)
+                               (m <= 64, CGS2 Arnoldi, Hessenberg/Givens in binary64
+                               on the GPU, right Jacobi or none; the monitor tests the
+                               compensated true residual once per restart).
+                               0: the drop-in path. */
 } hpb_solver_params;
 
 typedef struct hpb_solver_report {
@@ -347,6 +355,84 @@ int hpb_csr_solve_c64_host(const hpb_solver_params* p, int32_t rows, int64_t nnz
 int hpb_csr_solve_c128_host(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
                             const int32_t* col_ind, const void* val, const void* b, void* x,
                             hpb_solver_report* rep, double* history, int history_cap);
+
+/* ---------------------------------------------------------------------- */
+/* Mixed-precision iterative refinement (precision form; no counterpart in */
+/* the reference, whose solvers run in one precision).  Outer loop in       */
+/* binary64: r = b - A x with a compensated (Dot2) row sum, ||r|| in Dot2;  */
+/* inner correction solve in binary32 storage (complex<binary32> for        */
+/* c128) with binary32 SpMV and Dot2 reductions on the device-resident      */
+/* path; x += ||r|| d in binary64.                                          */
+/* ---------------------------------------------------------------------- */
+typedef struct hpb_ir_params {
+    int inner_method;       /* HPB_SOLVER_GMRES or HPB_SOLVER_BICGSTABL */
+    int inner_basis;        /* m of GMRES(m) / l of BiCGStab(l) */
+    double inner_rel_tol;   /* residual reduction asked of each inner solve */
+    int inner_max_iters;    /* per inner solve */
+    int precond;            /* none, Jacobi, or HPB_PRECOND_MATRIX (GMRES only) */
+    double rel_tol;         /* stop when ||b - A x|| <= rel_tol ||b|| (compensated) */
+    int max_refinements;
+} hpb_ir_params;
+
+typedef struct hpb_ir_report {
+    int converged;
+    int refinements;        /* outer steps taken */
+    int inner_iters;        /* inner iterations summed over all refinements */
+    int history_len;        /* (inner iterations so far, ||r||) pairs written */
+    double rhs_norm;        /* ||b|| (Dot2) */
+    double true_resid_norm; /* final compensated ||b - A x|| */
+    double seconds;
+} hpb_ir_report;
+
+int hpb_ir_params_default(hpb_ir_params* p);
+/* Device arrays.  val: binary64 values of A; val_f32: its binary32 copy
+ * (NULL: made inside); m_*: CSR of a binary32 right preconditioner M with
+ * A's shape (NULL unless precond == HPB_PRECOND_MATRIX); x: initial guess. */
+int hpb_ir_solve_f64(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                     const int32_t* col_ind, const double* val, const float* val_f32,
+                     const int32_t* m_row_ptr, const int32_t* m_col_ind, const float* m_val, int64_t m_nnz,
+                     const double* b, double* x, hpb_ir_report* rep, double* history, int history_cap);
+/* complex<binary64> outer, complex<binary32> inner (interleaved arrays). */
+int hpb_ir_solve_c128(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                      const int32_t* col_ind, const void* val, const void* val_c64,
+                      const int32_t* m_row_ptr, const int32_t* m_col_ind, const void* m_val, int64_t m_nnz,
+                      const void* b, void* x, hpb_ir_report* rep, double* history, int history_cap);
+
+/* ---------------------------------------------------------------------- */
+/* Learned sparse approximate inverse (no counterpart in the reference).   */
+/* A per-row MLP (16 -> 64 -> 64 -> 8, ReLU, bf16 weights, binary32        */
+/* accumulation) maps local features of row i of A to row i of M on A's    */
+/* pattern; M is a right preconditioner (HPB_PRECOND_MATRIX).  Trained by  */
+/* the library's own forward/backward kernels on                            */
+/*   w_F ||A M - I||_F^2 / n + w_R mean_s ||A M r_s - r_s||^2 / ||r_s||^2,  */
+/* r_s residual vectors of a plain solver.  Matrices must be symmetric.     */
+/* ---------------------------------------------------------------------- */
+typedef struct hpb_spai hpb_spai;
+typedef struct hpb_spai_system {
+    int32_t rows;
+    int64_t nnz;
+    const int32_t* row_ptr;    /* device, CSR of A, binary32 values */
+    const int32_t* col_ind;
+    const float* val;
+    int nres;                  /* residual samples (may be 0) */
+    const float* residuals;    /* device, nres x rows */
+} hpb_spai_system;
+
+/* offsets[nslot]: the stencil's column offsets col - row (e.g. -N^2, -N, -1,
+ * 0, 1, N, N^2); dslot: index of 0.  The untrained network is Jacobi. */
+int hpb_spai_create(hpb_spai** net, int nslot, int dslot, const int* offsets, uint64_t seed);
+int hpb_spai_destroy(hpb_spai* net);
+int hpb_spai_num_params(void);
+int hpb_spai_set_weights(hpb_spai* net, const float* w_host);
+int hpb_spai_get_weights(hpb_spai* net, float* w_host);
+/* m_val (device, nnz): M on A's pattern */
+int hpb_spai_assemble(hpb_spai* net, const hpb_spai_system* sys, float* m_val);
+/* loss[3] = (total, Frobenius, residual); adds the gradient to the
+ * network's accumulator; grad_host (optional, host, num_params) gets it. */
+int hpb_spai_loss_grad(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_resid, double* loss,
+                       float* grad_host);
+/* Adam step on scale * accumulated gradient, then clears the accumulator. */
+int hpb_spai_adam(hpb_spai* net, float lr, float scale);
 
 /* ---------------------------------------------------------------------- */
 /* Seeded input generators (host memory; no GPU needed)                    */

@@ -39,31 +39,31 @@ def test_axpy_family(gpu, t, n):
     S = lambda q: _lib.scalar(t, q)  # noqa: E731
     W = lambda q: q.astype(WIDE[t])  # noqa: E731
     cases = [
-        ("axpy", lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_axpy_{t}")(ctx.h, n, S(a), X, Y), "y",
+        ("axpy", lambda X, Y, Z, Wd, V: getattr(L, f"hpb_axpy_{t}")(ctx.h, n, S(a), X, Y), "y",
          a * W(x) + W(y), abs(a) * np.abs(W(x)) + np.abs(W(y))),
-        ("axpby", lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_axpby_{t}")(ctx.h, n, S(a), X, S(b), Y), "y",
+        ("axpby", lambda X, Y, Z, Wd, V: getattr(L, f"hpb_axpby_{t}")(ctx.h, n, S(a), X, S(b), Y), "y",
          a * W(x) + b * W(y), abs(a) * np.abs(W(x)) + abs(b) * np.abs(W(y))),
-        ("lincomb2", lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_lincomb2_{t}")(ctx.h, n, S(a), X, S(b), Y, Z), "z",
+        ("lincomb2", lambda X, Y, Z, Wd, V: getattr(L, f"hpb_lincomb2_{t}")(ctx.h, n, S(a), X, S(b), Y, Z), "z",
          a * W(x) + b * W(y), abs(a) * np.abs(W(x)) + abs(b) * np.abs(W(y))),
-        ("axpbypcz", lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_axpbypcz_{t}")(ctx.h, n, S(a), X, S(b), Y, S(c), Z),
+        ("axpbypcz", lambda X, Y, Z, Wd, V: getattr(L, f"hpb_axpbypcz_{t}")(ctx.h, n, S(a), X, S(b), Y, S(c), Z),
          "z", a * W(x) + b * W(y) + c * W(z), abs(a) * np.abs(W(x)) + abs(b) * np.abs(W(y)) + abs(c) * np.abs(W(z))),
         ("axpbypcwpdz",
-         lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_axpbypcwpdz_{t}")(ctx.h, n, S(a), X, S(b), Y, S(c), Wd, S(d), Z),
+         lambda X, Y, Z, Wd, V: getattr(L, f"hpb_axpbypcwpdz_{t}")(ctx.h, n, S(a), X, S(b), Y, S(c), Wd, S(d), Z),
          "z", a * W(x) + b * W(y) + c * W(w) + d * W(z),
          abs(a) * np.abs(W(x)) + abs(b) * np.abs(W(y)) + abs(c) * np.abs(W(w)) + abs(d) * np.abs(W(z))),
         ("lincomb4",
-         lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_lincomb4_{t}")(ctx.h, n, S(a), X, S(b), Y, S(c), V, S(d), Wd, Z),
+         lambda X, Y, Z, Wd, V: getattr(L, f"hpb_lincomb4_{t}")(ctx.h, n, S(a), X, S(b), Y, S(c), V, S(d), Wd, Z),
          "z", a * W(x) + b * W(y) + c * W(v) + d * W(w),
          abs(a) * np.abs(W(x)) + abs(b) * np.abs(W(y)) + abs(c) * np.abs(W(v)) + abs(d) * np.abs(W(w))),
-        ("scal", lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_scal_{t}")(ctx.h, n, S(a), X, Z), "z", a * W(x),
+        ("scal", lambda X, Y, Z, Wd, V: getattr(L, f"hpb_scal_{t}")(ctx.h, n, S(a), X, Z), "z", a * W(x),
          abs(a) * np.abs(W(x))),
-        ("add_scalar", lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_add_scalar_{t}")(ctx.h, n, S(b), S(a), Z), "z",
+        ("add_scalar", lambda X, Y, Z, Wd, V: getattr(L, f"hpb_add_scalar_{t}")(ctx.h, n, S(b), S(a), Z), "z",
          a * W(z) + b, abs(a) * np.abs(W(z)) + abs(b)),
-        ("fill", lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_fill_{t}")(ctx.h, n, S(a), Z), "z",
+        ("fill", lambda X, Y, Z, Wd, V: getattr(L, f"hpb_fill_{t}")(ctx.h, n, S(a), Z), "z",
          np.full(n, a, dtype=WIDE[t]), np.full(n, abs(a))),
-        ("mul_pointwise", lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_mul_pointwise_{t}")(ctx.h, n, S(a), X, S(b), Y, Z),
+        ("mul_pointwise", lambda X, Y, Z, Wd, V: getattr(L, f"hpb_mul_pointwise_{t}")(ctx.h, n, S(a), X, S(b), Y, Z),
          "z", (a * W(x)) * (b * W(y)), np.abs(a * W(x)) * np.abs(b * W(y)) * 2),
-        ("div_pointwise", lambda X, Y, Z, Wd, V: L.__getattr__(f"hpb_div_pointwise_{t}")(ctx.h, n, S(a), X, S(b), Y, Z),
+        ("div_pointwise", lambda X, Y, Z, Wd, V: getattr(L, f"hpb_div_pointwise_{t}")(ctx.h, n, S(a), X, S(b), Y, Z),
          "z", (a * W(x)) / (b * W(y)), np.abs((a * W(x)) / (b * W(y))) * 4),
     ]
     for name, call, out, want, scale in cases:
