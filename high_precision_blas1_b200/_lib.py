@@ -33,6 +33,7 @@ STATUS = {
     -5: "HPB_ERROR_BREAKDOWN",
     -6: "HPB_ERROR_NOT_FINITE",
     -7: "HPB_ERROR_NOT_CONVERGED",
+    -8: "HPB_ERROR_SIZE_LIMIT",
 }
 
 
@@ -100,6 +101,9 @@ for t in TYPES:
     for op in ("sum2", "asum2", "nrm2", "asum", "nrm2plain"):
         _sig(f"hpb_{op}_{t}", C.c_int, [P, I64, P, P])
         _sig(f"hpb_{op}_{t}_host", C.c_int, [P, I64, P, P])
+
+_sig("hpb_dot2_f64_noalloc", C.c_int, [I64, P, P, P, P])
+NOALLOC_MAX_N = 16777216
 
 # elementwise
 for t in TYPES:

@@ -110,6 +110,7 @@ const char* hpb_status_string(int status) {
         case HPB_ERROR_BREAKDOWN: return "HPB_ERROR_BREAKDOWN";
         case HPB_ERROR_NOT_FINITE: return "HPB_ERROR_NOT_FINITE";
         case HPB_ERROR_NOT_CONVERGED: return "HPB_ERROR_NOT_CONVERGED";
+        case HPB_ERROR_SIZE_LIMIT: return "HPB_ERROR_SIZE_LIMIT";
         default: return "HPB_UNKNOWN_STATUS";
     }
 }

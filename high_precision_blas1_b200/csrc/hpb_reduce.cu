@@ -22,6 +22,8 @@
 // so every combine of compensation terms runs in binary64.
 #include "hpb_common.cuh"
 
+#include <mutex>
+
 namespace hpb {
 
 enum RedOp { OP_DOT2 = 0, OP_SUM2, OP_ASUM2, OP_NRM2, OP_DOT, OP_ASUM, OP_NRM2P };
@@ -451,4 +453,80 @@ HPB_RED_ALL(HPB_RED1, nrm2, OP_NRM2)
 HPB_RED_ALL(HPB_RED2, dot, OP_DOT)
 HPB_RED_ALL(HPB_RED1, asum, OP_ASUM)
 HPB_RED_ALL(HPB_RED1, nrm2plain, OP_NRM2P)
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free Dot2 (hpb_dot2_f64_noalloc).
+//
+// For callers that cannot allocate device memory and therefore cannot hold
+// an hpb_context: code that runs under an external allocator owning the
+// whole device-memory budget, or on a path where cudaMalloc / cudaFree (which
+// can synchronise the device) are not allowed.  It launches the same
+// reduce_kernel<double, OP_DOT2> as hpb_dot2_f64; the block partials and the
+// ticket counter live in the file-scope array below instead of a context.
+//
+// Limits and sharing: the array holds kNoAllocMaxBlocks partial pairs plus
+// the ticket (128 KiB + 256 B, held by every GPU that loads the library until
+// the process exits); one block per 2048 elements, so n is limited to
+// kNoAllocMaxBlocks * 2048 = 16,777,216.  All calls share the array and it
+// keeps the last call's contents: the ticket is cleared before every launch,
+// and calls that overlap on the GPU (unordered streams) race.
+// The device address of the array is looked up once per device, with that
+// device current, by the first call on it.
+// ---------------------------------------------------------------------------
+namespace hpb {
+constexpr int kNoAllocMaxBlocks = 8192;
+constexpr int64_t kNoAllocElemsPerBlock = int64_t(kRedThreads) * kRedUnroll * 2;  // doubles per block
+constexpr size_t kNoAllocPartialBytes = size_t(kNoAllocMaxBlocks) * 2 * sizeof(double);
+constexpr size_t kNoAllocScratchBytes = kNoAllocPartialBytes + 256;  // + ticket, padded
+constexpr int kNoAllocMaxDevices = 64;
+static_assert(kNoAllocMaxBlocks * kNoAllocElemsPerBlock == HPB_DOT2_NOALLOC_MAX_N, "limit mismatch");
+}  // namespace hpb
+
+static __device__ __align__(256) unsigned char g_noalloc_dot2_scratch[hpb::kNoAllocScratchBytes];
+
+namespace {
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[hpb::kNoAllocMaxDevices] = {};
+
+// Device address of the static scratch on the current device (set-up on
+// first use per device).  Host code only sees a host-side stand-in for the
+// array's name, so the address must come from cudaGetSymbolAddress.
+cudaError_t noalloc_scratch(int* device, unsigned char** ptr) {
+    cudaError_t e = cudaGetDevice(device);
+    if (e != cudaSuccess) return e;
+    if (*device < 0 || *device >= hpb::kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_addr[*device] == nullptr) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_dot2_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_addr[*device] = p;
+    }
+    *ptr = static_cast<unsigned char*>(g_noalloc_addr[*device]);
+    return cudaSuccess;
+}
+}  // namespace
+
+extern "C" int hpb_dot2_f64_noalloc(int64_t n, const double* x, const double* y, double* out, void* stream) {
+    if (n < 0 || out == nullptr || (n > 0 && (x == nullptr || y == nullptr))) return HPB_ERROR_INVALID_VALUE;
+    if (n > HPB_DOT2_NOALLOC_MAX_N) return HPB_ERROR_SIZE_LIMIT;
+    if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(out)) %
+            sizeof(double) != 0)
+        return HPB_ERROR_INVALID_VALUE;
+    int device = 0;
+    unsigned char* scratch = nullptr;
+    if (noalloc_scratch(&device, &scratch) != cudaSuccess) return HPB_ERROR_CUDA;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned int* ticket = reinterpret_cast<unsigned int*>(scratch + hpb::kNoAllocPartialBytes);
+    if (cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s) != cudaSuccess) return HPB_ERROR_CUDA;
+    int64_t blocks = (n + hpb::kNoAllocElemsPerBlock - 1) / hpb::kNoAllocElemsPerBlock;
+    const int grid = int(blocks < 1 ? 1 : blocks);
+    const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
+    if (aligned)
+        hpb::reduce_kernel<double, hpb::OP_DOT2, true><<<grid, hpb::kRedThreads, 0, s>>>(n, x, y, scratch, ticket, out);
+    else
+        hpb::reduce_kernel<double, hpb::OP_DOT2, false><<<grid, hpb::kRedThreads, 0, s>>>(n, x, y, scratch, ticket, out);
+    hpb::count_launch();
+    return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
 }

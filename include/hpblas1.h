@@ -49,7 +49,8 @@ typedef enum hpb_status {
     HPB_ERROR_NOT_SUPPORTED = -4,   /* option the library does not provide */
     HPB_ERROR_BREAKDOWN = -5,       /* solver breakdown (rho == 0, ...) */
     HPB_ERROR_NOT_FINITE = -6,      /* NaN/Inf met where a finite value is required */
-    HPB_ERROR_NOT_CONVERGED = -7    /* solver stopped at max_iters above tolerance */
+    HPB_ERROR_NOT_CONVERGED = -7,   /* solver stopped at max_iters above tolerance */
+    HPB_ERROR_SIZE_LIMIT = -8       /* n above the stated maximum of an allocation-free entry point */
 } hpb_status;
 
 typedef struct hpb_context hpb_context;
@@ -113,6 +114,24 @@ int hpb_nrm2_f32(hpb_context* ctx, int64_t n, const float* x, double* out);
 int hpb_nrm2_f64(hpb_context* ctx, int64_t n, const double* x, double* out);
 int hpb_nrm2_c64(hpb_context* ctx, int64_t n, const void* x, double* out);
 int hpb_nrm2_c128(hpb_context* ctx, int64_t n, const void* x, double* out);
+
+/* Allocation-free Dot2 of float64 vectors.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory and so cannot
+ * hold an hpb_context: code running under an external allocator that owns
+ * the whole device-memory budget, or on a path where cudaMalloc/cudaFree
+ * (which can synchronise the device) are not allowed.  It allocates nothing:
+ * the same kernel as hpb_dot2_f64 keeps its block partials and ticket in a
+ * static device array of 128 KiB + 256 B, which every GPU that loads the
+ * library holds until the process exits.  out: device double[2] (hi, lo),
+ * as hpb_dot2_f64; x, y, out: device pointers aligned to 8 bytes; stream: a
+ * cudaStream_t or NULL.  n <= HPB_DOT2_NOALLOC_MAX_N, otherwise
+ * HPB_ERROR_SIZE_LIMIT.  The first call on a device sets up (looks up the
+ * array's device address with that device current); make that first call
+ * before any stream capture.  All calls share the array and it keeps the last
+ * call's contents; calls that overlap on the GPU (streams without an order
+ * between them) race and give wrong results. */
+#define HPB_DOT2_NOALLOC_MAX_N 16777216
+int hpb_dot2_f64_noalloc(int64_t n, const double* x, const double* y, double* out, void* stream);
 
 /* Plain ("standard precision") reductions: one FMA per term, plain tree,
  * same output layout with lo = 0.  Replace the cuBLAS ?dot/?dotc, ?asum and
