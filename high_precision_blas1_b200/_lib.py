@@ -183,6 +183,7 @@ _sig("hpb_spai_set_weights", C.c_int, [P, P])
 _sig("hpb_spai_get_weights", C.c_int, [P, P])
 _sig("hpb_spai_assemble", C.c_int, [P, C.POINTER(hpb_spai_system), P])
 _sig("hpb_spai_loss_grad", C.c_int, [P, C.POINTER(hpb_spai_system), C.c_float, C.c_float, P, P])
+_sig("hpb_spai_loss", C.c_int, [P, C.POINTER(hpb_spai_system), C.c_float, C.c_float, P])
 _sig("hpb_spai_adam", C.c_int, [P, C.c_float, C.c_float])
 
 

@@ -50,6 +50,9 @@ __host__ __device__ __forceinline__ bool s_is_zero(cd a) { return a.re == 0.0 &&
 __host__ __device__ __forceinline__ double conj_s(double a) { return a; }
 __host__ __device__ __forceinline__ cd conj_s(cd a) { return cd{a.re, -a.im}; }
 __host__ __device__ __forceinline__ double s_real(double a) { return a; }
+// sqrt of a sum of squares; clamps a negative rounding residue to 0 but keeps
+// NaN (fmax(NaN, 0) would turn a NaN norm into 0 and pass a stopping test)
+__host__ __device__ __forceinline__ double norm_sqrt(double v) { return sqrt(v < 0.0 ? 0.0 : v); }
 __host__ __device__ __forceinline__ double s_real(cd a) { return a.re; }
 // a*x + y with one rounding per component where possible
 __device__ __forceinline__ double s_fma(double a, double x, double y) { return fma(a, x, y); }

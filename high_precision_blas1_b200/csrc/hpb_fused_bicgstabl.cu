@@ -13,10 +13,11 @@
 //     and an optional Jacobi scaling (left preconditioning) is applied to
 //     the rows in the same kernel;
 //   * each modified-Gram-Schmidt pass of the MR part applies the previous
-//     projection and computes the next inner product(s) in one sweep;
+//     projection and computes the next inner product(s) in one sweep over
+//     the vectors, followed by a one-block combine of the block partials;
 //   * the closing update of x, r_0, u_0 also produces ||r_0|| (the monitor's
 //     residual), <rt, r_0> (next cycle's rho) and the finiteness of x;
-//   * one cycle = 4l + l(l+1)/2 + 1 kernels, captured once into a CUDA graph
+//   * one cycle = 4l + l(l+1) + 1 kernels, captured once into a CUDA graph
 //     and replayed; the host reads 16 bytes (||r_0||, breakdown, non-finite)
 //     per cycle to apply the monitor's test, as the reference does once per
 //     cycle (default_monitor.h:202-226).
@@ -100,7 +101,7 @@ __device__ void run_epi(const EpiArgs<S>& a, const S* v, bool bad) {
             break;
         }
         case EPI_FINAL: {  // v[0] = <rt, r_0>, v[1] = <r_0, r_0>
-            a.rep->rnorm = sqrt(fmax(s_real(v[1]), 0.0));
+            a.rep->rnorm = norm_sqrt(s_real(v[1]));
             a.rep->nonfinite = bad ? 1 : 0;
             st.rho = s_neg(s_mul(st.omega, st.rho));  // next cycle: rho = -omega rho
             if (s_is_zero(st.rho)) a.rep->breakdown = 1;
@@ -190,17 +191,23 @@ __global__ void __launch_bounds__(kThreads) k_upd_rx(int64_t n, int j, Vecs<E> V
 }
 
 // ------------------------------------------------------------ MR part
-// Pass k of the modified Gram-Schmidt sweep on r_j:
-//   if k > 1:  r_j -= tau[k-1][j] r_{k-1}
-//   if k < j:  tau[k][j] = <r_k, r_j> / sigma[k]
-//   if k == j: sigma[j] = <r_j, r_j>, gamma'_j = <r_j, r_0> / sigma[j]
+// Pass k of the modified Gram-Schmidt sweep on r_j, in two launches:
+//   k_mgs_part:   if k > 1:  r_j -= tau[k-1][j] r_{k-1}
+//                 if k < j:  block partials of <r_k, r_j>
+//                 if k == j: block partials of <r_j, r_j> and <r_j, r_0>
+//   k_mgs_finish: one block merges the partials in block order and sets
+//                 tau[k][j] = <r_k, r_j> / sigma[k], or sigma[j] and
+//                 gamma'_j = <r_j, r_0> / sigma[j] (then gamma, gamma'').
+// The combine is a separate launch (no ticket): the single-launch form with
+// a last-block epilogue stalled on B200 for this pass (every block's thread 0
+// stopped between the block barrier and the ticket atomic) and is not used.
 template <class E, int ND>
 __global__ void __launch_bounds__(kThreads)
-k_mgs(int64_t n, int k, int j, Vecs<E> V, BcgState<typename scalar_of<E>::type>* st,
-      typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
-      EpiArgs<typename scalar_of<E>::type> ea) {
+k_mgs_part(int64_t n, int k, int j, Vecs<E> V, const BcgState<typename scalar_of<E>::type>* st,
+           typename acc_of<typename scalar_of<E>::type>::type* partials) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
+    __shared__ A sh[ND * 32];
     const bool upd = k > 1;
     const S ntau = upd ? s_neg(st->tau[k - 1][j]) : s_zero(S{});
     E* rj = V.r[j];
@@ -223,7 +230,28 @@ k_mgs(int64_t n, int k, int j, Vecs<E> V, BcgState<typename scalar_of<E>::type>*
             dot_add(acc[ND - 1], v, to_s(ldE(r0, q)));
         }
     }
-    grid_finish<ND>(acc, false, partials, ticket, badflag, [&](const S* vals, bool bad) { run_epi(ea, vals, bad); });
+    block_merge<ND>(acc, sh);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int d = 0; d < ND; ++d) partials[size_t(d) * gridDim.x + blockIdx.x] = acc[d];
+}
+
+template <class S, int ND>
+__global__ void __launch_bounds__(kThreads)
+k_mgs_finish(int nb, const typename acc_of<S>::type* __restrict__ partials, EpiArgs<S> ea) {
+    using A = typename acc_of<S>::type;
+    __shared__ A sh[ND * 32];
+    A tot[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d)
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) merge(tot[d], partials[size_t(d) * nb + b]);
+    block_merge<ND>(tot, sh);
+    if (threadIdx.x == 0) {
+        S vals[ND];
+#pragma unroll
+        for (int d = 0; d < ND; ++d) vals[d] = acc_value(tot[d]);
+        run_epi(ea, vals, false);
+    }
 }
 
 // ------------------------------------------------------------ closing update
@@ -351,7 +379,7 @@ __global__ void __launch_bounds__(kThreads) k_norm(int64_t n, const E* __restric
         dot_add(acc[0], s, s);
     }
     grid_finish<1>(acc, false, partials, ticket, badflag,
-                   [&](const S* vals, bool) { out[0] = sqrt(fmax(s_real(vals[0]), 0.0)); });
+                   [&](const S* vals, bool) { out[0] = norm_sqrt(s_real(vals[0])); });
 }
 
 namespace {
@@ -476,13 +504,14 @@ int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     }
     for (int j = 1; j <= L; ++j)
         for (int k = 1; k <= j; ++k) {
-            if (k < j)
-                k_mgs<E, 1><<<g_ew, kThreads, 0, s>>>(n, k, j, V, st, partials, ticket, badflag,
-                                                      EpiArgs<S>{st, drep, EPI_TAU, k, j, L});
-            else
-                k_mgs<E, 2><<<g_ew, kThreads, 0, s>>>(n, k, j, V, st, partials, ticket, badflag,
-                                                      EpiArgs<S>{st, drep, EPI_SIGMA, k, j, L});
-            ++kernels;
+            if (k < j) {
+                k_mgs_part<E, 1><<<g_ew, kThreads, 0, s>>>(n, k, j, V, st, partials);
+                k_mgs_finish<S, 1><<<1, kThreads, 0, s>>>(g_ew, partials, EpiArgs<S>{st, drep, EPI_TAU, k, j, L});
+            } else {
+                k_mgs_part<E, 2><<<g_ew, kThreads, 0, s>>>(n, k, j, V, st, partials);
+                k_mgs_finish<S, 2><<<1, kThreads, 0, s>>>(g_ew, partials, EpiArgs<S>{st, drep, EPI_SIGMA, k, j, L});
+            }
+            kernels += 2;
         }
     k_final<E><<<g_ew, kThreads, 0, s>>>(n, L, 1, V, x, rt, st, partials, ticket, badflag,
                                          EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L});

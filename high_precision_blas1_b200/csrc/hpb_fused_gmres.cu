@@ -173,7 +173,7 @@ k_gs_update(int64_t n, int K, const E* __restrict__ V, const E* win, E* wout,
     if (!NORM) return;
     grid_finish<1>(acc, bad, partials, ticket, badflag, [&](const S* vals, bool anybad) {
         GmState<S>& g = *st;
-        const double hn = sqrt(fmax(s_real(vals[0]), 0.0));
+        const double hn = norm_sqrt(s_real(vals[0]));
         if (step < 0) {  // plain norm request
             g.rnorm = hn;
             g.nonfinite = anybad ? 1 : 0;
@@ -319,7 +319,7 @@ k_resid_comp(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __rest
         dot_add(nacc[0], rr, rr);
     }
     grid_finish<1>(nacc, bad, partials, ticket, badflag, [&](const S* vals, bool anybad) {
-        st->rnorm = sqrt(fmax(s_real(vals[0]), 0.0));
+        st->rnorm = norm_sqrt(s_real(vals[0]));
         st->nonfinite = anybad ? 1 : 0;
     });
 }
@@ -359,7 +359,7 @@ __global__ void __launch_bounds__(kGmThreads) k_gm_norm(int64_t n, const E* __re
         dot_add(acc[0], s, s);
     }
     grid_finish<1>(acc, false, partials, ticket, badflag,
-                   [&](const S* vals, bool) { out[0] = sqrt(fmax(s_real(vals[0]), 0.0)); });
+                   [&](const S* vals, bool) { out[0] = norm_sqrt(s_real(vals[0])); });
 }
 template <class S>
 __global__ void k_gm_reset(GmState<S>* st) {

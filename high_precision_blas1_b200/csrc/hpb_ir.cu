@@ -42,7 +42,7 @@ __global__ void k_ir_resid(int32_t rows, const int32_t* __restrict__ rp, const i
         dot_add(nacc[0], rv, rv);
     }
     grid_finish<1>(nacc, bad, partials, ticket, badflag, [&](const S* v, bool anybad) {
-        out[0] = sqrt(fmax(s_real(v[0]), 0.0));
+        out[0] = norm_sqrt(s_real(v[0]));
         out[1] = anybad ? 1.0 : 0.0;
     });
 }
@@ -84,7 +84,7 @@ __global__ void k_ir_norm(int64_t n, const E* __restrict__ v, double* out,
         dot_add(acc[0], s, s);
     }
     grid_finish<1>(acc, false, partials, ticket, badflag,
-                   [&](const S* vals, bool) { out[0] = sqrt(fmax(s_real(vals[0]), 0.0)); });
+                   [&](const S* vals, bool) { out[0] = norm_sqrt(s_real(vals[0])); });
 }
 
 template <class E, class L>

@@ -2,22 +2,32 @@
 //
 // A per-row MLP (16 -> 64 -> 64 -> 8, ReLU; weights held in bfloat16,
 // every product accumulated in binary32) reads local features of row i of
-// A and emits the entries of row i of M on A's pattern; M is used as a
-// right preconditioner (A M y = b, x = M y).  Training minimises
-//   w_F ||A M - I||_F^2 / n  +  w_R sum_s ||A M r_s - r_s||^2 / ||r_s||^2
-// over systems of the target family, the second term on residual vectors
-// r_s of the plain Jacobi iteration (the residual histories of a plain
-// solver).  Forward, backward, loss gradients and the Adam step are the
-// kernels below; nothing here calls a library.
+// the diagonally scaled matrix Ah = D^{-1/2} A D^{-1/2} (D = diag(A)) and
+// emits raw outputs o_{i,s}, one per stencil slot.  They define a symmetric,
+// diagonally dominant (hence positive definite) Mh on A's pattern:
+//   S_ij  = (tanh(o_{i,s}) + tanh(o_{j,s'})) / 4   for the edge i-j, where
+//           s is the slot of j in row i and s' the slot of i in row j,
+//   Mh_ij = S_ij,   Mh_ii = 1 + tanh(o_{i,d}) / 2 + sum_j |S_ij|,
+// and the right preconditioner M = D^{-1/2} Mh D^{-1/2}.  o = 0 gives
+// Mh = I, i.e. Jacobi.  Positive definiteness of Mh keeps the spectrum of
+// A M (similar to Mh^{1/2} Ah Mh^{1/2}) real and positive for SPD A, so the
+// learned preconditioner cannot stall GMRES with eigenvalues near or below
+// zero; an unconstrained Mh trained on the same loss did.
+//
+// Training minimises, in the scaled space,
+//   w_F ||Ah Mh - I||_F^2 / n  +  w_R mean_s ||Ah Mh rh_s - rh_s||^2 / ||rh_s||^2
+// with rh_s = D^{-1/2} r_s and r_s residual vectors of the plain Jacobi
+// iteration on A (the residual histories of a plain solver).  Forward,
+// backward, loss gradients and the Adam step are the kernels below; the
+// SpMVs of the residual term are this library's CSR kernel.
 //
 // Stencil slots: a row's entries are addressed by their column offset
 // col - row, one of `nslot` offsets (7 for a 3-D 7-point stencil, 5 for a
 // 2-D 5-point one) given by the caller; slot `dslot` is the diagonal.
-// Features of row i (16, zero padded): a_{i,s}/a_ii for the off-diagonal
-// slots, a_{j,j}/a_ii of each neighbour j, log(a_ii / mean diag), 1.
-// Outputs: o_s, with M_{i,i+off_s} = o_s / a_ii (so o = e_dslot is Jacobi).
-// The matrices of this path are symmetric (diffusion); the Frobenius
-// gradient uses A^T = A.
+// Features of row i (16, zero padded): Ah_{i,s} for the off-diagonal slots,
+// log(a_jj / a_ii) of each neighbour j, log(a_ii) - mean log(diag), 1.
+// The path's matrices have a symmetric pattern and symmetric values
+// (diffusion); the Frobenius gradient uses Ah^T = Ah.
 //
 // No counterpart in the reference (which has no learned component).
 #include <cmath>
@@ -46,6 +56,8 @@ struct Offsets {
     int sq[kMaxSlot][kMaxSlot];
     // index of off[q] - off[p] in sqoff (-1 if absent)
     int dq[kMaxSlot][kMaxSlot];
+    // slot of -off[s] (the transposed entry), -1 if absent
+    int rev[kMaxSlot];
 };
 
 struct Params {  // offsets (in floats) of each tensor in the parameter vector
@@ -59,6 +71,8 @@ __device__ __forceinline__ int slot_of(const Offsets& o, int d) {
 }
 
 // ---------------------------------------------------------------- features
+__device__ __forceinline__ float inv_sqrt_dd(float di, float dj) { return 1.f / sqrtf(fabsf(di * dj)); }
+
 __global__ void k_features(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                            const float* __restrict__ val, const float* __restrict__ diag, float mean_log_diag,
                            Offsets o, float* __restrict__ feat) {
@@ -75,10 +89,11 @@ __global__ void k_features(int32_t rows, const int32_t* __restrict__ rp, const i
         dj[s] = 0.f;
     }
     for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
-        int s = slot_of(o, ci[k] - i);
+        const int s = slot_of(o, ci[k] - i);
         if (s < 0) continue;
-        a[s] = val[k] / dii;
-        dj[s] = diag[ci[k]] / dii;
+        const float djj = diag[ci[k]];
+        a[s] = val[k] * inv_sqrt_dd(dii, djj);
+        dj[s] = logf(fabsf(djj / dii));
     }
     for (int s = 0; s < o.nslot; ++s)
         if (s != o.dslot) {
@@ -90,6 +105,15 @@ __global__ void k_features(int32_t rows, const int32_t* __restrict__ rp, const i
     f[2 * (o.nslot - 1) + 1] = 1.f;
 #pragma unroll
     for (int k = 0; k < kF; ++k) feat[size_t(i) * kF + k] = f[k];
+}
+
+// Ah values on A's pattern
+__global__ void k_scale_vals(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+                             const float* __restrict__ val, const float* __restrict__ diag, float* __restrict__ ah) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const float dii = diag[i];
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k) ah[k] = val[k] * inv_sqrt_dd(dii, diag[ci[k]]);
 }
 
 // ---------------------------------------------------------------- MLP
@@ -239,22 +263,25 @@ k_backward(int32_t rows, const float* __restrict__ feat, const __nv_bfloat16* __
     }
 }
 
-// grad[p] = scale * sum_b part[b][p] (fixed order: deterministic)
-__global__ void k_reduce_grad(int nblocks, const float* __restrict__ part, float scale, float* __restrict__ grad) {
+// g = sum_b part[b][p] (fixed order: deterministic); gsys[p] = g, gacc[p] += g
+__global__ void k_reduce_grad(int nblocks, const float* __restrict__ part, float* __restrict__ gsys,
+                              float* __restrict__ gacc) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= kNumParams) return;
     double s = 0.0;
     for (int b = 0; b < nblocks; ++b) s += part[size_t(b) * kNumParams + p];
-    grad[p] = float(s * scale);
+    gsys[p] = float(s);
+    gacc[p] += float(s);
 }
 
 // Adam on binary32 master weights, bf16 copy for the kernels
-__global__ void k_adam(int step, float lr, float b1, float b2, float eps, float* __restrict__ wm,
-                       float* __restrict__ m1, float* __restrict__ m2, const float* __restrict__ grad,
+__global__ void k_adam(int step, float lr, float scale, float b1, float b2, float eps, float* __restrict__ wm,
+                       float* __restrict__ m1, float* __restrict__ m2, float* __restrict__ grad,
                        __nv_bfloat16* __restrict__ wb) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= kNumParams) return;
-    const float g = grad[p];
+    const float g = grad[p] * scale;
+    grad[p] = 0.f;
     m1[p] = b1 * m1[p] + (1.f - b1) * g;
     m2[p] = b2 * m2[p] + (1.f - b2) * g * g;
     const float mh = m1[p] / (1.f - powf(b1, float(step)));
@@ -264,16 +291,34 @@ __global__ void k_adam(int step, float lr, float b1, float b2, float eps, float*
 }
 
 // ---------------------------------------------------------------- SPAI
-// M_{i, i+off_s} = out[i][s] / a_ii on A's pattern
+// Mh (scaled = true) or M = D^{-1/2} Mh D^{-1/2} on A's pattern
 __global__ void k_assemble(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                           const float* __restrict__ diag, const float* __restrict__ out, Offsets o,
+                           const float* __restrict__ diag, const float* __restrict__ out, Offsets o, bool scaled,
                            float* __restrict__ mval) {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
-    const float inv = 1.f / diag[i];
+    const float dii = diag[i];
+    float sum = 0.f;
+    int32_t kd = -1;
     for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
         const int s = slot_of(o, ci[k] - i);
-        mval[k] = s >= 0 ? out[size_t(i) * kO + s] * inv : 0.f;
+        if (s == o.dslot) {
+            kd = k;
+            continue;
+        }
+        const int rs = s >= 0 ? o.rev[s] : -1;
+        if (rs < 0) {
+            mval[k] = 0.f;
+            continue;
+        }
+        const int32_t j = ci[k];
+        const float S = 0.25f * (tanhf(out[size_t(i) * kO + s]) + tanhf(out[size_t(j) * kO + rs]));
+        sum += fabsf(S);
+        mval[k] = scaled ? S : S * inv_sqrt_dd(dii, diag[j]);
+    }
+    if (kd >= 0) {
+        const float m = 1.f + 0.5f * tanhf(out[size_t(i) * kO + o.dslot]) + sum;
+        mval[kd] = scaled ? m : m * inv_sqrt_dd(dii, dii);
     }
 }
 
@@ -347,20 +392,49 @@ __global__ void k_resid_grad(int32_t rows, const int32_t* __restrict__ rp, const
     for (int32_t kq = rp[k]; kq < rp[k + 1]; ++kq) dm[kq] += wr * 2.f * gk * r[ci[kq]];
 }
 
-// dout[i][s] = dM_{i, i+off_s} / a_ii
+// dout[i][s] = dL/do_{i,s} given dm = dL/dMh on A's pattern:
+//   off-diagonal slot s (neighbour j):  (1 - t^2)/4 * dS_ij,
+//     dS_ij = dm_ij + dm_ji + sign(S_ij) (dm_ii + dm_jj)
+//   diagonal slot: (1 - t^2)/2 * dm_ii
 __global__ void k_dout(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                       const float* __restrict__ diag, const float* __restrict__ dm, Offsets o,
+                       const float* __restrict__ out, const float* __restrict__ dm, Offsets o,
                        float* __restrict__ dout) {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
     float d[kO];
     for (int s = 0; s < kO; ++s) d[s] = 0.f;
-    const float inv = 1.f / diag[i];
+    int32_t kd = -1;
+    for (int32_t k = rp[i]; k < rp[i + 1]; ++k)
+        if (ci[k] == i) kd = k;
+    const float dmii = kd >= 0 ? dm[kd] : 0.f;
     for (int32_t k = rp[i]; k < rp[i + 1]; ++k) {
         const int s = slot_of(o, ci[k] - i);
-        if (s >= 0) d[s] = dm[k] * inv;
+        if (s < 0 || s == o.dslot) continue;
+        const int rs = o.rev[s];
+        if (rs < 0) continue;
+        const int32_t j = ci[k];
+        float dmji = 0.f, dmjj = 0.f;
+        for (int32_t kk = rp[j]; kk < rp[j + 1]; ++kk) {
+            if (ci[kk] == i) dmji = dm[kk];
+            if (ci[kk] == j) dmjj = dm[kk];
+        }
+        const float ti = tanhf(out[size_t(i) * kO + s]);
+        const float S = 0.25f * (ti + tanhf(out[size_t(j) * kO + rs]));
+        const float sg = S > 0.f ? 1.f : (S < 0.f ? -1.f : 0.f);
+        d[s] = 0.25f * (1.f - ti * ti) * (dm[k] + dmji + sg * (dmii + dmjj));
+    }
+    if (kd >= 0) {
+        const float td = tanhf(out[size_t(i) * kO + o.dslot]);
+        d[o.dslot] = 0.5f * (1.f - td * td) * dmii;
     }
     for (int s = 0; s < kO; ++s) dout[size_t(i) * kO + s] = d[s];
+}
+
+// rh = r / sqrt|d|
+__global__ void k_scale_res(int32_t n, const float* __restrict__ r, const float* __restrict__ diag,
+                            float* __restrict__ rh) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) rh[i] = r[i] / sqrtf(fabsf(diag[i]));
 }
 
 }  // namespace spai
@@ -382,6 +456,7 @@ struct hpb_spai {
     size_t cap_rows = 0, cap_nnz = 0;
     float *feat = nullptr, *h1 = nullptr, *h2 = nullptr, *out = nullptr, *dout = nullptr, *diag = nullptr;
     float *mval = nullptr, *dm = nullptr, *G = nullptr, *y = nullptr, *z = nullptr, *g = nullptr, *part = nullptr;
+    float *ahat = nullptr, *rh = nullptr;
     double* lpart = nullptr;
     int part_blocks = 0;
 };
@@ -393,7 +468,8 @@ constexpr int kGridMlp = 296;
 int grow(hpb_spai* net, int32_t rows, int64_t nnz) {
     using namespace hpb::spai;
     if (size_t(rows) <= net->cap_rows && size_t(nnz) <= net->cap_nnz) return HPB_SUCCESS;
-    float** fr[] = {&net->feat, &net->h1, &net->h2, &net->out, &net->dout, &net->diag, &net->y, &net->z, &net->g, &net->G};
+    float** fr[] = {&net->feat, &net->h1, &net->h2, &net->out, &net->dout, &net->diag,
+                    &net->y,    &net->z,  &net->g,  &net->G,   &net->rh,   &net->ahat};
     for (auto f : fr) {
         cudaFree(*f);
         *f = nullptr;
@@ -408,6 +484,7 @@ int grow(hpb_spai* net, int32_t rows, int64_t nnz) {
         cudaMalloc(&net->out, R * kO * 4) || cudaMalloc(&net->dout, R * kO * 4) || cudaMalloc(&net->diag, R * 4) ||
         cudaMalloc(&net->y, R * 4) || cudaMalloc(&net->z, R * 4) || cudaMalloc(&net->g, R * 4) ||
         cudaMalloc(&net->G, R * kMaxSq * 4) || cudaMalloc(&net->mval, Z * 4) || cudaMalloc(&net->dm, Z * 4) ||
+        cudaMalloc(&net->rh, R * 4) || cudaMalloc(&net->ahat, Z * 4) ||
         cudaMalloc(&net->lpart, ((R + kThreads - 1) / kThreads + 1) * 8)) {
         net->cap_rows = net->cap_nnz = 0;
         return HPB_ERROR_OUT_OF_MEMORY;
@@ -461,25 +538,30 @@ double host_sum(const double* dpart, int nb) {
     return s;
 }
 
-// forward + M for one system (binary32 CSR, device)
-int forward_system(hpb_spai* net, const hpb_spai_system& sys, bool keep) {
+// forward + Mh (scaled, training: also Ah) or M (scaled = false) for one
+// system (binary32 CSR, device)
+int forward_system(hpb_spai* net, const hpb_spai_system& sys, bool train) {
     using namespace hpb::spai;
     const int32_t n = sys.rows;
     int st = grow(net, n, sys.nnz);
     if (st) return st;
     const int gb = (n + 255) / 256;
     k_fdiag<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, net->diag);
-    // mean log|diag| (binary64 reduction via the partial-sum kernel)
+    // mean log|diag| over the rows (binary64 on the host)
     std::vector<float> hd(n);
     cudaMemcpy(hd.data(), net->diag, size_t(n) * 4, cudaMemcpyDeviceToHost);
     double ml = 0;
     for (float v : hd) ml += std::log(std::fabs(double(v)));
     ml /= std::max(1, n);
     k_features<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, net->diag, float(ml), net->off, net->feat);
-    k_forward<<<kGridMlp, kThreads, fwd_smem()>>>(n, net->feat, net->wb, keep ? net->h1 : nullptr,
-                                                 keep ? net->h2 : nullptr, net->out);
-    k_assemble<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, net->diag, net->out, net->off, net->mval);
+    k_forward<<<kGridMlp, kThreads, fwd_smem()>>>(n, net->feat, net->wb, train ? net->h1 : nullptr,
+                                                 train ? net->h2 : nullptr, net->out);
+    k_assemble<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, net->diag, net->out, net->off, train, net->mval);
     hpb::count_launch(4);
+    if (train) {
+        k_scale_vals<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, net->diag, net->ahat);
+        hpb::count_launch();
+    }
     return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
 }
 }  // namespace
@@ -519,9 +601,14 @@ int hpb_spai_create(hpb_spai** out, int nslot, int dslot, const int* offsets, ui
                 if (o.sqoff[u] == d) t = u;
             o.dq[p][q] = t;
         }
+    for (int p = 0; p < nslot; ++p) {
+        o.rev[p] = -1;
+        for (int q = 0; q < nslot; ++q)
+            if (o.off[q] == -o.off[p]) o.rev[p] = q;
+    }
     cudaGetDevice(&net->device);
-    // He-style init for the hidden layers (seeded), zero output layer with
-    // bias e_dslot: the untrained network is exactly Jacobi.
+    // He-style init for the hidden layers (seeded), zero output layer: the
+    // untrained network gives Mh = I, exactly Jacobi.
     std::vector<float> w(kNumParams, 0.f);
     uint64_t sd = seed * 0x9E3779B97F4A7C15ull + 1;
     auto rnd = [&]() {
@@ -536,7 +623,6 @@ int hpb_spai_create(hpb_spai** out, int nslot, int dslot, const int* offsets, ui
         w[Params::B1 + i] = 0.01f;
         w[Params::B2 + i] = 0.01f;
     }
-    w[Params::B3 + dslot] = 1.f;
     if (cudaMalloc(&net->w, kNumParams * 4) || cudaMalloc(&net->wb, kNumParams * 2) ||
         cudaMalloc(&net->m1, kNumParams * 4) || cudaMalloc(&net->m2, kNumParams * 4) ||
         cudaMalloc(&net->grad, kNumParams * 4) || cudaMalloc(&net->gtmp, kNumParams * 4) ||
@@ -566,7 +652,8 @@ int hpb_spai_destroy(hpb_spai* net) {
     if (!net) return HPB_SUCCESS;
     cudaDeviceSynchronize();
     void* ptrs[] = {net->w, net->wb, net->m1, net->m2, net->grad, net->gtmp, net->part, net->feat, net->h1, net->h2,
-                    net->out, net->dout, net->diag, net->mval, net->dm, net->G, net->y, net->z, net->g, net->lpart};
+                    net->out, net->dout, net->diag, net->mval, net->dm, net->G, net->y, net->z, net->g, net->lpart,
+                    net->ahat, net->rh};
     for (void* p : ptrs) cudaFree(p);
     if (net->ctx) hpb_destroy(net->ctx);
     delete net;
@@ -602,8 +689,11 @@ int hpb_spai_assemble(hpb_spai* net, const hpb_spai_system* sys, float* m_val) {
 // Loss of one system and its parameter gradient, added to the network's
 // accumulated gradient.  loss[0] = total, [1] = Frobenius part, [2] =
 // residual part.  grad_host (optional) receives this system's gradient.
-int hpb_spai_loss_grad(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_resid, double* loss,
-                       float* grad_host) {
+}  // extern "C"
+
+namespace {
+int loss_impl(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_resid, double* loss, float* grad_host,
+              bool grad) {
     using namespace hpb::spai;
     if (!net || !sys || sys->rows <= 0) return HPB_ERROR_INVALID_VALUE;
     int st = forward_system(net, *sys, true);
@@ -611,44 +701,50 @@ int hpb_spai_loss_grad(hpb_spai* net, const hpb_spai_system* sys, float w_frob, 
     const int32_t n = sys->rows;
     const int gb = (n + 255) / 256;
     cudaMemset(net->dm, 0, size_t(sys->nnz) * 4);
-    // Frobenius term (normalised by n)
-    k_frob_g<<<gb, kThreads>>>(n, sys->row_ptr, sys->col_ind, sys->val, net->mval, net->off, net->G, net->lpart);
+    // Frobenius term ||Ah Mh - I||^2 / n
+    k_frob_g<<<gb, kThreads>>>(n, sys->row_ptr, sys->col_ind, net->ahat, net->mval, net->off, net->G, net->lpart);
     const double lf = host_sum(net->lpart, gb) / n;
-    k_frob_grad<<<gb, 256>>>(n, sys->row_ptr, sys->col_ind, sys->val, net->G, net->off, w_frob / float(n), net->dm);
-    hpb::count_launch(2);
-    // residual-history term (normalised by the number of samples)
+    hpb::count_launch();
+    if (grad) {
+        k_frob_grad<<<gb, 256>>>(n, sys->row_ptr, sys->col_ind, net->ahat, net->G, net->off, w_frob / float(n),
+                                 net->dm);
+        hpb::count_launch();
+    }
+    // residual-history term on rh = D^{-1/2} r (normalised by the number of samples)
     double lr = 0.0;
     for (int sidx = 0; sidx < sys->nres; ++sidx) {
-        const float* r = sys->residuals + size_t(sidx) * n;
-        k_dot_partial<<<gb, 256>>>(n, r, r, net->lpart);
+        k_scale_res<<<gb, 256>>>(n, sys->residuals + size_t(sidx) * n, net->diag, net->rh);
+        k_dot_partial<<<gb, 256>>>(n, net->rh, net->rh, net->lpart);
+        hpb::count_launch(2);
         const double rr = host_sum(net->lpart, gb);
         if (!(rr > 0)) continue;
-        // y = M r ; z = A y - r ; g = A z   (A symmetric)
-        st = hpb_csr_spmv_f32(net->ctx, n, n, sys->nnz, sys->row_ptr, sys->col_ind, net->mval, 1.f, r, 0.f, net->y);
-        if (!st) st = hpb_csr_spmv_f32(net->ctx, n, n, sys->nnz, sys->row_ptr, sys->col_ind, sys->val, 1.f, net->y, 0.f, net->z);
+        // y = Mh rh ; z = Ah y - rh ; g = Ah z   (Ah symmetric)
+        st = hpb_csr_spmv_f32(net->ctx, n, n, sys->nnz, sys->row_ptr, sys->col_ind, net->mval, 1.f, net->rh, 0.f,
+                              net->y);
+        if (!st)
+            st = hpb_csr_spmv_f32(net->ctx, n, n, sys->nnz, sys->row_ptr, sys->col_ind, net->ahat, 1.f, net->y, 0.f,
+                                  net->z);
         if (st) return st;
-        k_sub<<<gb, 256>>>(n, net->z, r);
+        k_sub<<<gb, 256>>>(n, net->z, net->rh);
         k_dot_partial<<<gb, 256>>>(n, net->z, net->z, net->lpart);
         lr += host_sum(net->lpart, gb) / rr / sys->nres;
-        st = hpb_csr_spmv_f32(net->ctx, n, n, sys->nnz, sys->row_ptr, sys->col_ind, sys->val, 1.f, net->z, 0.f, net->g);
+        if (!grad) continue;
+        st = hpb_csr_spmv_f32(net->ctx, n, n, sys->nnz, sys->row_ptr, sys->col_ind, net->ahat, 1.f, net->z, 0.f,
+                              net->g);
         if (st) return st;
-        k_resid_grad<<<gb, 256>>>(n, sys->row_ptr, sys->col_ind, net->g, r, float(w_resid / (rr * sys->nres)), net->dm);
-        hpb::count_launch(4);
+        k_resid_grad<<<gb, 256>>>(n, sys->row_ptr, sys->col_ind, net->g, net->rh, float(w_resid / (rr * sys->nres)),
+                                  net->dm);
+        hpb::count_launch(3);
     }
-    k_dout<<<gb, 256>>>(n, sys->row_ptr, sys->col_ind, net->diag, net->dm, net->off, net->dout);
-    const int ntiles = (n + kTile - 1) / kTile;
-    const int grid = std::min(kGridMlp, ntiles);
-    k_backward<<<grid, kThreads, bwd_smem()>>>(n, net->feat, net->wb, net->h1, net->h2, net->dout, net->part);
-    k_reduce_grad<<<(kNumParams + 255) / 256, 256>>>(grid, net->part, 1.f, net->gtmp);
-    hpb::count_launch(3);
-    // grad += gtmp
-    {
-        std::vector<float> a(kNumParams), b(kNumParams);
-        cudaMemcpy(a.data(), net->gtmp, kNumParams * 4, cudaMemcpyDeviceToHost);
-        cudaMemcpy(b.data(), net->grad, kNumParams * 4, cudaMemcpyDeviceToHost);
-        for (int i = 0; i < kNumParams; ++i) b[i] += a[i];
-        cudaMemcpy(net->grad, b.data(), kNumParams * 4, cudaMemcpyHostToDevice);
-        if (grad_host) std::memcpy(grad_host, a.data(), kNumParams * 4);
+    if (grad) {
+        k_dout<<<gb, 256>>>(n, sys->row_ptr, sys->col_ind, net->out, net->dm, net->off, net->dout);
+        const int ntiles = (n + kTile - 1) / kTile;
+        const int grid = std::min(kGridMlp, ntiles);
+        k_backward<<<grid, kThreads, bwd_smem()>>>(n, net->feat, net->wb, net->h1, net->h2, net->dout, net->part);
+        k_reduce_grad<<<(kNumParams + 255) / 256, 256>>>(grid, net->part, net->gtmp, net->grad);
+        hpb::count_launch(3);
+        if (grad_host && cudaMemcpy(grad_host, net->gtmp, kNumParams * 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return HPB_ERROR_CUDA;
     }
     if (loss) {
         loss[0] = w_frob * lf + w_resid * lr;
@@ -658,21 +754,27 @@ int hpb_spai_loss_grad(hpb_spai* net, const hpb_spai_system* sys, float w_frob, 
     return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
 }
 
+}  // namespace
+
+extern "C" {
+
+int hpb_spai_loss_grad(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_resid, double* loss,
+                       float* grad_host) {
+    return loss_impl(net, sys, w_frob, w_resid, loss, grad_host, true);
+}
+
+int hpb_spai_loss(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_resid, double* loss) {
+    return loss_impl(net, sys, w_frob, w_resid, loss, nullptr, false);
+}
+
 // One Adam step with the accumulated gradient scaled by `scale`; clears it.
 int hpb_spai_adam(hpb_spai* net, float lr, float scale) {
     using namespace hpb::spai;
     if (!net) return HPB_ERROR_INVALID_VALUE;
-    if (scale != 1.f) {
-        std::vector<float> g(kNumParams);
-        cudaMemcpy(g.data(), net->grad, kNumParams * 4, cudaMemcpyDeviceToHost);
-        for (float& v : g) v *= scale;
-        cudaMemcpy(net->grad, g.data(), kNumParams * 4, cudaMemcpyHostToDevice);
-    }
     ++net->step;
-    k_adam<<<(kNumParams + 255) / 256, 256>>>(net->step, lr, 0.9f, 0.999f, 1e-8f, net->w, net->m1, net->m2, net->grad,
-                                              net->wb);
+    k_adam<<<(kNumParams + 255) / 256, 256>>>(net->step, lr, scale, 0.9f, 0.999f, 1e-8f, net->w, net->m1, net->m2,
+                                              net->grad, net->wb);
     hpb::count_launch();
-    cudaMemset(net->grad, 0, kNumParams * 4);
     return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
 }
 

@@ -27,7 +27,7 @@ I64 = C.c_int64
 hpb_spai_system = _lib.hpb_spai_system
 
 NUM_PARAMS = L.hpb_spai_num_params()
-# weights trained on the GPU by `python -m high_precision_blas1_b200.spai train`
+# weights trained on the GPU by `python -m high_precision_blas1_b200.spai train --systems 2000 --grid 24`
 WEIGHTS_FILE = Path(__file__).resolve().parent / "data" / "spai_lognormal3d_w64.npy"
 
 
@@ -122,6 +122,12 @@ class SpaiNet:
                                    g.ctypes.data if want_grad else None), "loss_grad")
         return loss, g
 
+    def loss(self, D: DeviceCSR, w_frob=1.0, w_resid=1.0):
+        out = np.zeros(3)
+        sysd = D.system()
+        check(L.hpb_spai_loss(self.h, C.byref(sysd), w_frob, w_resid, out.ctypes.data), "loss")
+        return out
+
     def adam(self, lr, scale=1.0):
         check(L.hpb_spai_adam(self.h, lr, scale), "adam")
 
@@ -138,24 +144,31 @@ def family(N: int, seed: int) -> problems.CSR:
     return problems.diffusion3d_lognormal(N, seed=seed, sigma=2.3, corr=8.0)
 
 
-def train(torch, n_systems=2000, N=24, epochs=2, batch=8, lr=3e-3, w_frob=1.0, w_resid=1.0, seed=1000,
+def train(torch, n_systems=2000, N=24, epochs=3, batch=8, lr=3e-3, w_frob=1.0, w_resid=1.0, seed=1000, n_val=32,
           log=print):
-    """Train on n_systems seeded systems of the family (seeds seed..seed+n-1,
-    disjoint from the evaluation seeds); returns (weights, history)."""
+    """Train on n_systems seeded systems of the family (seeds seed..seed+n-1);
+    n_val further seeds are held out and the weights of the epoch with the
+    lowest held-out loss are returned.  Returns (weights, history), history
+    = mean training loss per epoch."""
     from . import Context
     offs, dslot = stencil7(N)
     net = SpaiNet(offs, dslot, seed=7)
     hist = []
     with Context(0, torch.cuda.current_stream().cuda_stream) as ctx:
-        data = []
         t0 = time.time()
-        for s in range(n_systems):
+        data, val = [], []
+        for s in range(n_systems + n_val):
             D = DeviceCSR(torch, family(N, seed + s))
             jacobi_residuals(torch, ctx, D, seed=seed + s)
-            data.append(D)
-        log(f"generated {n_systems} systems of {N}^3 in {time.time() - t0:.1f}s")
+            (data if s < n_systems else val).append(D)
+        log(f"generated {n_systems} + {n_val} systems of {N}^3 in {time.time() - t0:.1f}s")
+
+        def val_loss():
+            return float(np.mean([net.loss(D, w_frob, w_resid)[0] for D in val])) if val else 0.0
+
+        best, best_w = val_loss(), net.weights()
+        log(f"untrained (Jacobi): held-out loss {best:.5f}")
         rng = np.random.default_rng(seed)
-        step = 0
         for ep in range(epochs):
             order = rng.permutation(n_systems)
             tot = 0.0
@@ -165,12 +178,14 @@ def train(torch, n_systems=2000, N=24, epochs=2, batch=8, lr=3e-3, w_frob=1.0, w
                     loss, _ = net.loss_grad(data[i], w_frob, w_resid)
                     tot += loss[0]
                 net.adam(lr, 1.0 / len(idx))
-                step += 1
             hist.append(tot / n_systems)
-            log(f"epoch {ep}: mean loss {tot / n_systems:.5f}")
-    w = net.weights()
+            vl = val_loss()
+            if vl < best or not val:
+                best, best_w = vl, net.weights()
+            log(f"epoch {ep}: mean training loss {tot / n_systems:.5f}, held-out {vl:.5f} "
+                f"({time.time() - t0:.1f}s)")
     net.close()
-    return w, hist
+    return best_w, hist
 
 
 def main(argv=None):
@@ -179,11 +194,12 @@ def main(argv=None):
     t = sub.add_parser("train")
     t.add_argument("--systems", type=int, default=2000)
     t.add_argument("--grid", type=int, default=24)
-    t.add_argument("--epochs", type=int, default=2)
+    t.add_argument("--epochs", type=int, default=3)
+    t.add_argument("--lr", type=float, default=3e-3)
     t.add_argument("--out", type=str, required=True)
     a = ap.parse_args(argv)
     import torch
-    w, hist = train(torch, n_systems=a.systems, N=a.grid, epochs=a.epochs)
+    w, hist = train(torch, n_systems=a.systems, N=a.grid, epochs=a.epochs, lr=a.lr)
     np.save(Path(a.out), w)
     print("saved", a.out, "loss history", hist)
 

@@ -420,11 +420,14 @@ int hpb_ir_solve_c128(const hpb_ir_params* p, int32_t rows, int64_t nnz, const i
 /* ---------------------------------------------------------------------- */
 /* Learned sparse approximate inverse (no counterpart in the reference).   */
 /* A per-row MLP (16 -> 64 -> 64 -> 8, ReLU, bf16 weights, binary32        */
-/* accumulation) maps local features of row i of A to row i of M on A's    */
-/* pattern; M is a right preconditioner (HPB_PRECOND_MATRIX).  Trained by  */
-/* the library's own forward/backward kernels on                            */
-/*   w_F ||A M - I||_F^2 / n + w_R mean_s ||A M r_s - r_s||^2 / ||r_s||^2,  */
-/* r_s residual vectors of a plain solver.  Matrices must be symmetric.     */
+/* accumulation) maps local features of row i of Ah = D^-1/2 A D^-1/2 to   */
+/* row i of a symmetric, diagonally dominant (so positive definite) Mh on  */
+/* A's pattern; M = D^-1/2 Mh D^-1/2 is a right preconditioner             */
+/* (HPB_PRECOND_MATRIX).  Trained by the library's own forward/backward    */
+/* kernels on                                                               */
+/*   w_F ||Ah Mh - I||_F^2 / n + w_R mean_s ||Ah Mh rh_s - rh_s||^2/||rh_s||^2, */
+/* rh_s = D^-1/2 r_s, r_s residual vectors of a plain solver on A.  A must */
+/* be symmetric with a positive diagonal.                                   */
 /* ---------------------------------------------------------------------- */
 typedef struct hpb_spai hpb_spai;
 typedef struct hpb_spai_system {
@@ -450,6 +453,8 @@ int hpb_spai_assemble(hpb_spai* net, const hpb_spai_system* sys, float* m_val);
  * network's accumulator; grad_host (optional, host, num_params) gets it. */
 int hpb_spai_loss_grad(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_resid, double* loss,
                        float* grad_host);
+/* loss[3] only (no gradient), e.g. on held-out systems. */
+int hpb_spai_loss(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_resid, double* loss);
 /* Adam step on scale * accumulated gradient, then clears the accumulator. */
 int hpb_spai_adam(hpb_spai* net, float lr, float scale);
 
