@@ -56,7 +56,7 @@ class ClockSampler:
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,clocks.mem,clocks.max.mem")
 
     def __init__(self, device_index: int):
         self.dev = device_index
@@ -94,7 +94,10 @@ class ClockSampler:
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        mem = [float(r[9]) for r in rows if len(r) > 10 and r[9].replace(".", "").isdigit()]
+        mmx = [float(r[10]) for r in rows if len(r) > 10 and r[10].replace(".", "").isdigit()]
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "mem_mhz": statistics.median(mem) if mem else None, "mem_max_mhz": max(mmx) if mmx else None,
                 "reasons": reasons, "samples": len(rows)}
 
 
@@ -321,37 +324,78 @@ def bench_dot2(args, ws, rank, local, torch, dist):
     }
 
 
+# DRAM bytes of one hpb_csr_spmv_dot2_f64 launch on the 1024^2 operator
+# (dram__bytes_read.sum + dram__bytes_write.sum), from the ncu capture in
+# profiles/spmv_dot2_f64_convdiff1024.md; None until captured.
+SPMV_DOT2_TRAFFIC = None
+
+
 def spmv_roofline(torch, L, ctx, A, reps=40):
-    """Live per-launch time of the CSR SpMV on the solver's matrix, two
-    matrix copies rotated (2 x 84 MB > L2)."""
+    """Live per-launch times, two matrix copies rotated (2 x 84 MB > L2), of
+    the fused solver's dominant operation -- y = A x with the Dot2 <w, y>
+    (hpb_csr_spmv_dot2_f64, the same row kernel and combine as the solver's
+    k_spmv_dot) -- and of the plain SpMV."""
     mats = []
     for _ in range(2):
         mats.append([torch.from_numpy(a).cuda() for a in (A.row_ptr, A.col_ind, A.val)])
     xs = [torch.rand(A.n, dtype=torch.float64, device="cuda") for _ in range(2)]
     ys = [torch.empty(A.n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    ws_ = [torch.rand(A.n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    out = torch.zeros(4, dtype=torch.float64, device="cuda")
     stream = torch.cuda.current_stream()
 
-    def launch(i):
+    def fused(i):
+        rp, ci, va = mats[i % 2]
+        ctx.check(L.hpb_csr_spmv_dot2_f64(ctx.h, A.n, A.n, A.nnz, rp.data_ptr(), ci.data_ptr(), va.data_ptr(),
+                                          xs[i % 2].data_ptr(), ys[i % 2].data_ptr(), ws_[i % 2].data_ptr(),
+                                          out.data_ptr()))
+
+    def plain(i):
         rp, ci, va = mats[i % 2]
         ctx.check(L.hpb_csr_spmv_f64(ctx.h, A.n, A.n, A.nnz, rp.data_ptr(), ci.data_ptr(), va.data_ptr(), 1.0,
                                      xs[i % 2].data_ptr(), 0.0, ys[i % 2].data_ptr()))
-    for i in range(4):
-        launch(i)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for i in range(reps):
-        launch(i)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    us = e0.elapsed_time(e1) * 1e3 / reps
-    alg = 12.0 * A.nnz + 4.0 * (A.n + 1) + 8.0 * A.n + 8.0 * A.n
+
+    def timed(launch):
+        for i in range(4):
+            launch(i)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(reps):
+            launch(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) * 1e3 / reps
+
+    us_f, us_p = timed(fused), timed(plain)
+    mat = 12.0 * A.nnz + 4.0 * (A.n + 1)
+    alg_f = mat + 3 * 8.0 * A.n  # read x, write y, read w
+    alg_p = mat + 2 * 8.0 * A.n
     hbm, src = peaks()
-    ach = alg / (us * 1e-6) / 1e9
-    return {"kernel": "csr_stream_kernel<double>", "bound": "hbm", "achieved": ach, "peak": hbm, "peak_source": src,
-            "unit": "GB/s", "frac": ach / hbm, "traffic": None, "algorithmic_bytes_per_launch": alg,
-            "avg_launch_us": us}
+    ach = alg_f / (us_f * 1e-6) / 1e9
+    ach_p = alg_p / (us_p * 1e-6) / 1e9
+    return {"kernel": "csr_row_dot_kernel<double> (hpb_csr_spmv_dot2_f64: y = A x and Dot2 <w, y>)", "bound": "hbm",
+            "achieved": ach, "peak": hbm, "peak_source": src, "unit": "GB/s", "frac": ach / hbm,
+            "traffic": SPMV_DOT2_TRAFFIC, "algorithmic_bytes_per_launch": alg_f, "avg_launch_us": us_f,
+            "plain_spmv": {"kernel": "csr_row_kernel<double>", "achieved": ach_p, "frac": ach_p / hbm,
+                           "algorithmic_bytes_per_launch": alg_p, "avg_launch_us": us_p}}
+
+
+def bicgstabl_cycle_bytes(n, nnz, L, elem=8):
+    """Algorithmic HBM bytes of one fused BiCGStab(L) cycle: 2L SpMVs (2L-1
+    with the Dot2 against rt), the u/r/x updates, the MGS passes and the
+    closing update, each vector read or written once per kernel."""
+    mat = (elem + 4.0) * nnz + 4.0 * (n + 1)
+    spmv = mat + 2.0 * elem * n
+    vec = elem * float(n)
+    passes = sum(3 * (j + 1) for j in range(L))            # u_i = r_i - beta u_i
+    passes += sum(3 * (j + 1) + 3 for j in range(L))       # r_i -= alpha u_{i+1}, x += alpha u_0
+    for j in range(1, L + 1):                              # MGS passes (k, j)
+        for k in range(1, j + 1):
+            passes += 2 if k == 1 else 4
+    passes += (2 + 2 * L + 2) + 3                          # closing update: reads, then x, r_0, u_0 written
+    return (2 * L) * spmv + (2 * L - 1) * vec + passes * vec
 
 
 def bench_solver(args, ws, rank, local, torch, dist):
@@ -435,6 +479,7 @@ def bench_solver(args, ws, rank, local, torch, dist):
                    "iters": iters, "true_rel_residual": rel, "cycles": [i // SOLVER_L for i in iters],
                    "plain_dropin": plain},
         "roofline": roof,
+        "solver_roofline": solver_roofline(A, iters, t_step, args.plain),
         "e2e": {"value": float(np.mean(e2e)), "unit": "s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(hx.nbytes)},
         "gpu_launches": int(launches // max(1, args.steps)),
@@ -442,6 +487,19 @@ def bench_solver(args, ws, rank, local, torch, dist):
         "clocks": clocks,
         "dot2": dot2,
     }
+
+
+def solver_roofline(A, iters, t_step, plain):
+    """Whole-solve HBM roofline of the fused BiCGStab(L): algorithmic bytes
+    per cycle x cycles / solve time (the plain path moves more: its
+    reductions and updates are separate kernels)."""
+    cycles = iters[-1] // SOLVER_L
+    per_cycle = bicgstabl_cycle_bytes(A.n, A.nnz, SOLVER_L)
+    hbm, src = peaks()
+    ach = per_cycle * cycles / t_step / 1e9
+    return {"bytes_per_cycle": per_cycle, "cycles": cycles, "achieved": ach, "peak": hbm, "peak_source": src,
+            "unit": "GB/s", "frac": ach / hbm, "bound_s": per_cycle * cycles / (hbm * 1e9),
+            "note": "fused-path byte model" + (" (timed path is the plain one)" if plain else "")}
 
 
 # ------------------------------------------------ precision / complex / learned forms
@@ -469,13 +527,14 @@ def fused_solve(torch, A, b, method, basis, tol, precond="none", complex_=False,
     return t, st, rep, x
 
 
-def ir_solve(torch, A, b, inner, basis, precond="none", M=None, complex_=False, inner_tol=1e-5, max_iters=5000):
+def ir_solve(torch, A, b, inner, basis, precond="none", M=None, complex_=False, inner_tol=1e-5, max_iters=5000,
+             max_refinements=40):
     from high_precision_blas1_b200 import _lib
     dt = np.complex128 if complex_ else np.float64
     d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (A.row_ptr, A.col_ind, A.val.astype(dt),
                                                                     b.astype(dt), np.zeros(A.n, dtype=dt))]
     p = _lib.ir_params(inner, basis=basis, inner_rel_tol=inner_tol, inner_max_iters=max_iters, precond=precond,
-                       rel_tol=SOLVER_TOL, max_refinements=40)
+                       rel_tol=SOLVER_TOL, max_refinements=max_refinements)
     rep = _lib.hpb_ir_report()
     mp = [None, None, None, 0] if M is None else [d[0].data_ptr(), d[1].data_ptr(), M.data_ptr(), A.nnz]
     f = _lib.lib.hpb_ir_solve_c128 if complex_ else _lib.lib.hpb_ir_solve_f64
@@ -534,10 +593,14 @@ def bench_forms(torch, log=lambda *a: None):
         A = spai.family(96, seed=424242)  # outside the training seeds
         b = problems.rhs_uniform(A.n, 505)
         res = {"n": A.n, "nnz": A.nnz}
+        # iteration budget of every run: 30000 GMRES(30) iterations
         t64, st64, r64, x64 = fused_solve(torch, A, b, "gmres", 30, SOLVER_TOL, max_iters=30000)
         res["plain_fp64_gmres30"] = {"s": t64, "status": st64, "iters": r64.iters, "true_rel_residual": _rel(A, b, x64)}
+        tj64, stj64, rj64, xj64 = fused_solve(torch, A, b, "gmres", 30, SOLVER_TOL, precond="jacobi", max_iters=30000)
+        res["fp64_gmres30_jacobi"] = {"s": tj64, "status": stj64, "iters": rj64.iters,
+                                      "true_rel_residual": _rel(A, b, xj64)}
         for pc in ("none", "jacobi"):
-            t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond=pc, max_iters=30000)
+            t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond=pc, max_iters=15000, max_refinements=10)
             res[f"fp32_dot2_gmres30_refined_{pc}"] = {"s": t, "status": st, "inner_iters": r.inner_iters,
                                                       "refinements": r.refinements, "true_rel_residual": _rel(A, b, x)}
         wfile = spai.WEIGHTS_FILE
@@ -546,13 +609,16 @@ def bench_forms(torch, log=lambda *a: None):
             net = spai.SpaiNet(offs, dslot)
             net.set_weights(np.load(wfile))
             tb, M = _timed(torch, lambda: net.assemble(torch, spai.DeviceCSR(torch, A)))
-            t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond="matrix", M=M, max_iters=30000)
+            t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond="matrix", M=M, max_iters=15000,
+                                   max_refinements=10)
             res["fp32_dot2_gmres30_refined_learned_spai"] = {
                 "s": t, "build_s": tb, "status": st, "inner_iters": r.inner_iters, "refinements": r.refinements,
                 "true_rel_residual": _rel(A, b, x)}
             net.close()
             if st == 0:
+                # plain FP64 without a preconditioner may not converge within the budget: then no ratio
                 res["speedup_learned_vs_plain_fp64"] = t64 / (t + tb) if st64 == 0 else None
+                res["speedup_learned_vs_fp64_jacobi"] = tj64 / (t + tb) if stj64 == 0 else None
         out["learned_pc_gmres30_lognormal96"] = res
     except Exception as e:
         out["learned_pc_gmres30_lognormal96"] = {"error": repr(e)}

@@ -122,6 +122,7 @@ for t in TYPES:
     _sig(f"hpb_abs_{t}", C.c_int, [P, I64, P, P])
     _sig(f"hpb_isfinite_{t}", C.c_int, [P, I64, P, C.POINTER(C.c_int)])
     _sig(f"hpb_csr_spmv_{t}", C.c_int, [P, I32, I32, I64, P, P, P, S, P, S, P])
+    _sig(f"hpb_csr_spmv_dot2_{t}", C.c_int, [P, I32, I32, I64, P, P, P, P, P, P, P])
     _sig(f"hpb_csr_diag_{t}", C.c_int, [P, I32, P, P, P, P])
     _sig(f"hpb_random_{t}", C.c_int, [P, I64, C.c_uint64, S, S, P])
 _sig("hpb_gendot_f64", C.c_int, [C.c_uint64, I64, C.c_double, P, P, C.POINTER(C.c_int64)])

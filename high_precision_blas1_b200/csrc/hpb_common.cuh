@@ -70,6 +70,30 @@ __device__ __forceinline__ cd ldE<cd>(const cd* p, int64_t i) {
     const double* q = reinterpret_cast<const double*>(p) + 2 * i;
     return cd{q[0], q[1]};
 }
+// Streaming load (evict-first: matrix values and indices, read once per
+// product) and read-only cached load (the gathered vector x).
+__device__ __forceinline__ float ldcsE(const float* p, int64_t i) { return __ldcs(p + i); }
+__device__ __forceinline__ double ldcsE(const double* p, int64_t i) { return __ldcs(p + i); }
+__device__ __forceinline__ cf ldcsE(const cf* p, int64_t i) {  // components: cf may be 4-byte aligned
+    const float* q = reinterpret_cast<const float*>(p) + 2 * i;
+    return cf{__ldcs(q), __ldcs(q + 1)};
+}
+__device__ __forceinline__ cd ldcsE(const cd* p, int64_t i) {
+    const double* q = reinterpret_cast<const double*>(p) + 2 * i;
+    return cd{__ldcs(q), __ldcs(q + 1)};
+}
+__device__ __forceinline__ int32_t ldcsI(const int32_t* p, int64_t i) { return __ldcs(p + i); }
+__device__ __forceinline__ float ldgE(const float* p, int64_t i) { return __ldg(p + i); }
+__device__ __forceinline__ double ldgE(const double* p, int64_t i) { return __ldg(p + i); }
+__device__ __forceinline__ cf ldgE(const cf* p, int64_t i) {
+    const float* q = reinterpret_cast<const float*>(p) + 2 * i;
+    return cf{__ldg(q), __ldg(q + 1)};
+}
+__device__ __forceinline__ cd ldgE(const cd* p, int64_t i) {
+    const double* q = reinterpret_cast<const double*>(p) + 2 * i;
+    return cd{__ldg(q), __ldg(q + 1)};
+}
+
 template <class E>
 __device__ __forceinline__ void stE(E* p, int64_t i, E v) { p[i] = v; }
 template <>

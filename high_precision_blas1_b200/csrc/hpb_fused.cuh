@@ -176,12 +176,12 @@ __device__ __forceinline__ void block_merge(A (&acc)[ND], A* sh /* [ND][32] */) 
 }
 
 // Cross-block finish: block partials -> ticket -> the last block merges all
-// partials in block order and runs `epi(values, bad)` on thread 0, where
-// values[d] = hi of dot d and bad = any block reported a non-finite entry.
-// Returns true in the last block's thread 0 only (after epi).
+// partials in block order and runs `epi(tot, bad)` on thread 0, where tot[d]
+// is the merged (s, c) accumulator of dot d and bad = any block reported a
+// non-finite entry.
 template <int ND, class A, class Epi>
-__device__ __forceinline__ void grid_finish(A (&acc)[ND], bool bad, A* partials, unsigned int* ticket, int* badflag,
-                                            Epi epi) {
+__device__ __forceinline__ void grid_finish_acc(A (&acc)[ND], bool bad, A* partials, unsigned int* ticket,
+                                                int* badflag, Epi epi) {
     __shared__ A sh[ND * 32 > 0 ? ND * 32 : 1];
     __shared__ bool am_last;
     if (ND > 0) block_merge<ND>(acc, sh);
@@ -205,13 +205,22 @@ __device__ __forceinline__ void grid_finish(A (&acc)[ND], bool bad, A* partials,
     __syncthreads();
     if (ND > 0) block_merge<ND>(tot, sh);
     if (threadIdx.x == 0) {
+        epi(static_cast<const A*>(tot), atomicExch(badflag, 0) != 0);
+        *ticket = 0;
+    }
+}
+
+// As grid_finish_acc, with epi(values, bad), values[d] = s + c of dot d.
+template <int ND, class A, class Epi>
+__device__ __forceinline__ void grid_finish(A (&acc)[ND], bool bad, A* partials, unsigned int* ticket, int* badflag,
+                                            Epi epi) {
+    grid_finish_acc<ND>(acc, bad, partials, ticket, badflag, [&](const A* tot, bool b) {
         using V = decltype(acc_value(tot[0]));
         V vals[ND > 0 ? ND : 1];
 #pragma unroll
         for (int d = 0; d < ND; ++d) vals[d] = acc_value(tot[d]);
-        epi(vals, atomicExch(badflag, 0) != 0);
-        *ticket = 0;
-    }
+        epi(static_cast<const V*>(vals), b);
+    });
 }
 
 // Right preconditioner of the fused GMRES: none, Jacobi (diagonal of A) or

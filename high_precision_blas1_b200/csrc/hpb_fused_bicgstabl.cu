@@ -125,30 +125,13 @@ k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
            EpiArgs<typename scalar_of<E>::type> ea) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
-    constexpr int kCap = 2048;
-    __shared__ E sv[kCap];
-    __shared__ int32_t sc[kCap];
-    const int32_t r0 = blockIdx.x * kThreads;
-    const int32_t r = r0 + threadIdx.x;
-    const int32_t rend = min(r0 + kThreads, rows);
-    const int32_t p0 = rp[r0];
-    const int32_t cnt = rp[rend] - p0;
-    int32_t b = 0, e = 0;
-    if (r < rows) {
-        b = rp[r];
-        e = rp[r + 1];
-    }
+    // one thread per row: streaming loads of the row's values and indices,
+    // x through the read-only path (the library SpMV's layout)
+    const int32_t r = blockIdx.x * kThreads + threadIdx.x;
     S acc = s_zero(S{});
-    if (cnt <= kCap) {
-#pragma unroll 4
-        for (int32_t k = threadIdx.x; k < cnt; k += kThreads) {
-            sv[k] = ldE(val, int64_t(p0) + k);
-            sc[k] = ci[p0 + k];
-        }
-        __syncthreads();
-        for (int32_t k = b - p0; k < e - p0; ++k) acc = s_fma(to_s(sv[k]), to_s(ldE(x, sc[k])), acc);
-    } else {
-        for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ldE(val, k)), to_s(ldE(x, ci[k])), acc);
+    if (r < rows) {
+        const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
+        for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ldcsE(val, k)), to_s(ldgE(x, ldcsI(ci, k))), acc);
     }
     A dacc[1];
     if (r < rows) {

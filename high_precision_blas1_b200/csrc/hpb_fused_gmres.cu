@@ -262,29 +262,12 @@ __global__ void __launch_bounds__(kGmThreads)
 k_gm_spmv(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const E* __restrict__ val,
           const E* __restrict__ x, E* __restrict__ y) {
     using S = typename scalar_of<E>::type;
-    constexpr int kCap = 2048;
-    __shared__ E sv[kCap];
-    __shared__ int32_t sidx[kCap];
-    const int32_t r0 = blockIdx.x * kGmThreads;
-    const int32_t r = r0 + threadIdx.x;
-    const int32_t rend = min(r0 + kGmThreads, rows);
-    const int32_t p0 = rp[r0];
-    const int32_t cnt = rp[rend] - p0;
-    int32_t b = 0, e = 0;
-    if (r < rows) {
-        b = rp[r];
-        e = rp[r + 1];
-    }
+    // one thread per row (the library SpMV's layout)
+    const int32_t r = blockIdx.x * kGmThreads + threadIdx.x;
     S acc = s_zero(S{});
-    if (cnt <= kCap) {
-        for (int32_t k = threadIdx.x; k < cnt; k += kGmThreads) {
-            sv[k] = ldE(val, int64_t(p0) + k);
-            sidx[k] = ci[p0 + k];
-        }
-        __syncthreads();
-        for (int32_t k = b - p0; k < e - p0; ++k) acc = s_fma(to_s(sv[k]), to_s(ldE(x, sidx[k])), acc);
-    } else {
-        for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ldE(val, k)), to_s(ldE(x, ci[k])), acc);
+    if (r < rows) {
+        const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
+        for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ldcsE(val, k)), to_s(ldgE(x, ldcsI(ci, k))), acc);
     }
     if (r < rows) stE(y, r, from_s<E>(acc));
 }
@@ -307,9 +290,10 @@ k_resid_comp(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __rest
         A ra;  // b_r - sum_k a_rk x_k as a Dot2 accumulation
         S bv = to_s(ldE(b, row));
         ra.s = bv;
-        for (int32_t k = rp[row]; k < rp[row + 1]; ++k) {
-            S a = to_s(ldE(val, k));
-            E xe = ldE(x, ci[k]);
+        const int32_t kb = __ldg(rp + row), ke = __ldg(rp + row + 1);
+        for (int32_t k = kb; k < ke; ++k) {
+            S a = to_s(ldcsE(val, k));
+            E xe = ldgE(x, ldcsI(ci, k));
             bad |= !finite_e(xe);
             dot_add(ra, s_neg(conj_s(a)), to_s(xe));  // conj(-conj(a)) * x = -a x
         }

@@ -32,10 +32,11 @@ __global__ void k_ir_resid(int32_t rows, const int32_t* __restrict__ rp, const i
     if (row < rows) {
         A ra;
         ra.s = to_s(ldE(b, row));
-        for (int32_t k = rp[row]; k < rp[row + 1]; ++k) {
-            E xe = ldE(x, ci[k]);
+        const int32_t kb = __ldg(rp + row), ke = __ldg(rp + row + 1);
+        for (int32_t k = kb; k < ke; ++k) {
+            E xe = ldgE(x, ldcsI(ci, k));
             bad |= !finite_e(xe);
-            dot_add(ra, s_neg(conj_s(to_s(ldE(val, k)))), to_s(xe));
+            dot_add(ra, s_neg(conj_s(to_s(ldcsE(val, k)))), to_s(xe));
         }
         S rv = acc_value(ra);
         stE(r, row, from_s<E>(rv));

@@ -283,6 +283,27 @@ int hpb_csr_spmv_c128(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
                       const int32_t* row_ptr, const int32_t* col_ind, const void* val,
                       hpb_c128 alpha, const void* x, hpb_c128 beta, void* y);
 
+/* Fused CSR product and compensated dot, one pass over A:
+ *   y = A x   (bit-identical to hpb_csr_spmv_* with alpha = 1, beta = 0)
+ *   out = Dot2 of <w, y> = sum conj(w_i) y_i, written like hpb_dot2_*
+ *         (device; real: hi, lo; complex: hi.re, hi.im, lo.re, lo.im).
+ * Replaces the pair csr::gpu_matrix::axpy + gpu_vector_operations::
+ * scalar_prod that the reference's solvers issue back to back
+ * (common/csr/gpu_matrix.h:322-375, common/gpu_vector_operations.h:257-269;
+ * e.g. numerical_algos/lin_solvers/bicgstabl.h:213-216). */
+int hpb_csr_spmv_dot2_f32(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
+                          const int32_t* row_ptr, const int32_t* col_ind, const float* val,
+                          const float* x, float* y, const float* w, double* out);
+int hpb_csr_spmv_dot2_f64(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
+                          const int32_t* row_ptr, const int32_t* col_ind, const double* val,
+                          const double* x, double* y, const double* w, double* out);
+int hpb_csr_spmv_dot2_c64(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
+                          const int32_t* row_ptr, const int32_t* col_ind, const void* val,
+                          const void* x, void* y, const void* w, double* out);
+int hpb_csr_spmv_dot2_c128(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz,
+                           const int32_t* row_ptr, const int32_t* col_ind, const void* val,
+                           const void* x, void* y, const void* w, double* out);
+
 /* diag[r] := A(r, r) (0 if row r stores no diagonal entry); used by the
  * Jacobi preconditioner (the diagonal scaling of linear_operator.hpp:59-91). */
 int hpb_csr_diag_f32(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,

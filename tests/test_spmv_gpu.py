@@ -113,3 +113,59 @@ def test_csr_diagonal(gpu):
     want = np.array([A.val[A.row_ptr[r]:A.row_ptr[r + 1]][A.col_ind[A.row_ptr[r]:A.row_ptr[r + 1]] == r][0]
                      for r in range(A.n)])
     assert np.array_equal(host(d), want)
+
+
+def spmv_dot2(ctx, torch, t, A, x, w):
+    d = [dev(torch, a) for a in (A.row_ptr, A.col_ind, A.val.astype(DT[t]), x.astype(DT[t]), np.zeros(A.n, DT[t]),
+                                 w.astype(DT[t]))]
+    out = torch.full((4,), np.nan, dtype=torch.float64, device="cuda")
+    st = getattr(_lib.lib, f"hpb_csr_spmv_dot2_{t}")(ctx.h, A.n, x.shape[0], A.nnz, d[0].data_ptr(),
+                                                    d[1].data_ptr(), d[2].data_ptr(), d[3].data_ptr(),
+                                                    d[4].data_ptr(), d[5].data_ptr(), out.data_ptr())
+    ctx.check(st, "spmv_dot2")
+    torch.cuda.synchronize()
+    return host(d[4]), host(out)
+
+
+@pytest.mark.parametrize("t", ["f32", "f64", "c64", "c128"])
+def test_spmv_dot2_fused(gpu, t):
+    """y bit-identical to hpb_csr_spmv (alpha 1, beta 0); <w, y> within the
+    compensated Dot2 bound of the exact dot of the rounded y (oracle)."""
+    import oracle
+    ctx, torch = gpu
+    rng = np.random.default_rng(5)
+    for A in (problems.convdiff2d(300), random_csr(rng, 3001, 2900, 0.003, long_rows=(7,), empty_rows=(0, 11)),
+              problems.convdiff2d(1024)):
+        x = rng.standard_normal(2900 if A.n == 3001 else A.n)
+        w = rng.standard_normal(A.n)
+        if t in ("c64", "c128"):
+            x = x + 1j * rng.standard_normal(x.shape[0])
+            w = w + 1j * rng.standard_normal(A.n)
+        y, out = spmv_dot2(ctx, torch, t, A, x, w)
+        y_ref = spmv(ctx, torch, t, A, 1.0, x, 0.0, np.zeros(A.n))
+        assert np.array_equal(y.view(np.uint8), y_ref.view(np.uint8))
+        wd, yd = w.astype(DT[t]).astype(WIDE[t]), y.astype(WIDE[t])
+        if t in ("f32", "f64"):
+            hi, _ = oracle.exact_dot(wd, yd)
+            scale = float(np.sum(np.abs(wd * yd)))
+            assert abs(out[0] - hi) <= oracle.bound_dot2(A.n, scale / abs(hi)) * abs(hi) + 2 * np.spacing(abs(hi))
+        else:
+            hc, _ = oracle.exact_dot(wd, yd)
+            hr, hi_ = hc.real, hc.imag
+            scale = float(np.sum(np.abs(wd) * np.abs(yd)))
+            b = oracle.bound_dot2(A.n, 1.0, complex_=True) * scale
+            assert abs(out[0] - hr) <= b + 2 * np.spacing(abs(hr)) and abs(out[1] - hi_) <= b + 2 * np.spacing(abs(hi_))
+
+
+def test_spmv_dot2_bad_args(gpu):
+    ctx, torch = gpu
+    A = problems.convdiff2d(8)
+    d = [dev(torch, a) for a in (A.row_ptr, A.col_ind, A.val, np.ones(A.n), np.zeros(A.n), np.ones(A.n))]
+    out = torch.zeros(2, dtype=torch.float64, device="cuda")
+    f = _lib.lib.hpb_csr_spmv_dot2_f64
+    p = [a.data_ptr() for a in d]
+    assert f(ctx.h, A.n, A.n, A.nnz, p[0], p[1], p[2], p[3], p[4], p[5], None) == -1
+    assert f(ctx.h, -1, A.n, A.nnz, p[0], p[1], p[2], p[3], p[4], p[5], out.data_ptr()) == -1
+    assert f(ctx.h, A.n, A.n, A.nnz, p[0], p[1], p[2] + 4, p[3], p[4], p[5], out.data_ptr()) == -1
+    # zero rows: out is the empty sum
+    assert f(ctx.h, 0, 0, 0, p[0], None, None, None, None, None, out.data_ptr()) == 0
