@@ -384,16 +384,16 @@ def spmv_roofline(torch, L, ctx, A, reps=40):
 
 def bicgstabl_cycle_bytes(n, nnz, L, elem=8):
     """Algorithmic HBM bytes of one fused BiCGStab(L) cycle: 2L SpMVs (2L-1
-    with the Dot2 against rt), the u/r/x updates, the MGS passes and the
-    closing update, each vector read or written once per kernel."""
+    with the Dot2 against rt), the u/r/x updates, the L modified Gram-Schmidt
+    sweeps and the closing update, each vector read or written once per
+    kernel."""
     mat = (elem + 4.0) * nnz + 4.0 * (n + 1)
     spmv = mat + 2.0 * elem * n
     vec = elem * float(n)
     passes = sum(3 * (j + 1) for j in range(L))            # u_i = r_i - beta u_i
     passes += sum(3 * (j + 1) + 3 for j in range(L))       # r_i -= alpha u_{i+1}, x += alpha u_0
-    for j in range(1, L + 1):                              # MGS passes (k, j)
-        for k in range(1, j + 1):
-            passes += 2 if k == 1 else 4
+    for k in range(1, L + 1):                              # right-looking MGS sweep k
+        passes += (L + 1) if k == 1 else (L - k + 3) + (L - k + 1)
     passes += (2 + 2 * L + 2) + 3                          # closing update: reads, then x, r_0, u_0 written
     return (2 * L) * spmv + (2 * L - 1) * vec + passes * vec
 
@@ -427,13 +427,14 @@ def bench_solver(args, ws, rank, local, torch, dist):
     clk.start()
     launches0 = L.hpb_launch_count()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    iters, rel = [], []
+    iters, rel, inner = [], [], []
     for i in range(args.steps):
         evs[i][0].record(stream)
         one()
         evs[i][1].record(stream)
         iters.append(rep.iters)
         rel.append(rep.true_resid_norm / rep.true_rhs_norm)
+        inner.append(rep.seconds)
     torch.cuda.synchronize()
     launches = L.hpb_launch_count() - launches0
     clocks = clk.stop()
@@ -477,7 +478,7 @@ def bench_solver(args, ws, rank, local, torch, dist):
         "solver": {"path": "plain drop-in (host-synchronised reductions)" if args.plain else
                    "fused device-resident BiCGStab(4): scalars on the GPU, SpMV+Dot2 fused, one CUDA graph per cycle",
                    "iters": iters, "true_rel_residual": rel, "cycles": [i // SOLVER_L for i in iters],
-                   "plain_dropin": plain},
+                   "step_s": times, "solve_loop_s": inner, "plain_dropin": plain},
         "roofline": roof,
         "solver_roofline": solver_roofline(A, iters, t_step, args.plain),
         "e2e": {"value": float(np.mean(e2e)), "unit": "s", "h2d_bytes_per_step": int(h2d),
@@ -559,7 +560,8 @@ def bench_forms(torch, log=lambda *a: None):
         b = problems.rhs_uniform(A.n, 303)
         t64, st64, r64, x64 = fused_solve(torch, A, b, "gmres", 50, SOLVER_TOL)
         _, sto, ro, xo = fused_solve(torch, A, b, "gmres", 50, 1e-13, max_iters=40000)
-        tir, stir, rir, xir = ir_solve(torch, A, b, "gmres", 50)
+        # one binary32 GMRES(50) cycle per binary64 refinement
+        tir, stir, rir, xir = ir_solve(torch, A, b, "gmres", 50, inner_tol=0.0, max_iters=0, max_refinements=400)
         nx = np.linalg.norm(xo)
         out["precision_gmres50_poisson3d_aniso128"] = {
             "n": A.n, "nnz": A.nnz,
@@ -599,8 +601,9 @@ def bench_forms(torch, log=lambda *a: None):
         tj64, stj64, rj64, xj64 = fused_solve(torch, A, b, "gmres", 30, SOLVER_TOL, precond="jacobi", max_iters=30000)
         res["fp64_gmres30_jacobi"] = {"s": tj64, "status": stj64, "iters": rj64.iters,
                                       "true_rel_residual": _rel(A, b, xj64)}
-        for pc in ("none", "jacobi"):
-            t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond=pc, max_iters=15000, max_refinements=10)
+        for pc in ("none", "jacobi"):  # one binary32 GMRES(30) cycle per refinement, same 30000-iteration budget
+            t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond=pc, inner_tol=0.0, max_iters=0,
+                                   max_refinements=1000)
             res[f"fp32_dot2_gmres30_refined_{pc}"] = {"s": t, "status": st, "inner_iters": r.inner_iters,
                                                       "refinements": r.refinements, "true_rel_residual": _rel(A, b, x)}
         wfile = spai.WEIGHTS_FILE
@@ -609,8 +612,8 @@ def bench_forms(torch, log=lambda *a: None):
             net = spai.SpaiNet(offs, dslot)
             net.set_weights(np.load(wfile))
             tb, M = _timed(torch, lambda: net.assemble(torch, spai.DeviceCSR(torch, A)))
-            t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond="matrix", M=M, max_iters=15000,
-                                   max_refinements=10)
+            t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond="matrix", M=M, inner_tol=0.0, max_iters=0,
+                                   max_refinements=1000)
             res["fp32_dot2_gmres30_refined_learned_spai"] = {
                 "s": t, "build_s": tb, "status": st, "inner_iters": r.inner_iters, "refinements": r.refinements,
                 "true_rel_residual": _rel(A, b, x)}

@@ -166,6 +166,7 @@ for t in TYPES:
              [C.POINTER(hpb_solver_params), I32, I64, P, P, P, P, P, C.POINTER(hpb_solver_report), P, C.c_int])
 
 
+_sig("hpb_solver_memory_release", C.c_int, [])
 _sig("hpb_ir_params_default", C.c_int, [C.POINTER(hpb_ir_params)])
 for _n in ("hpb_ir_solve_f64", "hpb_ir_solve_c128"):
     _sig(_n, C.c_int, [C.POINTER(hpb_ir_params), I32, I64, P, P, P, P, P, P, P, I64, P, P,

@@ -12,6 +12,9 @@
 
 #include "hpb_common.cuh"
 
+#include <memory>
+#include <vector>
+
 namespace hpb {
 namespace fused {
 
@@ -153,6 +156,27 @@ __device__ __forceinline__ AccC ldcg_acc(const AccC* p) {
     return r;
 }
 
+// This thread's share of a combine over nb block partials: entries
+// threadIdx.x, + blockDim.x, + 2 blockDim.x, ... merged in that order, four
+// loads issued before their merges (the order, hence the result, is that of
+// a plain strided loop).
+template <class A>
+__device__ __forceinline__ A merge_partials(const A* p, int nb) {
+    A t{};
+    const int bd = blockDim.x;
+    int b = threadIdx.x;
+    for (; b + 3 * bd < nb; b += 4 * bd) {
+        const A p0 = ldcg_acc(p + b), p1 = ldcg_acc(p + b + bd), p2 = ldcg_acc(p + b + 2 * bd),
+                p3 = ldcg_acc(p + b + 3 * bd);
+        merge(t, p0);
+        merge(t, p1);
+        merge(t, p2);
+        merge(t, p3);
+    }
+    for (; b < nb; b += bd) merge(t, ldcg_acc(p + b));
+    return t;
+}
+
 // Block-wide merge of ND accumulators (result valid in thread 0).
 template <int ND, class A>
 __device__ __forceinline__ void block_merge(A (&acc)[ND], A* sh /* [ND][32] */) {
@@ -198,10 +222,7 @@ __device__ __forceinline__ void grid_finish_acc(A (&acc)[ND], bool bad, A* parti
     __threadfence();
     A tot[ND > 0 ? ND : 1];
 #pragma unroll
-    for (int d = 0; d < ND; ++d) {
-        tot[d] = A{};
-        for (int b = threadIdx.x; b < int(gridDim.x); b += blockDim.x) merge(tot[d], ldcg_acc(partials + size_t(d) * gridDim.x + b));
-    }
+    for (int d = 0; d < ND; ++d) tot[d] = merge_partials<A>(partials + size_t(d) * gridDim.x, int(gridDim.x));
     __syncthreads();
     if (ND > 0) block_merge<ND>(tot, sh);
     if (threadIdx.x == 0) {
@@ -223,6 +244,26 @@ __device__ __forceinline__ void grid_finish(A (&acc)[ND], bool bad, A* partials,
     });
 }
 
+// ------------------------------------------------------------ workspace
+// Device scratch, stream, event, pinned read-back slot and cycle graph of one
+// solver plan (hpb_pool.cu): device memory comes stream-ordered from a
+// library-owned pool that keeps freed blocks for the next plan; pinned slots
+// are cached per host thread.  open() first, then alloc().
+void* pool_alloc(size_t bytes, cudaStream_t stream);
+void pool_free(void* p, cudaStream_t stream);
+
+struct SolverWorkspace {
+    std::vector<void*> dev;
+    void* pinned = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int open(size_t pinned_bytes);
+    void* alloc(size_t bytes);
+    ~SolverWorkspace();
+};
+
 // Right preconditioner of the fused GMRES: none, Jacobi (diagonal of A) or
 // a general CSR matrix M with the storage type of the iteration.
 template <class E>
@@ -236,13 +277,40 @@ struct RightPrec {
 };
 
 // Device-resident GMRES(m) (hpb_fused_gmres.cu); E in {float, double, cf, cd}.
+// A plan holds the workspace and the captured restart-cycle graph for one
+// matrix, one preconditioner and fixed b / x addresses; run() solves from
+// x's current content and can be called repeatedly (iterative refinement
+// rewrites b and x in place between calls).
+template <class E>
+struct GmPlan {
+    GmPlan();
+    ~GmPlan();
+    int init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
+             const E* val, const RightPrec<E>& M, const E* b, E* x, int max_cycles);
+    int run(hpb_solver_report* rep, double* hist, int cap);
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+};
 template <class E>
 int solve_gmres(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
                 const E* val, const RightPrec<E>& M, const E* b, E* x, hpb_solver_report* rep, double* hist, int cap,
                 int max_cycles);
 
 // Device-resident BiCGStab(l) (hpb_fused_bicgstabl.cu); E in {float,
-// double, cf, cd}.
+// double, cf, cd}.  A plan holds the workspace and the captured cycle graph
+// for one matrix and one solution vector x; run() solves for a right-hand
+// side from x's current content and can be called repeatedly (the inner
+// solves of iterative refinement).
+template <class E>
+struct BcgPlan {
+    BcgPlan();
+    ~BcgPlan();
+    int init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
+             const E* val, E* x);
+    int run(const E* b, hpb_solver_report* rep, double* hist, int cap);
+    struct Impl;
+    std::unique_ptr<Impl> impl_;
+};
 template <class E>
 int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
                     const E* val, const E* b, E* x, hpb_solver_report* rep, double* hist, int cap);

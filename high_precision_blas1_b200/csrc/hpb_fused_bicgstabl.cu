@@ -12,12 +12,12 @@
 //     (u_{j+1} = A u_j with <rt, u_{j+1}>, r_{j+1} = A r_j with <rt, r_{j+1}>),
 //     and an optional Jacobi scaling (left preconditioning) is applied to
 //     the rows in the same kernel;
-//   * each modified-Gram-Schmidt pass of the MR part applies the previous
-//     projection and computes the next inner product(s) in one sweep over
-//     the vectors, followed by a one-block combine of the block partials;
+//   * the MR part's modified Gram-Schmidt runs in l sweeps (right-looking:
+//     sweep k finishes r_k, projects r_{k-1} out of r_k..r_l and forms all
+//     inner products with r_k), each followed by a one-block combine;
 //   * the closing update of x, r_0, u_0 also produces ||r_0|| (the monitor's
 //     residual), <rt, r_0> (next cycle's rho) and the finiteness of x;
-//   * one cycle = 4l + l(l+1) + 1 kernels, captured once into a CUDA graph
+//   * one cycle = 6l + 1 kernels, captured once into a CUDA graph
 //     and replayed; the host reads 16 bytes (||r_0||, breakdown, non-finite)
 //     per cycle to apply the monitor's test, as the reference does once per
 //     cycle (default_monitor.h:202-226).
@@ -26,6 +26,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <memory>
+#include <new>
 #include <vector>
 
 #include "hpb_fused.cuh"
@@ -56,7 +58,7 @@ struct Vecs {
     E* u[kMaxL + 1];
 };
 
-enum Epi { EPI_NONE = 0, EPI_ALPHA, EPI_BETA, EPI_TAU, EPI_SIGMA, EPI_FINAL };
+enum Epi { EPI_NONE = 0, EPI_ALPHA, EPI_BETA, EPI_STEP, EPI_FINAL };
 
 template <class S>
 struct EpiArgs {
@@ -77,14 +79,12 @@ __device__ void run_epi(const EpiArgs<S>& a, const S* v, bool bad) {
             st.beta = s_div(s_mul(st.alpha, v[0]), st.rho);
             st.rho = v[0];
             break;
-        case EPI_TAU:  // tau[k][j] = <r_k, r_j> / sigma[k]
-            st.tau[a.k][a.j] = s_div(v[0], st.sigma[a.k]);
-            break;
-        case EPI_SIGMA: {  // sigma[j] = <r_j, r_j>; gamma'_j = <r_j, r_0> / sigma[j]
-            st.sigma[a.j] = v[0];
-            st.gam1[a.j] = s_div(v[1], v[0]);
-            if (a.j == a.L) {
-                const int L = a.L;
+        case EPI_STEP: {  // sweep k: v = (<r_k, r_k>, <r_k, r_0>, <r_k, r_{k+1}>, ..., <r_k, r_L>)
+            const int k = a.k, L = a.L;
+            st.sigma[k] = v[0];
+            st.gam1[k] = s_div(v[1], v[0]);
+            for (int j = k + 1; j <= L; ++j) st.tau[k][j] = s_div(v[1 + j - k], v[0]);
+            if (k == L) {  // gamma = T^{-1} gamma', gamma'' (the MR part of bicgstabl.h)
                 st.gam[L] = st.gam1[L];
                 st.omega = st.gam[L];
                 for (int jj = L - 1; jj >= 1; --jj) {
@@ -174,44 +174,55 @@ __global__ void __launch_bounds__(kThreads) k_upd_rx(int64_t n, int j, Vecs<E> V
 }
 
 // ------------------------------------------------------------ MR part
-// Pass k of the modified Gram-Schmidt sweep on r_j, in two launches:
-//   k_mgs_part:   if k > 1:  r_j -= tau[k-1][j] r_{k-1}
-//                 if k < j:  block partials of <r_k, r_j>
-//                 if k == j: block partials of <r_j, r_j> and <r_j, r_0>
+// Modified Gram-Schmidt on r_1..r_L in right-looking order: sweep k
+// (k = 1..L) finishes r_k and projects it out of the later vectors.  Per
+// vector r_j the operations are those of the column-by-column loop of
+// bicgstabl.h (r_j -= tau[1][j] r_1, then tau[2][j] from the updated r_j,
+// ...), so the results are the same; the L(L+1)/2 passes become L sweeps.
+//   k_mgs_step:   r_j -= tau[k-1][j] r_{k-1} for j = k..L (k > 1), then block
+//                 partials of <r_k, r_k>, <r_k, r_0>, <r_k, r_j> (j > k);
 //   k_mgs_finish: one block merges the partials in block order and sets
-//                 tau[k][j] = <r_k, r_j> / sigma[k], or sigma[j] and
-//                 gamma'_j = <r_j, r_0> / sigma[j] (then gamma, gamma'').
+//                 sigma[k], gamma'_k, tau[k][j > k] (and, at k = L, gamma
+//                 and gamma'').
 // The combine is a separate launch (no ticket): the single-launch form with
 // a last-block epilogue stalled on B200 for this pass (every block's thread 0
 // stopped between the block barrier and the ticket atomic) and is not used.
-template <class E, int ND>
+template <class E, int ND>  // ND = L - k + 2 inner products
 __global__ void __launch_bounds__(kThreads)
-k_mgs_part(int64_t n, int k, int j, Vecs<E> V, const BcgState<typename scalar_of<E>::type>* st,
+k_mgs_step(int64_t n, int k, Vecs<E> V, const BcgState<typename scalar_of<E>::type>* st,
            typename acc_of<typename scalar_of<E>::type>::type* partials) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
+    constexpr int NV = ND - 1;  // r_k .. r_L
     __shared__ A sh[ND * 32];
     const bool upd = k > 1;
-    const S ntau = upd ? s_neg(st->tau[k - 1][j]) : s_zero(S{});
-    E* rj = V.r[j];
+    S ntau[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) ntau[i] = upd ? s_neg(st->tau[k - 1][k + i]) : s_zero(S{});
     const E* rprev = upd ? V.r[k - 1] : nullptr;
-    const E* rk = V.r[k];
     const E* r0 = V.r[0];
     A acc[ND];
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
-        S v = to_s(ldE(rj, q));
+        E ve[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) ve[i] = ldE(V.r[k + i], q);
+        const S z = to_s(ldE(r0, q));
         if (upd) {
-            E ve = from_s<E>(s_fma(ntau, to_s(ldE(rprev, q)), v));
-            stE(rj, q, ve);
-            v = to_s(ve);
+            const S pv = to_s(ldE(rprev, q));
+#pragma unroll
+            for (int i = 0; i < NV; ++i) {
+                ve[i] = from_s<E>(s_fma(ntau[i], pv, to_s(ve[i])));
+                stE(V.r[k + i], q, ve[i]);
+            }
         }
-        if (ND == 1) {
-            dot_add(acc[0], to_s(ldE(rk, q)), v);
-        } else {
-            dot_add(acc[0], v, v);
-            dot_add(acc[ND - 1], v, to_s(ldE(r0, q)));
-        }
+        S v[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] = to_s(ve[i]);
+        dot_add(acc[0], v[0], v[0]);
+        dot_add(acc[1], v[0], z);
+#pragma unroll
+        for (int i = 1; i < NV; ++i) dot_add(acc[1 + i], v[0], v[i]);
     }
     block_merge<ND>(acc, sh);
     if (threadIdx.x == 0)
@@ -226,8 +237,7 @@ k_mgs_finish(int nb, const typename acc_of<S>::type* __restrict__ partials, EpiA
     __shared__ A sh[ND * 32];
     A tot[ND];
 #pragma unroll
-    for (int d = 0; d < ND; ++d)
-        for (int b = threadIdx.x; b < nb; b += blockDim.x) merge(tot[d], partials[size_t(d) * nb + b]);
+    for (int d = 0; d < ND; ++d) tot[d] = merge_partials<A>(partials + size_t(d) * nb, nb);
     block_merge<ND>(tot, sh);
     if (threadIdx.x == 0) {
         S vals[ND];
@@ -240,20 +250,22 @@ k_mgs_finish(int nb, const typename acc_of<S>::type* __restrict__ partials, EpiA
 // ------------------------------------------------------------ closing update
 // x += gamma_1 r_0 + sum_{j<L} gamma''_j r_j ; r_0 -= sum_j gamma'_j r_j ;
 // u_0 -= sum_j gamma_j u_j ; then <rt, r_0>, <r_0, r_0>, finiteness of x.
-template <class E>
+// L is a template parameter so the gamma coefficients live in registers.
+template <class E, int L>
 __global__ void __launch_bounds__(kThreads)
-k_final(int64_t n, int L, int update, Vecs<E> V, E* __restrict__ x, const E* __restrict__ rt,
+k_final(int64_t n, int update, Vecs<E> V, E* __restrict__ x, const E* __restrict__ rt,
         BcgState<typename scalar_of<E>::type>* st, typename acc_of<typename scalar_of<E>::type>::type* partials,
         unsigned int* ticket, int* badflag, EpiArgs<typename scalar_of<E>::type> ea) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
-    S g[kMaxL + 1], g1[kMaxL + 1], g2[kMaxL + 1];
-    if (update)
-        for (int i = 1; i <= L; ++i) {
-            g[i] = s_neg(st->gam[i]);
-            g1[i] = s_neg(st->gam1[i]);
-            g2[i] = st->gam2[i];
-        }
+    S g[L + 1], g1[L + 1], g2[L + 1];
+#pragma unroll
+    for (int i = 1; i <= L; ++i) {
+        g[i] = update ? s_neg(st->gam[i]) : s_zero(S{});
+        g1[i] = update ? s_neg(st->gam1[i]) : s_zero(S{});
+        g2[i] = update ? st->gam2[i] : s_zero(S{});
+    }
+    const S gam_1 = update ? st->gam[1] : s_zero(S{});
     A acc[2];
     bool bad = false;
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
@@ -261,15 +273,23 @@ k_final(int64_t n, int L, int update, Vecs<E> V, E* __restrict__ x, const E* __r
         E r0e = ldE(V.r[0], q);
         E xe = ldE(x, q);
         if (update) {
+            E re[L + 1], ue[L + 1];
+#pragma unroll
+            for (int j = 1; j <= L; ++j) {
+                re[j] = ldE(V.r[j], q);
+                ue[j] = ldE(V.u[j], q);
+            }
+            ue[0] = ldE(V.u[0], q);
             S r0 = to_s(r0e);
-            S xs = s_fma(st->gam[1], r0, to_s(xe));
-            r0 = s_fma(g1[L], to_s(ldE(V.r[L], q)), r0);
-            S u0 = s_fma(g[L], to_s(ldE(V.u[L], q)), to_s(ldE(V.u[0], q)));
+            S xs = s_fma(gam_1, r0, to_s(xe));
+            r0 = s_fma(g1[L], to_s(re[L]), r0);
+            S u0 = s_fma(g[L], to_s(ue[L]), to_s(ue[0]));
+#pragma unroll
             for (int jj = 1; jj < L; ++jj) {
-                S rj = to_s(ldE(V.r[jj], q));
+                const S rj = to_s(re[jj]);
                 xs = s_fma(g2[jj], rj, xs);
                 r0 = s_fma(g1[jj], rj, r0);
-                u0 = s_fma(g[jj], to_s(ldE(V.u[jj], q)), u0);
+                u0 = s_fma(g[jj], to_s(ue[jj]), u0);
             }
             xe = from_s<E>(xs);
             r0e = from_s<E>(r0);
@@ -283,7 +303,6 @@ k_final(int64_t n, int L, int update, Vecs<E> V, E* __restrict__ x, const E* __r
         bad |= !finite_e(xe);
     }
     grid_finish<2>(acc, bad, partials, ticket, badflag, [&](const S* vals, bool b) { run_epi(ea, vals, b); });
-    (void)A{};
 }
 
 // ------------------------------------------------------------ small kernels
@@ -365,110 +384,188 @@ __global__ void __launch_bounds__(kThreads) k_norm(int64_t n, const E* __restric
                    [&](const S* vals, bool) { out[0] = norm_sqrt(s_real(vals[0])); });
 }
 
-namespace {
-struct Workspace {
-    std::vector<void*> dev;
-    void* pinned = nullptr;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    ~Workspace() {
-        if (stream) cudaStreamSynchronize(stream);
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        for (void* p : dev) cudaFree(p);
-        if (pinned) cudaFreeHost(pinned);
-        if (ev) cudaEventDestroy(ev);
-        if (stream) cudaStreamDestroy(stream);
-    }
-    void* alloc(size_t bytes) {
-        void* p = nullptr;
-        if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return nullptr;
-        dev.push_back(p);
-        return p;
-    }
-};
-}  // namespace
+// Resident blocks per SM (the least over a kernel set): grids are one full
+// wave, so no SM idles in a partial second wave.  The light streaming
+// kernels and the register-heavier reduction kernels (closing update, MGS
+// sweeps) get separate grids.
+inline int occupancy_of(const void* f) {
+    int o = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, kThreads, 0) == cudaSuccess && o > 0 ? o : 1;
+}
 
 template <class E>
-int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
-                    const E* val, const E* b, E* x, hpb_solver_report* rep, double* hist, int cap) {
+int light_occupancy() {
+    int occ = occupancy_of(reinterpret_cast<const void*>(k_upd_u<E>));
+    occ = std::min(occ, occupancy_of(reinterpret_cast<const void*>(k_upd_rx<E>)));
+    occ = std::min(occ, occupancy_of(reinterpret_cast<const void*>(k_norm<E>)));
+    return occ;
+}
+
+template <class E>
+int reduction_occupancy(int L) {
+    int occ = 64;
+#define HPB_OCC_F(LL) \
+    case LL: occ = occupancy_of(reinterpret_cast<const void*>(k_final<E, LL>)); break;
+    switch (L) {
+        HPB_OCC_F(1) HPB_OCC_F(2) HPB_OCC_F(3) HPB_OCC_F(4) HPB_OCC_F(5) HPB_OCC_F(6) HPB_OCC_F(7) HPB_OCC_F(8)
+        default: break;
+    }
+#undef HPB_OCC_F
+#define HPB_OCC_S(ND) \
+    if (ND <= L + 1) occ = std::min(occ, occupancy_of(reinterpret_cast<const void*>(k_mgs_step<E, ND>)));
+    HPB_OCC_S(2) HPB_OCC_S(3) HPB_OCC_S(4) HPB_OCC_S(5) HPB_OCC_S(6) HPB_OCC_S(7) HPB_OCC_S(8) HPB_OCC_S(9)
+#undef HPB_OCC_S
+    return occ;
+}
+
+// launch helpers: compile-time L / number of inner products
+template <class E>
+void launch_final(int L, int grid, cudaStream_t s, int64_t n, int update, const Vecs<E>& V, E* x, const E* rt,
+                  BcgState<typename scalar_of<E>::type>* st,
+                  typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
+                  EpiArgs<typename scalar_of<E>::type> ea) {
+#define HPB_FINAL(LL) \
+    case LL: k_final<E, LL><<<grid, kThreads, 0, s>>>(n, update, V, x, rt, st, partials, ticket, badflag, ea); break;
+    switch (L) {
+        HPB_FINAL(1) HPB_FINAL(2) HPB_FINAL(3) HPB_FINAL(4) HPB_FINAL(5) HPB_FINAL(6) HPB_FINAL(7) HPB_FINAL(8)
+        default: break;
+    }
+#undef HPB_FINAL
+}
+
+template <class E>
+void launch_mgs_step(int nd, int grid, cudaStream_t s, int64_t n, int k, const Vecs<E>& V,
+                     const BcgState<typename scalar_of<E>::type>* st,
+                     typename acc_of<typename scalar_of<E>::type>::type* partials,
+                     EpiArgs<typename scalar_of<E>::type> ea) {
+    using S = typename scalar_of<E>::type;
+#define HPB_STEP(ND)                                                        \
+    case ND:                                                                \
+        k_mgs_step<E, ND><<<grid, kThreads, 0, s>>>(n, k, V, st, partials); \
+        k_mgs_finish<S, ND><<<1, kThreads, 0, s>>>(grid, partials, ea);     \
+        break;
+    switch (nd) {
+        HPB_STEP(2) HPB_STEP(3) HPB_STEP(4) HPB_STEP(5) HPB_STEP(6) HPB_STEP(7) HPB_STEP(8) HPB_STEP(9)
+        default: break;
+    }
+#undef HPB_STEP
+}
+
+template <class E>
+struct BcgPlan<E>::Impl {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
+    hpb_solver_params p{};
+    int L = 2;
+    bool jac = false;
+    int32_t rows = 0;
+    int64_t n = 0;
+    const int32_t *rp = nullptr, *ci = nullptr;
+    const E* val = nullptr;
+    E* x = nullptr;
+    int g_ew = 1, g_red = 1, g_sp = 1, kernels = 0;
+    SolverWorkspace ws;
+    Vecs<E> V{};
+    E *rt = nullptr, *tmp = nullptr, *diag = nullptr;
+    BcgState<S>* st = nullptr;
+    Report* drep = nullptr;
+    A* partials = nullptr;
+    unsigned int* ticket = nullptr;
+    int* badflag = nullptr;
+    double* dnorm = nullptr;
+    Report* hrep = nullptr;
+    double* hnorm = nullptr;
+};
+
+template <class E>
+BcgPlan<E>::BcgPlan() = default;
+template <class E>
+BcgPlan<E>::~BcgPlan() = default;
+
+// Workspace, the Jacobi diagonal and the captured cycle graph: everything
+// that depends on A and x's address but not on b.
+template <class E>
+int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
+                     const E* val, E* x) {
+    using S = typename Impl::S;
+    using A = typename Impl::A;
+    (void)nnz;
     const int L = p->basis > 0 ? p->basis : 2;
     if (L > kMaxL) return HPB_ERROR_NOT_SUPPORTED;
     const bool jac = p->precond == HPB_PRECOND_JACOBI;
     if (!jac && p->precond != HPB_PRECOND_NONE) return HPB_ERROR_NOT_SUPPORTED;
     if (!p->high_precision) return HPB_ERROR_NOT_SUPPORTED;  // the fused path carries Dot2 only
-    (void)nnz;
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return HPB_ERROR_CUDA;
+    impl_.reset(new (std::nothrow) Impl());
+    if (!impl_) return HPB_ERROR_OUT_OF_MEMORY;
+    Impl& P = *impl_;
+    P.p = *p;
+    P.L = L;
+    P.jac = jac;
+    P.rows = rows;
+    P.n = rows;
+    P.rp = rp;
+    P.ci = ci;
+    P.val = val;
+    P.x = x;
     const int64_t n = rows;
-    const int g_ew = int(std::max<int64_t>(1, std::min<int64_t>((n + kThreads - 1) / kThreads, int64_t(sms) * 8)));
-    const int g_sp = (rows + kThreads - 1) / kThreads;
-
-    Workspace ws;
-    Vecs<E> V{};
+    const int64_t need = (n + kThreads - 1) / kThreads;
+    P.g_ew = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * light_occupancy<E>())));
+    P.g_red = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * reduction_occupancy<E>(L))));
+    P.g_sp = int(std::max<int64_t>(1, need));
+    const int g_ew = P.g_ew, g_red = P.g_red, g_sp = P.g_sp;
+    SolverWorkspace& ws = P.ws;
+    Vecs<E>& V = P.V;
     const size_t vb = size_t(n) * sizeof(E);
+    int wst = ws.open(sizeof(Report) + 8 * sizeof(double));
+    if (wst != HPB_SUCCESS) return wst;
+    cudaStream_t s = ws.stream;
+    // allocations and the diagonal run after the caller's work on the legacy default stream
+    if (cudaEventRecord(ws.ev, 0) != cudaSuccess || cudaStreamWaitEvent(s, ws.ev, 0) != cudaSuccess)
+        return HPB_ERROR_CUDA;
     for (int i = 0; i <= L; ++i) {
         V.r[i] = static_cast<E*>(ws.alloc(vb));
         V.u[i] = static_cast<E*>(ws.alloc(vb));
         if (!V.r[i] || !V.u[i]) return HPB_ERROR_OUT_OF_MEMORY;
     }
-    E* rt = static_cast<E*>(ws.alloc(vb));
-    E* tmp = static_cast<E*>(ws.alloc(vb));
-    E* diag = jac ? static_cast<E*>(ws.alloc(vb)) : nullptr;
-    auto* st = static_cast<BcgState<S>*>(ws.alloc(sizeof(BcgState<S>)));
-    auto* drep = static_cast<Report*>(ws.alloc(sizeof(Report)));
-    auto* partials = static_cast<A*>(ws.alloc(2 * size_t(std::max(g_ew, g_sp)) * sizeof(A)));
-    auto* ticket = static_cast<unsigned int*>(ws.alloc(64));
-    auto* badflag = static_cast<int*>(ws.alloc(64));
-    auto* dnorm = static_cast<double*>(ws.alloc(4 * sizeof(double)));
-    if (!rt || !tmp || (jac && !diag) || !st || !drep || !partials || !ticket || !badflag || !dnorm)
+    P.rt = static_cast<E*>(ws.alloc(vb));
+    P.tmp = static_cast<E*>(ws.alloc(vb));
+    P.diag = jac ? static_cast<E*>(ws.alloc(vb)) : nullptr;
+    P.st = static_cast<BcgState<S>*>(ws.alloc(sizeof(BcgState<S>)));
+    P.drep = static_cast<Report*>(ws.alloc(sizeof(Report)));
+    // block partials: ND dots x grid blocks for the largest producer -- the
+    // SpMV+Dot2 (1 x g_sp), the norms (1 x g_ew), the closing update
+    // (2 x g_red) and the first MGS sweep (L + 1 x g_red)
+    const size_t npart =
+        std::max<size_t>(std::max<size_t>(size_t(g_sp), size_t(g_ew)), size_t(L + 1) * size_t(g_red));
+    P.partials = static_cast<A*>(ws.alloc(npart * sizeof(A)));
+    P.ticket = static_cast<unsigned int*>(ws.alloc(64));
+    P.badflag = static_cast<int*>(ws.alloc(64));
+    P.dnorm = static_cast<double*>(ws.alloc(4 * sizeof(double)));
+    if (!P.rt || !P.tmp || (jac && !P.diag) || !P.st || !P.drep || !P.partials || !P.ticket || !P.badflag || !P.dnorm)
         return HPB_ERROR_OUT_OF_MEMORY;
-    if (cudaMallocHost(&ws.pinned, sizeof(Report) + 8 * sizeof(double)) != cudaSuccess) return HPB_ERROR_OUT_OF_MEMORY;
-    Report* hrep = static_cast<Report*>(ws.pinned);
-    double* hnorm = reinterpret_cast<double*>(static_cast<char*>(ws.pinned) + sizeof(Report));
-    if (cudaStreamCreateWithFlags(&ws.stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ws.ev, cudaEventDisableTiming) != cudaSuccess)
-        return HPB_ERROR_CUDA;
-    cudaStream_t s = ws.stream;
-    // run after the caller's work on the legacy default stream
-    if (cudaEventRecord(ws.ev, 0) != cudaSuccess || cudaStreamWaitEvent(s, ws.ev, 0) != cudaSuccess)
-        return HPB_ERROR_CUDA;
-    auto t0 = std::chrono::steady_clock::now();
-
-    cudaMemsetAsync(ticket, 0, 64, s);
-    cudaMemsetAsync(badflag, 0, 64, s);
-    cudaMemsetAsync(V.u[0], 0, vb, s);
-    k_init_state<S><<<1, 1, 0, s>>>(st, drep);
-    EpiArgs<S> none{st, drep, EPI_NONE, 0, 0, L};
-    if (jac) k_diag<E><<<(rows + 255) / 256, 256, 0, s>>>(rows, rp, ci, val, diag);
-    // monitor base ||P b||
-    const E* pb = b;
+    P.hrep = static_cast<Report*>(ws.pinned);
+    P.hnorm = reinterpret_cast<double*>(static_cast<char*>(ws.pinned) + sizeof(Report));
+    cudaMemsetAsync(P.ticket, 0, 64, s);
+    cudaMemsetAsync(P.badflag, 0, 64, s);
     if (jac) {
-        k_scale_inv<E><<<g_ew, kThreads, 0, s>>>(n, b, diag, tmp);
-        pb = tmp;
+        k_diag<E><<<(rows + 255) / 256, 256, 0, s>>>(rows, rp, ci, val, P.diag);
+        count_launch();
     }
-    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, pb, dnorm, partials, ticket, badflag);
-    // r0 = P (b - A x), rt = r0 / ||r0||
-    k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, nullptr, x, tmp, nullptr, partials, ticket,
-                                                   badflag, none);
-    k_residual_finish<E><<<g_ew, kThreads, 0, s>>>(n, b, tmp, diag, V.r[0]);
-    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[0], dnorm + 1, partials, ticket, badflag);
-    k_scale_by_inv_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[0], dnorm + 1, rt);
-    // ||r0||, <rt, r0>, finiteness of x, and the first cycle's beta / rho
-    k_final<E><<<g_ew, kThreads, 0, s>>>(n, L, 0, V, x, rt, st, partials, ticket, badflag,
-                                         EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L});
-    cudaMemcpyAsync(hrep, drep, sizeof(Report), cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(hnorm, dnorm, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return HPB_ERROR_CUDA;
-    count_launch(jac ? 9 : 6);
 
     // ---- one cycle as a CUDA graph
+    BcgState<S>* st = P.st;
+    Report* drep = P.drep;
+    A* partials = P.partials;
+    unsigned int* ticket = P.ticket;
+    int* badflag = P.badflag;
+    E* diag = P.diag;
+    E* rt = P.rt;
+    EpiArgs<S> none{st, drep, EPI_NONE, 0, 0, L};
     int kernels = 0;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HPB_ERROR_CUDA;
     for (int j = 0; j < L; ++j) {
@@ -485,23 +582,63 @@ int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
                                                            partials, ticket, badflag, none);
         kernels += 4;
     }
-    for (int j = 1; j <= L; ++j)
-        for (int k = 1; k <= j; ++k) {
-            if (k < j) {
-                k_mgs_part<E, 1><<<g_ew, kThreads, 0, s>>>(n, k, j, V, st, partials);
-                k_mgs_finish<S, 1><<<1, kThreads, 0, s>>>(g_ew, partials, EpiArgs<S>{st, drep, EPI_TAU, k, j, L});
-            } else {
-                k_mgs_part<E, 2><<<g_ew, kThreads, 0, s>>>(n, k, j, V, st, partials);
-                k_mgs_finish<S, 2><<<1, kThreads, 0, s>>>(g_ew, partials, EpiArgs<S>{st, drep, EPI_SIGMA, k, j, L});
-            }
-            kernels += 2;
-        }
-    k_final<E><<<g_ew, kThreads, 0, s>>>(n, L, 1, V, x, rt, st, partials, ticket, badflag,
-                                         EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L});
+    for (int k = 1; k <= L; ++k) {
+        launch_mgs_step<E>(L - k + 2, g_red, s, n, k, V, st, partials, EpiArgs<S>{st, drep, EPI_STEP, k, 0, L});
+        kernels += 2;
+    }
+    launch_final<E>(L, g_red, s, n, 1, V, x, rt, st, partials, ticket, badflag,
+                    EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L});
     ++kernels;
-    cudaMemcpyAsync(hrep, drep, sizeof(Report), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(P.hrep, drep, sizeof(Report), cudaMemcpyDeviceToHost, s);
     if (cudaStreamEndCapture(s, &ws.graph) != cudaSuccess) return HPB_ERROR_CUDA;
     if (cudaGraphInstantiate(&ws.exec, ws.graph, 0) != cudaSuccess) return HPB_ERROR_CUDA;
+    P.kernels = kernels;
+    return HPB_SUCCESS;
+}
+
+// One solve A x = b from the current content of x (the x given to init).
+template <class E>
+int BcgPlan<E>::run(const E* b, hpb_solver_report* rep, double* hist, int cap) {
+    using S = typename Impl::S;
+    if (!impl_) return HPB_ERROR_INVALID_VALUE;
+    Impl& P = *impl_;
+    const hpb_solver_params* p = &P.p;
+    const int L = P.L;
+    const int32_t rows = P.rows;
+    const int64_t n = P.n;
+    const int g_ew = P.g_ew, g_sp = P.g_sp;
+    Vecs<E>& V = P.V;
+    E* x = P.x;
+    Report* hrep = P.hrep;
+    double* hnorm = P.hnorm;
+    cudaStream_t s = P.ws.stream;
+    EpiArgs<S> none{P.st, P.drep, EPI_NONE, 0, 0, L};
+    // run after the caller's work on the legacy default stream
+    if (cudaEventRecord(P.ws.ev, 0) != cudaSuccess || cudaStreamWaitEvent(s, P.ws.ev, 0) != cudaSuccess)
+        return HPB_ERROR_CUDA;
+    auto t0 = std::chrono::steady_clock::now();
+    cudaMemsetAsync(V.u[0], 0, size_t(n) * sizeof(E), s);
+    k_init_state<S><<<1, 1, 0, s>>>(P.st, P.drep);
+    // monitor base ||P b||
+    const E* pb = b;
+    if (P.jac) {
+        k_scale_inv<E><<<g_ew, kThreads, 0, s>>>(n, b, P.diag, P.tmp);
+        pb = P.tmp;
+    }
+    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, pb, P.dnorm, P.partials, P.ticket, P.badflag);
+    // r0 = P (b - A x), rt = r0 / ||r0||
+    k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, P.rp, P.ci, P.val, nullptr, x, P.tmp, nullptr, P.partials,
+                                                   P.ticket, P.badflag, none);
+    k_residual_finish<E><<<g_ew, kThreads, 0, s>>>(n, b, P.tmp, P.diag, V.r[0]);
+    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[0], P.dnorm + 1, P.partials, P.ticket, P.badflag);
+    k_scale_by_inv_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[0], P.dnorm + 1, P.rt);
+    // ||r0||, <rt, r0>, finiteness of x, and the first cycle's beta / rho
+    launch_final<E>(L, P.g_red, s, n, 0, V, x, P.rt, P.st, P.partials, P.ticket, P.badflag,
+                    EpiArgs<S>{P.st, P.drep, EPI_FINAL, 0, 0, L});
+    cudaMemcpyAsync(hrep, P.drep, sizeof(Report), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hnorm, P.dnorm, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HPB_ERROR_CUDA;
+    count_launch(P.jac ? 8 : 7);
 
     // ---- monitor loop (default_monitor semantics, one test per cycle)
     const double rhs = hnorm[0];
@@ -522,9 +659,9 @@ int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     };
     bool finished = record();
     while (!finished) {
-        if (cudaGraphLaunch(ws.exec, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+        if (cudaGraphLaunch(P.ws.exec, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
             return HPB_ERROR_CUDA;
-        count_launch(uint64_t(kernels));
+        count_launch(uint64_t(P.kernels));
         iters += L;
         if (hrep->breakdown) {
             breakdown = true;
@@ -535,12 +672,12 @@ int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     auto t1 = std::chrono::steady_clock::now();
 
     // true residual ||b - A x|| and ||b|| (compensated)
-    k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, nullptr, x, tmp, nullptr, partials, ticket,
-                                                   badflag, none);
-    k_residual_finish<E><<<g_ew, kThreads, 0, s>>>(n, b, tmp, nullptr, V.r[1]);
-    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[1], dnorm + 2, partials, ticket, badflag);
-    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, b, dnorm + 3, partials, ticket, badflag);
-    cudaMemcpyAsync(hnorm + 2, dnorm + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
+    k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, P.rp, P.ci, P.val, nullptr, x, P.tmp, nullptr, P.partials,
+                                                   P.ticket, P.badflag, none);
+    k_residual_finish<E><<<g_ew, kThreads, 0, s>>>(n, b, P.tmp, nullptr, V.r[1]);
+    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[1], P.dnorm + 2, P.partials, P.ticket, P.badflag);
+    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, b, P.dnorm + 3, P.partials, P.ticket, P.badflag);
+    cudaMemcpyAsync(hnorm + 2, P.dnorm + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return HPB_ERROR_CUDA;
     count_launch(4);
 
@@ -557,6 +694,19 @@ int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     return conv ? HPB_SUCCESS : (breakdown ? HPB_ERROR_BREAKDOWN : HPB_ERROR_NOT_CONVERGED);
 }
 
+template <class E>
+int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
+                    const E* val, const E* b, E* x, hpb_solver_report* rep, double* hist, int cap) {
+    BcgPlan<E> plan;
+    int st = plan.init(p, rows, nnz, rp, ci, val, x);
+    if (st != HPB_SUCCESS) return st;
+    return plan.run(b, rep, hist, cap);
+}
+
+template struct BcgPlan<float>;
+template struct BcgPlan<double>;
+template struct BcgPlan<cf>;
+template struct BcgPlan<cd>;
 template int solve_bicgstabl<float>(const hpb_solver_params*, int32_t, int64_t, const int32_t*, const int32_t*,
                                     const float*, const float*, float*, hpb_solver_report*, double*, int);
 template int solve_bicgstabl<double>(const hpb_solver_params*, int32_t, int64_t, const int32_t*, const int32_t*,

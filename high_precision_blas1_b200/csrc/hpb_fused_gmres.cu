@@ -18,6 +18,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <memory>
+#include <new>
 #include <vector>
 
 #include "hpb_fused.cuh"
@@ -358,38 +360,41 @@ struct GmHostView {
     double bnorm;
 };
 
-namespace {
-struct GmWorkspace {
-    std::vector<void*> dev;
-    void* pinned = nullptr;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    ~GmWorkspace() {
-        if (stream) cudaStreamSynchronize(stream);
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        for (void* p : dev) cudaFree(p);
-        if (pinned) cudaFreeHost(pinned);
-        if (ev) cudaEventDestroy(ev);
-        if (stream) cudaStreamDestroy(stream);
-    }
-    void* alloc(size_t bytes) {
-        void* p = nullptr;
-        if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return nullptr;
-        dev.push_back(p);
-        return p;
-    }
-};
-}  // namespace
-
 template <class E>
-int solve_gmres(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
-                const E* val, const RightPrec<E>& M, const E* b, E* x, hpb_solver_report* rep, double* hist, int cap,
-                int max_cycles) {
+struct GmPlan<E>::Impl {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
+    hpb_solver_params p{};
+    int m = 30, max_cycles = 0;
+    int32_t rows = 0;
+    int64_t n = 0;
+    const int32_t *rp = nullptr, *ci = nullptr;
+    const E* val = nullptr;
+    const E* b = nullptr;
+    E* x = nullptr;
+    int g_ew = 1, g_md = 1, g_sp = 1, kernels = 0;
+    SolverWorkspace ws;
+    E *V = nullptr, *W = nullptr, *Z = nullptr, *R = nullptr, *diag = nullptr;
+    GmState<S>* st = nullptr;
+    A* partials = nullptr;
+    unsigned int* ticket = nullptr;
+    int* badflag = nullptr;
+    double* dnorm = nullptr;
+    GmHostView* hv = nullptr;
+};
+
+template <class E>
+GmPlan<E>::GmPlan() = default;
+template <class E>
+GmPlan<E>::~GmPlan() = default;
+
+// Workspace, the Jacobi diagonal and the captured restart-cycle graph for
+// one matrix, one preconditioner and fixed b / x addresses.
+template <class E>
+int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
+                    const E* val, const RightPrec<E>& M, const E* b, E* x, int max_cycles) {
+    using S = typename Impl::S;
+    using A = typename Impl::A;
     (void)nnz;
     const int m = p->basis > 0 ? p->basis : 30;
     if (m > kGmMaxM) return HPB_ERROR_NOT_SUPPORTED;
@@ -398,52 +403,54 @@ int solve_gmres(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
         return HPB_ERROR_CUDA;
+    impl_.reset(new (std::nothrow) Impl());
+    if (!impl_) return HPB_ERROR_OUT_OF_MEMORY;
+    Impl& P = *impl_;
+    P.p = *p;
+    P.m = m;
+    P.max_cycles = max_cycles;
+    P.rows = rows;
+    P.n = rows;
+    P.rp = rp;
+    P.ci = ci;
+    P.val = val;
+    P.b = b;
+    P.x = x;
     const int64_t n = rows;
-    const int g_ew = int(std::max<int64_t>(1, std::min<int64_t>((n + kGmThreads - 1) / kGmThreads, int64_t(sms) * 8)));
-    const int g_md = int(std::max<int64_t>(1, std::min<int64_t>((n + 4095) / 4096, int64_t(sms) * 2)));
-    const int g_sp = (rows + kGmThreads - 1) / kGmThreads;
-
-    GmWorkspace ws;
+    const int g_ew = P.g_ew =
+        int(std::max<int64_t>(1, std::min<int64_t>((n + kGmThreads - 1) / kGmThreads, int64_t(sms) * 8)));
+    const int g_md = P.g_md = int(std::max<int64_t>(1, std::min<int64_t>((n + 4095) / 4096, int64_t(sms) * 2)));
+    const int g_sp = P.g_sp = int(std::max<int64_t>(1, (int64_t(rows) + kGmThreads - 1) / kGmThreads));
+    SolverWorkspace& ws = P.ws;
     const size_t vb = size_t(n) * sizeof(E);
-    E* V = static_cast<E*>(ws.alloc(vb * size_t(m + 1)));
-    E* W = static_cast<E*>(ws.alloc(vb));
-    E* Z = M.kind ? static_cast<E*>(ws.alloc(vb)) : nullptr;
-    E* R = static_cast<E*>(ws.alloc(vb));
-    E* diag = M.kind == 1 ? static_cast<E*>(ws.alloc(vb)) : nullptr;
-    auto* st = static_cast<GmState<S>*>(ws.alloc(sizeof(GmState<S>)));
-    const size_t np = std::max<size_t>(size_t(m + 1) * g_md, std::max<size_t>(g_ew, g_sp));
-    auto* partials = static_cast<A*>(ws.alloc(np * sizeof(A)));
-    auto* ticket = static_cast<unsigned int*>(ws.alloc(64));
-    auto* badflag = static_cast<int*>(ws.alloc(64));
-    auto* dnorm = static_cast<double*>(ws.alloc(8 * sizeof(double)));
-    if (!V || !W || (M.kind && !Z) || !R || (M.kind == 1 && !diag) || !st || !partials || !ticket || !badflag ||
-        !dnorm)
-        return HPB_ERROR_OUT_OF_MEMORY;
-    if (cudaMallocHost(&ws.pinned, sizeof(GmHostView)) != cudaSuccess) return HPB_ERROR_OUT_OF_MEMORY;
-    auto* hv = static_cast<GmHostView*>(ws.pinned);
-    if (cudaStreamCreateWithFlags(&ws.stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ws.ev, cudaEventDisableTiming) != cudaSuccess)
-        return HPB_ERROR_CUDA;
+    int wst = ws.open(sizeof(GmHostView));
+    if (wst != HPB_SUCCESS) return wst;
     cudaStream_t s = ws.stream;
+    // allocations and the diagonal run after the caller's work on the legacy default stream
     if (cudaEventRecord(ws.ev, 0) != cudaSuccess || cudaStreamWaitEvent(s, ws.ev, 0) != cudaSuccess)
         return HPB_ERROR_CUDA;
-    auto t0 = std::chrono::steady_clock::now();
+    E* V = P.V = static_cast<E*>(ws.alloc(vb * size_t(m + 1)));
+    E* W = P.W = static_cast<E*>(ws.alloc(vb));
+    E* Z = P.Z = M.kind ? static_cast<E*>(ws.alloc(vb)) : nullptr;
+    E* R = P.R = static_cast<E*>(ws.alloc(vb));
+    E* diag = P.diag = M.kind == 1 ? static_cast<E*>(ws.alloc(vb)) : nullptr;
+    auto* st = P.st = static_cast<GmState<S>*>(ws.alloc(sizeof(GmState<S>)));
+    const size_t np = std::max<size_t>(size_t(m + 1) * g_md, std::max<size_t>(g_ew, g_sp));
+    auto* partials = P.partials = static_cast<A*>(ws.alloc(np * sizeof(A)));
+    auto* ticket = P.ticket = static_cast<unsigned int*>(ws.alloc(64));
+    auto* badflag = P.badflag = static_cast<int*>(ws.alloc(64));
+    P.dnorm = static_cast<double*>(ws.alloc(8 * sizeof(double)));
+    if (!V || !W || (M.kind && !Z) || !R || (M.kind == 1 && !diag) || !st || !partials || !ticket || !badflag ||
+        !P.dnorm)
+        return HPB_ERROR_OUT_OF_MEMORY;
+    auto* hv = P.hv = static_cast<GmHostView*>(ws.pinned);
     cudaMemsetAsync(ticket, 0, 64, s);
     cudaMemsetAsync(badflag, 0, 64, s);
-    cudaMemsetAsync(st, 0, sizeof(GmState<S>), s);
-    if (M.kind == 1) k_gm_diag<E><<<(rows + 255) / 256, 256, 0, s>>>(rows, rp, ci, val, diag);
-    k_gm_norm<E><<<g_ew, kGmThreads, 0, s>>>(n, b, dnorm, partials, ticket, badflag);
-    k_resid_comp<E, E><<<g_sp, kGmThreads, 0, s>>>(rows, rp, ci, val, x, b, R, st, partials, ticket, badflag);
-    auto pull = [&]() {
-        cudaMemcpyAsync(&hv->rnorm, &st->rnorm, sizeof(double), cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(&hv->est, &st->est, sizeof(double), cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(&hv->nsteps, &st->nsteps, sizeof(int), cudaMemcpyDeviceToHost, s);
-        cudaMemcpyAsync(&hv->nonfinite, &st->nonfinite, sizeof(int), cudaMemcpyDeviceToHost, s);
-    };
-    pull();
-    cudaMemcpyAsync(&hv->bnorm, dnorm, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (M.kind == 1) {
+        k_gm_diag<E><<<(rows + 255) / 256, 256, 0, s>>>(rows, rp, ci, val, diag);
+        count_launch();
+    }
     if (cudaStreamSynchronize(s) != cudaSuccess) return HPB_ERROR_CUDA;
-    count_launch(M.kind == 1 ? 3 : 2);
 
     // ---- one restart cycle as a CUDA graph
     int kernels = 0;
@@ -493,9 +500,41 @@ int solve_gmres(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int
     }
     k_resid_comp<E, E><<<g_sp, kGmThreads, 0, s>>>(rows, rp, ci, val, x, b, R, st, partials, ticket, badflag);
     ++kernels;
-    pull();
+    cudaMemcpyAsync(&hv->rnorm, &st->rnorm, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&hv->est, &st->est, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&hv->nsteps, &st->nsteps, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&hv->nonfinite, &st->nonfinite, sizeof(int), cudaMemcpyDeviceToHost, s);
     if (cudaStreamEndCapture(s, &ws.graph) != cudaSuccess) return HPB_ERROR_CUDA;
     if (cudaGraphInstantiate(&ws.exec, ws.graph, 0) != cudaSuccess) return HPB_ERROR_CUDA;
+    P.kernels = kernels;
+    return HPB_SUCCESS;
+}
+
+// One solve A x = b (the b and x given to init) from x's current content.
+template <class E>
+int GmPlan<E>::run(hpb_solver_report* rep, double* hist, int cap) {
+    using S = typename Impl::S;
+    if (!impl_) return HPB_ERROR_INVALID_VALUE;
+    Impl& P = *impl_;
+    const hpb_solver_params* p = &P.p;
+    const int m = P.m;
+    cudaStream_t s = P.ws.stream;
+    GmState<S>* st = P.st;
+    GmHostView* hv = P.hv;
+    if (cudaEventRecord(P.ws.ev, 0) != cudaSuccess || cudaStreamWaitEvent(s, P.ws.ev, 0) != cudaSuccess)
+        return HPB_ERROR_CUDA;
+    auto t0 = std::chrono::steady_clock::now();
+    cudaMemsetAsync(st, 0, sizeof(GmState<S>), s);
+    k_gm_norm<E><<<P.g_ew, kGmThreads, 0, s>>>(P.n, P.b, P.dnorm, P.partials, P.ticket, P.badflag);
+    k_resid_comp<E, E><<<P.g_sp, kGmThreads, 0, s>>>(P.rows, P.rp, P.ci, P.val, P.x, P.b, P.R, st, P.partials,
+                                                     P.ticket, P.badflag);
+    cudaMemcpyAsync(&hv->rnorm, &st->rnorm, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&hv->est, &st->est, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&hv->nsteps, &st->nsteps, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&hv->nonfinite, &st->nonfinite, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(&hv->bnorm, P.dnorm, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return HPB_ERROR_CUDA;
+    count_launch(2);
 
     // ---- monitor loop: the true residual is tested once per cycle
     const double bnorm = hv->bnorm;
@@ -510,13 +549,13 @@ int solve_gmres(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int
             hist[2 * hl + 1] = hv->rnorm;
             ++hl;
         }
-        return !valid || conv || iters >= p->max_iters || (max_cycles > 0 && cycles >= max_cycles);
+        return !valid || conv || iters >= p->max_iters || (P.max_cycles > 0 && cycles >= P.max_cycles);
     };
     bool finished = record();
     while (!finished) {
-        if (cudaGraphLaunch(ws.exec, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+        if (cudaGraphLaunch(P.ws.exec, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
             return HPB_ERROR_CUDA;
-        count_launch(uint64_t(kernels));
+        count_launch(uint64_t(P.kernels));
         iters += hv->nsteps > 0 ? hv->nsteps : m;
         ++cycles;
         finished = record();
@@ -535,6 +574,21 @@ int solve_gmres(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int
     if (cudaGetLastError() != cudaSuccess) return HPB_ERROR_CUDA;
     return conv ? HPB_SUCCESS : HPB_ERROR_NOT_CONVERGED;
 }
+
+template <class E>
+int solve_gmres(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
+                const E* val, const RightPrec<E>& M, const E* b, E* x, hpb_solver_report* rep, double* hist, int cap,
+                int max_cycles) {
+    GmPlan<E> plan;
+    int st = plan.init(p, rows, nnz, rp, ci, val, M, b, x, max_cycles);
+    if (st != HPB_SUCCESS) return st;
+    return plan.run(rep, hist, cap);
+}
+
+template struct GmPlan<float>;
+template struct GmPlan<double>;
+template struct GmPlan<cf>;
+template struct GmPlan<cd>;
 
 #define HPB_GM_INST(E)                                                                                          \
     template int solve_gmres<E>(const hpb_solver_params*, int32_t, int64_t, const int32_t*, const int32_t*, const E*, \

@@ -109,18 +109,19 @@ int ir_solve(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* r
     const int64_t n = rows;
     const int g_ew = int(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, int64_t(sms) * 8)));
     const int g_row = (rows + 255) / 256;
+    // scratch from the solvers' pool, stream-ordered on the legacy default
+    // stream that this loop's kernels run on
     std::vector<void*> allocs;
     auto dalloc = [&](size_t bytes) -> void* {
-        void* q = nullptr;
-        if (cudaMalloc(&q, bytes ? bytes : 16) != cudaSuccess) return nullptr;
-        allocs.push_back(q);
+        void* q = pool_alloc(bytes, nullptr);
+        if (q) allocs.push_back(q);
         return q;
     };
     struct Cleanup {
         std::vector<void*>& a;
         ~Cleanup() {
-            cudaDeviceSynchronize();
-            for (void* q : a) cudaFree(q);
+            for (void* q : a) pool_free(q, nullptr);
+            cudaStreamSynchronize(nullptr);
         }
     } cleanup{allocs};
     E* r = static_cast<E*>(dalloc(size_t(n) * sizeof(E)));
@@ -139,8 +140,8 @@ int ir_solve(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* r
     int* badflag = static_cast<int*>(dalloc(64));
     double* dn = static_cast<double*>(dalloc(8 * sizeof(double)));
     if (!r || !rlo || !dlo || !partials || !ticket || !badflag || !dn) return HPB_ERROR_OUT_OF_MEMORY;
-    cudaMemset(ticket, 0, 64);
-    cudaMemset(badflag, 0, 64);
+    cudaMemsetAsync(ticket, 0, 64, nullptr);
+    cudaMemsetAsync(badflag, 0, 64, nullptr);
     auto t0 = std::chrono::steady_clock::now();
     double hn[2];
     k_ir_norm<E><<<g_ew, 256>>>(n, b, dn + 2, partials, ticket, badflag);
@@ -155,7 +156,10 @@ int ir_solve(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* r
     ip.basis = p->inner_basis;
     ip.rel_tol = p->inner_rel_tol;
     ip.abs_tol = 0.0;
-    ip.max_iters = p->inner_max_iters > 0 ? p->inner_max_iters : 10000;
+    // inner_max_iters = 0: one restart cycle per refinement for GMRES,
+    // 10000 iterations for BiCGStab(l)
+    ip.max_iters = p->inner_max_iters > 0 ? p->inner_max_iters
+                                          : (p->inner_method == HPB_SOLVER_GMRES ? std::max(1, p->inner_basis) : 10000);
     ip.precond = p->precond == HPB_PRECOND_JACOBI ? HPB_PRECOND_JACOBI : HPB_PRECOND_NONE;
     ip.high_precision = 1;
     ip.fused = 1;
@@ -169,6 +173,17 @@ int ir_solve(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* r
         M.ci = m_ci;
         M.val = m_val;
     }
+
+    // the inner solver is planned once (workspace, graph) for rlo -> dlo and
+    // re-run for every refinement
+    GmPlan<L> gm;
+    BcgPlan<L> bcg;
+    int pst = HPB_ERROR_NOT_SUPPORTED;
+    if (p->inner_method == HPB_SOLVER_GMRES)
+        pst = gm.init(&ip, rows, nnz, rp, ci, vlo, M, rlo, dlo, 0);
+    else if (p->inner_method == HPB_SOLVER_BICGSTABL)
+        pst = bcg.init(&ip, rows, nnz, rp, ci, vlo, dlo);
+    if (pst != HPB_SUCCESS) return pst;
 
     int refinements = 0, inner_iters = 0, hl = 0;
     bool conv = false, valid = true;
@@ -187,16 +202,10 @@ int ir_solve(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* r
         }
         if (conv || !valid || refinements >= p->max_refinements) break;
         k_ir_scale_down<E, L><<<g_ew, 256>>>(n, r, dn, rlo);
-        cudaMemset(dlo, 0, size_t(n) * sizeof(L));
+        cudaMemsetAsync(dlo, 0, size_t(n) * sizeof(L), nullptr);
         count_launch();
         hpb_solver_report irep{};
-        int st;
-        if (p->inner_method == HPB_SOLVER_GMRES)
-            st = solve_gmres<L>(&ip, rows, nnz, rp, ci, vlo, M, rlo, dlo, &irep, nullptr, 0, 0);
-        else if (p->inner_method == HPB_SOLVER_BICGSTABL)
-            st = solve_bicgstabl<L>(&ip, rows, nnz, rp, ci, vlo, rlo, dlo, &irep, nullptr, 0);
-        else
-            return HPB_ERROR_NOT_SUPPORTED;
+        const int st = p->inner_method == HPB_SOLVER_GMRES ? gm.run(&irep, nullptr, 0) : bcg.run(rlo, &irep, nullptr, 0);
         if (st != HPB_SUCCESS && st != HPB_ERROR_NOT_CONVERGED && st != HPB_ERROR_BREAKDOWN) return st;
         inner_iters += irep.iters;
         k_ir_update<E, L><<<g_ew, 256>>>(n, x, dlo, dn);
@@ -226,13 +235,15 @@ extern "C" {
 int hpb_ir_params_default(hpb_ir_params* p) {
     if (!p) return HPB_ERROR_INVALID_VALUE;
     *p = hpb_ir_params{};
+    // GMRES inner: one binary32 restart cycle per refinement (the binary64
+    // residual and solution replace GMRES's own at every restart)
     p->inner_method = HPB_SOLVER_GMRES;
     p->inner_basis = 50;
-    p->inner_rel_tol = 1e-5;
-    p->inner_max_iters = 5000;
+    p->inner_rel_tol = 0.0;
+    p->inner_max_iters = 0;
     p->precond = HPB_PRECOND_NONE;
     p->rel_tol = 1e-10;
-    p->max_refinements = 30;
+    p->max_refinements = 2000;
     return HPB_SUCCESS;
 }
 

@@ -325,10 +325,26 @@ reduce_kernel(int64_t n, const E* __restrict__ x, const E* __restrict__ y, void*
     // Last block: combine the per-block pairs in block order.
     __threadfence();
     W S = wzero<W>(), C = wzero<W>();
-    for (int b = threadIdx.x; b < int(gridDim.x); b += blockDim.x) {
-        W sb = ldcg_w(part + 2 * b);
-        W cb = ldcg_w(part + 2 * b + 1);
-        merge<COMP>(S, C, sb, cb);
+    {
+        // four blocks' pairs loaded before their merges; same merge order as
+        // a plain strided loop
+        const int bd = blockDim.x, nb = gridDim.x;
+        int b = threadIdx.x;
+        for (; b + 3 * bd < nb; b += 4 * bd) {
+            W sv[4], cv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                sv[u] = ldcg_w(part + 2 * (b + u * bd));
+                cv[u] = ldcg_w(part + 2 * (b + u * bd) + 1);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) merge<COMP>(S, C, sv[u], cv[u]);
+        }
+        for (; b < nb; b += bd) {
+            W sb = ldcg_w(part + 2 * b);
+            W cb = ldcg_w(part + 2 * b + 1);
+            merge<COMP>(S, C, sb, cb);
+        }
     }
     __syncthreads();  // `sh` is reused
     block_combine<COMP>(S, C, sh);

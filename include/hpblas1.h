@@ -396,19 +396,31 @@ int hpb_csr_solve_c128_host(const hpb_solver_params* p, int32_t rows, int64_t nn
                             const int32_t* col_ind, const void* val, const void* b, void* x,
                             hpb_solver_report* rep, double* history, int history_cap);
 
+/* The device-resident solvers and the refinement loop take their scratch
+ * (Krylov vectors: (l + 1) or (m + 1) vectors of n elements, plus a few)
+ * from a library-owned stream-ordered memory pool per device that keeps
+ * freed blocks for the next solve, so repeated solves neither call
+ * cudaMalloc/cudaFree nor synchronise the device.  This returns the pool's
+ * unused memory to the device (no counterpart in the reference, whose
+ * vector objects allocate and free their own buffers). */
+int hpb_solver_memory_release(void);
+
 /* ---------------------------------------------------------------------- */
 /* Mixed-precision iterative refinement (precision form; no counterpart in */
 /* the reference, whose solvers run in one precision).  Outer loop in       */
 /* binary64: r = b - A x with a compensated (Dot2) row sum, ||r|| in Dot2;  */
 /* inner correction solve in binary32 storage (complex<binary32> for        */
 /* c128) with binary32 SpMV and Dot2 reductions on the device-resident      */
-/* path; x += ||r|| d in binary64.                                          */
+/* path; x += ||r|| d in binary64.  With a GMRES inner solver and         */
+/* inner_max_iters = 0 (the default) each refinement is one binary32        */
+/* restart cycle: restarted GMRES(m) whose restart residual and solution    */
+/* are binary64, so it keeps GMRES(m)'s iteration count at binary32 cost.  */
 /* ---------------------------------------------------------------------- */
 typedef struct hpb_ir_params {
     int inner_method;       /* HPB_SOLVER_GMRES or HPB_SOLVER_BICGSTABL */
     int inner_basis;        /* m of GMRES(m) / l of BiCGStab(l) */
     double inner_rel_tol;   /* residual reduction asked of each inner solve */
-    int inner_max_iters;    /* per inner solve */
+    int inner_max_iters;    /* per inner solve; 0: one GMRES cycle / 10000 */
     int precond;            /* none, Jacobi, or HPB_PRECOND_MATRIX (GMRES only) */
     double rel_tol;         /* stop when ||b - A x|| <= rel_tol ||b|| (compensated) */
     int max_refinements;

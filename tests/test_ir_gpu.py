@@ -56,6 +56,24 @@ def test_ir_gmres_f32_inner_reaches_1e10_aniso_poisson(gpu):
     assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-6
 
 
+def test_ir_one_cycle_refinement_keeps_gmres_iteration_count(gpu):
+    """inner_max_iters = 0: each refinement is one binary32 GMRES(m) cycle with
+    binary64 restart residual and solution -- restarted GMRES(m) at binary32
+    cost; its iteration count stays within two cycles of binary64 GMRES(m)."""
+    ctx, torch = gpu
+    A = problems.poisson3d_aniso(24, eps=(1.0, 1e-2, 1e-4))
+    b = problems.rhs_uniform(A.n, 9)
+    p = _lib.ir_params("gmres", basis=30, inner_rel_tol=0.0, inner_max_iters=0, rel_tol=1e-10, max_refinements=500)
+    st, rep, x, hist = ir(torch, A, b, p, cap=600)
+    assert st == 0 and rel_res(A, b, x) <= 1.05e-10
+    assert rep.inner_iters == 30 * rep.refinements
+    p64 = _lib.solver_params("gmres", basis=30, rel_tol=1e-10, max_iters=100000, fused=True)
+    rep64 = _lib.hpb_solver_report()
+    d = [dev(torch, a) for a in (A.row_ptr, A.col_ind, A.val, b, np.zeros(A.n))]
+    assert _lib.lib.hpb_csr_solve_f64(C.byref(p64), A.n, A.nnz, *[a.data_ptr() for a in d], C.byref(rep64), None, 0) == 0
+    assert rep.inner_iters <= rep64.iters + 60, (rep.inner_iters, rep64.iters)
+
+
 def test_ir_jacobi_and_matrix_preconditioner_agree(gpu):
     ctx, torch = gpu
     A = problems.diffusion3d_lognormal(16, seed=7, sigma=2.3, corr=4.0)
