@@ -700,6 +700,20 @@ def cpu_baseline_dot2():
             "sample": f"{tot} sequential Dot2 calls (n=2^20), ~5 s"}
 
 
+def profile_solve(torch, max_iters):
+    """One fused BiCGStab(4) solve of the solver workload capped at
+    max_iters iterations (a short, complete run of the hot path for ncu)."""
+    import ctypes as C
+    from high_precision_blas1_b200 import _lib
+    A, b = solver_problem(0)
+    d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (A.row_ptr, A.col_ind, A.val, b, np.zeros(A.n))]
+    p = _lib.solver_params("bicgstabl", basis=SOLVER_L, rel_tol=SOLVER_TOL, max_iters=max_iters, fused=True)
+    rep = _lib.hpb_solver_report()
+    st = _lib.lib.hpb_csr_solve_f64(C.byref(p), A.n, A.nnz, *[a.data_ptr() for a in d], C.byref(rep), None, 0)
+    torch.cuda.synchronize()
+    print(f"profile solve: status {st}, iterations {rep.iters}, relative residual {rep.resid_norm / rep.rhs_norm:.3e}")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -710,6 +724,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", action="store_true", help="time the plain drop-in solver path instead of the fused one")
     ap.add_argument("--no-forms", action="store_true", help="skip the precision / complex / learned-preconditioner runs")
+    ap.add_argument("--profile-solve", type=int, default=0, metavar="K",
+                    help="profiling aid: run one fused solve of the solver workload capped at K iterations, "
+                         "print its report and exit (no bench line)")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 200 if args.workload == "dot2" else 3
@@ -723,6 +740,9 @@ def main():
         return
 
     import torch
+    if args.profile_solve > 0:
+        profile_solve(torch, args.profile_solve)
+        return
     dist = None
     if ws > 1:
         import datetime
