@@ -235,6 +235,36 @@ def solver_config():
 
 
 # ------------------------------------------------------------------ our arm
+def dot2_by_n(torch, L, ctx):
+    """Dot2 f64 throughput by length, back-to-back calls over pairs rotated
+    so each call reads from HBM (working set > L2)."""
+    hbm, _ = peaks()
+    res = {}
+    for lg in (20, 22, 24, 26):
+        n = 1 << lg
+        R = max(2, int(np.ceil(2.0 * L2_BYTES / (16.0 * n))))
+        g = torch.Generator(device="cuda").manual_seed(lg)
+        xs = [torch.rand(n, dtype=torch.float64, device="cuda", generator=g) for _ in range(R)]
+        ys = [torch.rand(n, dtype=torch.float64, device="cuda", generator=g) for _ in range(R)]
+        out = torch.zeros(4, dtype=torch.float64, device="cuda")
+        reps = max(20, min(400, int(4e9 / (16 * n))))
+        for i in range(4):
+            ctx.check(L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(), out.data_ptr()))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for i in range(reps):
+            ctx.check(L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(), out.data_ptr()))
+        e1.record()
+        torch.cuda.synchronize()
+        us = e0.elapsed_time(e1) * 1e3 / reps
+        gbs = 16.0 * n / (us * 1e-6) / 1e9
+        res[str(n)] = {"us_per_call": us, "GB/s": gbs, "frac_of_hbm": gbs / hbm}
+        del xs, ys
+    return res
+
+
 def bench_dot2(args, ws, rank, local, torch, dist):
     from high_precision_blas1_b200 import Context, _lib
     L = _lib.lib
@@ -256,22 +286,33 @@ def bench_dot2(args, ws, rank, local, torch, dist):
         torch.cuda.synchronize()
         clk = ClockSampler(local)
         clk.start()
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        # back-to-back calls (the kernels overlap launch and drain through
+        # programmatic dependent launch); per-launch time = total / steps
         t_all0 = torch.cuda.Event(enable_timing=True)
         t_all1 = torch.cuda.Event(enable_timing=True)
         launches0 = L.hpb_launch_count()
         t_all0.record(stream)
         for i in range(args.steps):
-            evs[i][0].record(stream)
             ctx.check(L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(),
                                      out.data_ptr() + 32 * (i % 8)))
-            evs[i][1].record(stream)
         t_all1.record(stream)
         torch.cuda.synchronize()
         launches = L.hpb_launch_count() - launches0
         clocks = clk.stop()
         total_ms = t_all0.elapsed_time(t_all1)
-        per_launch_ms = [a.elapsed_time(b) for a, b in evs]
+        per_launch_ms = [total_ms / args.steps]
+        # one isolated launch (events on both sides), for the cold single-call latency
+        i0 = torch.cuda.Event(enable_timing=True)
+        i1 = torch.cuda.Event(enable_timing=True)
+        iso = []
+        for i in range(10):
+            torch.cuda.synchronize()
+            i0.record(stream)
+            ctx.check(L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(), out.data_ptr()))
+            i1.record(stream)
+            torch.cuda.synchronize()
+            iso.append(i0.elapsed_time(i1))
+        by_n = dot2_by_n(torch, L, ctx)
         if dist:
             tt = torch.tensor([total_ms], device="cuda")
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -315,7 +356,8 @@ def bench_dot2(args, ws, rank, local, torch, dist):
         "roofline": {"kernel": "reduce_kernel<double,DOT2>", "bound": "hbm", "achieved": achieved, "peak": hbm,
                      "peak_source": src, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": None, "algorithmic_bytes_per_launch": bytes_step,
-                     "avg_launch_us": kern_ms * 1e3},
+                     "avg_launch_us": kern_ms * 1e3, "isolated_launch_us": float(np.median(iso)) * 1e3},
+        "by_n": by_n,
         "e2e": {"value": bytes_step * args.steps / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s",
                 "h2d_bytes_per_step": int(2 * 8 * n), "d2h_bytes_per_step": 32},
         "gpu_launches": int(launches),
@@ -653,7 +695,8 @@ def dot2_probe(torch, L, ctx, reps=200):
     hbm, src = peaks()
     gbs = 16.0 * n / (us * 1e-6) / 1e9
     return {"workload": "dot2 f64 GenDot n=1048576 cond~1e20, 16 pairs rotated (268 MB > L2)",
-            "value": gbs, "unit": "GB/s", "us_per_call": us, "frac_of_hbm": gbs / hbm, "peak_source": src}
+            "value": gbs, "unit": "GB/s", "us_per_call": us, "frac_of_hbm": gbs / hbm, "peak_source": src,
+            "by_n": dot2_by_n(torch, L, ctx)}
 
 
 def cpu_baseline_solver(t_gpu_iters):

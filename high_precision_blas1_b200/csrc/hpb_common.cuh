@@ -11,6 +11,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <utility>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -32,6 +33,37 @@ struct hpb_context {
 };
 
 namespace hpb {
+
+// ------------------------------------------------ programmatic dependent launch
+// Library kernels are launched with programmatic stream serialisation
+// (launch_pdl): a kernel may be scheduled while its predecessor on the
+// stream drains, hiding the launch gap between back-to-back kernels.  Each
+// such kernel calls pdl_enter() first: it waits until the predecessor grid
+// has completed and its memory is visible
+// (griddepcontrol.wait) -- so nothing is read early -- and then lets its own
+// successor be scheduled (griddepcontrol.launch_dependents).  Launched
+// normally, the wait returns at once.
+__device__ __forceinline__ void pdl_enter() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+    cudaGridDependencySynchronize();
+    cudaTriggerProgrammaticLaunchCompletion();
+#endif
+}
+
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(cudaStream_t s, int grid, int block, void (*kernel)(KArgs...), Args&&... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(unsigned(block));
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 extern std::atomic<uint64_t> g_launches;
 

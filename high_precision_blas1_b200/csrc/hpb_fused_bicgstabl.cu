@@ -125,16 +125,17 @@ k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
            EpiArgs<typename scalar_of<E>::type> ea) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
-    // one thread per row: streaming loads of the row's values and indices,
-    // x through the read-only path (the library SpMV's layout)
-    const int32_t r = blockIdx.x * kThreads + threadIdx.x;
-    S acc = s_zero(S{});
-    if (r < rows) {
-        const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
-        for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ldcsE(val, k)), to_s(ldgE(x, ldcsI(ci, k))), acc);
-    }
+    // rows in a grid-stride loop, consecutive threads on consecutive rows:
+    // streaming loads of the values and indices, x through the read-only
+    // path.  Launched with one row per thread without the dot; with it, on
+    // 6 blocks per SM (B200, 1024^2: 20.5 us against 26.7 us for one row
+    // per thread, whose 4096 blocks each hold their warps at the merge).
     A dacc[1];
-    if (r < rows) {
+    const int32_t stride = gridDim.x * kThreads;
+    for (int32_t r = blockIdx.x * kThreads + threadIdx.x; r < rows; r += stride) {
+        const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
+        S acc = s_zero(S{});
+        for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ldcsE(val, k)), to_s(ldgE(x, ldcsI(ci, k))), acc);
         if (diag) acc = s_div(acc, to_s(ldE(diag, r)));
         E out = from_s<E>(acc);
         stE(y, r, out);
@@ -395,10 +396,8 @@ inline int occupancy_of(const void* f) {
 
 template <class E>
 int light_occupancy() {
-    int occ = occupancy_of(reinterpret_cast<const void*>(k_upd_u<E>));
-    occ = std::min(occ, occupancy_of(reinterpret_cast<const void*>(k_upd_rx<E>)));
-    occ = std::min(occ, occupancy_of(reinterpret_cast<const void*>(k_norm<E>)));
-    return occ;
+    return std::min(occupancy_of(reinterpret_cast<const void*>(k_upd_u<E>)),
+                    occupancy_of(reinterpret_cast<const void*>(k_upd_rx<E>)));
 }
 
 template <class E>
@@ -439,10 +438,10 @@ void launch_mgs_step(int nd, int grid, cudaStream_t s, int64_t n, int k, const V
                      typename acc_of<typename scalar_of<E>::type>::type* partials,
                      EpiArgs<typename scalar_of<E>::type> ea) {
     using S = typename scalar_of<E>::type;
-#define HPB_STEP(ND)                                                        \
-    case ND:                                                                \
-        k_mgs_step<E, ND><<<grid, kThreads, 0, s>>>(n, k, V, st, partials); \
-        k_mgs_finish<S, ND><<<1, kThreads, 0, s>>>(grid, partials, ea);     \
+#define HPB_STEP(ND)                                                                         \
+    case ND:                                                                                 \
+        k_mgs_step<E, ND><<<grid, kThreads, 0, s>>>(n, k, V, st, partials);                  \
+        k_mgs_finish<S, ND><<<1, kThreads, 0, s>>>(grid, partials, ea);                      \
         break;
     switch (nd) {
         HPB_STEP(2) HPB_STEP(3) HPB_STEP(4) HPB_STEP(5) HPB_STEP(6) HPB_STEP(7) HPB_STEP(8) HPB_STEP(9)
@@ -463,7 +462,7 @@ struct BcgPlan<E>::Impl {
     const int32_t *rp = nullptr, *ci = nullptr;
     const E* val = nullptr;
     E* x = nullptr;
-    int g_ew = 1, g_red = 1, g_sp = 1, kernels = 0;
+    int g_ew = 1, g_red = 1, g_sp = 1, g_spd = 1, g_nrm = 1, kernels = 0;
     SolverWorkspace ws;
     Vecs<E> V{};
     E *rt = nullptr, *tmp = nullptr, *diag = nullptr;
@@ -516,7 +515,10 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     P.g_ew = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * light_occupancy<E>())));
     P.g_red = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * reduction_occupancy<E>(L))));
     P.g_sp = int(std::max<int64_t>(1, need));
-    const int g_ew = P.g_ew, g_red = P.g_red, g_sp = P.g_sp;
+    P.g_spd = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * 6)));
+    P.g_nrm = int(std::max<int64_t>(
+        1, std::min<int64_t>(need, int64_t(sms) * occupancy_of(reinterpret_cast<const void*>(k_norm<E>)))));
+    const int g_ew = P.g_ew, g_red = P.g_red, g_sp = P.g_sp, g_spd = P.g_spd;
     SolverWorkspace& ws = P.ws;
     Vecs<E>& V = P.V;
     const size_t vb = size_t(n) * sizeof(E);
@@ -537,10 +539,9 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     P.st = static_cast<BcgState<S>*>(ws.alloc(sizeof(BcgState<S>)));
     P.drep = static_cast<Report*>(ws.alloc(sizeof(Report)));
     // block partials: ND dots x grid blocks for the largest producer -- the
-    // SpMV+Dot2 (1 x g_sp), the norms (1 x g_ew), the closing update
+    // SpMV+Dot2 (1 x g_spd), the norms (1 x g_nrm), the closing update
     // (2 x g_red) and the first MGS sweep (L + 1 x g_red)
-    const size_t npart =
-        std::max<size_t>(std::max<size_t>(size_t(g_sp), size_t(g_ew)), size_t(L + 1) * size_t(g_red));
+    const size_t npart = std::max<size_t>(std::max<size_t>(size_t(g_spd), size_t(P.g_nrm)), size_t(L + 1) * size_t(g_red));
     P.partials = static_cast<A*>(ws.alloc(npart * sizeof(A)));
     P.ticket = static_cast<unsigned int*>(ws.alloc(64));
     P.badflag = static_cast<int*>(ws.alloc(64));
@@ -570,13 +571,13 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HPB_ERROR_CUDA;
     for (int j = 0; j < L; ++j) {
         k_upd_u<E><<<g_ew, kThreads, 0, s>>>(n, j, V, st);
-        k_spmv_dot<E, true><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt, partials,
-                                                      ticket, badflag, EpiArgs<S>{st, drep, EPI_ALPHA, 0, j, L});
+        k_spmv_dot<E, true><<<g_spd, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt, partials,
+                                                       ticket, badflag, EpiArgs<S>{st, drep, EPI_ALPHA, 0, j, L});
         k_upd_rx<E><<<g_ew, kThreads, 0, s>>>(n, j, V, x, st);
         if (j + 1 < L)
-            k_spmv_dot<E, true><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.r[j], V.r[j + 1], rt,
-                                                          partials, ticket, badflag,
-                                                          EpiArgs<S>{st, drep, EPI_BETA, 0, j, L});
+            k_spmv_dot<E, true><<<g_spd, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.r[j], V.r[j + 1], rt,
+                                                           partials, ticket, badflag,
+                                                           EpiArgs<S>{st, drep, EPI_BETA, 0, j, L});
         else
             k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.r[j], V.r[j + 1], nullptr,
                                                            partials, ticket, badflag, none);
@@ -625,12 +626,12 @@ int BcgPlan<E>::run(const E* b, hpb_solver_report* rep, double* hist, int cap) {
         k_scale_inv<E><<<g_ew, kThreads, 0, s>>>(n, b, P.diag, P.tmp);
         pb = P.tmp;
     }
-    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, pb, P.dnorm, P.partials, P.ticket, P.badflag);
+    k_norm<E><<<P.g_nrm, kThreads, 0, s>>>(n, pb, P.dnorm, P.partials, P.ticket, P.badflag);
     // r0 = P (b - A x), rt = r0 / ||r0||
     k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, P.rp, P.ci, P.val, nullptr, x, P.tmp, nullptr, P.partials,
                                                    P.ticket, P.badflag, none);
     k_residual_finish<E><<<g_ew, kThreads, 0, s>>>(n, b, P.tmp, P.diag, V.r[0]);
-    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[0], P.dnorm + 1, P.partials, P.ticket, P.badflag);
+    k_norm<E><<<P.g_nrm, kThreads, 0, s>>>(n, V.r[0], P.dnorm + 1, P.partials, P.ticket, P.badflag);
     k_scale_by_inv_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[0], P.dnorm + 1, P.rt);
     // ||r0||, <rt, r0>, finiteness of x, and the first cycle's beta / rho
     launch_final<E>(L, P.g_red, s, n, 0, V, x, P.rt, P.st, P.partials, P.ticket, P.badflag,
@@ -675,8 +676,8 @@ int BcgPlan<E>::run(const E* b, hpb_solver_report* rep, double* hist, int cap) {
     k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, P.rp, P.ci, P.val, nullptr, x, P.tmp, nullptr, P.partials,
                                                    P.ticket, P.badflag, none);
     k_residual_finish<E><<<g_ew, kThreads, 0, s>>>(n, b, P.tmp, nullptr, V.r[1]);
-    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[1], P.dnorm + 2, P.partials, P.ticket, P.badflag);
-    k_norm<E><<<g_ew, kThreads, 0, s>>>(n, b, P.dnorm + 3, P.partials, P.ticket, P.badflag);
+    k_norm<E><<<P.g_nrm, kThreads, 0, s>>>(n, V.r[1], P.dnorm + 2, P.partials, P.ticket, P.badflag);
+    k_norm<E><<<P.g_nrm, kThreads, 0, s>>>(n, b, P.dnorm + 3, P.partials, P.ticket, P.badflag);
     cudaMemcpyAsync(hnorm + 2, P.dnorm + 2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (cudaStreamSynchronize(s) != cudaSuccess) return HPB_ERROR_CUDA;
     count_launch(4);

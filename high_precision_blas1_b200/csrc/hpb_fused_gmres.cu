@@ -360,6 +360,23 @@ struct GmHostView {
     double bnorm;
 };
 
+// Blocks per SM of the restart cycle's streaming kernels (the least of them):
+// their grid is one resident wave.
+template <class E>
+int gm_occupancy() {
+    auto occ = [](const void* f) {
+        int o = 0;
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, kGmThreads, 0) == cudaSuccess && o > 0 ? o : 1;
+    };
+    int o = occ(reinterpret_cast<const void*>(k_gs_update<E, false>));
+    o = std::min(o, occ(reinterpret_cast<const void*>(k_gs_update<E, true>)));
+    o = std::min(o, occ(reinterpret_cast<const void*>(k_gm_scale<E>)));
+    o = std::min(o, occ(reinterpret_cast<const void*>(k_gm_jacobi<E>)));
+    o = std::min(o, occ(reinterpret_cast<const void*>(k_gm_start<E>)));
+    o = std::min(o, occ(reinterpret_cast<const void*>(k_gm_norm<E>)));
+    return o;
+}
+
 template <class E>
 struct GmPlan<E>::Impl {
     using S = typename scalar_of<E>::type;
@@ -417,8 +434,8 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     P.b = b;
     P.x = x;
     const int64_t n = rows;
-    const int g_ew = P.g_ew =
-        int(std::max<int64_t>(1, std::min<int64_t>((n + kGmThreads - 1) / kGmThreads, int64_t(sms) * 8)));
+    const int g_ew = P.g_ew = int(
+        std::max<int64_t>(1, std::min<int64_t>((n + kGmThreads - 1) / kGmThreads, int64_t(sms) * gm_occupancy<E>())));
     const int g_md = P.g_md = int(std::max<int64_t>(1, std::min<int64_t>((n + 4095) / 4096, int64_t(sms) * 2)));
     const int g_sp = P.g_sp = int(std::max<int64_t>(1, (int64_t(rows) + kGmThreads - 1) / kGmThreads));
     SolverWorkspace& ws = P.ws;

@@ -265,6 +265,7 @@ reduce_kernel(int64_t n, const E* __restrict__ x, const E* __restrict__ y, void*
     using W = typename T::Wide;
     constexpr bool COMP = op_is_comp(OP);
     constexpr int K = VEC ? VecOf<E>::k : 1;
+    pdl_enter();  // inputs and the ticket are read only after the previous kernel on the stream completed
 
     Acc s{}, c{};
     const int64_t gtid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -406,12 +407,13 @@ int launch_reduce(hpb_context* ctx, int64_t n, const E* x, const E* y, double* o
         int grid = grid_for(ctx, work, kRedThreads, 1 << 20);
         int cap = max_blocks_for<E, OP, true>(ctx);
         if (grid > cap) grid = cap;
-        reduce_kernel<E, OP, true><<<grid, kRedThreads, 0, ctx->stream>>>(n, x, y, ctx->partials, ctx->ticket, out);
+        launch_pdl(ctx->stream, grid, kRedThreads, reduce_kernel<E, OP, true>, n, x, y, ctx->partials, ctx->ticket, out);
     } else {
         int grid = grid_for(ctx, work, kRedThreads, 1 << 20);
         int cap = max_blocks_for<E, OP, false>(ctx);
         if (grid > cap) grid = cap;
-        reduce_kernel<E, OP, false><<<grid, kRedThreads, 0, ctx->stream>>>(n, x, y, ctx->partials, ctx->ticket, out);
+        launch_pdl(ctx->stream, grid, kRedThreads, reduce_kernel<E, OP, false>, n, x, y, ctx->partials, ctx->ticket,
+                   out);
     }
     count_launch();
     return check_launch(ctx, name);

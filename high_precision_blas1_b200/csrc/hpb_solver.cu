@@ -160,18 +160,21 @@ template <class T>
 int solve_host(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
                const T* val, const T* b, T* x, hpb_solver_report* rep, double* hist, int cap) {
     if (rows < 0 || nnz < 0) return HPB_ERROR_INVALID_VALUE;
-    void *d_rp = nullptr, *d_ci = nullptr, *d_val = nullptr, *d_b = nullptr, *d_x = nullptr;
-    auto cleanup = [&]() {
-        cudaFree(d_rp);
-        cudaFree(d_ci);
-        cudaFree(d_val);
-        cudaFree(d_b);
-        cudaFree(d_x);
-    };
+    // device copies from the solvers' memory pool, stream-ordered on the
+    // legacy default stream (no cudaMalloc/cudaFree per call)
+    using hpb::fused::pool_alloc;
+    using hpb::fused::pool_free;
     const size_t n = size_t(rows);
-    if (cudaMalloc(&d_rp, (n + 1) * 4) != cudaSuccess || cudaMalloc(&d_ci, size_t(nnz ? nnz : 1) * 4) != cudaSuccess ||
-        cudaMalloc(&d_val, size_t(nnz ? nnz : 1) * sizeof(T)) != cudaSuccess ||
-        cudaMalloc(&d_b, (n ? n : 1) * sizeof(T)) != cudaSuccess || cudaMalloc(&d_x, (n ? n : 1) * sizeof(T)) != cudaSuccess) {
+    void* d_rp = pool_alloc((n + 1) * 4, nullptr);
+    void* d_ci = pool_alloc(size_t(nnz ? nnz : 1) * 4, nullptr);
+    void* d_val = pool_alloc(size_t(nnz ? nnz : 1) * sizeof(T), nullptr);
+    void* d_b = pool_alloc((n ? n : 1) * sizeof(T), nullptr);
+    void* d_x = pool_alloc((n ? n : 1) * sizeof(T), nullptr);
+    auto cleanup = [&]() {
+        for (void* q : {d_rp, d_ci, d_val, d_b, d_x}) pool_free(q, nullptr);
+        cudaStreamSynchronize(nullptr);
+    };
+    if (!d_rp || !d_ci || !d_val || !d_b || !d_x) {
         cleanup();
         return HPB_ERROR_OUT_OF_MEMORY;
     }
