@@ -743,14 +743,21 @@ def cpu_baseline_dot2():
             "sample": f"{tot} sequential Dot2 calls (n=2^20), ~5 s"}
 
 
-def profile_solve(torch, max_iters):
-    """One fused BiCGStab(4) solve of the solver workload capped at
-    max_iters iterations (a short, complete run of the hot path for ncu)."""
+def profile_solve(torch, max_iters, method="bicgstabl"):
+    """One fused solve capped at max_iters iterations (a short, complete run
+    of the hot path for ncu): BiCGStab(4) on the config-2 system, or
+    GMRES(30) + Jacobi on the config-5 system."""
     import ctypes as C
-    from high_precision_blas1_b200 import _lib
-    A, b = solver_problem(0)
+    from high_precision_blas1_b200 import _lib, spai, problems
+    if method == "gmres":
+        A = spai.family(96, seed=424242)
+        b = problems.rhs_uniform(A.n, 505)
+        p = _lib.solver_params("gmres", basis=30, rel_tol=SOLVER_TOL, max_iters=max_iters, precond="jacobi",
+                               fused=True)
+    else:
+        A, b = solver_problem(0)
+        p = _lib.solver_params("bicgstabl", basis=SOLVER_L, rel_tol=SOLVER_TOL, max_iters=max_iters, fused=True)
     d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (A.row_ptr, A.col_ind, A.val, b, np.zeros(A.n))]
-    p = _lib.solver_params("bicgstabl", basis=SOLVER_L, rel_tol=SOLVER_TOL, max_iters=max_iters, fused=True)
     rep = _lib.hpb_solver_report()
     st = _lib.lib.hpb_csr_solve_f64(C.byref(p), A.n, A.nnz, *[a.data_ptr() for a in d], C.byref(rep), None, 0)
     torch.cuda.synchronize()
@@ -770,6 +777,9 @@ def main():
     ap.add_argument("--profile-solve", type=int, default=0, metavar="K",
                     help="profiling aid: run one fused solve of the solver workload capped at K iterations, "
                          "print its report and exit (no bench line)")
+    ap.add_argument("--profile-method", choices=["bicgstabl", "gmres"], default="bicgstabl",
+                    help="with --profile-solve: BiCGStab(4) on the config-2 system, or GMRES(30) + Jacobi on the "
+                         "config-5 lognormal 96^3 system")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 200 if args.workload == "dot2" else 3
@@ -784,7 +794,7 @@ def main():
 
     import torch
     if args.profile_solve > 0:
-        profile_solve(torch, args.profile_solve)
+        profile_solve(torch, args.profile_solve, args.profile_method)
         return
     dist = None
     if ws > 1:

@@ -63,6 +63,27 @@ def oro():
     return _ORO
 
 
+_REF_GPU = None
+
+
+def ref_gpu():
+    """The reference's own GPU compensated reductions (built for sm_100a), or
+    None if _ref was not built.  Needs a CUDA device at call time."""
+    global _REF_GPU
+    if _REF_GPU is None:
+        so = HERE / "_ref" / "libhpb_ref_gpu.so"
+        if not so.exists():
+            return None
+        lib = C.CDLL(str(so))
+        for name, args in (("ref_gpu_dot2_f64", [I64, P, P, P]), ("ref_gpu_sum2_f64", [I64, P, P]),
+                           ("ref_gpu_dot2_c128", [I64, P, P, P])):
+            f = getattr(lib, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        _REF_GPU = lib
+    return _REF_GPU
+
+
 def ref():
     """The reference's own CPU reductions, or None if _ref was not built."""
     global _REF

@@ -227,3 +227,45 @@ def test_inf_nan_propagate(gpu):
     x[517] = np.nan
     o = red(ctx, "sum2", dev(torch, x))
     assert np.isnan(o[0])
+
+
+@pytest.mark.parametrize("n", [1001, 65537, 1 << 20, (1 << 20) + 3])
+def test_dot2_sum2_match_reference_gpu_kernels(gpu, n):
+    """Against the reference's own GPU Ogita kernels (gpu_reduction_ogita,
+    built for sm_100a into oracle/_ref) on the same device data: both within
+    the compensated bound of the exact value, and within 2 ulp of each other
+    where the condition number is <= 1e8 (n stays below the size at which
+    the reference's in-place later passes race)."""
+    rg = oracle.ref_gpu()
+    if rg is None:
+        pytest.skip("reference GPU reductions not built")
+    ctx, torch = gpu
+    rng = np.random.default_rng(n)
+    cases = [(rng.standard_normal(n), rng.standard_normal(n))]
+    if n >= 65537:
+        cases.append(gendot(29, n, 1e16))
+    for x, y in cases:
+        xd, yd = dev(torch, x), dev(torch, y)
+        ours = red(ctx, "dot2", xd, yd)
+        theirs = np.zeros(2)
+        assert rg.ref_gpu_dot2_f64(n, xd.data_ptr(), yd.data_ptr(), theirs.ctypes.data) == 0
+        torch.cuda.synchronize()
+        hi, _ = oracle.exact_dot(x, y)
+        cond = oracle.condition_dot(x, y)
+        bound = oracle.bound_dot2(n, cond) * abs(hi) + 2 * ulp(hi)
+        assert abs(ours[0] - hi) <= bound and abs(theirs[0] - hi) <= bound
+        if cond <= 1e8:
+            assert abs(ours[0] - theirs[0]) <= 2 * ulp(theirs[0]), (ours[0], theirs[0])
+    # Sum2
+    x = rng.standard_normal(n) * np.exp2(rng.integers(-30, 30, n))
+    xd = dev(torch, x)
+    ours = red(ctx, "sum2", xd)
+    theirs = np.zeros(1)
+    assert rg.ref_gpu_sum2_f64(n, xd.data_ptr(), theirs.ctypes.data) == 0
+    torch.cuda.synchronize()
+    hi, _ = oracle.exact_sum(x)
+    scale = float(np.sum(np.abs(x)))
+    bound = oracle.bound_sum2(n, scale / abs(hi)) * abs(hi) + 2 * ulp(hi)
+    assert abs(ours[0] - hi) <= bound and abs(theirs[0] - hi) <= bound
+    if scale / abs(hi) <= 1e8:
+        assert abs(ours[0] - theirs[0]) <= 2 * ulp(theirs[0])
