@@ -101,6 +101,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(torch, dist, value, device):
+    """The largest of each rank's value (the job's time is its slowest
+    replica); every rank takes this collective at the same point."""
+    if dist is None:
+        return value
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_init(args):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -313,10 +323,7 @@ def bench_dot2(args, ws, rank, local, torch, dist):
             torch.cuda.synchronize()
             iso.append(i0.elapsed_time(i1))
         by_n = dot2_by_n(torch, L, ctx)
-        if dist:
-            tt = torch.tensor([total_ms], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            total_ms = tt.item()
+        total_ms = max_over_ranks(torch, dist, total_ms, "cuda")
 
         # e2e: pinned host inputs -> H2D -> Dot2 -> D2H of (hi, lo), every step
         hx = torch.from_numpy(x).pin_memory()
@@ -482,10 +489,7 @@ def bench_solver(args, ws, rank, local, torch, dist):
     clocks = clk.stop()
     times = [a.elapsed_time(bb) * 1e-3 for a, bb in evs]
     t_step = float(np.mean(times))
-    if dist:
-        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_step = tt.item()
+    t_step = max_over_ranks(torch, dist, t_step, "cuda")
     # the plain drop-in path (host-synchronised reductions) on the same system, for comparison
     plain = None
     if not args.plain:
@@ -777,6 +781,8 @@ def main():
     ap.add_argument("--profile-solve", type=int, default=0, metavar="K",
                     help="profiling aid: run one fused solve of the solver workload capped at K iterations, "
                          "print its report and exit (no bench line)")
+    ap.add_argument("--profile-spmv-dot2", type=int, default=0, metavar="K",
+                    help="profiling aid: K launches of hpb_csr_spmv_dot2_f64 on the config-2 matrix, then exit")
     ap.add_argument("--profile-method", choices=["bicgstabl", "gmres"], default="bicgstabl",
                     help="with --profile-solve: BiCGStab(4) on the config-2 system, or GMRES(30) + Jacobi on the "
                          "config-5 lognormal 96^3 system")
@@ -795,6 +801,13 @@ def main():
     import torch
     if args.profile_solve > 0:
         profile_solve(torch, args.profile_solve, args.profile_method)
+        return
+    if args.profile_spmv_dot2 > 0:
+        from high_precision_blas1_b200 import Context, _lib
+        A, _ = solver_problem(0)
+        with Context(0, torch.cuda.current_stream().cuda_stream) as ctx:
+            r = spmv_roofline(torch, _lib.lib, ctx, A, reps=args.profile_spmv_dot2)
+        print(f"profile spmv+dot2: {r['avg_launch_us']:.2f} us per launch")
         return
     dist = None
     if ws > 1:

@@ -177,6 +177,63 @@ __device__ __forceinline__ A merge_partials(const A* p, int nb) {
     return t;
 }
 
+// Per-thread accumulators by storage type.  binary32 storage (float,
+// complex<float>) accumulates each thread's Dot2 in binary32 -- TwoProd by
+// fmaf, TwoSum in binary32, the reference's own f32 arithmetic -- and is
+// widened to binary64 only for the block and cross-block combines; binary64
+// storage accumulates in binary64.  (On B200 binary64 issues at a small
+// fraction of binary32's rate; a multi-dot over K basis vectors spends
+// about ten operations per element and vector in the error-free
+// transformations, which in binary64 would bound a binary32 inner solve by
+// arithmetic instead of memory.)
+struct Acc2f {
+    float s = 0.f, c = 0.f;
+};
+struct AccCf {
+    cf s{0.f, 0.f}, c{0.f, 0.f};
+};
+template <class E> struct pacc_of;
+template <> struct pacc_of<float> { using type = Acc2f; };
+template <> struct pacc_of<double> { using type = Acc2; };
+template <> struct pacc_of<cf> { using type = AccCf; };
+template <> struct pacc_of<cd> { using type = AccC; };
+
+__device__ __forceinline__ void pdot_add(Acc2f& a, float x, float y) {
+    float t, e;
+    const float p = two_prod(x, y, t);
+    a.s = two_sum(a.s, p, e);
+    a.c = add_rn(a.c, add_rn(t, e));
+}
+__device__ __forceinline__ void pdot_add(AccCf& a, cf x, cf y) {  // conj(x) * y
+    float tR1, tR2, tI1, tI2, t1, t2, e;
+    const float pR1 = two_prod(x.re, y.re, tR1);
+    const float pR2 = two_prod(x.im, y.im, tR2);
+    const float pI1 = two_prod(x.re, y.im, tI1);
+    const float pI2 = two_prod(-x.im, y.re, tI2);
+    const float pR = two_sum(pR1, pR2, t1);
+    const float pI = two_sum(pI1, pI2, t2);
+    a.s.re = two_sum(a.s.re, pR, e);
+    a.c.re = add_rn(a.c.re, add_rn(add_rn(add_rn(tR1, tR2), t1), e));
+    a.s.im = two_sum(a.s.im, pI, e);
+    a.c.im = add_rn(a.c.im, add_rn(add_rn(add_rn(tI1, tI2), t2), e));
+}
+__device__ __forceinline__ void pdot_add(Acc2& a, double x, double y) { dot_add(a, x, y); }
+__device__ __forceinline__ void pdot_add(AccC& a, cd x, cd y) { dot_add(a, x, y); }
+__device__ __forceinline__ Acc2 widen_acc(const Acc2f& a) {
+    Acc2 r;
+    r.s = double(a.s);
+    r.c = double(a.c);
+    return r;
+}
+__device__ __forceinline__ AccC widen_acc(const AccCf& a) {
+    AccC r;
+    r.s = cd{double(a.s.re), double(a.s.im)};
+    r.c = cd{double(a.c.re), double(a.c.im)};
+    return r;
+}
+__device__ __forceinline__ Acc2 widen_acc(const Acc2& a) { return a; }
+__device__ __forceinline__ AccC widen_acc(const AccC& a) { return a; }
+
 // Block-wide merge of ND accumulators (result valid in thread 0).
 template <int ND, class A>
 __device__ __forceinline__ void block_merge(A (&acc)[ND], A* sh /* [ND][32] */) {

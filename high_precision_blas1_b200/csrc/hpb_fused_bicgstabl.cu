@@ -130,7 +130,7 @@ k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
     // path.  Launched with one row per thread without the dot; with it, on
     // 6 blocks per SM (B200, 1024^2: 20.5 us against 26.7 us for one row
     // per thread, whose 4096 blocks each hold their warps at the merge).
-    A dacc[1];
+    typename pacc_of<E>::type pacc;
     const int32_t stride = gridDim.x * kThreads;
     for (int32_t r = blockIdx.x * kThreads + threadIdx.x; r < rows; r += stride) {
         const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
@@ -139,9 +139,12 @@ k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
         if (diag) acc = s_div(acc, to_s(ldE(diag, r)));
         E out = from_s<E>(acc);
         stE(y, r, out);
-        if (DOT) dot_add(dacc[0], to_s(ldE(w, r)), to_s(out));
+        if (DOT) pdot_add(pacc, ldE(w, r), out);
     }
-    if (DOT) grid_finish<1>(dacc, false, partials, ticket, badflag, [&](const S* v, bool bad) { run_epi(ea, v, bad); });
+    if (DOT) {
+        A dacc[1] = {widen_acc(pacc)};
+        grid_finish<1>(dacc, false, partials, ticket, badflag, [&](const S* v, bool bad) { run_epi(ea, v, bad); });
+    }
 }
 
 // ------------------------------------------------------------ BiCG updates
@@ -202,13 +205,13 @@ k_mgs_step(int64_t n, int k, Vecs<E> V, const BcgState<typename scalar_of<E>::ty
     for (int i = 0; i < NV; ++i) ntau[i] = upd ? s_neg(st->tau[k - 1][k + i]) : s_zero(S{});
     const E* rprev = upd ? V.r[k - 1] : nullptr;
     const E* r0 = V.r[0];
-    A acc[ND];
+    typename pacc_of<E>::type pacc[ND];
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
         E ve[NV];
 #pragma unroll
         for (int i = 0; i < NV; ++i) ve[i] = ldE(V.r[k + i], q);
-        const S z = to_s(ldE(r0, q));
+        const E z = ldE(r0, q);
         if (upd) {
             const S pv = to_s(ldE(rprev, q));
 #pragma unroll
@@ -217,14 +220,14 @@ k_mgs_step(int64_t n, int k, Vecs<E> V, const BcgState<typename scalar_of<E>::ty
                 stE(V.r[k + i], q, ve[i]);
             }
         }
-        S v[NV];
+        pdot_add(pacc[0], ve[0], ve[0]);
+        pdot_add(pacc[1], ve[0], z);
 #pragma unroll
-        for (int i = 0; i < NV; ++i) v[i] = to_s(ve[i]);
-        dot_add(acc[0], v[0], v[0]);
-        dot_add(acc[1], v[0], z);
-#pragma unroll
-        for (int i = 1; i < NV; ++i) dot_add(acc[1 + i], v[0], v[i]);
+        for (int i = 1; i < NV; ++i) pdot_add(pacc[1 + i], ve[0], ve[i]);
     }
+    A acc[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) acc[d] = widen_acc(pacc[d]);
     block_merge<ND>(acc, sh);
     if (threadIdx.x == 0)
 #pragma unroll
@@ -267,7 +270,7 @@ k_final(int64_t n, int update, Vecs<E> V, E* __restrict__ x, const E* __restrict
         g2[i] = update ? st->gam2[i] : s_zero(S{});
     }
     const S gam_1 = update ? st->gam[1] : s_zero(S{});
-    A acc[2];
+    typename pacc_of<E>::type pacc[2];
     bool bad = false;
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
@@ -298,11 +301,11 @@ k_final(int64_t n, int update, Vecs<E> V, E* __restrict__ x, const E* __restrict
             stE(V.r[0], q, r0e);
             stE(V.u[0], q, from_s<E>(u0));
         }
-        S rs = to_s(r0e);
-        dot_add(acc[0], to_s(ldE(rt, q)), rs);
-        dot_add(acc[1], rs, rs);
+        pdot_add(pacc[0], ldE(rt, q), r0e);
+        pdot_add(pacc[1], r0e, r0e);
         bad |= !finite_e(xe);
     }
+    A acc[2] = {widen_acc(pacc[0]), widen_acc(pacc[1])};
     grid_finish<2>(acc, bad, partials, ticket, badflag, [&](const S* vals, bool b) { run_epi(ea, vals, b); });
 }
 
@@ -375,12 +378,13 @@ __global__ void __launch_bounds__(kThreads) k_norm(int64_t n, const E* __restric
                                                    unsigned int* ticket, int* badflag) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
-    A acc[1];
+    typename pacc_of<E>::type pacc;
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
-        S s = to_s(ldE(v, q));
-        dot_add(acc[0], s, s);
+        const E e = ldE(v, q);
+        pdot_add(pacc, e, e);
     }
+    A acc[1] = {widen_acc(pacc)};
     grid_finish<1>(acc, false, partials, ticket, badflag,
                    [&](const S* vals, bool) { out[0] = norm_sqrt(s_real(vals[0])); });
 }

@@ -92,55 +92,66 @@ __device__ __forceinline__ double s_abs(double v) { return fabs(v); }
 __device__ __forceinline__ double s_abs(cd v) { return cabs_(v); }
 
 // ------------------------------------------------------------ multi-dot
-// out[k] = <V_k, w> for k < K (Dot2).  Warp w of a block owns basis vectors
-// k = w, w + 8, ...; the block owns a contiguous chunk of rows.
+// out[k] = <V_k, w> for k < K (Dot2), in two launches:
+//   k_multidot:     threads stream rows in a grid-stride loop; each pass
+//                   takes md_tile basis vectors, so w[q] is loaded once per
+//                   pass and every V_k once; block partials per k;
+//   k_mdot_finish:  one block per k merges its block partials in block
+//                   order.
+// (A warp-per-basis-vector layout left 12 warps per SM resident and the
+// Arnoldi step latency-bound.)
+// basis vectors per pass: binary64 storage 4 (its binary64 Dot2 arithmetic
+// needs registers; 48 per thread keeps 5 blocks per SM), binary32 storage 8
+// (binary32 arithmetic, w loaded half as often) -- the faster of 4 and 8 for
+// each on B200 (GMRES(30)/(50) solves of configs 3 and 5)
+template <class E> struct md_tile { static constexpr int value = 8; };
+template <> struct md_tile<double> { static constexpr int value = 4; };
+template <> struct md_tile<cd> { static constexpr int value = 4; };
+
 template <class E>
 __global__ void __launch_bounds__(kGmThreads)
 k_multidot(int64_t n, int K, const E* __restrict__ V, const E* __restrict__ w,
-           typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket,
-           typename scalar_of<E>::type* out) {
+           typename acc_of<typename scalar_of<E>::type>::type* partials) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
-    constexpr int NW = kGmThreads / 32;
-    constexpr int KPW = (kGmMaxM + 1 + NW - 1) / NW;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t chunk = (n + gridDim.x - 1) / gridDim.x;
-    const int64_t q0 = int64_t(blockIdx.x) * chunk;
-    const int64_t q1 = min(n, q0 + chunk);
-    A acc[KPW];
+    __shared__ A sh[md_tile<E>::value * 32];
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    using PA = typename pacc_of<E>::type;
+    constexpr int kMdTile = md_tile<E>::value;
+    for (int kb = 0; kb < K; kb += kMdTile) {
+        PA pacc[kMdTile];
+        for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+            const E wq = ldE(w, q);
+            E vk[kMdTile];
 #pragma unroll
-    for (int t = 0; t < KPW; ++t) {
-        const int k = warp + t * NW;
-        if (k < K) {
-            const E* vk = V + size_t(k) * n;
-            for (int64_t q = q0 + lane; q < q1; q += 32) dot_add(acc[t], to_s(ldE(vk, q)), to_s(ldE(w, q)));
+            for (int t = 0; t < kMdTile; ++t)
+                if (kb + t < K) vk[t] = ldE(V + size_t(kb + t) * n, q);
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) merge(acc[t], shfl_acc(acc[t], off));
-            if (lane == 0) partials[size_t(k) * gridDim.x + blockIdx.x] = acc[t];
+            for (int t = 0; t < kMdTile; ++t)
+                if (kb + t < K) pdot_add(pacc[t], vk[t], wq);
         }
-    }
-    __shared__ bool am_last;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        am_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!am_last) return;
-    __threadfence();
+        A acc[kMdTile];
 #pragma unroll
-    for (int t = 0; t < KPW; ++t) {
-        const int k = warp + t * NW;
-        if (k < K) {
-            A tot{};
-            for (int b = lane; b < int(gridDim.x); b += 32) merge(tot, ldcg_acc(partials + size_t(k) * gridDim.x + b));
+        for (int t = 0; t < kMdTile; ++t) acc[t] = widen_acc(pacc[t]);
+        __syncthreads();  // sh is reused across passes
+        block_merge<kMdTile>(acc, sh);
+        if (threadIdx.x == 0)
 #pragma unroll
-            for (int off = 16; off > 0; off >>= 1) merge(tot, shfl_acc(tot, off));
-            if (lane == 0) out[k] = acc_value(tot);
-        }
+            for (int t = 0; t < kMdTile; ++t)
+                if (kb + t < K) partials[size_t(kb + t) * gridDim.x + blockIdx.x] = acc[t];
     }
-    __syncthreads();
-    if (threadIdx.x == 0) *ticket = 0;
+}
+
+template <class S>
+__global__ void __launch_bounds__(kGmThreads)
+k_mdot_finish(int nb, const typename acc_of<S>::type* __restrict__ partials, S* __restrict__ out) {
+    using A = typename acc_of<S>::type;
+    __shared__ A sh[32];
+    const int k = blockIdx.x;
+    A t[1];
+    t[0] = merge_partials<A>(partials + size_t(k) * nb, nb);
+    block_merge<1>(t, sh);
+    if (threadIdx.x == 0) out[k] = acc_value(t[0]);
 }
 
 // ------------------------------------------------------------ updates
@@ -158,7 +169,7 @@ k_gs_update(int64_t n, int K, const E* __restrict__ V, const E* win, E* wout,
     __shared__ S sc[kGmMaxM + 1];
     for (int k = threadIdx.x; k < K; k += blockDim.x) sc[k] = s_neg(coef[k]);
     __syncthreads();
-    A acc[1];
+    typename pacc_of<E>::type pacc;
     bool bad = false;
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
@@ -167,12 +178,12 @@ k_gs_update(int64_t n, int K, const E* __restrict__ V, const E* win, E* wout,
         E ve = from_s<E>(v);
         stE(wout, q, ve);
         if (NORM) {
-            S vs = to_s(ve);
-            dot_add(acc[0], vs, vs);
+            pdot_add(pacc, ve, ve);
             bad |= !finite_e(ve);
         }
     }
     if (!NORM) return;
+    A acc[1] = {widen_acc(pacc)};
     grid_finish<1>(acc, bad, partials, ticket, badflag, [&](const S* vals, bool anybad) {
         GmState<S>& g = *st;
         const double hn = norm_sqrt(s_real(vals[0]));
@@ -338,12 +349,13 @@ __global__ void __launch_bounds__(kGmThreads) k_gm_norm(int64_t n, const E* __re
                                                       unsigned int* ticket, int* badflag) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
-    A acc[1];
+    typename pacc_of<E>::type pacc;
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
-        S s = to_s(ldE(v, q));
-        dot_add(acc[0], s, s);
+        const E e = ldE(v, q);
+        pdot_add(pacc, e, e);
     }
+    A acc[1] = {widen_acc(pacc)};
     grid_finish<1>(acc, false, partials, ticket, badflag,
                    [&](const S* vals, bool) { out[0] = norm_sqrt(s_real(vals[0])); });
 }
@@ -436,7 +448,12 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     const int64_t n = rows;
     const int g_ew = P.g_ew = int(
         std::max<int64_t>(1, std::min<int64_t>((n + kGmThreads - 1) / kGmThreads, int64_t(sms) * gm_occupancy<E>())));
-    const int g_md = P.g_md = int(std::max<int64_t>(1, std::min<int64_t>((n + 4095) / 4096, int64_t(sms) * 2)));
+    int occ_md = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_md, reinterpret_cast<const void*>(k_multidot<E>), kGmThreads,
+                                                      0) != cudaSuccess || occ_md < 1)
+        occ_md = 1;
+    const int g_md = P.g_md = int(
+        std::max<int64_t>(1, std::min<int64_t>((n + kGmThreads - 1) / kGmThreads, int64_t(sms) * occ_md)));
     const int g_sp = P.g_sp = int(std::max<int64_t>(1, (int64_t(rows) + kGmThreads - 1) / kGmThreads));
     SolverWorkspace& ws = P.ws;
     const size_t vb = size_t(n) * sizeof(E);
@@ -488,14 +505,16 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
             ++kernels;
         }
         k_gm_spmv<E><<<g_sp, kGmThreads, 0, s>>>(rows, rp, ci, val, src, W);
-        k_multidot<E><<<g_md, kGmThreads, 0, s>>>(n, i + 1, V, W, partials, ticket, st->h1);
+        k_multidot<E><<<g_md, kGmThreads, 0, s>>>(n, i + 1, V, W, partials);
+        k_mdot_finish<S><<<i + 1, kGmThreads, 0, s>>>(g_md, partials, st->h1);
         k_gs_update<E, false><<<g_ew, kGmThreads, 0, s>>>(n, i + 1, V, W, W, st->h1, st, m, i, partials, ticket,
                                                            badflag);
-        k_multidot<E><<<g_md, kGmThreads, 0, s>>>(n, i + 1, V, W, partials, ticket, st->h2);
+        k_multidot<E><<<g_md, kGmThreads, 0, s>>>(n, i + 1, V, W, partials);
+        k_mdot_finish<S><<<i + 1, kGmThreads, 0, s>>>(g_md, partials, st->h2);
         k_gs_update<E, true><<<g_ew, kGmThreads, 0, s>>>(n, i + 1, V, W, W, st->h2, st, m, i, partials, ticket,
                                                           badflag);
         k_gm_scale<E><<<g_ew, kGmThreads, 0, s>>>(n, W, V + size_t(i + 1) * n, st);
-        kernels += 6;
+        kernels += 8;
     }
     k_gm_solve<S><<<1, 1, 0, s>>>(st, m);
     ++kernels;

@@ -38,6 +38,7 @@
 #include <cuda_bf16.h>
 
 #include "hpb_common.cuh"
+#include "hpb_fused.cuh"
 
 namespace hpb {
 namespace spai {
@@ -538,30 +539,55 @@ double host_sum(const double* dpart, int nb) {
     return s;
 }
 
-// forward + Mh (scaled, training: also Ah) or M (scaled = false) for one
-// system (binary32 CSR, device)
-int forward_system(hpb_spai* net, const hpb_spai_system& sys, bool train) {
+__global__ void k_logabs(int32_t n, const float* __restrict__ d, double* __restrict__ out) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = log(fabs(double(d[i])));
+}
+
+// mean log|diag| over the rows: binary64 logs summed with Sum2 (deterministic)
+int mean_log_diag(hpb_spai* net, int32_t n, const float* diag, double* scratch, double* mean) {
+    k_logabs<<<(n + 255) / 256, 256>>>(n, diag, scratch);
+    hpb::count_launch();
+    double r[2] = {0.0, 0.0};
+    const int st = hpb_sum2_f64_host(net->ctx, n, scratch, r);
+    *mean = r[0] / std::max(1, n);
+    return st;
+}
+
+// Features and the MLP forward pass of one system (binary32 CSR, device),
+// into feat / out; diag receives diag(A).  h1, h2 (post-ReLU) are kept for
+// the backward pass when not null.
+int forward_rows(hpb_spai* net, const hpb_spai_system& sys, float* diag, float* feat, float* out, float* h1, float* h2,
+                 double* scratch) {
+    using namespace hpb::spai;
+    const int32_t n = sys.rows;
+    const int gb = (n + 255) / 256;
+    k_fdiag<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, diag);
+    hpb::count_launch();
+    double ml = 0.0;
+    int st = mean_log_diag(net, n, diag, scratch, &ml);
+    if (st) return st;
+    k_features<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, diag, float(ml), net->off, feat);
+    k_forward<<<kGridMlp, kThreads, fwd_smem()>>>(n, feat, net->wb, h1, h2, out);
+    hpb::count_launch(2);
+    return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
+}
+
+// training: forward with h1/h2 kept, Mh (scaled) and Ah into the network's workspace
+int forward_system(hpb_spai* net, const hpb_spai_system& sys) {
     using namespace hpb::spai;
     const int32_t n = sys.rows;
     int st = grow(net, n, sys.nnz);
     if (st) return st;
+    double* scratch = static_cast<double*>(hpb::fused::pool_alloc(size_t(n ? n : 1) * sizeof(double), nullptr));
+    if (!scratch) return HPB_ERROR_OUT_OF_MEMORY;
+    st = forward_rows(net, sys, net->diag, net->feat, net->out, net->h1, net->h2, scratch);
+    hpb::fused::pool_free(scratch, nullptr);
+    if (st) return st;
     const int gb = (n + 255) / 256;
-    k_fdiag<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, net->diag);
-    // mean log|diag| over the rows (binary64 on the host)
-    std::vector<float> hd(n);
-    cudaMemcpy(hd.data(), net->diag, size_t(n) * 4, cudaMemcpyDeviceToHost);
-    double ml = 0;
-    for (float v : hd) ml += std::log(std::fabs(double(v)));
-    ml /= std::max(1, n);
-    k_features<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, net->diag, float(ml), net->off, net->feat);
-    k_forward<<<kGridMlp, kThreads, fwd_smem()>>>(n, net->feat, net->wb, train ? net->h1 : nullptr,
-                                                 train ? net->h2 : nullptr, net->out);
-    k_assemble<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, net->diag, net->out, net->off, train, net->mval);
-    hpb::count_launch(4);
-    if (train) {
-        k_scale_vals<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, net->diag, net->ahat);
-        hpb::count_launch();
-    }
+    k_assemble<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, net->diag, net->out, net->off, true, net->mval);
+    k_scale_vals<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, net->diag, net->ahat);
+    hpb::count_launch(2);
     return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
 }
 }  // namespace
@@ -679,11 +705,31 @@ int hpb_spai_get_weights(hpb_spai* net, float* w_host) {
 
 // M on A's pattern for one binary32 system: m_val[nnz] (device)
 int hpb_spai_assemble(hpb_spai* net, const hpb_spai_system* sys, float* m_val) {
-    if (!net || !sys || !m_val) return HPB_ERROR_INVALID_VALUE;
-    int st = forward_system(net, *sys, false);
-    if (st) return st;
-    return cudaMemcpy(m_val, net->mval, size_t(sys->nnz) * 4, cudaMemcpyDeviceToDevice) ? HPB_ERROR_CUDA
-                                                                                           : HPB_SUCCESS;
+    using namespace hpb::spai;
+    if (!net || !sys || !m_val || sys->rows < 0) return HPB_ERROR_INVALID_VALUE;
+    const int32_t n = sys->rows;
+    if (n == 0) return HPB_SUCCESS;
+    // inference needs only features, outputs and the diagonal: scratch from
+    // the solvers' pool on the legacy stream (no training workspace)
+    using hpb::fused::pool_alloc;
+    using hpb::fused::pool_free;
+    const size_t R = size_t(n);
+    float* diag = static_cast<float*>(pool_alloc(R * 4, nullptr));
+    float* feat = static_cast<float*>(pool_alloc(R * kF * 4, nullptr));
+    float* out = static_cast<float*>(pool_alloc(R * kO * 4, nullptr));
+    double* scratch = static_cast<double*>(pool_alloc(R * 8, nullptr));
+    int st = (diag && feat && out && scratch) ? HPB_SUCCESS : HPB_ERROR_OUT_OF_MEMORY;
+    if (st == HPB_SUCCESS) st = forward_rows(net, *sys, diag, feat, out, nullptr, nullptr, scratch);
+    if (st == HPB_SUCCESS) {
+        k_assemble<<<(n + 255) / 256, 256>>>(n, sys->row_ptr, sys->col_ind, diag, out, net->off, false, m_val);
+        hpb::count_launch();
+        if (cudaGetLastError() != cudaSuccess) st = HPB_ERROR_CUDA;
+    }
+    for (void* q : {static_cast<void*>(diag), static_cast<void*>(feat), static_cast<void*>(out),
+                    static_cast<void*>(scratch)})
+        pool_free(q, nullptr);
+    if (cudaStreamSynchronize(nullptr) != cudaSuccess && st == HPB_SUCCESS) st = HPB_ERROR_CUDA;
+    return st;
 }
 
 // Loss of one system and its parameter gradient, added to the network's
@@ -696,7 +742,7 @@ int loss_impl(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_r
               bool grad) {
     using namespace hpb::spai;
     if (!net || !sys || sys->rows <= 0) return HPB_ERROR_INVALID_VALUE;
-    int st = forward_system(net, *sys, true);
+    int st = forward_system(net, *sys);
     if (st) return st;
     const int32_t n = sys->rows;
     const int gb = (n + 255) / 256;
