@@ -375,8 +375,9 @@ def bench_dot2(args, ws, rank, local, torch, dist):
 
 # DRAM bytes of one hpb_csr_spmv_dot2_f64 launch on the 1024^2 operator
 # (dram__bytes_read.sum + dram__bytes_write.sum), from the ncu capture in
-# profiles/spmv_dot2_f64_convdiff1024.md; None until captured.
-SPMV_DOT2_TRAFFIC = None
+# profiles/spmv_dot2_f64_convdiff1024.md (83,859,456 B read + 5,346,048 B
+# written; part of y is still in L2 when the launch ends).
+SPMV_DOT2_TRAFFIC = 89205504
 
 
 def spmv_roofline(torch, L, ctx, A, reps=40):

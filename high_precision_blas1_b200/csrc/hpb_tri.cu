@@ -1,0 +1,681 @@
+// Sparse triangular solves and ILU(0) on CSR matrices (the analysis, the
+// solve and the factorization kernels, and their C ABI).  The design is
+// described at the top of hpb_tri.cuh.
+//
+// Arithmetic.  Every operation goes through the round-to-nearest intrinsics
+// (a - l*u as one FMA per real product, complex products and quotients by
+// the textbook formulas spelled out below), so a row's result does not
+// depend on compiler contraction and equals the CPU restatement
+// (oracle/oro.c, oro_csr_trsv_* / oro_csr_ilu0_*) bit for bit: each row is
+// computed by one thread, over its entries in index order, whatever the
+// schedule.
+#include <algorithm>
+#include <climits>
+#include <mutex>
+#include <vector>
+
+#include "hpb_tri.cuh"
+
+namespace hpb {
+namespace tri {
+namespace {
+
+constexpr int kLvThreads = 512;
+constexpr int kPre = 4;                          // dependencies per row prefetched into registers
+constexpr long long kSpinShared = 1ll << 24;     // polls of the tile's level counter (shared memory)
+constexpr long long kSpinGlobal = 1ll << 20;     // polls of another tile's row flag (L2)
+
+// ---- arithmetic -----------------------------------------------------------
+__device__ __forceinline__ float fms(float a, float l, float u) { return __fmaf_rn(-l, u, a); }
+__device__ __forceinline__ double fms(double a, double l, double u) { return __fma_rn(-l, u, a); }
+// a - l*u with l*u = (lr ur - li ui) + i (lr ui + li ur)
+__device__ __forceinline__ cf fms(cf a, cf l, cf u) {
+    return cf{__fmaf_rn(-l.re, u.re, __fmaf_rn(l.im, u.im, a.re)), __fmaf_rn(-l.re, u.im, __fmaf_rn(-l.im, u.re, a.im))};
+}
+__device__ __forceinline__ cd fms(cd a, cd l, cd u) {
+    return cd{__fma_rn(-l.re, u.re, __fma_rn(l.im, u.im, a.re)), __fma_rn(-l.re, u.im, __fma_rn(-l.im, u.re, a.im))};
+}
+__device__ __forceinline__ float scale(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double scale(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ cf scale(cf a, cf b) {
+    return cf{__fmaf_rn(a.re, b.re, -__fmul_rn(a.im, b.im)), __fmaf_rn(a.re, b.im, __fmul_rn(a.im, b.re))};
+}
+__device__ __forceinline__ cd scale(cd a, cd b) {
+    return cd{__fma_rn(a.re, b.re, -__dmul_rn(a.im, b.im)), __fma_rn(a.re, b.im, __dmul_rn(a.im, b.re))};
+}
+__device__ __forceinline__ float quot(float a, float d) { return __fdiv_rn(a, d); }
+__device__ __forceinline__ double quot(double a, double d) { return __ddiv_rn(a, d); }
+// a / d = (a conj(d)) / |d|^2
+__device__ __forceinline__ cf quot(cf a, cf d) {
+    const float den = __fmaf_rn(d.re, d.re, __fmul_rn(d.im, d.im));
+    return cf{__fdiv_rn(__fmaf_rn(a.re, d.re, __fmul_rn(a.im, d.im)), den),
+              __fdiv_rn(__fmaf_rn(a.im, d.re, -__fmul_rn(a.re, d.im)), den)};
+}
+__device__ __forceinline__ cd quot(cd a, cd d) {
+    const double den = __fma_rn(d.re, d.re, __dmul_rn(d.im, d.im));
+    return cd{__ddiv_rn(__fma_rn(a.re, d.re, __dmul_rn(a.im, d.im)), den),
+              __ddiv_rn(__fma_rn(a.im, d.re, -__dmul_rn(a.re, d.im)), den)};
+}
+__device__ __forceinline__ bool zero_of(float a) { return a == 0.0f; }
+__device__ __forceinline__ bool zero_of(double a) { return a == 0.0; }
+__device__ __forceinline__ bool zero_of(cf a) { return a.re == 0.0f && a.im == 0.0f; }
+__device__ __forceinline__ bool zero_of(cd a) { return a.re == 0.0 && a.im == 0.0; }
+
+// L2 loads (values another block or warp wrote during this kernel)
+__device__ __forceinline__ float ldcgE(const float* p, int64_t i) { return __ldcg(p + i); }
+__device__ __forceinline__ double ldcgE(const double* p, int64_t i) { return __ldcg(p + i); }
+__device__ __forceinline__ cf ldcgE(const cf* p, int64_t i) {
+    const float* q = reinterpret_cast<const float*>(p + i);
+    return cf{__ldcg(q), __ldcg(q + 1)};
+}
+__device__ __forceinline__ cd ldcgE(const cd* p, int64_t i) {
+    const double* q = reinterpret_cast<const double*>(p + i);
+    return cd{__ldcg(q), __ldcg(q + 1)};
+}
+
+__device__ __forceinline__ void stcgE(float* p, int64_t i, float v) { __stcg(p + i, v); }
+__device__ __forceinline__ void stcgE(double* p, int64_t i, double v) { __stcg(p + i, v); }
+__device__ __forceinline__ void stcgE(cf* p, int64_t i, cf v) {
+    float* q = reinterpret_cast<float*>(p + i);
+    __stcg(q, v.re);
+    __stcg(q + 1, v.im);
+}
+__device__ __forceinline__ void stcgE(cd* p, int64_t i, cd v) {
+    double* q = reinterpret_cast<double*>(p + i);
+    __stcg(q, v.re);
+    __stcg(q + 1, v.im);
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Wait (bounded) until row j of another tile is published.
+__device__ __forceinline__ void wait_row(const unsigned* flags, int32_t j, int* err) {
+    long long it = 0;
+    while (ld_acquire(flags + j) == 0u) {
+        if (++it > kSpinGlobal) {
+            atomicOr(err, kErrTimeout);
+            return;
+        }
+    }
+}
+
+// Lane 0 waits (bounded) until the tile's levels [0, l) are complete; then
+// the warp may read what those levels wrote.
+__device__ __forceinline__ void wait_levels(volatile int* done, int l, int lane, int* err) {
+    if (lane == 0) {
+        long long it = 0;
+        while (*done < l) {
+            if (++it > kSpinShared) {
+                atomicOr(err, kErrTimeout);
+                break;
+            }
+        }
+    }
+    __syncwarp();
+    __threadfence_block();
+}
+
+// ---- analysis -------------------------------------------------------------
+// Per row: validate the structure (row pointers monotone and within nnz,
+// columns in range and strictly increasing), locate the diagonal, and the
+// dependency range: strictly lower part [rp[i], first column >= i) or
+// strictly upper part (first column > i, rp[i+1]).
+__global__ void k_tri_rows(int32_t n, int64_t nnz, int upper, const int32_t* __restrict__ rp,
+                           const int32_t* __restrict__ ci, int32_t* __restrict__ beg, int32_t* __restrict__ cnt,
+                           int32_t* __restrict__ dpos, int* err, int* missing) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int32_t b = rp[i], e = rp[i + 1];
+    int bad = 0;
+    if (b < 0 || e < b || int64_t(e) > nnz) {
+        bad |= kErrColumn;
+        b = e = 0;
+    }
+    int32_t prev = -1, dp = -1, ge = e, gt = e;
+    for (int32_t k = b; k < e; ++k) {
+        const int32_t c = ci[k];
+        if (c < 0 || c >= n) bad |= kErrColumn;
+        if (c <= prev) bad |= kErrUnsorted;
+        prev = c;
+        if (c == i) dp = k;
+        if (c >= i && ge == e) ge = k;
+        if (c > i && gt == e) gt = k;
+    }
+    if (bad) atomicOr(err, bad);
+    if (dp < 0) atomicAdd(missing, 1);
+    beg[i] = upper ? gt : b;
+    cnt[i] = upper ? e - gt : ge - b;
+    dpos[i] = dp;
+}
+
+// Per tile (one block): level of each row = 1 + the largest level of its
+// in-tile dependencies (0 if none), by relaxation sweeps over contiguous
+// per-thread segments walked in dependency order, until a sweep changes
+// nothing (levels only grow and are bounded by the tile's row count);
+// then a counting sort of the tile's rows by level into desc.
+template <bool UPPER>
+__global__ void __launch_bounds__(kLvThreads)
+k_tri_levels(int32_t n, const int32_t* __restrict__ ci, const int32_t* __restrict__ beg,
+             const int32_t* __restrict__ cnt, const int32_t* __restrict__ dpos, int4* __restrict__ desc,
+             int32_t* __restrict__ lvlptr, int32_t* __restrict__ nlev) {
+    extern __shared__ int sh[];
+    volatile int* lev = sh;          // kTriTile
+    int* hist = sh + kTriTile;       // kTriTile + 1
+    __shared__ int part[kLvThreads];
+    __shared__ int s_max;
+    const int t = blockIdx.x;
+    const int32_t base = int32_t(t) * kTriTile;
+    const int32_t m = min(kTriTile, n - base);
+    for (int r = threadIdx.x; r < m; r += blockDim.x) lev[r] = 0;
+    if (threadIdx.x == 0) s_max = 0;
+    __syncthreads();
+    const int seg = (m + blockDim.x - 1) / blockDim.x;
+    const int s0 = min(m, int(threadIdx.x) * seg), s1 = min(m, s0 + seg);
+    int changed, sweeps = 0;
+    do {
+        changed = 0;
+        for (int k = 0; k < s1 - s0; ++k) {
+            const int r = UPPER ? s1 - 1 - k : s0 + k;
+            const int32_t i = base + r;
+            const int32_t b = __ldg(beg + i), c = __ldg(cnt + i);
+            int lv = 0;
+            for (int32_t e = b; e < b + c; ++e) {
+                const int32_t j = __ldg(ci + e) - base;
+                // only dependencies in the solve's direction: the graph stays acyclic
+                // (and the sweeps finite) even before the structure checks are read
+                if (j >= 0 && j < m && (UPPER ? j > r : j < r)) lv = max(lv, lev[j] + 1);
+            }
+            if (lv > lev[r]) {
+                lev[r] = lv;
+                changed = 1;
+            }
+        }
+    } while (__syncthreads_or(changed) && ++sweeps <= m);
+
+    int mx = 0;
+    for (int r = threadIdx.x; r < m; r += blockDim.x) mx = max(mx, lev[r]);
+    atomicMax(&s_max, mx);
+    for (int r = threadIdx.x; r <= m; r += blockDim.x) hist[r] = 0;
+    __syncthreads();
+    const int L = s_max + 1;
+    for (int r = threadIdx.x; r < m; r += blockDim.x) atomicAdd(&hist[lev[r]], 1);
+    __syncthreads();
+    const int cs = (L + blockDim.x - 1) / blockDim.x;
+    const int c0 = min(L, int(threadIdx.x) * cs), c1 = min(L, c0 + cs);
+    int sum = 0;
+    for (int l = c0; l < c1; ++l) sum += hist[l];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int w = 0; w < int(blockDim.x); ++w) {
+            const int v = part[w];
+            part[w] = acc;
+            acc += v;
+        }
+    }
+    __syncthreads();
+    int run = part[threadIdx.x];
+    int32_t* lp = lvlptr + size_t(t) * (kTriTile + 1);
+    for (int l = c0; l < c1; ++l) {
+        const int v = hist[l];
+        hist[l] = run;
+        lp[l] = run;
+        run += v;
+    }
+    if (threadIdx.x == 0) {
+        lp[L] = m;
+        nlev[t] = L;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+        const int pos = atomicAdd(&hist[lev[r]], 1);
+        const int32_t i = base + r;
+        desc[base + pos] = make_int4(i, __ldg(beg + i), __ldg(cnt + i), __ldg(dpos + i));
+    }
+}
+
+// ---- solve ----------------------------------------------------------------
+template <class E, bool UPPER, bool UNIT>
+__global__ void __launch_bounds__(kTriThreads)
+k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int32_t* __restrict__ lvlptr,
+       const int32_t* __restrict__ nlev, const int32_t* __restrict__ ci, const E* __restrict__ val, E alpha,
+       const E* b, E* x, unsigned* flags, int* err) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    E* xs = reinterpret_cast<E*>(smraw);
+    __shared__ int s_tile;
+    __shared__ int s_done;
+    if (threadIdx.x == 0) {
+        const int tk = int(atomicAdd(flags + n, 1u));
+        s_tile = UPPER ? ntiles - 1 - tk : tk;
+        s_done = 0;
+    }
+    __syncthreads();
+    const int t = s_tile;
+    if (t < 0 || t >= ntiles) return;
+    const int32_t base = int32_t(t) * kTriTile;
+    const int32_t m = min(kTriTile, n - base);
+    const int L = nlev[t];
+    const int32_t* lp = lvlptr + size_t(t) * (kTriTile + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int W = kTriThreads / 32;
+    volatile int* done = &s_done;
+    auto fetch = [&](int32_t j) -> E {
+        const int32_t jl = j - base;
+        if (jl >= 0 && jl < m) return xs[jl];
+        wait_row(flags, j, err);
+        return ldcgE(x, j);
+    };
+    for (int l = warp; l < L; l += W) {
+        const int32_t p0 = lp[l], p1 = lp[l + 1];
+        int32_t last_row = -1;
+        for (int32_t q = p0; q < p1; q += 32) {
+            const int32_t p = q + lane;
+            const bool act = p < p1;
+            // the row's data does not depend on the solve: load it before waiting
+            int4 d = make_int4(0, 0, 0, -1);
+            if (act) d = desc[base + p];
+            E rhs{}, dg{};
+            int32_t col[kPre];
+            E v[kPre];
+#pragma unroll
+            for (int k = 0; k < kPre; ++k) {
+                col[k] = 0;
+                v[k] = E{};
+            }
+            if (act) {
+                rhs = scale(alpha, ldE(b, d.x));
+                if (!UNIT) dg = ldE(val, d.w);
+#pragma unroll
+                for (int k = 0; k < kPre; ++k)
+                    if (k < d.z) {
+                        col[k] = __ldg(ci + d.y + k);
+                        v[k] = ldE(val, d.y + k);
+                    }
+            }
+            if (q == p0) wait_levels(done, l, lane, err);
+            if (act) {
+                E acc = rhs;
+#pragma unroll
+                for (int k = 0; k < kPre; ++k)
+                    if (k < d.z) acc = fms(acc, v[k], fetch(col[k]));
+                for (int32_t e = d.y + kPre; e < d.y + d.z; ++e) acc = fms(acc, ldE(val, e), fetch(__ldg(ci + e)));
+                if (!UNIT) acc = quot(acc, dg);
+                xs[d.x - base] = acc;
+                stE(x, d.x, acc);
+                if (q + 32 < p1)
+                    st_release(flags + d.x, 1u);  // more chunks follow in this level: publish now
+                else
+                    last_row = d.x;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            *done = l + 1;
+        }
+        // publish to other tiles after the in-tile announcement (the release
+        // makes this thread's store of x visible first)
+        if (last_row >= 0) st_release(flags + last_row, 1u);
+    }
+}
+
+// ---- ILU(0) ---------------------------------------------------------------
+// Row i, for each strictly lower entry k (ascending): l_ik = a_ik / u_kk,
+// then a_ij -= l_ik u_kj for every j > k present in both rows (the IKJ
+// variant of ILU(0), Saad, Iterative Methods for Sparse Linear Systems,
+// 2nd ed., Algorithm 10.4).  Rows k are complete when read: earlier levels
+// of the tile (level counter) or other tiles (row flags).  All accesses to
+// val go to L2 (ld.cg / st.cg): rows finished by other warps and blocks are
+// read there, and no L1 line of a neighbouring row can go stale.
+template <class E>
+__global__ void __launch_bounds__(kTriThreads)
+k_ilu0(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int32_t* __restrict__ lvlptr,
+       const int32_t* __restrict__ nlev, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+       const int32_t* __restrict__ dpos, E* val, unsigned* flags, int* err, int* err_row) {
+    __shared__ int s_tile;
+    __shared__ int s_done;
+    if (threadIdx.x == 0) {
+        s_tile = int(atomicAdd(flags + n, 1u));
+        s_done = 0;
+    }
+    __syncthreads();
+    const int t = s_tile;
+    if (t < 0 || t >= ntiles) return;
+    const int32_t base = int32_t(t) * kTriTile;
+    const int32_t m = min(kTriTile, n - base);
+    const int L = nlev[t];
+    const int32_t* lp = lvlptr + size_t(t) * (kTriTile + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int W = kTriThreads / 32;
+    volatile int* done = &s_done;
+    for (int l = warp; l < L; l += W) {
+        const int32_t p0 = lp[l], p1 = lp[l + 1];
+        wait_levels(done, l, lane, err);
+        for (int32_t q = p0; q < p1; q += 32) {
+            const int32_t p = q + lane;
+            if (p >= p1) continue;
+            const int4 d = desc[base + p];
+            const int32_t i = d.x, e_end = __ldg(rp + i + 1);
+            for (int32_t e = d.y; e < d.y + d.z; ++e) {
+                const int32_t k = __ldg(ci + e);
+                const int32_t kl = k - base;
+                if (!(kl >= 0 && kl < m)) wait_row(flags, k, err);
+                const int32_t dk = __ldg(dpos + k);
+                const E lik = quot(ldcgE(val, e), ldcgE(val, dk));
+                stcgE(val, e, lik);
+                int32_t pi = e + 1, pk = dk + 1;
+                const int32_t pk_end = __ldg(rp + k + 1);
+                while (pi < e_end && pk < pk_end) {
+                    const int32_t ca = __ldg(ci + pi), cb = __ldg(ci + pk);
+                    if (ca == cb) {
+                        stcgE(val, pi, fms(ldcgE(val, pi), lik, ldcgE(val, pk)));
+                        ++pi;
+                        ++pk;
+                    } else if (ca < cb) {
+                        ++pi;
+                    } else {
+                        ++pk;
+                    }
+                }
+            }
+            if (zero_of(ldcgE(val, d.w))) {
+                atomicOr(err, kErrZeroPivot);
+                atomicMin(err_row, i);
+            }
+            __threadfence();
+            st_release(flags + i, 1u);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence();
+            *done = l + 1;
+        }
+    }
+}
+
+template <class K>
+void allow_smem(K kernel, size_t bytes) {
+    if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+}
+
+}  // namespace
+
+int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* rp, const int32_t* ci, Plan* P) {
+    *P = Plan{};
+    P->upper = upper ? 1 : 0;
+    P->n = n;
+    P->nnz = nnz;
+    P->rp = rp;
+    P->ci = ci;
+    P->ntiles = int32_t((int64_t(n) + kTriTile - 1) / kTriTile);
+    cudaGetDevice(&P->device);
+    cudaStream_t s = ctx->stream;
+    int32_t *beg = nullptr, *cnt = nullptr;
+    int* missing = nullptr;
+    auto fail = [&](int status, const char* what) {
+        cudaFree(beg);
+        cudaFree(cnt);
+        cudaFree(missing);
+        release(P);
+        return set_error(ctx, status, "hpb_csr_tri_create: %s", what);
+    };
+    const size_t nn = size_t(n);
+    if (cudaMalloc(&P->desc, nn * sizeof(int4)) != cudaSuccess ||
+        cudaMalloc(&P->lvlptr, size_t(P->ntiles) * (kTriTile + 1) * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&P->nlev, size_t(P->ntiles) * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&P->dpos, nn * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&P->flags, (nn + 1) * sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&P->err, 2 * sizeof(int)) != cudaSuccess || cudaMalloc(&beg, nn * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&cnt, nn * sizeof(int32_t)) != cudaSuccess || cudaMalloc(&missing, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HPB_ERROR_OUT_OF_MEMORY, "device allocation failed");
+    }
+    P->err_row = P->err + 1;
+    const int init[2] = {0, INT_MAX};
+    cudaMemcpyAsync(P->err, init, sizeof(init), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(missing, 0, sizeof(int), s);
+    k_tri_rows<<<(n + 255) / 256, 256, 0, s>>>(n, nnz, P->upper, rp, ci, beg, cnt, P->dpos, P->err, missing);
+    const size_t lv_smem = (2 * size_t(kTriTile) + 1) * sizeof(int);
+    if (P->upper) {
+        allow_smem(k_tri_levels<true>, lv_smem);
+        k_tri_levels<true><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, ci, beg, cnt, P->dpos, P->desc, P->lvlptr,
+                                                                   P->nlev);
+    } else {
+        allow_smem(k_tri_levels<false>, lv_smem);
+        k_tri_levels<false><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, ci, beg, cnt, P->dpos, P->desc, P->lvlptr,
+                                                                    P->nlev);
+    }
+    count_launch(2);
+    if (cudaGetLastError() != cudaSuccess) return fail(HPB_ERROR_CUDA, "analysis launch failed");
+    int host_err = 0, host_missing = 0;
+    std::vector<int32_t> lev(size_t(P->ntiles));
+    if (cudaMemcpyAsync(&host_err, P->err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(&host_missing, missing, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(lev.data(), P->nlev, lev.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(HPB_ERROR_CUDA, "analysis failed");
+    cudaFree(beg);
+    cudaFree(cnt);
+    cudaFree(missing);
+    beg = cnt = nullptr;
+    missing = nullptr;
+    if (host_err & kErrColumn) return fail(HPB_ERROR_INVALID_VALUE, "row pointer or column index out of range");
+    if (host_err & kErrUnsorted)
+        return fail(HPB_ERROR_INVALID_VALUE, "column indices of a row are not strictly increasing");
+    P->all_diag = host_missing == 0;
+    for (int32_t v : lev) {
+        P->max_levels = std::max(P->max_levels, v);
+        P->sum_levels += v;
+    }
+    return HPB_SUCCESS;
+}
+
+void release(Plan* P) {
+    cudaFree(P->desc);
+    cudaFree(P->lvlptr);
+    cudaFree(P->nlev);
+    cudaFree(P->dpos);
+    cudaFree(P->flags);
+    cudaFree(P->err);
+    P->desc = nullptr;
+    P->lvlptr = P->nlev = P->dpos = nullptr;
+    P->flags = nullptr;
+    P->err = P->err_row = nullptr;
+}
+
+template <class E>
+cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E* b, E* x, cudaStream_t s) {
+    if (P.n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(P.flags, 0, (size_t(P.n) + 1) * sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    const size_t sm = size_t(kTriTile) * sizeof(E);
+    static std::once_flag once;
+    std::call_once(once, [&] {
+        allow_smem(k_trsv<E, false, false>, sm);
+        allow_smem(k_trsv<E, false, true>, sm);
+        allow_smem(k_trsv<E, true, false>, sm);
+        allow_smem(k_trsv<E, true, true>, sm);
+    });
+    auto k = P.upper ? (unit ? k_trsv<E, true, true> : k_trsv<E, true, false>)
+                     : (unit ? k_trsv<E, false, true> : k_trsv<E, false, false>);
+    k<<<P.ntiles, kTriThreads, sm, s>>>(P.n, P.ntiles, P.desc, P.lvlptr, P.nlev, P.ci, val, alpha, b, x, P.flags,
+                                        P.err);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template <class E>
+cudaError_t launch_ilu0(const Plan& P, E* val, cudaStream_t s) {
+    if (P.n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(P.flags, 0, (size_t(P.n) + 1) * sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    k_ilu0<E><<<P.ntiles, kTriThreads, 0, s>>>(P.n, P.ntiles, P.desc, P.lvlptr, P.nlev, P.rp, P.ci, P.dpos, val,
+                                               P.flags, P.err, P.err_row);
+    count_launch();
+    return cudaGetLastError();
+}
+
+template cudaError_t launch_trsv<float>(const Plan&, int, const float*, float, const float*, float*, cudaStream_t);
+template cudaError_t launch_trsv<double>(const Plan&, int, const double*, double, const double*, double*,
+                                         cudaStream_t);
+template cudaError_t launch_trsv<cf>(const Plan&, int, const cf*, cf, const cf*, cf*, cudaStream_t);
+template cudaError_t launch_trsv<cd>(const Plan&, int, const cd*, cd, const cd*, cd*, cudaStream_t);
+template cudaError_t launch_ilu0<float>(const Plan&, float*, cudaStream_t);
+template cudaError_t launch_ilu0<double>(const Plan&, double*, cudaStream_t);
+template cudaError_t launch_ilu0<cf>(const Plan&, cf*, cudaStream_t);
+template cudaError_t launch_ilu0<cd>(const Plan&, cd*, cudaStream_t);
+
+}  // namespace tri
+
+namespace {
+
+bool aligned(const void* p, size_t a) { return reinterpret_cast<uintptr_t>(p) % a == 0; }
+
+template <class E>
+int trsv_impl(hpb_context* ctx, const hpb_csr_tri* tri, int unit, const E* val, E alpha, const E* b, E* x,
+              const char* name) {
+    HPB_CHECK_CTX(ctx);
+    if (tri == nullptr) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null analysis", name);
+    const tri::Plan& P = tri->plan;
+    if (P.n == 0) return HPB_SUCCESS;
+    if (val == nullptr || b == nullptr || x == nullptr)
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null pointer", name);
+    constexpr size_t kA = sizeof(typename real_of<E>::type);
+    if (!aligned(val, kA) || !aligned(b, kA) || !aligned(x, kA))
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: pointer not aligned to its element type", name);
+    if (!unit && !P.all_diag)
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: a row stores no diagonal entry (structural zero)", name);
+    HPB_CUDA_TRY(ctx, tri::launch_trsv<E>(P, unit, val, alpha, b, x, ctx->stream));
+    return HPB_SUCCESS;
+}
+
+template <class E>
+int ilu0_impl(hpb_context* ctx, const hpb_csr_tri* tri, E* val, const char* name) {
+    HPB_CHECK_CTX(ctx);
+    if (tri == nullptr) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null analysis", name);
+    const tri::Plan& P = tri->plan;
+    if (P.upper) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: needs the analysis of the lower triangle", name);
+    if (P.n == 0) return HPB_SUCCESS;
+    if (val == nullptr) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null pointer", name);
+    if (!aligned(val, sizeof(typename real_of<E>::type)))
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: pointer not aligned to its element type", name);
+    if (!P.all_diag)
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: a row stores no diagonal entry (structural zero)", name);
+    const int init[2] = {0, INT_MAX};
+    HPB_CUDA_TRY(ctx, cudaMemcpyAsync(P.err, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    HPB_CUDA_TRY(ctx, tri::launch_ilu0<E>(P, val, ctx->stream));
+    int h[2] = {0, 0};
+    HPB_CUDA_TRY(ctx, cudaMemcpyAsync(h, P.err, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    HPB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h[0] & tri::kErrTimeout)
+        return set_error(ctx, HPB_ERROR_TIMEOUT, "%s: a bounded device-side wait gave up", name);
+    if (h[0] & tri::kErrZeroPivot) return set_error(ctx, HPB_ERROR_BREAKDOWN, "%s: zero pivot in row %d", name, h[1]);
+    return HPB_SUCCESS;
+}
+
+}  // namespace
+}  // namespace hpb
+
+using hpb::cd;
+using hpb::cf;
+
+extern "C" {
+
+int hpb_csr_tri_create(hpb_context* ctx, int upper, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                       const int32_t* col_ind, hpb_csr_tri** tri) {
+    HPB_CHECK_CTX(ctx);
+    if (tri == nullptr) return hpb::set_error(ctx, HPB_ERROR_INVALID_VALUE, "hpb_csr_tri_create: null output");
+    *tri = nullptr;
+    if (rows < 0 || nnz < 0 || nnz > INT32_MAX)
+        return hpb::set_error(ctx, HPB_ERROR_INVALID_VALUE, "hpb_csr_tri_create: invalid dimensions");
+    if (rows > 0 && (row_ptr == nullptr || (nnz > 0 && col_ind == nullptr)))
+        return hpb::set_error(ctx, HPB_ERROR_INVALID_VALUE, "hpb_csr_tri_create: null pointer");
+    auto* h = new (std::nothrow) hpb_csr_tri;
+    if (h == nullptr) return hpb::set_error(ctx, HPB_ERROR_OUT_OF_MEMORY, "hpb_csr_tri_create: host allocation");
+    if (rows == 0) {
+        h->plan = hpb::tri::Plan{};
+        h->plan.upper = upper ? 1 : 0;
+        h->plan.all_diag = 1;
+        *tri = h;
+        return HPB_SUCCESS;
+    }
+    const int st = hpb::tri::analyse(ctx, upper, rows, nnz, row_ptr, col_ind, &h->plan);
+    if (st != HPB_SUCCESS) {
+        delete h;
+        return st;
+    }
+    *tri = h;
+    return HPB_SUCCESS;
+}
+
+int hpb_csr_tri_destroy(hpb_csr_tri* tri) {
+    if (tri == nullptr) return HPB_SUCCESS;
+    hpb::tri::release(&tri->plan);
+    delete tri;
+    return HPB_SUCCESS;
+}
+
+int hpb_csr_tri_info(const hpb_csr_tri* tri, int32_t* tiles, int32_t* max_levels, int64_t* sum_levels,
+                     int* has_diagonal) {
+    if (tri == nullptr) return HPB_ERROR_INVALID_VALUE;
+    if (tiles) *tiles = tri->plan.ntiles;
+    if (max_levels) *max_levels = tri->plan.max_levels;
+    if (sum_levels) *sum_levels = tri->plan.sum_levels;
+    if (has_diagonal) *has_diagonal = tri->plan.all_diag;
+    return HPB_SUCCESS;
+}
+
+int hpb_csr_tri_check(hpb_context* ctx, const hpb_csr_tri* tri) {
+    HPB_CHECK_CTX(ctx);
+    if (tri == nullptr) return hpb::set_error(ctx, HPB_ERROR_INVALID_VALUE, "hpb_csr_tri_check: null analysis");
+    if (tri->plan.err == nullptr) return HPB_SUCCESS;
+    int h = 0;
+    HPB_CUDA_TRY(ctx, cudaMemcpyAsync(&h, tri->plan.err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    HPB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h & hpb::tri::kErrTimeout)
+        return hpb::set_error(ctx, HPB_ERROR_TIMEOUT, "hpb_csr_tri_check: a bounded device-side wait gave up");
+    return HPB_SUCCESS;
+}
+
+int hpb_csr_trsv_f32(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const float* val, float alpha,
+                     const float* b, float* x) {
+    return hpb::trsv_impl<float>(ctx, tri, unit_diag, val, alpha, b, x, "hpb_csr_trsv_f32");
+}
+int hpb_csr_trsv_f64(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const double* val, double alpha,
+                     const double* b, double* x) {
+    return hpb::trsv_impl<double>(ctx, tri, unit_diag, val, alpha, b, x, "hpb_csr_trsv_f64");
+}
+int hpb_csr_trsv_c64(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const void* val, hpb_c64 alpha,
+                     const void* b, void* x) {
+    return hpb::trsv_impl<cf>(ctx, tri, unit_diag, static_cast<const cf*>(val), cf{alpha.re, alpha.im},
+                              static_cast<const cf*>(b), static_cast<cf*>(x), "hpb_csr_trsv_c64");
+}
+int hpb_csr_trsv_c128(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const void* val, hpb_c128 alpha,
+                      const void* b, void* x) {
+    return hpb::trsv_impl<cd>(ctx, tri, unit_diag, static_cast<const cd*>(val), cd{alpha.re, alpha.im},
+                              static_cast<const cd*>(b), static_cast<cd*>(x), "hpb_csr_trsv_c128");
+}
+
+int hpb_csr_ilu0_f32(hpb_context* ctx, const hpb_csr_tri* lower, float* val) {
+    return hpb::ilu0_impl<float>(ctx, lower, val, "hpb_csr_ilu0_f32");
+}
+int hpb_csr_ilu0_f64(hpb_context* ctx, const hpb_csr_tri* lower, double* val) {
+    return hpb::ilu0_impl<double>(ctx, lower, val, "hpb_csr_ilu0_f64");
+}
+int hpb_csr_ilu0_c64(hpb_context* ctx, const hpb_csr_tri* lower, void* val) {
+    return hpb::ilu0_impl<cf>(ctx, lower, static_cast<cf*>(val), "hpb_csr_ilu0_c64");
+}
+int hpb_csr_ilu0_c128(hpb_context* ctx, const hpb_csr_tri* lower, void* val) {
+    return hpb::ilu0_impl<cd>(ctx, lower, static_cast<cd*>(val), "hpb_csr_ilu0_c128");
+}
+
+}  // extern "C"

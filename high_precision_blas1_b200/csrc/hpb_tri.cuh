@@ -1,0 +1,77 @@
+// Sparse triangular solves and the ILU(0) factorization on CSR matrices.
+//
+// Replaces csr::gpu_matrix::triangular_solve_lower / triangular_solve_upper
+// (common/csr/gpu_matrix.h:142-311: cuSPARSE csrsv2 with a per-call
+// analysis and cudaMalloc'd buffer) and gives csr::preconditioner
+// (common/csr/preconditioner.h:32-85) and csr::gpu_ilu0_preconditioner
+// (common/csr/gpu_ilu0_preconditioner.h:32-80) their factors.
+//
+// An analysis (hpb_csr_tri) is made once per sparsity pattern and triangle:
+// rows are cut into tiles of kTriTile consecutive rows; inside a tile each
+// row gets its level (longest chain of in-tile dependencies), and the tile's
+// rows are stored in level order as packed descriptors.  A solve is one
+// kernel: each block takes the next tile by ticket (ascending for a lower,
+// descending for an upper triangle), keeps the tile's solution in shared
+// memory, and its warps take the tile's levels round-robin, so a warp loads
+// the rows of its next level while earlier levels finish.  Dependencies on
+// other tiles wait on per-row flags (release/acquire at GPU scope); every
+// wait has an iteration limit after which the kernel records a timeout and
+// carries on, so a solve always ends.
+#pragma once
+
+#include "hpb_common.cuh"
+
+namespace hpb {
+namespace tri {
+
+constexpr int kTriTile = 8192;      // rows per tile
+constexpr int kTriThreads = 512;    // threads per solve block (16 warps)
+
+// Error bits of Plan::err (device).
+constexpr int kErrUnsorted = 1;     // column indices of a row not strictly increasing
+constexpr int kErrColumn = 2;       // column index outside [0, rows)
+constexpr int kErrTimeout = 4;      // a bounded wait gave up
+constexpr int kErrZeroPivot = 8;    // ILU(0): zero pivot
+
+struct Plan {
+    int device = 0;
+    int upper = 0;                  // 0: strictly lower part, 1: strictly upper part
+    int all_diag = 0;               // every row stores its diagonal
+    int32_t n = 0;
+    int64_t nnz = 0;
+    int32_t ntiles = 0;
+    int32_t max_levels = 0;         // largest level count of a tile
+    int64_t sum_levels = 0;         // levels summed over tiles
+    const int32_t* rp = nullptr;    // caller's structure; must stay valid and unchanged
+    const int32_t* ci = nullptr;
+    int4* desc = nullptr;           // n: (row, first dependency, dependency count, diagonal position) in level order
+    int32_t* lvlptr = nullptr;      // ntiles * (kTriTile + 1): level starts within the tile
+    int32_t* nlev = nullptr;        // ntiles
+    int32_t* dpos = nullptr;        // n: position of the diagonal entry of each row, -1 if absent
+    unsigned* flags = nullptr;      // n + 1: per-row done flags, then the tile ticket
+    int* err = nullptr;             // error bits
+    int* err_row = nullptr;         // ILU(0): first row with a zero pivot
+};
+
+int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* rp, const int32_t* ci, Plan* P);
+void release(Plan* P);
+
+// x := op^-1 (alpha b) for the plan's triangle; unit: the diagonal is taken
+// as 1 (stored diagonal entries are ignored).  Stream-ordered, no host sync;
+// b may equal x.  The flag reset and the solve are two graph-capturable
+// operations.
+template <class E>
+cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E* b, E* x, cudaStream_t s);
+
+// ILU(0) in place on val (lower plan): val := L\U with L unit lower
+// (strictly lower entries stored) and U upper (diagonal included).
+template <class E>
+cudaError_t launch_ilu0(const Plan& P, E* val, cudaStream_t s);
+
+}  // namespace tri
+}  // namespace hpb
+
+// The C ABI handle is the plan.
+struct hpb_csr_tri {
+    hpb::tri::Plan plan;
+};
