@@ -34,6 +34,7 @@ STATUS = {
     -6: "HPB_ERROR_NOT_FINITE",
     -7: "HPB_ERROR_NOT_CONVERGED",
     -8: "HPB_ERROR_SIZE_LIMIT",
+    -9: "HPB_ERROR_TIMEOUT",
 }
 
 
@@ -125,6 +126,14 @@ for t in TYPES:
     _sig(f"hpb_csr_spmv_dot2_{t}", C.c_int, [P, I32, I32, I64, P, P, P, P, P, P, P])
     _sig(f"hpb_csr_diag_{t}", C.c_int, [P, I32, P, P, P, P])
     _sig(f"hpb_random_{t}", C.c_int, [P, I64, C.c_uint64, S, S, P])
+# sparse triangular solves and ILU(0)
+_sig("hpb_csr_tri_create", C.c_int, [P, C.c_int, I32, I64, P, P, C.POINTER(P)])
+_sig("hpb_csr_tri_destroy", C.c_int, [P])
+_sig("hpb_csr_tri_info", C.c_int, [P, C.POINTER(I32), C.POINTER(I32), C.POINTER(I64), C.POINTER(C.c_int)])
+_sig("hpb_csr_tri_check", C.c_int, [P, P])
+for t in TYPES:
+    _sig(f"hpb_csr_trsv_{t}", C.c_int, [P, P, C.c_int, P, SCALAR[t], P, P])
+    _sig(f"hpb_csr_ilu0_{t}", C.c_int, [P, P, P])
 _sig("hpb_gendot_f64", C.c_int, [C.c_uint64, I64, C.c_double, P, P, C.POINTER(C.c_int64)])
 _sig("hpb_gendot_c128", C.c_int, [C.c_uint64, I64, C.c_double, P, P])
 _sig("hpb_copy", C.c_int, [P, I64, C.c_size_t, P, P])

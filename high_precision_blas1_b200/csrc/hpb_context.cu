@@ -111,6 +111,7 @@ const char* hpb_status_string(int status) {
         case HPB_ERROR_NOT_FINITE: return "HPB_ERROR_NOT_FINITE";
         case HPB_ERROR_NOT_CONVERGED: return "HPB_ERROR_NOT_CONVERGED";
         case HPB_ERROR_SIZE_LIMIT: return "HPB_ERROR_SIZE_LIMIT";
+        case HPB_ERROR_TIMEOUT: return "HPB_ERROR_TIMEOUT";
         default: return "HPB_UNKNOWN_STATUS";
     }
 }

@@ -22,8 +22,13 @@ namespace {
 
 constexpr int kLvThreads = 512;
 constexpr int kPre = 4;                          // dependencies per row prefetched into registers
-constexpr long long kSpinShared = 1ll << 24;     // polls of the tile's level counter (shared memory)
-constexpr long long kSpinGlobal = 1ll << 20;     // polls of another tile's row flag (L2)
+constexpr int kMerge = 8;                        // ILU(0): update pairs per batch of loads
+// Every wait ends after kWaitNs of GPU time (%globaltimer) at the latest.
+// A legitimate wait lasts at most as long as the launch itself (a tile waits
+// for rows of tiles that started earlier), so a launch whose waits run out
+// is either broken or a factorization / solve whose dependency chain takes
+// seconds; both report HPB_ERROR_TIMEOUT.
+constexpr unsigned long long kWaitNs = 4000000000ull;
 
 // ---- arithmetic -----------------------------------------------------------
 __device__ __forceinline__ float fms(float a, float l, float u) { return __fmaf_rn(-l, u, a); }
@@ -95,28 +100,54 @@ __device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// A timeout is sticky: once one wait has given up, every later wait of the
+// launch returns at its next check of the error word, so a failed launch
+// ends within about one wait limit instead of one limit per waiting row.
+__device__ __forceinline__ bool timed_out(const int* err) {
+    return (*reinterpret_cast<const volatile int*>(err) & kErrTimeout) != 0;
+}
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Deadline bookkeeping for one wait: check() every `every` polls; true when
+// the wait must stop (limit reached, recorded; or another wait timed out).
+struct Waiter {
+    unsigned long long t0 = 0;
+    long long it = 0;
+    __device__ __forceinline__ bool check(int* err, int every_mask) {
+        if ((++it & every_mask) != 0) return false;
+        if (timed_out(err)) return true;
+        const unsigned long long now = gtimer();
+        if (t0 == 0) {
+            t0 = now;
+            return false;
+        }
+        if (now - t0 > kWaitNs) {
+            atomicOr(err, kErrTimeout);
+            return true;
+        }
+        return false;
+    }
+};
+
 // Wait (bounded) until row j of another tile is published.
 __device__ __forceinline__ void wait_row(const unsigned* flags, int32_t j, int* err) {
-    long long it = 0;
-    while (ld_acquire(flags + j) == 0u) {
-        if (++it > kSpinGlobal) {
-            atomicOr(err, kErrTimeout);
-            return;
-        }
-    }
+    Waiter w;
+    while (ld_acquire(flags + j) == 0u)
+        if (w.check(err, 63)) return;
 }
 
 // Lane 0 waits (bounded) until the tile's levels [0, l) are complete; then
 // the warp may read what those levels wrote.
 __device__ __forceinline__ void wait_levels(volatile int* done, int l, int lane, int* err) {
     if (lane == 0) {
-        long long it = 0;
-        while (*done < l) {
-            if (++it > kSpinShared) {
-                atomicOr(err, kErrTimeout);
-                break;
-            }
-        }
+        Waiter w;
+        while (*done < l)
+            if (w.check(err, 1023)) break;
     }
     __syncwarp();
     __threadfence_block();
@@ -164,7 +195,7 @@ template <bool UPPER>
 __global__ void __launch_bounds__(kLvThreads)
 k_tri_levels(int32_t n, const int32_t* __restrict__ ci, const int32_t* __restrict__ beg,
              const int32_t* __restrict__ cnt, const int32_t* __restrict__ dpos, int4* __restrict__ desc,
-             int32_t* __restrict__ lvlptr, int32_t* __restrict__ nlev) {
+             int4* __restrict__ dcol, int32_t* __restrict__ lvlptr, int32_t* __restrict__ nlev) {
     extern __shared__ int sh[];
     volatile int* lev = sh;          // kTriTile
     int* hist = sh + kTriTile;       // kTriTile + 1
@@ -238,22 +269,133 @@ k_tri_levels(int32_t n, const int32_t* __restrict__ ci, const int32_t* __restric
     for (int r = threadIdx.x; r < m; r += blockDim.x) {
         const int pos = atomicAdd(&hist[lev[r]], 1);
         const int32_t i = base + r;
-        desc[base + pos] = make_int4(i, __ldg(beg + i), __ldg(cnt + i), __ldg(dpos + i));
+        const int32_t b = __ldg(beg + i), c = __ldg(cnt + i);
+        desc[base + pos] = make_int4(i, b, c, __ldg(dpos + i));
+        dcol[base + pos] = make_int4(c > 0 ? __ldg(ci + b) : -1, c > 1 ? __ldg(ci + b + 1) : -1,
+                                     c > 2 ? __ldg(ci + b + 2) : -1, c > 3 ? __ldg(ci + b + 3) : -1);
     }
 }
 
 // ---- solve ----------------------------------------------------------------
+// Rows of other tiles are read from x itself: the solve first fills x with
+// a signalling-NaN sentinel, which no arithmetic operation returns (IEEE
+// 754 operations deliver quiet NaNs), and every row's value is stored once
+// with a relaxed store of the whole (8- or 4-byte) word.  A reader that
+// loads anything but the sentinel therefore holds the final value: one L2
+// round trip per dependency, issued with the row's other loads before the
+// warp waits for its level, instead of a flag acquire followed by the load.
+constexpr unsigned long long kSent64 = 0x7FF0DEAD0000BEEFull;  // exponent all ones, quiet bit 0
+constexpr unsigned kSent32 = 0x7F80BEEFu;
+
+__device__ __forceinline__ unsigned long long ld_relaxed64(const void* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned ld_relaxed32(const void* p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed64(void* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed32(void* p, unsigned v) {
+    asm volatile("st.relaxed.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Published values: load / store / fill / "still the sentinel" per element
+// type (complex: per component; a component is final once it is not the
+// sentinel).
+template <class E> struct Pub;
+template <> struct Pub<double> {
+    static __device__ __forceinline__ double load(const double* x, int64_t j) {
+        return __longlong_as_double(static_cast<long long>(ld_relaxed64(x + j)));
+    }
+    static __device__ __forceinline__ void store(double* x, int64_t i, double v) {
+        st_relaxed64(x + i, static_cast<unsigned long long>(__double_as_longlong(v)));
+    }
+    static __device__ __forceinline__ bool pending(double v) {
+        return static_cast<unsigned long long>(__double_as_longlong(v)) == kSent64;
+    }
+    static __device__ __forceinline__ void fill(double* x, int64_t i) {
+        x[i] = __longlong_as_double(static_cast<long long>(kSent64));
+    }
+};
+template <> struct Pub<float> {
+    static __device__ __forceinline__ float load(const float* x, int64_t j) {
+        return __uint_as_float(ld_relaxed32(x + j));
+    }
+    static __device__ __forceinline__ void store(float* x, int64_t i, float v) {
+        st_relaxed32(x + i, __float_as_uint(v));
+    }
+    static __device__ __forceinline__ bool pending(float v) { return __float_as_uint(v) == kSent32; }
+    static __device__ __forceinline__ void fill(float* x, int64_t i) { x[i] = __uint_as_float(kSent32); }
+};
+template <> struct Pub<cd> {
+    static __device__ __forceinline__ cd load(const cd* x, int64_t j) {
+        const double* q = reinterpret_cast<const double*>(x + j);
+        return cd{Pub<double>::load(q, 0), Pub<double>::load(q, 1)};
+    }
+    static __device__ __forceinline__ void store(cd* x, int64_t i, cd v) {
+        double* q = reinterpret_cast<double*>(x + i);
+        Pub<double>::store(q, 0, v.re);
+        Pub<double>::store(q, 1, v.im);
+    }
+    static __device__ __forceinline__ bool pending(cd v) { return Pub<double>::pending(v.re) || Pub<double>::pending(v.im); }
+    static __device__ __forceinline__ void fill(cd* x, int64_t i) {
+        double* q = reinterpret_cast<double*>(x + i);
+        Pub<double>::fill(q, 0);
+        Pub<double>::fill(q, 1);
+    }
+};
+template <> struct Pub<cf> {
+    static __device__ __forceinline__ cf load(const cf* x, int64_t j) {
+        const float* q = reinterpret_cast<const float*>(x + j);
+        return cf{Pub<float>::load(q, 0), Pub<float>::load(q, 1)};
+    }
+    static __device__ __forceinline__ void store(cf* x, int64_t i, cf v) {
+        float* q = reinterpret_cast<float*>(x + i);
+        Pub<float>::store(q, 0, v.re);
+        Pub<float>::store(q, 1, v.im);
+    }
+    static __device__ __forceinline__ bool pending(cf v) { return Pub<float>::pending(v.re) || Pub<float>::pending(v.im); }
+    static __device__ __forceinline__ void fill(cf* x, int64_t i) {
+        float* q = reinterpret_cast<float*>(x + i);
+        Pub<float>::fill(q, 0);
+        Pub<float>::fill(q, 1);
+    }
+};
+
+// Wait (bounded) until x[j], as last loaded into v, is published.
+template <class E>
+__device__ __forceinline__ E await_value(const E* x, int32_t j, E v, int* err) {
+    Waiter w;
+    while (Pub<E>::pending(v)) {
+        if (w.check(err, 63)) break;
+        v = Pub<E>::load(x, j);
+    }
+    return v;
+}
+
+template <class E>
+__global__ void k_tri_fill(int32_t n, E* __restrict__ x, unsigned* ticket) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *ticket = 0u;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        Pub<E>::fill(x, i);
+}
+
 template <class E, bool UPPER, bool UNIT>
 __global__ void __launch_bounds__(kTriThreads)
-k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int32_t* __restrict__ lvlptr,
-       const int32_t* __restrict__ nlev, const int32_t* __restrict__ ci, const E* __restrict__ val, E alpha,
-       const E* b, E* x, unsigned* flags, int* err) {
+k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int4* __restrict__ dcol,
+       const int32_t* __restrict__ lvlptr, const int32_t* __restrict__ nlev, const int32_t* __restrict__ ci,
+       const E* __restrict__ val, E alpha, const E* __restrict__ b, E* x, unsigned* ticket, int* err) {
     extern __shared__ __align__(16) unsigned char smraw[];
     E* xs = reinterpret_cast<E*>(smraw);
     __shared__ int s_tile;
     __shared__ int s_done;
     if (threadIdx.x == 0) {
-        const int tk = int(atomicAdd(flags + n, 1u));
+        const int tk = int(atomicAdd(ticket, 1u));
         s_tile = UPPER ? ntiles - 1 - tk : tk;
         s_done = 0;
     }
@@ -267,28 +409,29 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int32_t* 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int W = kTriThreads / 32;
     volatile int* done = &s_done;
-    auto fetch = [&](int32_t j) -> E {
-        const int32_t jl = j - base;
-        if (jl >= 0 && jl < m) return xs[jl];
-        wait_row(flags, j, err);
-        return ldcgE(x, j);
-    };
     for (int l = warp; l < L; l += W) {
         const int32_t p0 = lp[l], p1 = lp[l + 1];
-        int32_t last_row = -1;
+        int32_t pub_row = -1;
+        E pub_val{};
         for (int32_t q = p0; q < p1; q += 32) {
             const int32_t p = q + lane;
             const bool act = p < p1;
-            // the row's data does not depend on the solve: load it before waiting
-            int4 d = make_int4(0, 0, 0, -1);
-            if (act) d = desc[base + p];
+            // The row's data and its other-tile dependencies, loaded before
+            // the wait: the descriptor and the first dependency columns
+            // (one round trip), then b, the values and x of other tiles
+            // (a second one).
+            int4 d = make_int4(0, 0, 0, -1), c4 = make_int4(-1, -1, -1, -1);
+            if (act) {
+                d = desc[base + p];
+                c4 = dcol[base + p];
+            }
+            const int32_t col[kPre] = {c4.x, c4.y, c4.z, c4.w};
             E rhs{}, dg{};
-            int32_t col[kPre];
-            E v[kPre];
+            E v[kPre], xv[kPre];
 #pragma unroll
             for (int k = 0; k < kPre; ++k) {
-                col[k] = 0;
                 v[k] = E{};
+                xv[k] = E{};
             }
             if (act) {
                 rhs = scale(alpha, ldE(b, d.x));
@@ -296,8 +439,9 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int32_t* 
 #pragma unroll
                 for (int k = 0; k < kPre; ++k)
                     if (k < d.z) {
-                        col[k] = __ldg(ci + d.y + k);
                         v[k] = ldE(val, d.y + k);
+                        const int32_t jl = col[k] - base;
+                        if (!(jl >= 0 && jl < m)) xv[k] = Pub<E>::load(x, col[k]);
                     }
             }
             if (q == p0) wait_levels(done, l, lane, err);
@@ -305,15 +449,24 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int32_t* 
                 E acc = rhs;
 #pragma unroll
                 for (int k = 0; k < kPre; ++k)
-                    if (k < d.z) acc = fms(acc, v[k], fetch(col[k]));
-                for (int32_t e = d.y + kPre; e < d.y + d.z; ++e) acc = fms(acc, ldE(val, e), fetch(__ldg(ci + e)));
+                    if (k < d.z) {
+                        const int32_t jl = col[k] - base;
+                        const E xj = (jl >= 0 && jl < m) ? xs[jl] : await_value(x, col[k], xv[k], err);
+                        acc = fms(acc, v[k], xj);
+                    }
+                for (int32_t e = d.y + kPre; e < d.y + d.z; ++e) {
+                    const int32_t j = __ldg(ci + e), jl = j - base;
+                    const E xj = (jl >= 0 && jl < m) ? xs[jl] : await_value(x, j, Pub<E>::load(x, j), err);
+                    acc = fms(acc, ldE(val, e), xj);
+                }
                 if (!UNIT) acc = quot(acc, dg);
                 xs[d.x - base] = acc;
-                stE(x, d.x, acc);
-                if (q + 32 < p1)
-                    st_release(flags + d.x, 1u);  // more chunks follow in this level: publish now
-                else
-                    last_row = d.x;
+                if (q + 32 < p1) {
+                    Pub<E>::store(x, d.x, acc);  // more chunks follow in this level
+                } else {
+                    pub_row = d.x;
+                    pub_val = acc;
+                }
             }
         }
         __syncwarp();
@@ -321,9 +474,9 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int32_t* 
             __threadfence_block();
             *done = l + 1;
         }
-        // publish to other tiles after the in-tile announcement (the release
-        // makes this thread's store of x visible first)
-        if (last_row >= 0) st_release(flags + last_row, 1u);
+        // the global store after the in-tile announcement, so the block fence
+        // above never waits on it
+        if (pub_row >= 0) Pub<E>::store(x, pub_row, pub_val);
     }
 }
 
@@ -371,19 +524,37 @@ k_ilu0(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int32_t* 
                 const int32_t dk = __ldg(dpos + k);
                 const E lik = quot(ldcgE(val, e), ldcgE(val, dk));
                 stcgE(val, e, lik);
+                // Merge the columns after e in row i with those after the
+                // diagonal in row k; the matching pairs are collected first
+                // (columns only, read-only path) and their values then loaded
+                // as one batch, so a batch costs one L2 round trip.
                 int32_t pi = e + 1, pk = dk + 1;
                 const int32_t pk_end = __ldg(rp + k + 1);
-                while (pi < e_end && pk < pk_end) {
-                    const int32_t ca = __ldg(ci + pi), cb = __ldg(ci + pk);
-                    if (ca == cb) {
-                        stcgE(val, pi, fms(ldcgE(val, pi), lik, ldcgE(val, pk)));
-                        ++pi;
-                        ++pk;
-                    } else if (ca < cb) {
-                        ++pi;
-                    } else {
-                        ++pk;
+                for (;;) {
+                    int32_t P[kMerge], Q[kMerge];
+                    int np = 0;
+                    while (np < kMerge && pi < e_end && pk < pk_end) {
+                        const int32_t ca = __ldg(ci + pi), cb = __ldg(ci + pk);
+                        if (ca == cb) {
+                            P[np] = pi++;
+                            Q[np++] = pk++;
+                        } else if (ca < cb) {
+                            ++pi;
+                        } else {
+                            ++pk;
+                        }
                     }
+                    E a[kMerge], u[kMerge];
+#pragma unroll
+                    for (int j = 0; j < kMerge; ++j)
+                        if (j < np) {
+                            a[j] = ldcgE(val, P[j]);
+                            u[j] = ldcgE(val, Q[j]);
+                        }
+#pragma unroll
+                    for (int j = 0; j < kMerge; ++j)
+                        if (j < np) stcgE(val, P[j], fms(a[j], lik, u[j]));
+                    if (np < kMerge) break;
                 }
             }
             if (zero_of(ldcgE(val, d.w))) {
@@ -428,7 +599,7 @@ int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* 
         return set_error(ctx, status, "hpb_csr_tri_create: %s", what);
     };
     const size_t nn = size_t(n);
-    if (cudaMalloc(&P->desc, nn * sizeof(int4)) != cudaSuccess ||
+    if (cudaMalloc(&P->desc, nn * sizeof(int4)) != cudaSuccess || cudaMalloc(&P->dcol, nn * sizeof(int4)) != cudaSuccess ||
         cudaMalloc(&P->lvlptr, size_t(P->ntiles) * (kTriTile + 1) * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&P->nlev, size_t(P->ntiles) * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&P->dpos, nn * sizeof(int32_t)) != cudaSuccess ||
@@ -446,12 +617,12 @@ int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* 
     const size_t lv_smem = (2 * size_t(kTriTile) + 1) * sizeof(int);
     if (P->upper) {
         allow_smem(k_tri_levels<true>, lv_smem);
-        k_tri_levels<true><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, ci, beg, cnt, P->dpos, P->desc, P->lvlptr,
-                                                                   P->nlev);
+        k_tri_levels<true><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, ci, beg, cnt, P->dpos, P->desc, P->dcol,
+                                                                   P->lvlptr, P->nlev);
     } else {
         allow_smem(k_tri_levels<false>, lv_smem);
-        k_tri_levels<false><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, ci, beg, cnt, P->dpos, P->desc, P->lvlptr,
-                                                                    P->nlev);
+        k_tri_levels<false><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, ci, beg, cnt, P->dpos, P->desc, P->dcol,
+                                                                    P->lvlptr, P->nlev);
     }
     count_launch(2);
     if (cudaGetLastError() != cudaSuccess) return fail(HPB_ERROR_CUDA, "analysis launch failed");
@@ -481,11 +652,15 @@ int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* 
 
 void release(Plan* P) {
     cudaFree(P->desc);
+    cudaFree(P->dcol);
+    P->dcol = nullptr;
     cudaFree(P->lvlptr);
     cudaFree(P->nlev);
     cudaFree(P->dpos);
     cudaFree(P->flags);
     cudaFree(P->err);
+    cudaFree(P->scratch);
+    P->scratch = nullptr;
     P->desc = nullptr;
     P->lvlptr = P->nlev = P->dpos = nullptr;
     P->flags = nullptr;
@@ -495,8 +670,8 @@ void release(Plan* P) {
 template <class E>
 cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E* b, E* x, cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(P.flags, 0, (size_t(P.n) + 1) * sizeof(unsigned), s);
-    if (e != cudaSuccess) return e;
+    const int fill_grid = int(std::min<int64_t>((int64_t(P.n) + 255) / 256, 148 * 8));
+    k_tri_fill<E><<<fill_grid, 256, 0, s>>>(P.n, x, P.flags + P.n);
     const size_t sm = size_t(kTriTile) * sizeof(E);
     static std::once_flag once;
     std::call_once(once, [&] {
@@ -507,9 +682,9 @@ cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E*
     });
     auto k = P.upper ? (unit ? k_trsv<E, true, true> : k_trsv<E, true, false>)
                      : (unit ? k_trsv<E, false, true> : k_trsv<E, false, false>);
-    k<<<P.ntiles, kTriThreads, sm, s>>>(P.n, P.ntiles, P.desc, P.lvlptr, P.nlev, P.ci, val, alpha, b, x, P.flags,
-                                        P.err);
-    count_launch();
+    k<<<P.ntiles, kTriThreads, sm, s>>>(P.n, P.ntiles, P.desc, P.dcol, P.lvlptr, P.nlev, P.ci, val, alpha, b, x,
+                                        P.flags + P.n, P.err);
+    count_launch(2);
     return cudaGetLastError();
 }
 
@@ -554,6 +729,23 @@ int trsv_impl(hpb_context* ctx, const hpb_csr_tri* tri, int unit, const E* val, 
         return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: pointer not aligned to its element type", name);
     if (!unit && !P.all_diag)
         return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: a row stores no diagonal entry (structural zero)", name);
+    const size_t bytes = size_t(P.n) * sizeof(E);
+    const char* bb = reinterpret_cast<const char*>(b);
+    const char* xb = reinterpret_cast<const char*>(x);
+    if (b != x && bb < xb + bytes && xb < bb + bytes)
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: b and x overlap without being equal", name);
+    if (b == x) {  // in place: solve into the analysis' scratch, then copy back
+        tri::Plan& Pm = const_cast<tri::Plan&>(P);
+        if (Pm.scratch == nullptr && cudaMalloc(&Pm.scratch, size_t(P.n) * 16) != cudaSuccess) {
+            cudaGetLastError();
+            Pm.scratch = nullptr;
+            return set_error(ctx, HPB_ERROR_OUT_OF_MEMORY, "%s: in-place scratch allocation failed", name);
+        }
+        E* tmp = static_cast<E*>(Pm.scratch);
+        HPB_CUDA_TRY(ctx, tri::launch_trsv<E>(P, unit, val, alpha, b, tmp, ctx->stream));
+        HPB_CUDA_TRY(ctx, cudaMemcpyAsync(x, tmp, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+        return HPB_SUCCESS;
+    }
     HPB_CUDA_TRY(ctx, tri::launch_trsv<E>(P, unit, val, alpha, b, x, ctx->stream));
     return HPB_SUCCESS;
 }

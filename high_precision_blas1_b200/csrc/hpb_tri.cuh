@@ -14,9 +14,11 @@
 // descending for an upper triangle), keeps the tile's solution in shared
 // memory, and its warps take the tile's levels round-robin, so a warp loads
 // the rows of its next level while earlier levels finish.  Dependencies on
-// other tiles wait on per-row flags (release/acquire at GPU scope); every
-// wait has an iteration limit after which the kernel records a timeout and
-// carries on, so a solve always ends.
+// other tiles poll the value itself (x is pre-filled with a signalling-NaN
+// sentinel); the factorization, whose rows are read as a whole, uses per-row
+// flags (release/acquire at GPU scope).  Every wait has an iteration limit
+// after which the kernel records a timeout and carries on, so a launch
+// always ends.
 #pragma once
 
 #include "hpb_common.cuh"
@@ -45,10 +47,12 @@ struct Plan {
     const int32_t* rp = nullptr;    // caller's structure; must stay valid and unchanged
     const int32_t* ci = nullptr;
     int4* desc = nullptr;           // n: (row, first dependency, dependency count, diagonal position) in level order
+    int4* dcol = nullptr;           // n: columns of the first four dependencies (-1: none), in level order
     int32_t* lvlptr = nullptr;      // ntiles * (kTriTile + 1): level starts within the tile
     int32_t* nlev = nullptr;        // ntiles
     int32_t* dpos = nullptr;        // n: position of the diagonal entry of each row, -1 if absent
-    unsigned* flags = nullptr;      // n + 1: per-row done flags, then the tile ticket
+    unsigned* flags = nullptr;      // n + 1: per-row done flags (factorization), then the tile ticket
+    void* scratch = nullptr;        // n * 16 bytes, allocated on the first in-place solve
     int* err = nullptr;             // error bits
     int* err_row = nullptr;         // ILU(0): first row with a zero pivot
 };
@@ -58,8 +62,8 @@ void release(Plan* P);
 
 // x := op^-1 (alpha b) for the plan's triangle; unit: the diagonal is taken
 // as 1 (stored diagonal entries are ignored).  Stream-ordered, no host sync;
-// b may equal x.  The flag reset and the solve are two graph-capturable
-// operations.
+// b and x must not overlap.  Two graph-capturable launches (the sentinel
+// fill of x, the solve).
 template <class E>
 cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E* b, E* x, cudaStream_t s);
 

@@ -50,7 +50,8 @@ typedef enum hpb_status {
     HPB_ERROR_BREAKDOWN = -5,       /* solver breakdown (rho == 0, ...) */
     HPB_ERROR_NOT_FINITE = -6,      /* NaN/Inf met where a finite value is required */
     HPB_ERROR_NOT_CONVERGED = -7,   /* solver stopped at max_iters above tolerance */
-    HPB_ERROR_SIZE_LIMIT = -8       /* n above the stated maximum of an allocation-free entry point */
+    HPB_ERROR_SIZE_LIMIT = -8,      /* n above the stated maximum of an allocation-free entry point */
+    HPB_ERROR_TIMEOUT = -9          /* a bounded device-side wait gave up (results not valid) */
 } hpb_status;
 
 typedef struct hpb_context hpb_context;
@@ -314,6 +315,59 @@ int hpb_csr_diag_c64(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, con
                      const void* val, void* diag);
 int hpb_csr_diag_c128(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,
                       const void* val, void* diag);
+
+/* ---------------------------------------------------------------------- */
+/* Sparse triangular solves and ILU(0) (replace csr::gpu_matrix::          */
+/* triangular_solve_lower / triangular_solve_upper, common/csr/           */
+/* gpu_matrix.h:142-311, i.e. cuSPARSE csrsv2 with a per-call analysis    */
+/* and cudaMalloc'd buffer; and the factors csr::preconditioner           */
+/* (common/csr/preconditioner.h:32-85) and csr::gpu_ilu0_preconditioner    */
+/* (common/csr/gpu_ilu0_preconditioner.h:32-80) apply).                    */
+/*                                                                          */
+/* An analysis of one triangle of a CSR pattern (0-based, int32, columns   */
+/* strictly increasing in each row) is made once and reused for any values */
+/* on that pattern.  It keeps row_ptr / col_ind by address: they must stay  */
+/* valid and unchanged while the analysis is used.  upper = 0: the strictly */
+/* lower part is used (entries with column > row are ignored); upper = 1:  */
+/* the strictly upper part.                                                 */
+/* ---------------------------------------------------------------------- */
+typedef struct hpb_csr_tri hpb_csr_tri;
+int hpb_csr_tri_create(hpb_context* ctx, int upper, int32_t rows, int64_t nnz, const int32_t* row_ptr,
+                       const int32_t* col_ind, hpb_csr_tri** tri);
+int hpb_csr_tri_destroy(hpb_csr_tri* tri);
+/* Row tiles, the largest level count of a tile, levels summed over tiles,
+ * and whether every row stores its diagonal (any argument may be NULL). */
+int hpb_csr_tri_info(const hpb_csr_tri* tri, int32_t* tiles, int32_t* max_levels, int64_t* sum_levels,
+                     int* has_diagonal);
+/* x := T^-1 (alpha b), T the analysed triangle of (row_ptr, col_ind, val)
+ * with its stored diagonal, or with a unit diagonal when unit_diag != 0
+ * (stored diagonal entries then ignored, as CUSPARSE_DIAG_TYPE_UNIT).
+ * Stream-ordered on the context's stream, no host synchronisation; b may
+ * equal x (in place: the analysis allocates an n-element scratch on the
+ * first such call), other overlaps are refused.  A zero diagonal gives
+ * Inf/NaN in x (csrsv2 reports it as a numerical zero and continues
+ * likewise).  Not safe for concurrent calls with the same analysis. */
+int hpb_csr_trsv_f32(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const float* val, float alpha,
+                     const float* b, float* x);
+int hpb_csr_trsv_f64(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const double* val, double alpha,
+                     const double* b, double* x);
+int hpb_csr_trsv_c64(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const void* val, hpb_c64 alpha,
+                     const void* b, void* x);
+int hpb_csr_trsv_c128(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const void* val, hpb_c128 alpha,
+                      const void* b, void* x);
+/* Blocking: HPB_ERROR_TIMEOUT if a bounded device-side wait of an earlier
+ * solve with this analysis gave up (cannot happen for a valid analysis). */
+int hpb_csr_tri_check(hpb_context* ctx, const hpb_csr_tri* tri);
+/* ILU(0) in place (lower analysis of the pattern; every row must store its
+ * diagonal): val := L\U, L unit lower (strictly lower entries stored), U
+ * upper with its diagonal, the incomplete factors on A's pattern (IKJ
+ * variant).  Then apply M^-1 = U^-1 L^-1 by hpb_csr_trsv_* with the lower
+ * analysis (unit_diag = 1) and an upper analysis (unit_diag = 0) on the
+ * same val.  Blocking; HPB_ERROR_BREAKDOWN on a zero pivot. */
+int hpb_csr_ilu0_f32(hpb_context* ctx, const hpb_csr_tri* lower, float* val);
+int hpb_csr_ilu0_f64(hpb_context* ctx, const hpb_csr_tri* lower, double* val);
+int hpb_csr_ilu0_c64(hpb_context* ctx, const hpb_csr_tri* lower, void* val);
+int hpb_csr_ilu0_c128(hpb_context* ctx, const hpb_csr_tri* lower, void* val);
 
 /* ---------------------------------------------------------------------- */
 /* Krylov solvers on a CSR matrix (the reference's bicgstabl.h, gmres.h,   */

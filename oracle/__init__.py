@@ -59,6 +59,13 @@ def oro():
             getattr(lib, name).restype = D
         lib.oro_bound_dot2_block_real.argtypes = [D, D, D, D]
         lib.oro_bound_dot2_block_real.restype = D
+        for suf in ("f32", "f64", "c64", "c128"):
+            f = getattr(lib, "oro_csr_trsv_" + suf)
+            f.argtypes = [C.c_int32, P, P, P, C.c_int, C.c_int, P, P, P]
+            f.restype = C.c_int
+            f = getattr(lib, "oro_csr_ilu0_" + suf)
+            f.argtypes = [C.c_int32, P, P, P]
+            f.restype = C.c_int32
         _ORO = lib
     return _ORO
 
@@ -247,3 +254,38 @@ def bound_dot2(n: int, cond: float, complex_: bool = False, eps: float = 2.0 ** 
 
 def bound_sum2(n: int, cond: float, eps: float = 2.0 ** -52) -> float:
     return oro().oro_bound_sum2(float(max(n, 2)), float(cond), eps)
+
+
+_TRI_SUFFIX = {np.dtype(np.float32): "f32", np.dtype(np.float64): "f64", np.dtype(np.complex64): "c64",
+               np.dtype(np.complex128): "c128"}
+
+
+def csr_trsv(row_ptr: np.ndarray, col_ind: np.ndarray, val: np.ndarray, b: np.ndarray, upper: bool, unit: bool,
+             alpha=1.0) -> np.ndarray:
+    """x = T^-1 (alpha b) for the lower (upper=False) or upper triangle of a
+    CSR matrix, by forward / backward substitution (oracle/tri.c)."""
+    suf = _TRI_SUFFIX[val.dtype]
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    ci = np.ascontiguousarray(col_ind, dtype=np.int32)
+    v = np.ascontiguousarray(val)
+    bb = np.ascontiguousarray(b, dtype=val.dtype)
+    x = np.zeros_like(bb)
+    a = np.array([alpha], dtype=val.dtype)
+    st = getattr(oro(), "oro_csr_trsv_" + suf)(len(rp) - 1, _ptr(rp), _ptr(ci), _ptr(v), int(upper), int(unit),
+                                               _ptr(a), _ptr(bb), _ptr(x))
+    if st != 0:
+        raise ValueError("a row stores no diagonal")
+    return x
+
+
+def csr_ilu0(row_ptr: np.ndarray, col_ind: np.ndarray, val: np.ndarray):
+    """ILU(0) factors on A's pattern (L unit lower, U upper, stored in one
+    array like the input), and the first zero-pivot row (-1 if none)."""
+    suf = _TRI_SUFFIX[val.dtype]
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    ci = np.ascontiguousarray(col_ind, dtype=np.int32)
+    lu = np.array(val, copy=True)
+    r = getattr(oro(), "oro_csr_ilu0_" + suf)(len(rp) - 1, _ptr(rp), _ptr(ci), _ptr(lu))
+    if r == -2:
+        raise ValueError("a row stores no diagonal")
+    return lu, int(r)
