@@ -154,7 +154,7 @@ class hpb_solver_report(C.Structure):
 
 
 SOLVER = {"bicgstabl": 0, "gmres": 1, "bicgstab": 2}
-PRECOND = {"none": 0, "jacobi": 1, "matrix": 2}
+PRECOND = {"none": 0, "jacobi": 1, "matrix": 2, "ilu0": 3}
 
 
 class hpb_ir_params(C.Structure):

@@ -11,6 +11,7 @@
 #pragma once
 
 #include "hpb_common.cuh"
+#include "hpb_tri.cuh"
 
 #include <memory>
 #include <vector>
@@ -325,12 +326,14 @@ struct SolverWorkspace {
 // a general CSR matrix M with the storage type of the iteration.
 template <class E>
 struct RightPrec {
-    int kind = 0;  // 0 none, 1 Jacobi, 2 CSR matrix
+    int kind = 0;  // 0 none, 1 Jacobi, 2 CSR matrix, 3 ILU(0) factors
     int32_t rows = 0;
     int64_t nnz = 0;
     const int32_t* rp = nullptr;
     const int32_t* ci = nullptr;
-    const E* val = nullptr;
+    const E* val = nullptr;                 // kind 2: M; kind 3: L\U on A's pattern
+    const hpb_csr_tri* lower = nullptr;     // kind 3: analyses of A's triangles
+    const hpb_csr_tri* upper = nullptr;
 };
 
 // Device-resident GMRES(m) (hpb_fused_gmres.cu); E in {float, double, cf, cd}.

@@ -503,6 +503,11 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
             k_gm_spmv<E><<<(M.rows + kGmThreads - 1) / kGmThreads, kGmThreads, 0, s>>>(M.rows, M.rp, M.ci, M.val, vi, Z);
             src = Z;
             ++kernels;
+        } else if (M.kind == 3) {  // z = U^-1 L^-1 v_i (R is free inside the cycle)
+            tri::launch_trsv<E>(M.lower->plan, 1, M.val, unit_of<E>(), vi, R, s);
+            tri::launch_trsv<E>(M.upper->plan, 0, M.val, unit_of<E>(), R, Z, s);
+            src = Z;
+            kernels += 4;
         }
         k_gm_spmv<E><<<g_sp, kGmThreads, 0, s>>>(rows, rp, ci, val, src, W);
         k_multidot<E><<<g_md, kGmThreads, 0, s>>>(n, i + 1, V, W, partials);
@@ -527,10 +532,15 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
         cudaMemsetAsync(W, 0, vb, s);
         k_gs_update<E, false><<<g_ew, kGmThreads, 0, s>>>(n, m, V, W, W, st->neg_y, st, m, -1, partials, ticket,
                                                            badflag);
-        if (M.kind == 1)
+        if (M.kind == 1) {
             k_gm_jacobi<E><<<g_ew, kGmThreads, 0, s>>>(n, W, diag, Z);
-        else
+        } else if (M.kind == 2) {
             k_gm_spmv<E><<<(M.rows + kGmThreads - 1) / kGmThreads, kGmThreads, 0, s>>>(M.rows, M.rp, M.ci, M.val, W, Z);
+        } else {
+            tri::launch_trsv<E>(M.lower->plan, 1, M.val, unit_of<E>(), W, R, s);
+            tri::launch_trsv<E>(M.upper->plan, 0, M.val, unit_of<E>(), R, Z, s);
+            kernels += 3;
+        }
         k_gm_axpy<E><<<g_ew, kGmThreads, 0, s>>>(n, x, Z);
         kernels += 3;
     }

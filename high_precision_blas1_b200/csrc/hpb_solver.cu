@@ -9,7 +9,9 @@
 #include <memory>
 #include <new>
 #include <stdexcept>
+#include <type_traits>
 
+#include <common/csr/gpu_ilu0_preconditioner.h>
 #include <common/csr/gpu_matrix.h>
 #include <common/csr/linear_operator.h>
 #include <common/csr/preconditioner.h>
@@ -34,7 +36,62 @@ struct Stack {
     using MAT = csr::gpu_matrix<VO, cublas_wrap>;
     using LO = csr::linear_operator<VO, MAT>;
     using PJ = csr::jacobi_preconditioner<VO, LO, MAT>;
+    using PI = csr::gpu_ilu0_preconditioner<VO, LO, MAT>;
     using MON = hpb::solvers::default_monitor<VO>;
+};
+
+// The preconditioner the solver templates are instantiated with: Jacobi
+// (D^-1) or ILU(0) ((L U)^-1 by two sparse triangular solves).
+template <class S>
+struct AnyPrec {
+    std::unique_ptr<typename S::PJ> jac;
+    std::unique_ptr<typename S::PI> ilu;
+    void set_operator(const typename S::LO*) {}
+    void apply(typename S::VO::vector_type& x) const {
+        if (jac)
+            jac->apply(x);
+        else if (ilu)
+            ilu->apply(x);
+    }
+};
+
+// ILU(0) factors of A for the fused GMRES: a copy of the values (from the
+// solvers' memory pool) factored in place, and the analyses of both
+// triangles; released when the solve returns.
+template <class E>
+struct IluFactors {
+    hpb_context* ctx = nullptr;
+    hpb_csr_tri* lower = nullptr;
+    hpb_csr_tri* upper = nullptr;
+    E* lu = nullptr;
+    int build(int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci, const E* val) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || hpb_create(&ctx, dev, nullptr) != HPB_SUCCESS)
+            return HPB_ERROR_CUDA;
+        lu = static_cast<E*>(hpb::fused::pool_alloc(size_t(nnz ? nnz : 1) * sizeof(E), nullptr));
+        if (lu == nullptr) return HPB_ERROR_OUT_OF_MEMORY;
+        if (cudaMemcpyAsync(lu, val, size_t(nnz) * sizeof(E), cudaMemcpyDeviceToDevice, nullptr) != cudaSuccess)
+            return HPB_ERROR_CUDA;
+        int st = hpb_csr_tri_create(ctx, 0, rows, nnz, rp, ci, &lower);
+        if (st == HPB_SUCCESS) st = hpb_csr_tri_create(ctx, 1, rows, nnz, rp, ci, &upper);
+        if (st != HPB_SUCCESS) return st;
+        if (std::is_same<E, float>::value)
+            st = hpb_csr_ilu0_f32(ctx, lower, reinterpret_cast<float*>(lu));
+        else if (std::is_same<E, double>::value)
+            st = hpb_csr_ilu0_f64(ctx, lower, reinterpret_cast<double*>(lu));
+        else if (std::is_same<E, hpb::cf>::value)
+            st = hpb_csr_ilu0_c64(ctx, lower, lu);
+        else
+            st = hpb_csr_ilu0_c128(ctx, lower, lu);
+        return st;
+    }
+    ~IluFactors() {
+        hpb_csr_tri_destroy(lower);
+        hpb_csr_tri_destroy(upper);
+        if (lu) hpb::fused::pool_free(lu, nullptr);
+        if (ctx) hpb_destroy(ctx);
+        cudaStreamSynchronize(nullptr);
+    }
 };
 
 template <class Solver, class Mon>
@@ -71,10 +128,19 @@ int solve_device(const hpb_solver_params* p, int32_t rows, int64_t nnz, const in
                                                   cap);
         if (p->method == HPB_SOLVER_GMRES) {
             hpb::fused::RightPrec<E> M;
-            if (p->precond == HPB_PRECOND_JACOBI)
+            IluFactors<E> F;
+            if (p->precond == HPB_PRECOND_JACOBI) {
                 M.kind = 1;
-            else if (p->precond != HPB_PRECOND_NONE)
+            } else if (p->precond == HPB_PRECOND_ILU0) {
+                const int st = F.build(rows, nnz, rp, ci, reinterpret_cast<const E*>(val));
+                if (st != HPB_SUCCESS) return st;
+                M.kind = 3;
+                M.val = F.lu;
+                M.lower = F.lower;
+                M.upper = F.upper;
+            } else if (p->precond != HPB_PRECOND_NONE) {
                 return HPB_ERROR_NOT_SUPPORTED;
+            }
             return hpb::fused::solve_gmres<E>(p, rows, nnz, rp, ci, reinterpret_cast<const E*>(val), M,
                                               reinterpret_cast<const E*>(b), reinterpret_cast<E*>(x), rep, hist, cap,
                                               0);
@@ -91,10 +157,15 @@ int solve_device(const hpb_solver_params* p, int32_t rows, int64_t nnz, const in
         typename S::MAT A;
         A.attach(rows, rows, int(nnz), rp, ci, val);
         typename S::LO op(&ops, &A);
-        std::unique_ptr<typename S::PJ> jac;
+        std::unique_ptr<AnyPrec<S> > jac;
         if (p->precond == HPB_PRECOND_JACOBI) {
-            jac.reset(new typename S::PJ(&ops));
-            jac->set_matrix(&A);
+            jac.reset(new AnyPrec<S>);
+            jac->jac.reset(new typename S::PJ(&ops));
+            jac->jac->set_matrix(&A);
+        } else if (p->precond == HPB_PRECOND_ILU0) {
+            jac.reset(new AnyPrec<S>);
+            jac->ilu.reset(new typename S::PI(&ops));
+            jac->ilu->set_matrix(A);
         } else if (p->precond != HPB_PRECOND_NONE) {
             return HPB_ERROR_NOT_SUPPORTED;
         }
@@ -103,7 +174,7 @@ int solve_device(const hpb_solver_params* p, int32_t rows, int64_t nnz, const in
         auto t0 = std::chrono::steady_clock::now();
         bool ok = false;
         if (p->method == HPB_SOLVER_BICGSTABL) {
-            hpb::solvers::bicgstabl<typename S::LO, typename S::PJ, typename S::VO, typename S::MON> sv(&ops);
+            hpb::solvers::bicgstabl<typename S::LO, AnyPrec<S>, typename S::VO, typename S::MON> sv(&ops);
             sv.set_basis_size(p->basis > 0 ? p->basis : 2);
             sv.set_resid_recalc_freq(p->resid_recalc_freq);
             if (jac) sv.set_preconditioner(jac.get());
@@ -112,7 +183,7 @@ int solve_device(const hpb_solver_params* p, int32_t rows, int64_t nnz, const in
             rep->breakdown = sv.breakdown_flag() < 0 ? 1 : 0;
             fill_report<decltype(sv)>(sv.monitor(), rep, hist, cap);
         } else if (p->method == HPB_SOLVER_GMRES) {
-            hpb::solvers::gmres<typename S::LO, typename S::PJ, typename S::VO, typename S::MON> sv(&ops);
+            hpb::solvers::gmres<typename S::LO, AnyPrec<S>, typename S::VO, typename S::MON> sv(&ops);
             sv.set_restarts(unsigned(p->basis > 0 ? p->basis : 30));
             sv.set_reorthogonalization(p->reorthogonalize != 0);
             sv.set_early_exit(p->early_exit != 0);
@@ -121,7 +192,7 @@ int solve_device(const hpb_solver_params* p, int32_t rows, int64_t nnz, const in
             ok = sv.solve(op, bm, x);
             fill_report<decltype(sv)>(sv.monitor(), rep, hist, cap);
         } else if (p->method == HPB_SOLVER_BICGSTAB) {
-            hpb::solvers::bicgstab<typename S::LO, typename S::PJ, typename S::VO, typename S::MON> sv(&ops);
+            hpb::solvers::bicgstab<typename S::LO, AnyPrec<S>, typename S::VO, typename S::MON> sv(&ops);
             sv.set_resid_recalc_freq(p->resid_recalc_freq);
             if (jac) sv.set_preconditioner(jac.get());
             sv.monitor().init(R(p->rel_tol), R(p->abs_tol), p->max_iters, 0, false, cap > 0);

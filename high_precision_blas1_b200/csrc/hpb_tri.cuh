@@ -73,6 +73,14 @@ template <class E>
 cudaError_t launch_ilu0(const Plan& P, E* val, cudaStream_t s);
 
 }  // namespace tri
+
+// 1 in each element type (the alpha of a plain solve)
+template <class E> inline E unit_of();
+template <> inline float unit_of<float>() { return 1.0f; }
+template <> inline double unit_of<double>() { return 1.0; }
+template <> inline cf unit_of<cf>() { return cf{1.0f, 0.0f}; }
+template <> inline cd unit_of<cd>() { return cd{1.0, 0.0}; }
+
 }  // namespace hpb
 
 // The C ABI handle is the plan.

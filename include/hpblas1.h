@@ -384,7 +384,9 @@ typedef enum hpb_solver_method {
 typedef enum hpb_precond_kind {
     HPB_PRECOND_NONE = 0,
     HPB_PRECOND_JACOBI = 1,     /* D^{-1}: left for BiCGStab(l), right for the fused GMRES */
-    HPB_PRECOND_MATRIX = 2      /* a given CSR matrix M as right preconditioner (refinement, GMRES) */
+    HPB_PRECOND_MATRIX = 2,     /* a given CSR matrix M as right preconditioner (refinement, GMRES) */
+    HPB_PRECOND_ILU0 = 3        /* ILU(0) of A ((L U)^-1 by two sparse triangular solves): left for the
+                                   drop-in path (csr::gpu_ilu0_preconditioner), right for the fused GMRES */
 } hpb_precond_kind;
 
 typedef struct hpb_solver_params {

@@ -12,8 +12,12 @@
 // off-by-one.  Here the operator is rows x columns from set_dim(); without
 // set_dim the matrix is taken square with rows = size_row - 1.
 // Only 0-based int32 indices are supported (the configs' matrices).
-// Triangular solves (the csrsv2 path, removed from CUDA 12) and the
-// transposed product report "not supported".
+// Triangular solves (triangular_solve_lower / _upper, csr/gpu_matrix.h:
+// 142-311, there cuSPARSE csrsv2 with an analysis and a cudaMalloc'd buffer
+// per call) run the library's level-scheduled kernel (hpb_csr_trsv_*); the
+// analysis of each triangle is made on the first solve and kept until the
+// matrix is set again or destroyed.  Transposed solves and the transposed
+// product report "not supported".
 #ifndef __CSR__GPU_MATRIX_H__
 #define __CSR__GPU_MATRIX_H__
 
@@ -21,6 +25,7 @@
 
 #include <cstdint>
 #include <stdexcept>
+#include <string>
 #include <type_traits>
 
 #include <common/gpu_vector_operations.h>
@@ -58,6 +63,7 @@ public:
     }
     gpu_matrix& operator=(const gpu_matrix&) = delete;
     ~gpu_matrix() {
+        drop_analyses();
         if (owns_) {
             cudaFree(data);
             cudaFree(col_ind);
@@ -93,6 +99,7 @@ public:
     // upload host arrays (values, column indices, row pointers)
     void set(const T_vec data_, const I_vec col_ind_, const I_vec row_ptr_) {
         if (!initialized) throw std::runtime_error("csr::gpu_matrix: trying to set an uninitialized matrix.");
+        drop_analyses();
         h2d(data, data_, size_t(nnz) * sizeof(T));
         h2d(col_ind, col_ind_, size_t(size_col) * sizeof(I));
         h2d(row_ptr, row_ptr_, size_t(size_row) * sizeof(I));
@@ -114,11 +121,16 @@ public:
                                   y_),
                           ctx, "csr::gpu_matrix::axpy");
     }
-    void triangular_solve_lower(const T_vec&, T_vec&, const T& = T(1.0), bool = false) const {
-        throw std::logic_error("csr::gpu_matrix: triangular solves are not supported by this library");
+    // L x = alpha b, L the lower triangle with a unit diagonal (stored
+    // diagonal and upper entries ignored), as the reference's csrsv2 call
+    // with CUSPARSE_DIAG_TYPE_UNIT (csr/gpu_matrix.h:150-225).
+    void triangular_solve_lower(const T_vec& b_, T_vec& x_, const T& alpha_ = T(1.0), bool transpose_ = false) const {
+        tri_solve(false, true, b_, x_, alpha_, transpose_, "csr::gpu_matrix::triangular_solve_lower");
     }
-    void triangular_solve_upper(const T_vec&, T_vec&, const T& = T(1.0), bool = false) const {
-        throw std::logic_error("csr::gpu_matrix: triangular solves are not supported by this library");
+    // U x = alpha b, U the upper triangle with its stored diagonal
+    // (csr/gpu_matrix.h:236-311).
+    void triangular_solve_upper(const T_vec& b_, T_vec& x_, const T& alpha_ = T(1.0), bool transpose_ = false) const {
+        tri_solve(true, false, b_, x_, alpha_, transpose_, "csr::gpu_matrix::triangular_solve_upper");
     }
 
     // ------------------------------------------------------------ extensions
@@ -145,6 +157,17 @@ public:
         using A = hpb_dropin::abi<T>;
         hpb_dropin::check(A::diag(ctx, get_dim().rows, row_ptr, col_ind, data, d), ctx, "csr::gpu_matrix::diagonal");
     }
+    // Replace the values by the ILU(0) factors on the same pattern (L unit
+    // lower in the strictly lower entries, U upper with the diagonal), so
+    // that triangular_solve_lower then triangular_solve_upper apply
+    // (L U)^-1.  Every row must store its diagonal, the columns of each row
+    // must be increasing; a zero pivot throws.  On an attached matrix the
+    // caller's value array is overwritten.
+    void ilu0() {
+        if (!initialized) throw std::runtime_error("csr::gpu_matrix::ilu0: matrix not set");
+        using A = hpb_dropin::abi<T>;
+        hpb_dropin::check(A::ilu0(ctx, analysis(false), data), ctx, "csr::gpu_matrix::ilu0");
+    }
 
 protected:
     T_vec data = nullptr;
@@ -158,6 +181,32 @@ private:
     CudaBlas* cublas;
     hpb_context* ctx = nullptr;
     bool owns_ = true;
+    mutable hpb_csr_tri* tri_[2] = {nullptr, nullptr};  // analyses of the lower / upper triangle
+
+    void drop_analyses() {
+        for (auto& t : tri_) {
+            hpb_csr_tri_destroy(t);
+            t = nullptr;
+        }
+    }
+    hpb_csr_tri* analysis(bool upper) const {
+        hpb_csr_tri*& t = tri_[upper ? 1 : 0];
+        if (t == nullptr)
+            hpb_dropin::check(hpb_csr_tri_create(ctx, upper ? 1 : 0, get_dim().rows, nnz, row_ptr, col_ind, &t), ctx,
+                              "csr::gpu_matrix: triangular analysis");
+        return t;
+    }
+    void tri_solve(bool upper, bool unit, const T_vec& b_, T_vec& x_, const T& alpha_, bool transpose_,
+                   const char* what) const {
+        if (transpose_) throw std::logic_error(std::string(what) + ": transposed solve is not supported");
+        if (!initialized) throw std::runtime_error(std::string(what) + ": matrix not set");
+        using A = hpb_dropin::abi<T>;
+        hpb_csr_tri* t = analysis(upper);
+        hpb_dropin::check(A::trsv(ctx, t, unit ? 1 : 0, data, A::s(alpha_), b_, x_), ctx, what);
+        // blocking, like the reference's call (its cudaFree of the work buffer
+        // synchronises); also reports a solve whose bounded waits gave up
+        hpb_dropin::check(hpb_csr_tri_check(ctx, t), ctx, what);
+    }
 
     static void* dalloc(size_t b) {
         void* p = nullptr;

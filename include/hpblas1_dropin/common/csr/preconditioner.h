@@ -2,9 +2,12 @@
 //
 // csr::preconditioner keeps the reference's interface (set_operator,
 // set_matrix(L, U), in-place apply) (csr/preconditioner.h:32-85).  With no
-// factors set, apply is the identity, as in the reference.  Applying L/U
-// factors needs sparse triangular solves (the reference's csrsv2 path, which
-// no longer compiles with CUDA 12): apply then reports "not supported".
+// factors set, apply is the identity, as in the reference; with factors,
+// apply is x := U^-1 L^-1 x by the same two calls the reference makes
+// (triangular_solve_lower with a unit diagonal into a work vector, then
+// triangular_solve_upper back into x), here on the library's sparse
+// triangular-solve kernel instead of csrsv2.  L and U may be the same
+// matrix holding both factors (the layout csr::gpu_matrix::ilu0 produces).
 //
 // csr::jacobi_preconditioner is the diagonal scaling x := D^{-1} x of A,
 // the GPU analogue of the reference's constant-diagonal prec_operator for
@@ -22,7 +25,16 @@ struct preconditioner {
     using T = typename VectorOperations::scalar_type;
     using T_vec = typename VectorOperations::vector_type;
 
-    explicit preconditioner(const VectorOperations* vec_ops_) : vec_ops(vec_ops_) {}
+    explicit preconditioner(const VectorOperations* vec_ops_) : vec_ops(vec_ops_) {
+        vec_ops->init_vector(y);
+        vec_ops->start_use_vector(y);
+    }
+    ~preconditioner() {
+        vec_ops->stop_use_vector(y);
+        vec_ops->free_vector(y);
+    }
+    preconditioner(const preconditioner&) = delete;
+    preconditioner& operator=(const preconditioner&) = delete;
     void set_operator(const LinearOperator* lin_op_) {
         lin_op = lin_op_;
         operator_set = true;
@@ -33,11 +45,13 @@ struct preconditioner {
         matrix_set = true;
     }
     void apply(T_vec& x) const {
-        if (matrix_set) throw std::logic_error("csr::preconditioner: triangular-factor application is not supported");
-        (void)x;
+        if (!matrix_set) return;
+        matL->triangular_solve_lower(x, y);
+        matU->triangular_solve_upper(y, x);
     }
 
 private:
+    mutable T_vec y = nullptr;
     bool operator_set = false;
     bool matrix_set = false;
     const VectorOperations* vec_ops;

@@ -129,6 +129,11 @@ template <class T> struct abi;
                         T* d) {                                                                           \
             return hpb_csr_diag_##SUF(c, rows, rp, ci, v, d);                                             \
         }                                                                                                 \
+        static int trsv(hpb_context* c, const hpb_csr_tri* t, int unit, const T* v, S a, const T* b,      \
+                        T* x) {                                                                           \
+            return hpb_csr_trsv_##SUF(c, t, unit, v, a, b, x);                                            \
+        }                                                                                                 \
+        static int ilu0(hpb_context* c, const hpb_csr_tri* t, T* v) { return hpb_csr_ilu0_##SUF(c, t, v); } \
     };
 
 HPB_DROPIN_ABI(float, f32, float, v)

@@ -8,6 +8,7 @@
 // oracle/_ref/ from the reference sources where they lie (oracle/Makefile).
 // A GPU test runs it beside the library's own solvers on the same device
 // arrays: same recurrences, same kernels -> same iterates.
+#include <common/csr/gpu_ilu0_preconditioner.h>
 #include <common/csr/gpu_matrix.h>
 #include <common/csr/linear_operator.h>
 #include <common/csr/preconditioner.h>
@@ -24,32 +25,18 @@ using vec_ops_t = gpu_vector_operations<double>;
 using mat_t = csr::gpu_matrix<vec_ops_t, cublas_wrap>;
 using lin_op_t = csr::linear_operator<vec_ops_t, mat_t>;
 using prec_t = csr::preconditioner<vec_ops_t, lin_op_t, mat_t>;
+using ilu_t = csr::gpu_ilu0_preconditioner<vec_ops_t, lin_op_t, mat_t>;
 using log_t = utils::log_std;
 using mon_t = numerical_algos::lin_solvers::default_monitor<vec_ops_t, log_t>;
-}  // namespace
 
-extern "C" {
-
-// method 0: bicgstabl(basis), 1: gmres(basis).  Device arrays; x holds the
-// initial guess.  Returns 1 if the reference's monitor reports convergence.
-int ref_dropin_solve_f64(int method, int rows, int64_t nnz, const int* rp, const int* ci, const double* val,
-                         double* b, double* x, int basis, double rel_tol, int max_iters, int high_prec,
-                         int* iters_out, double* resid_out) {
-    cublas_wrap cublas(false);
-    vec_ops_t vec_ops(size_t(rows), &cublas);
-    if (high_prec)
-        vec_ops.use_high_precision();
-    else
-        vec_ops.use_standard_precision();
-    mat_t mat(&cublas);
-    mat.attach(rows, rows, int(nnz), rp, ci, val);
-    lin_op_t lin_op(&vec_ops, &mat);
-    prec_t prec(&vec_ops);
+template <class Prec>
+int run_solver(Prec& prec, vec_ops_t& vec_ops, lin_op_t& lin_op, int method, double* b, double* x, int basis,
+               double rel_tol, int max_iters, int* iters_out, double* resid_out) {
     log_t log;
     log.set_verbosity(0);
     bool ok = false;
     if (method == 0) {
-        numerical_algos::lin_solvers::bicgstabl<lin_op_t, prec_t, vec_ops_t, mon_t, log_t> s(&vec_ops, &log);
+        numerical_algos::lin_solvers::bicgstabl<lin_op_t, Prec, vec_ops_t, mon_t, log_t> s(&vec_ops, &log);
         s.set_preconditioner(&prec);
         s.set_basis_size(basis);
         s.monitor().init(rel_tol, 0.0, max_iters);
@@ -57,7 +44,7 @@ int ref_dropin_solve_f64(int method, int rows, int64_t nnz, const int* rp, const
         *iters_out = s.monitor().iters_performed();
         *resid_out = s.monitor().resid_norm();
     } else {
-        numerical_algos::lin_solvers::gmres<lin_op_t, prec_t, vec_ops_t, mon_t, log_t, 300> s(&vec_ops, &log);
+        numerical_algos::lin_solvers::gmres<lin_op_t, Prec, vec_ops_t, mon_t, log_t, 300> s(&vec_ops, &log);
         s.set_preconditioner(&prec);
         s.set_restarts(unsigned(basis));
         s.set_reorthogonalization(false);
@@ -68,6 +55,42 @@ int ref_dropin_solve_f64(int method, int rows, int64_t nnz, const int* rp, const
     }
     vec_ops.sync();
     return ok ? 1 : 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+// method 0: bicgstabl(basis), 1: gmres(basis); precond 0: csr::preconditioner
+// without factors (the identity), 1: csr::gpu_ilu0_preconditioner of A.
+// Device arrays; x holds the initial guess.  Returns 1 if the reference's
+// monitor reports convergence.
+int ref_dropin_solve_prec_f64(int method, int precond, int rows, int64_t nnz, const int* rp, const int* ci,
+                              const double* val, double* b, double* x, int basis, double rel_tol, int max_iters,
+                              int high_prec, int* iters_out, double* resid_out) {
+    cublas_wrap cublas(false);
+    vec_ops_t vec_ops(size_t(rows), &cublas);
+    if (high_prec)
+        vec_ops.use_high_precision();
+    else
+        vec_ops.use_standard_precision();
+    mat_t mat(&cublas);
+    mat.attach(rows, rows, int(nnz), rp, ci, val);
+    lin_op_t lin_op(&vec_ops, &mat);
+    if (precond == 1) {
+        ilu_t prec(&vec_ops);
+        prec.set_matrix(mat);
+        return run_solver(prec, vec_ops, lin_op, method, b, x, basis, rel_tol, max_iters, iters_out, resid_out);
+    }
+    prec_t prec(&vec_ops);
+    return run_solver(prec, vec_ops, lin_op, method, b, x, basis, rel_tol, max_iters, iters_out, resid_out);
+}
+
+int ref_dropin_solve_f64(int method, int rows, int64_t nnz, const int* rp, const int* ci, const double* val,
+                         double* b, double* x, int basis, double rel_tol, int max_iters, int high_prec,
+                         int* iters_out, double* resid_out) {
+    return ref_dropin_solve_prec_f64(method, 0, rows, nnz, rp, ci, val, b, x, basis, rel_tol, max_iters, high_prec,
+                                     iters_out, resid_out);
 }
 
 }  // extern "C"

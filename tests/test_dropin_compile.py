@@ -14,6 +14,7 @@ SRC = r'''
 #include <common/csr/gpu_matrix.h>
 #include <common/csr/linear_operator.h>
 #include <common/csr/preconditioner.h>
+#include <common/csr/gpu_ilu0_preconditioner.h>
 #include <numerical_algos/lin_solvers/default_monitor.h>
 #include <numerical_algos/lin_solvers/bicgstabl.h>
 #include <numerical_algos/lin_solvers/bicgstab.h>
@@ -42,6 +43,17 @@ template <class T> int run(int n) {
     T *x, *b; vec_ops.init_vector(x); vec_ops.start_use_vector(x); vec_ops.init_vector(b); vec_ops.start_use_vector(b);
     vec_ops.use_high_precision();
     bool ok = s1.solve(lin_op, b, x) && s2.solve(lin_op, b, x) && s3.solve(lin_op, b, x);
+    // triangular factors: csr::preconditioner with L/U set, the ILU(0) preconditioner
+    using ilu_t = csr::gpu_ilu0_preconditioner<vec_ops_t, lin_op_t, mat_t>;
+    prec_t lu_prec(&vec_ops);
+    lu_prec.set_matrix(&mat, &mat);
+    ilu_t ilu(&vec_ops);
+    ilu.set_matrix(mat);
+    numerical_algos::lin_solvers::bicgstabl<lin_op_t, ilu_t, vec_ops_t, mon_t, log_t> s4(&vec_ops, &log);
+    s4.set_preconditioner(&ilu); s4.set_basis_size(2); s4.monitor().init(1e-10, 0, 100);
+    ok = ok && s4.solve(lin_op, b, x);
+    mat.triangular_solve_lower(b, x);
+    mat.triangular_solve_upper(x, b, T(2.0));
     vec_ops.free_vector(x); vec_ops.free_vector(b);
     return ok;
 }
