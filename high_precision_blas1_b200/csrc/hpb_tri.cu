@@ -154,6 +154,11 @@ __device__ __forceinline__ void wait_levels(volatile int* done, int l, int lane,
 }
 
 // ---- analysis -------------------------------------------------------------
+// column c is a dependency on another tile (c >= 0: a dependency at all)
+__device__ __forceinline__ int is_ext(int32_t c, int32_t base, int32_t m) {
+    return c >= 0 && (c < base || c >= base + m) ? 1 : 0;
+}
+
 // Per row: validate the structure (row pointers monotone and within nnz,
 // columns in range and strictly increasing), locate the diagonal, and the
 // dependency range: strictly lower part [rp[i], first column >= i) or
@@ -195,17 +200,21 @@ template <bool UPPER>
 __global__ void __launch_bounds__(kLvThreads)
 k_tri_levels(int32_t n, const int32_t* __restrict__ ci, const int32_t* __restrict__ beg,
              const int32_t* __restrict__ cnt, const int32_t* __restrict__ dpos, int4* __restrict__ desc,
-             int4* __restrict__ dcol, int32_t* __restrict__ lvlptr, int32_t* __restrict__ nlev) {
+             int4* __restrict__ dcol, int32_t* __restrict__ lvlptr, int32_t* __restrict__ nlev,
+             int32_t* __restrict__ hcount) {
     extern __shared__ int sh[];
     volatile int* lev = sh;          // kTriTile
     int* hist = sh + kTriTile;       // kTriTile + 1
     __shared__ int part[kLvThreads];
-    __shared__ int s_max;
+    __shared__ int s_max, s_ext;
     const int t = blockIdx.x;
     const int32_t base = int32_t(t) * kTriTile;
     const int32_t m = min(kTriTile, n - base);
     for (int r = threadIdx.x; r < m; r += blockDim.x) lev[r] = 0;
-    if (threadIdx.x == 0) s_max = 0;
+    if (threadIdx.x == 0) {
+        s_max = 0;
+        s_ext = 0;
+    }
     __syncthreads();
     const int seg = (m + blockDim.x - 1) / blockDim.x;
     const int s0 = min(m, int(threadIdx.x) * seg), s1 = min(m, s0 + seg);
@@ -266,13 +275,66 @@ k_tri_levels(int32_t n, const int32_t* __restrict__ ci, const int32_t* __restric
         nlev[t] = L;
     }
     __syncthreads();
+    int ext = 0;
     for (int r = threadIdx.x; r < m; r += blockDim.x) {
         const int pos = atomicAdd(&hist[lev[r]], 1);
         const int32_t i = base + r;
         const int32_t b = __ldg(beg + i), c = __ldg(cnt + i);
         desc[base + pos] = make_int4(i, b, c, __ldg(dpos + i));
-        dcol[base + pos] = make_int4(c > 0 ? __ldg(ci + b) : -1, c > 1 ? __ldg(ci + b + 1) : -1,
-                                     c > 2 ? __ldg(ci + b + 2) : -1, c > 3 ? __ldg(ci + b + 3) : -1);
+        const int4 c4 = make_int4(c > 0 ? __ldg(ci + b) : -1, c > 1 ? __ldg(ci + b + 1) : -1,
+                                  c > 2 ? __ldg(ci + b + 2) : -1, c > 3 ? __ldg(ci + b + 3) : -1);
+        dcol[base + pos] = c4;
+        ext += is_ext(c4.x, base, m) + is_ext(c4.y, base, m) + is_ext(c4.z, base, m) + is_ext(c4.w, base, m);
+    }
+    atomicAdd(&s_ext, ext);
+    __syncthreads();
+    if (threadIdx.x == 0) hcount[t] = s_ext;
+}
+
+// Per tile (one block): number, in level order, the tile's dependencies on
+// other tiles among each row's first kPre (the rows whose values the solve's
+// receiver warp fetches): dslot holds the slot of each such dependency (-1:
+// none, in the tile, or past kPre), hrow the row each slot is filled from.
+__global__ void __launch_bounds__(kLvThreads)
+k_tri_halo(int32_t n, const int4* __restrict__ dcol, const int32_t* __restrict__ hoff, int4* __restrict__ dslot,
+           int32_t* __restrict__ hrow) {
+    __shared__ int part[kLvThreads];
+    const int t = blockIdx.x;
+    const int32_t base = int32_t(t) * kTriTile;
+    const int32_t m = min(kTriTile, n - base);
+    const int seg = (m + blockDim.x - 1) / blockDim.x;
+    const int s0 = min(m, int(threadIdx.x) * seg), s1 = min(m, s0 + seg);
+    int cnt = 0;
+    for (int p = s0; p < s1; ++p) {
+        const int4 c4 = dcol[base + p];
+        cnt += is_ext(c4.x, base, m) + is_ext(c4.y, base, m) + is_ext(c4.z, base, m) + is_ext(c4.w, base, m);
+    }
+    part[threadIdx.x] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int w = 0; w < int(blockDim.x); ++w) {
+            const int v = part[w];
+            part[w] = acc;
+            acc += v;
+        }
+    }
+    __syncthreads();
+    int slot = part[threadIdx.x];
+    int32_t* hr = hrow + hoff[t];
+    for (int p = s0; p < s1; ++p) {
+        const int4 c4 = dcol[base + p];
+        const int c[4] = {c4.x, c4.y, c4.z, c4.w};
+        int o[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            o[k] = -1;
+            if (is_ext(c[k], base, m)) {
+                hr[slot] = c[k];
+                o[k] = slot++;
+            }
+        }
+        dslot[base + p] = make_int4(o[0], o[1], o[2], o[3]);
     }
 }
 
@@ -385,99 +447,267 @@ __global__ void k_tri_fill(int32_t n, E* __restrict__ x, unsigned* ticket) {
         Pub<E>::fill(x, i);
 }
 
+// Cross-tile values come through a receiver warp: the block's last warp
+// polls the tile's other-tile dependencies (numbered in level order by the
+// analysis, kHalo<E> of them at most) from x, 128 in flight, and stores each
+// arrived value into a shared-memory slot.  The slots are pre-filled with
+// the sentinel, so -- as for x in global memory -- a slot that no longer
+// holds it holds the final value (component-wise single-copy stores), and a
+// row waits on shared memory with neither a flag nor a fence, instead of an
+// L2 round trip; the producing tile runs only a few levels ahead, so that
+// round trip would otherwise sit on the critical path of nearly every level.
+template <class E> struct kHalo { static constexpr int value = 8192; };
+template <> struct kHalo<float> { static constexpr int value = 16384; };
+template <> struct kHalo<cd> { static constexpr int value = 4096; };
+
+template <class E>
+constexpr size_t trsv_smem() {
+    return size_t(kTriTile + kHalo<E>::value) * sizeof(E);
+}
+
+// Shared-memory slot access, one volatile access per component.
+__device__ __forceinline__ float vload(const float* p) { return *reinterpret_cast<const volatile float*>(p); }
+__device__ __forceinline__ double vload(const double* p) { return *reinterpret_cast<const volatile double*>(p); }
+__device__ __forceinline__ cf vload(const cf* p) {
+    const volatile float* q = reinterpret_cast<const volatile float*>(p);
+    return cf{q[0], q[1]};
+}
+__device__ __forceinline__ cd vload(const cd* p) {
+    const volatile double* q = reinterpret_cast<const volatile double*>(p);
+    return cd{q[0], q[1]};
+}
+__device__ __forceinline__ void vstore(float* p, float v) { *reinterpret_cast<volatile float*>(p) = v; }
+__device__ __forceinline__ void vstore(double* p, double v) { *reinterpret_cast<volatile double*>(p) = v; }
+__device__ __forceinline__ void vstore(cf* p, cf v) {
+    volatile float* q = reinterpret_cast<volatile float*>(p);
+    q[0] = v.re;
+    q[1] = v.im;
+}
+__device__ __forceinline__ void vstore(cd* p, cd v) {
+    volatile double* q = reinterpret_cast<volatile double*>(p);
+    q[0] = v.re;
+    q[1] = v.im;
+}
+
+// Level handoff inside a tile: the warp that finishes level l arrives on
+// named barrier 1 + l % kSolveWarps, the warp of level l + 1 syncs on it
+// (64 threads: the two warps).  A barrier orders the shared-memory writes
+// of the arriving warp before the reads of the syncing one, with no
+// separate fence; the pair of warps behind each barrier id is fixed because
+// levels go round-robin over kSolveWarps warps.
+constexpr int kSolveWarps = kTriThreads / 32 - 1;  // 15; the 16th warp receives
+__device__ __forceinline__ void level_arrive(int l) {
+    asm volatile("bar.arrive %0, 64;" ::"r"(1 + l % kSolveWarps) : "memory");
+}
+__device__ __forceinline__ void level_sync(int l) {
+    asm volatile("bar.sync %0, 64;" ::"r"(1 + l % kSolveWarps) : "memory");
+}
+
+// One row of a chunk, gathered before it can be solved: its index, the
+// source of each of its first kPre dependencies (>= 0: position in the
+// tile's shared-memory solution; <= -2: halo slot -(src + 2); -1: another
+// tile's row without a slot, read from x), alpha b_i, the diagonal and the
+// dependency values.
+template <class E>
+struct RowData {
+    int32_t row, e0, nd;  // row index, first dependency entry, dependency count (-1 row: inactive)
+    int32_t src[kPre];
+    E rhs, dg, v[kPre];
+};
+
+// Levels whose first chunk a warp gathers ahead (registers permitting).
+template <class E> struct kLook { static constexpr int value = 3; };
+template <> struct kLook<cd> { static constexpr int value = 2; };
+
+template <class E, bool UNIT>
+__device__ __forceinline__ void gather_row(RowData<E>& r, int32_t p, int32_t p1, int32_t base, int32_t m,
+                                           const int4* __restrict__ desc, const int4* __restrict__ dcol,
+                                           const int4* __restrict__ dslot, const E* __restrict__ val, E alpha,
+                                           const E* __restrict__ b) {
+    constexpr int H = kHalo<E>::value;
+    r.row = -1;
+    r.e0 = 0;
+    r.nd = 0;
+    r.rhs = E{};
+    r.dg = E{};
+#pragma unroll
+    for (int k = 0; k < kPre; ++k) {
+        r.src[k] = -1;
+        r.v[k] = E{};
+    }
+    if (p >= p1) return;
+    const int4 d = desc[base + p], c4 = dcol[base + p], s4 = dslot[base + p];
+    const int32_t c[kPre] = {c4.x, c4.y, c4.z, c4.w};
+    const int32_t sl[kPre] = {s4.x, s4.y, s4.z, s4.w};
+    r.row = d.x;
+    r.e0 = d.y;
+    r.nd = d.z;
+#pragma unroll
+    for (int k = 0; k < kPre; ++k) {
+        const int32_t jl = c[k] - base;
+        r.src[k] = (jl >= 0 && jl < m) ? jl : (sl[k] >= 0 && sl[k] < H ? -(sl[k] + 2) : -1);
+    }
+    r.rhs = scale(alpha, ldE(b, d.x));
+    if (!UNIT) r.dg = ldE(val, d.w);
+#pragma unroll
+    for (int k = 0; k < kPre; ++k)
+        if (k < d.z) r.v[k] = ldE(val, d.y + k);
+}
+
+// Solve one gathered row; returns x_row.
+template <class E, bool UNIT>
+__device__ __forceinline__ E solve_row(const RowData<E>& r, int32_t base, int32_t m, const E* xs, const E* halo,
+                                       const int32_t* __restrict__ ci, const E* __restrict__ val, const E* x,
+                                       int* err) {
+    E acc = r.rhs;
+#pragma unroll
+    for (int k = 0; k < kPre; ++k)
+        if (k < r.nd) {
+            const int32_t sk = r.src[k];
+            E xj;
+            if (sk >= 0) {
+                xj = xs[sk];
+            } else if (sk <= -2) {
+                const E* slot = halo + (-sk - 2);
+                xj = vload(slot);
+                if (Pub<E>::pending(xj)) {
+                    Waiter w;
+                    do {
+                        if (w.check(err, 255)) break;
+                        xj = vload(slot);
+                    } while (Pub<E>::pending(xj));
+                }
+            } else {
+                const int32_t j = __ldg(ci + r.e0 + k);
+                xj = await_value(x, j, Pub<E>::load(x, j), err);
+            }
+            acc = fms(acc, r.v[k], xj);
+        }
+    for (int32_t e = r.e0 + kPre; e < r.e0 + r.nd; ++e) {
+        const int32_t j = __ldg(ci + e), jl = j - base;
+        const E xj = (jl >= 0 && jl < m) ? xs[jl] : await_value(x, j, Pub<E>::load(x, j), err);
+        acc = fms(acc, ldE(val, e), xj);
+    }
+    if (!UNIT) acc = quot(acc, r.dg);
+    return acc;
+}
+
 template <class E, bool UPPER, bool UNIT>
 __global__ void __launch_bounds__(kTriThreads)
 k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int4* __restrict__ dcol,
+       const int4* __restrict__ dslot, const int32_t* __restrict__ hoff, const int32_t* __restrict__ hrow,
        const int32_t* __restrict__ lvlptr, const int32_t* __restrict__ nlev, const int32_t* __restrict__ ci,
        const E* __restrict__ val, E alpha, const E* __restrict__ b, E* x, unsigned* ticket, int* err) {
+    constexpr int H = kHalo<E>::value;
+    constexpr int D = kLook<E>::value;
     extern __shared__ __align__(16) unsigned char smraw[];
     E* xs = reinterpret_cast<E*>(smraw);
+    E* halo = xs + kTriTile;
     __shared__ int s_tile;
-    __shared__ int s_done;
     if (threadIdx.x == 0) {
         const int tk = int(atomicAdd(ticket, 1u));
         s_tile = UPPER ? ntiles - 1 - tk : tk;
-        s_done = 0;
     }
+    for (int i = threadIdx.x; i < H; i += blockDim.x) Pub<E>::fill(halo, i);
     __syncthreads();
     const int t = s_tile;
     if (t < 0 || t >= ntiles) return;
     const int32_t base = int32_t(t) * kTriTile;
     const int32_t m = min(kTriTile, n - base);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int W = kSolveWarps;
+
+    if (warp == W) {  // ---- receiver warp
+        const int32_t h0 = hoff[t];
+        const int32_t nsl = min(hoff[t + 1] - h0, H);
+        const int32_t* hr = hrow + h0;
+        int32_t s0 = 0;
+        unsigned pend = 0xFu;  // bit j: slot s0 + lane + 32 j not yet delivered
+        int32_t row[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) row[j] = s0 + lane + 32 * j < nsl ? hr[s0 + lane + 32 * j] : 0;
+        Waiter w;
+        while (s0 < nsl) {
+            E v[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (((pend >> j) & 1u) && s0 + lane + 32 * j < nsl) v[j] = Pub<E>::load(x, row[j]);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int32_t sl = s0 + lane + 32 * j;
+                if (!((pend >> j) & 1u)) continue;
+                if (sl >= nsl) {
+                    pend &= ~(1u << j);
+                } else if (!Pub<E>::pending(v[j])) {
+                    vstore(halo + sl, v[j]);
+                    pend &= ~(1u << j);
+                }
+            }
+            if (__all_sync(0xffffffffu, (pend & 1u) == 0u)) {  // the window's first 32 slots are in: slide
+                s0 += 32;
+                pend = (pend >> 1) | 0x8u;
+                row[0] = row[1];
+                row[1] = row[2];
+                row[2] = row[3];
+                row[3] = s0 + lane + 96 < nsl ? hr[s0 + lane + 96] : 0;
+                w = Waiter();
+            } else {
+                const bool stop = w.check(err, 15);  // every lane checks, the warp leaves together
+                if (__any_sync(0xffffffffu, stop)) break;
+            }
+        }
+        return;
+    }
+
+    // ---- solve warps: levels round-robin.  A warp holds the gathered first
+    // chunk (32 rows) of its next D levels; within a level, the next chunk is
+    // gathered while the current one is solved.
     const int L = nlev[t];
     const int32_t* lp = lvlptr + size_t(t) * (kTriTile + 1);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int W = kTriThreads / 32;
-    volatile int* done = &s_done;
+    RowData<E> ahead[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) {
+        const int lj = warp + j * W;
+        const int32_t a0 = lj < L ? lp[lj] : 0, a1 = lj < L ? lp[lj + 1] : 0;
+        gather_row<E, UNIT>(ahead[j], a0 + lane, a1, base, m, desc, dcol, dslot, val, alpha, b);
+    }
     for (int l = warp; l < L; l += W) {
         const int32_t p0 = lp[l], p1 = lp[l + 1];
+        RowData<E> cur = ahead[0];
+#pragma unroll
+        for (int j = 0; j + 1 < D; ++j) ahead[j] = ahead[j + 1];
+        {
+            const int lj = l + D * W;
+            const int32_t a0 = lj < L ? lp[lj] : 0, a1 = lj < L ? lp[lj + 1] : 0;
+            gather_row<E, UNIT>(ahead[D - 1], a0 + lane, a1, base, m, desc, dcol, dslot, val, alpha, b);
+        }
         int32_t pub_row = -1;
         E pub_val{};
+        if (l > 0) level_sync(l - 1);  // levels < l of the tile are complete
         for (int32_t q = p0; q < p1; q += 32) {
-            const int32_t p = q + lane;
-            const bool act = p < p1;
-            // The row's data and its other-tile dependencies, loaded before
-            // the wait: the descriptor and the first dependency columns
-            // (one round trip), then b, the values and x of other tiles
-            // (a second one).
-            int4 d = make_int4(0, 0, 0, -1), c4 = make_int4(-1, -1, -1, -1);
-            if (act) {
-                d = desc[base + p];
-                c4 = dcol[base + p];
-            }
-            const int32_t col[kPre] = {c4.x, c4.y, c4.z, c4.w};
-            E rhs{}, dg{};
-            E v[kPre], xv[kPre];
-#pragma unroll
-            for (int k = 0; k < kPre; ++k) {
-                v[k] = E{};
-                xv[k] = E{};
-            }
-            if (act) {
-                rhs = scale(alpha, ldE(b, d.x));
-                if (!UNIT) dg = ldE(val, d.w);
-#pragma unroll
-                for (int k = 0; k < kPre; ++k)
-                    if (k < d.z) {
-                        v[k] = ldE(val, d.y + k);
-                        const int32_t jl = col[k] - base;
-                        if (!(jl >= 0 && jl < m)) xv[k] = Pub<E>::load(x, col[k]);
-                    }
-            }
-            if (q == p0) wait_levels(done, l, lane, err);
-            if (act) {
-                E acc = rhs;
-#pragma unroll
-                for (int k = 0; k < kPre; ++k)
-                    if (k < d.z) {
-                        const int32_t jl = col[k] - base;
-                        const E xj = (jl >= 0 && jl < m) ? xs[jl] : await_value(x, col[k], xv[k], err);
-                        acc = fms(acc, v[k], xj);
-                    }
-                for (int32_t e = d.y + kPre; e < d.y + d.z; ++e) {
-                    const int32_t j = __ldg(ci + e), jl = j - base;
-                    const E xj = (jl >= 0 && jl < m) ? xs[jl] : await_value(x, j, Pub<E>::load(x, j), err);
-                    acc = fms(acc, ldE(val, e), xj);
-                }
-                if (!UNIT) acc = quot(acc, dg);
-                xs[d.x - base] = acc;
-                if (q + 32 < p1) {
-                    Pub<E>::store(x, d.x, acc);  // more chunks follow in this level
+            const bool more = q + 32 < p1;
+            RowData<E> nxt;
+            if (more) gather_row<E, UNIT>(nxt, q + 32 + lane, p1, base, m, desc, dcol, dslot, val, alpha, b);
+            if (cur.row >= 0) {
+                const E acc = solve_row<E, UNIT>(cur, base, m, xs, halo, ci, val, x, err);
+                xs[cur.row - base] = acc;
+                if (more) {
+                    Pub<E>::store(x, cur.row, acc);  // more chunks follow in this level
                 } else {
-                    pub_row = d.x;
+                    pub_row = cur.row;
                     pub_val = acc;
                 }
             }
+            if (more) cur = nxt;
         }
         __syncwarp();
-        if (lane == 0) {
-            __threadfence_block();
-            *done = l + 1;
-        }
-        // the global store after the in-tile announcement, so the block fence
-        // above never waits on it
+        level_arrive(l);
+        // the global store after the in-tile announcement
         if (pub_row >= 0) Pub<E>::store(x, pub_row, pub_val);
     }
+    // the warp that would take level L syncs on the last arrival, so that no
+    // barrier is left half-arrived when the block ends
+    if (L > 0 && warp == L % W) level_sync(L - 1);
 }
 
 // ---- ILU(0) ---------------------------------------------------------------
@@ -602,6 +832,8 @@ int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* 
     if (cudaMalloc(&P->desc, nn * sizeof(int4)) != cudaSuccess || cudaMalloc(&P->dcol, nn * sizeof(int4)) != cudaSuccess ||
         cudaMalloc(&P->lvlptr, size_t(P->ntiles) * (kTriTile + 1) * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&P->nlev, size_t(P->ntiles) * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&P->hoff, (size_t(P->ntiles) + 1) * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&P->dslot, nn * sizeof(int4)) != cudaSuccess ||
         cudaMalloc(&P->dpos, nn * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&P->flags, (nn + 1) * sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&P->err, 2 * sizeof(int)) != cudaSuccess || cudaMalloc(&beg, nn * sizeof(int32_t)) != cudaSuccess ||
@@ -618,21 +850,43 @@ int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* 
     if (P->upper) {
         allow_smem(k_tri_levels<true>, lv_smem);
         k_tri_levels<true><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, ci, beg, cnt, P->dpos, P->desc, P->dcol,
-                                                                   P->lvlptr, P->nlev);
+                                                                   P->lvlptr, P->nlev, P->hoff);
     } else {
         allow_smem(k_tri_levels<false>, lv_smem);
         k_tri_levels<false><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, ci, beg, cnt, P->dpos, P->desc, P->dcol,
-                                                                    P->lvlptr, P->nlev);
+                                                                    P->lvlptr, P->nlev, P->hoff);
     }
     count_launch(2);
     if (cudaGetLastError() != cudaSuccess) return fail(HPB_ERROR_CUDA, "analysis launch failed");
     int host_err = 0, host_missing = 0;
-    std::vector<int32_t> lev(size_t(P->ntiles));
+    std::vector<int32_t> lev(size_t(P->ntiles)), hc(size_t(P->ntiles) + 1, 0);
+    // the per-tile halo counts were written into hoff[0, ntiles)
     if (cudaMemcpyAsync(&host_err, P->err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaMemcpyAsync(&host_missing, missing, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
         cudaMemcpyAsync(lev.data(), P->nlev, lev.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s) !=
             cudaSuccess ||
+        cudaMemcpyAsync(hc.data(), P->hoff, size_t(P->ntiles) * sizeof(int32_t), cudaMemcpyDeviceToHost, s) !=
+            cudaSuccess ||
         cudaStreamSynchronize(s) != cudaSuccess)
+        return fail(HPB_ERROR_CUDA, "analysis failed");
+    // counts -> offsets; slots of other-tile dependencies in level order
+    int64_t total = 0;
+    for (int32_t t = 0; t < P->ntiles; ++t) {
+        const int32_t c = hc[size_t(t)];
+        hc[size_t(t)] = int32_t(total);
+        total += c;
+    }
+    if (total > INT32_MAX) return fail(HPB_ERROR_INVALID_VALUE, "too many dependencies between row tiles");
+    hc[size_t(P->ntiles)] = int32_t(total);
+    if (cudaMalloc(&P->hrow, size_t(total > 0 ? total : 1) * sizeof(int32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HPB_ERROR_OUT_OF_MEMORY, "device allocation failed");
+    }
+    if (cudaMemcpyAsync(P->hoff, hc.data(), hc.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return fail(HPB_ERROR_CUDA, "analysis failed");
+    k_tri_halo<<<P->ntiles, kLvThreads, 0, s>>>(n, P->dcol, P->hoff, P->dslot, P->hrow);
+    count_launch();
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
         return fail(HPB_ERROR_CUDA, "analysis failed");
     cudaFree(beg);
     cudaFree(cnt);
@@ -653,7 +907,11 @@ int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* 
 void release(Plan* P) {
     cudaFree(P->desc);
     cudaFree(P->dcol);
-    P->dcol = nullptr;
+    cudaFree(P->dslot);
+    cudaFree(P->hoff);
+    cudaFree(P->hrow);
+    P->dcol = P->dslot = nullptr;
+    P->hoff = P->hrow = nullptr;
     cudaFree(P->lvlptr);
     cudaFree(P->nlev);
     cudaFree(P->dpos);
@@ -672,7 +930,7 @@ cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E*
     if (P.n == 0) return cudaSuccess;
     const int fill_grid = int(std::min<int64_t>((int64_t(P.n) + 255) / 256, 148 * 8));
     k_tri_fill<E><<<fill_grid, 256, 0, s>>>(P.n, x, P.flags + P.n);
-    const size_t sm = size_t(kTriTile) * sizeof(E);
+    constexpr size_t sm = trsv_smem<E>();
     static std::once_flag once;
     std::call_once(once, [&] {
         allow_smem(k_trsv<E, false, false>, sm);
@@ -682,8 +940,8 @@ cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E*
     });
     auto k = P.upper ? (unit ? k_trsv<E, true, true> : k_trsv<E, true, false>)
                      : (unit ? k_trsv<E, false, true> : k_trsv<E, false, false>);
-    k<<<P.ntiles, kTriThreads, sm, s>>>(P.n, P.ntiles, P.desc, P.dcol, P.lvlptr, P.nlev, P.ci, val, alpha, b, x,
-                                        P.flags + P.n, P.err);
+    k<<<P.ntiles, kTriThreads, sm, s>>>(P.n, P.ntiles, P.desc, P.dcol, P.dslot, P.hoff, P.hrow, P.lvlptr,
+                                             P.nlev, P.ci, val, alpha, b, x, P.flags + P.n, P.err);
     count_launch(2);
     return cudaGetLastError();
 }

@@ -14,11 +14,12 @@
 // descending for an upper triangle), keeps the tile's solution in shared
 // memory, and its warps take the tile's levels round-robin, so a warp loads
 // the rows of its next level while earlier levels finish.  Dependencies on
-// other tiles poll the value itself (x is pre-filled with a signalling-NaN
-// sentinel); the factorization, whose rows are read as a whole, uses per-row
-// flags (release/acquire at GPU scope).  Every wait has an iteration limit
-// after which the kernel records a timeout and carries on, so a launch
-// always ends.
+// other tiles are read from x itself (x is pre-filled with a signalling-NaN
+// sentinel), by a receiver warp per block that streams them into shared
+// memory ahead of need; the factorization, whose rows are read as a whole,
+// uses per-row flags (release/acquire at GPU scope).  Every wait has a time
+// limit after which the kernel records a timeout and carries on, so a
+// launch always ends.
 #pragma once
 
 #include "hpb_common.cuh"
@@ -48,6 +49,9 @@ struct Plan {
     const int32_t* ci = nullptr;
     int4* desc = nullptr;           // n: (row, first dependency, dependency count, diagonal position) in level order
     int4* dcol = nullptr;           // n: columns of the first four dependencies (-1: none), in level order
+    int4* dslot = nullptr;          // n: halo slot of each of those that lies in another tile (-1: none)
+    int32_t* hoff = nullptr;        // ntiles + 1: first halo slot of each tile in hrow
+    int32_t* hrow = nullptr;        // halo slots: the other-tile row each one is filled from
     int32_t* lvlptr = nullptr;      // ntiles * (kTriTile + 1): level starts within the tile
     int32_t* nlev = nullptr;        // ntiles
     int32_t* dpos = nullptr;        // n: position of the diagonal entry of each row, -1 if absent
