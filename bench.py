@@ -672,7 +672,75 @@ def bench_forms(torch, log=lambda *a: None):
         out["learned_pc_gmres30_lognormal96"] = res
     except Exception as e:
         out["learned_pc_gmres30_lognormal96"] = {"error": repr(e)}
+    # ---- ILU(0): the triangular-solve preconditioner of the drop-in (the
+    # reference's csrsv2 path), on the config-2 system
+    try:
+        A = problems.convdiff2d(1024)
+        b = problems.rhs_uniform(A.n, 606)
+        res = {"kernels": ilu0_probe(torch, A)}
+        for pc in ("none", "jacobi", "ilu0"):
+            t, st, r, x = fused_solve(torch, A, b, "gmres", 30, SOLVER_TOL, precond=pc, max_iters=30000)
+            res[f"fp64_gmres30_{pc}"] = {"s": t, "status": st, "iters": r.iters, "true_rel_residual": _rel(A, b, x)}
+        A5 = spai.family(96, seed=424242)
+        b5 = problems.rhs_uniform(A5.n, 505)
+        t, st, r, x = fused_solve(torch, A5, b5, "gmres", 30, SOLVER_TOL, precond="ilu0", max_iters=30000)
+        res["lognormal96_fp64_gmres30_ilu0"] = {"s": t, "status": st, "iters": r.iters,
+                                                "true_rel_residual": _rel(A5, b5, x)}
+        out["ilu0_convdiff1024"] = res
+    except Exception as e:
+        out["ilu0_convdiff1024"] = {"error": repr(e)}
     return out
+
+
+def ilu0_probe(torch, A, reps=10):
+    """Sparse triangular solves and ILU(0) on the CSR system A (f64): the
+    analyses, the factorization, and per-solve times of the two triangular
+    solves (CUDA events, back to back).  These kernels are latency-bound --
+    a solve is a chain of dependent levels -- so the figure that explains
+    them is the time per level on the critical path, reported beside the
+    algorithmic bytes."""
+    from high_precision_blas1_b200 import Context, _lib
+    L = _lib.lib
+    ctx = Context(0, torch.cuda.current_stream().cuda_stream)
+    rp, ci = (torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (A.row_ptr, A.col_ind))
+    val = torch.from_numpy(A.val.astype(np.float64)).cuda()
+    out = {"n": A.n, "nnz": A.nnz}
+    tris = []
+    try:
+        for upper in (0, 1):
+            h = C.c_void_p()
+            t, st = _timed(torch, lambda: L.hpb_csr_tri_create(ctx.h, upper, A.n, A.nnz, rp.data_ptr(), ci.data_ptr(),
+                                                                C.byref(h)))
+            ctx.check(st, "hpb_csr_tri_create")
+            tris.append(h)
+            tl, ml, sl, _ = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int()
+            L.hpb_csr_tri_info(h, C.byref(tl), C.byref(ml), C.byref(sl), None)
+            out["upper" if upper else "lower"] = {"analysis_s": t, "tiles": tl.value, "max_levels_per_tile": ml.value}
+        lu = val.clone()
+        t, st = _timed(torch, lambda: L.hpb_csr_ilu0_f64(ctx.h, tris[0], lu.data_ptr()))
+        ctx.check(st, "hpb_csr_ilu0_f64")
+        out["ilu0_factor_s"] = t
+        bvec = torch.randn(A.n, dtype=torch.float64, device="cuda")
+        x = torch.empty_like(bvec)
+        rows = np.repeat(np.arange(A.n), np.diff(A.row_ptr))
+        for upper, unit in ((0, 1), (1, 0)):
+            f = lambda: L.hpb_csr_trsv_f64(ctx.h, tris[upper], unit, lu.data_ptr(), 1.0, bvec.data_ptr(), x.data_ptr())
+            for _ in range(3):
+                ctx.check(f(), "trsv")
+            t, _ = _timed(torch, lambda: [f() for _ in range(reps)])
+            ctx.check(L.hpb_csr_tri_check(ctx.h, tris[upper]), "trsv")
+            tri_nnz = int(np.count_nonzero(A.col_ind > rows if upper else A.col_ind < rows))
+            # algorithmic bytes: the triangle's values and columns, b read, x written,
+            # and the diagonal for the non-unit solve
+            alg = tri_nnz * 12 + A.n * (16 + (0 if unit else 12))
+            key = "upper" if upper else "lower"
+            out[key].update({"solve_us": t / reps * 1e6, "triangle_nnz": tri_nnz, "algorithmic_bytes": alg,
+                             "achieved_GBs": alg / (t / reps) / 1e9})
+        return out
+    finally:
+        for h in tris:
+            L.hpb_csr_tri_destroy(h)
+        ctx.close()
 
 
 def dot2_probe(torch, L, ctx, reps=200):

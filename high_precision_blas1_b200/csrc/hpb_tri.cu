@@ -191,29 +191,63 @@ __global__ void k_tri_rows(int32_t n, int64_t nnz, int upper, const int32_t* __r
     dpos[i] = dp;
 }
 
-// Per tile (one block): level of each row = 1 + the largest level of its
-// in-tile dependencies (0 if none), by relaxation sweeps over contiguous
-// per-thread segments walked in dependency order, until a sweep changes
-// nothing (levels only grow and are bounded by the tile's row count);
-// then a counting sort of the tile's rows by level into desc.
+// Per tile (one block): the global level of each row -- the longest chain
+// of dependencies ending at it over the whole triangle -- and the tile's rows
+// sorted by it.  Tiles are taken by ticket in the solve's order (ascending
+// for a lower, descending for an upper triangle) and each waits (bounded)
+// for the previous one to publish its levels, so the levels of every
+// other-tile dependency are final when read.  In the tile: start from
+// 1 + the largest other-tile dependency level, then relaxation sweeps over
+// contiguous per-thread segments walked in dependency order until a sweep
+// changes nothing (a sweep that changes something brings one more row of
+// the longest in-tile chain to its final value, so at most m + 1 sweeps).
+// Then a bitonic sort of (level, row) and a dense renumbering of the
+// distinct levels: the solve's levels of the tile, in global order.  Rows
+// of the tile then never wait on an other-tile row that is late in its own
+// tile merely because of where the tile boundary falls.
 template <bool UPPER>
 __global__ void __launch_bounds__(kLvThreads)
-k_tri_levels(int32_t n, const int32_t* __restrict__ ci, const int32_t* __restrict__ beg,
-             const int32_t* __restrict__ cnt, const int32_t* __restrict__ dpos, int4* __restrict__ desc,
-             int4* __restrict__ dcol, int32_t* __restrict__ lvlptr, int32_t* __restrict__ nlev,
-             int32_t* __restrict__ hcount) {
-    extern __shared__ int sh[];
-    volatile int* lev = sh;          // kTriTile
-    int* hist = sh + kTriTile;       // kTriTile + 1
+k_tri_levels(int32_t n, int32_t ntiles, const int32_t* __restrict__ ci, const int32_t* __restrict__ beg,
+             const int32_t* __restrict__ cnt, const int32_t* __restrict__ dpos, int32_t* glev,
+             int4* __restrict__ desc, int4* __restrict__ dcol, int32_t* __restrict__ lvlptr,
+             int32_t* __restrict__ nlev, int32_t* __restrict__ hcount, unsigned* chain, int* err) {
+    extern __shared__ __align__(16) unsigned char shraw[];
+    unsigned long long* key = reinterpret_cast<unsigned long long*>(shraw);  // kTriTile
+    volatile int* lev = reinterpret_cast<volatile int*>(key + kTriTile);      // kTriTile
+    int* ext = reinterpret_cast<int*>(key);  // aliases key until the sort
     __shared__ int part[kLvThreads];
-    __shared__ int s_max, s_ext;
-    const int t = blockIdx.x;
+    __shared__ int s_tile, s_ext;
+    if (threadIdx.x == 0) {
+        const int tk = int(atomicAdd(chain + ntiles, 1u));
+        s_tile = UPPER ? ntiles - 1 - tk : tk;
+        s_ext = 0;
+    }
+    __syncthreads();
+    const int t = s_tile;
+    if (t < 0 || t >= ntiles) return;
     const int32_t base = int32_t(t) * kTriTile;
     const int32_t m = min(kTriTile, n - base);
-    for (int r = threadIdx.x; r < m; r += blockDim.x) lev[r] = 0;
-    if (threadIdx.x == 0) {
-        s_max = 0;
-        s_ext = 0;
+    const int prev = UPPER ? t + 1 : t - 1;
+    if (prev >= 0 && prev < ntiles) {
+        if (threadIdx.x == 0) {
+            Waiter w;
+            while (ld_acquire(chain + prev) == 0u)
+                if (w.check(err, 63)) break;
+        }
+        __syncthreads();
+    }
+    // lower bound from the other-tile dependencies (final levels)
+    for (int r = threadIdx.x; r < m; r += blockDim.x) {
+        const int32_t i = base + r;
+        const int32_t b = __ldg(beg + i), c = __ldg(cnt + i);
+        int e = 0;
+        for (int32_t k = b; k < b + c; ++k) {
+            const int32_t j = __ldg(ci + k), jl = j - base;
+            // (a column outside [0, n) is reported by k_tri_rows; never read through it)
+            if (!(jl >= 0 && jl < m) && j >= 0 && j < n) e = max(e, __ldcg(glev + j) + 1);
+        }
+        ext[r] = e;
+        lev[r] = e;
     }
     __syncthreads();
     const int seg = (m + blockDim.x - 1) / blockDim.x;
@@ -225,7 +259,7 @@ k_tri_levels(int32_t n, const int32_t* __restrict__ ci, const int32_t* __restric
             const int r = UPPER ? s1 - 1 - k : s0 + k;
             const int32_t i = base + r;
             const int32_t b = __ldg(beg + i), c = __ldg(cnt + i);
-            int lv = 0;
+            int lv = ext[r];
             for (int32_t e = b; e < b + c; ++e) {
                 const int32_t j = __ldg(ci + e) - base;
                 // only dependencies in the solve's direction: the graph stays acyclic
@@ -238,20 +272,35 @@ k_tri_levels(int32_t n, const int32_t* __restrict__ ci, const int32_t* __restric
             }
         }
     } while (__syncthreads_or(changed) && ++sweeps <= m);
+    // publish the tile's levels for the tiles after it
+    for (int r = threadIdx.x; r < m; r += blockDim.x) __stcg(glev + base + r, lev[r]);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) st_release(chain + t, 1u);
 
-    int mx = 0;
-    for (int r = threadIdx.x; r < m; r += blockDim.x) mx = max(mx, lev[r]);
-    atomicMax(&s_max, mx);
-    for (int r = threadIdx.x; r <= m; r += blockDim.x) hist[r] = 0;
+    // sort the tile's rows by (level, row): bitonic over kTriTile keys
+    for (int r = threadIdx.x; r < kTriTile; r += blockDim.x)
+        key[r] = r < m ? (static_cast<unsigned long long>(lev[r]) << 13) | static_cast<unsigned long long>(r)
+                       : ~0ull;
     __syncthreads();
-    const int L = s_max + 1;
-    for (int r = threadIdx.x; r < m; r += blockDim.x) atomicAdd(&hist[lev[r]], 1);
-    __syncthreads();
-    const int cs = (L + blockDim.x - 1) / blockDim.x;
-    const int c0 = min(L, int(threadIdx.x) * cs), c1 = min(L, c0 + cs);
-    int sum = 0;
-    for (int l = c0; l < c1; ++l) sum += hist[l];
-    part[threadIdx.x] = sum;
+    for (int k = 2; k <= kTriTile; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < kTriTile; i += blockDim.x) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long a = key[i], b = key[ixj];
+                    if ((a > b) == ((i & k) == 0)) {
+                        key[i] = b;
+                        key[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    // dense level numbers: a new level starts where the level value changes
+    int nf = 0;
+    for (int i = s0; i < s1; ++i) nf += (i == 0 || (key[i] >> 13) != (key[i - 1] >> 13)) ? 1 : 0;
+    part[threadIdx.x] = nf;
     __syncthreads();
     if (threadIdx.x == 0) {
         int acc = 0;
@@ -260,33 +309,24 @@ k_tri_levels(int32_t n, const int32_t* __restrict__ ci, const int32_t* __restric
             part[w] = acc;
             acc += v;
         }
+        nlev[t] = acc;
+        lvlptr[size_t(t) * (kTriTile + 1) + acc] = m;
     }
     __syncthreads();
-    int run = part[threadIdx.x];
     int32_t* lp = lvlptr + size_t(t) * (kTriTile + 1);
-    for (int l = c0; l < c1; ++l) {
-        const int v = hist[l];
-        hist[l] = run;
-        lp[l] = run;
-        run += v;
-    }
-    if (threadIdx.x == 0) {
-        lp[L] = m;
-        nlev[t] = L;
-    }
-    __syncthreads();
-    int ext = 0;
-    for (int r = threadIdx.x; r < m; r += blockDim.x) {
-        const int pos = atomicAdd(&hist[lev[r]], 1);
-        const int32_t i = base + r;
-        const int32_t b = __ldg(beg + i), c = __ldg(cnt + i);
-        desc[base + pos] = make_int4(i, b, c, __ldg(dpos + i));
+    int d = part[threadIdx.x];
+    int ext_n = 0;
+    for (int i = s0; i < s1; ++i) {
+        if (i == 0 || (key[i] >> 13) != (key[i - 1] >> 13)) lp[d++] = i;
+        const int32_t row = base + int32_t(key[i] & 8191ull);
+        const int32_t b = __ldg(beg + row), c = __ldg(cnt + row);
+        desc[base + i] = make_int4(row, b, c, __ldg(dpos + row));
         const int4 c4 = make_int4(c > 0 ? __ldg(ci + b) : -1, c > 1 ? __ldg(ci + b + 1) : -1,
                                   c > 2 ? __ldg(ci + b + 2) : -1, c > 3 ? __ldg(ci + b + 3) : -1);
-        dcol[base + pos] = c4;
-        ext += is_ext(c4.x, base, m) + is_ext(c4.y, base, m) + is_ext(c4.z, base, m) + is_ext(c4.w, base, m);
+        dcol[base + i] = c4;
+        ext_n += is_ext(c4.x, base, m) + is_ext(c4.y, base, m) + is_ext(c4.z, base, m) + is_ext(c4.w, base, m);
     }
-    atomicAdd(&s_ext, ext);
+    atomicAdd(&s_ext, ext_n);
     __syncthreads();
     if (threadIdx.x == 0) hcount[t] = s_ext;
 }
@@ -456,9 +496,10 @@ __global__ void k_tri_fill(int32_t n, E* __restrict__ x, unsigned* ticket) {
 // row waits on shared memory with neither a flag nor a fence, instead of an
 // L2 round trip; the producing tile runs only a few levels ahead, so that
 // round trip would otherwise sit on the critical path of nearly every level.
-template <class E> struct kHalo { static constexpr int value = 8192; };
-template <> struct kHalo<float> { static constexpr int value = 16384; };
-template <> struct kHalo<cd> { static constexpr int value = 4096; };
+template <class E> struct kHalo { static constexpr int value = 12288; };
+template <> struct kHalo<float> { static constexpr int value = 24576; };
+template <> struct kHalo<cd> { static constexpr int value = 5632; };
+constexpr int kRecv = 8;  // slots in flight per receiver lane
 
 template <class E>
 constexpr size_t trsv_smem() {
@@ -515,43 +556,60 @@ struct RowData {
     E rhs, dg, v[kPre];
 };
 
-// Levels whose first chunk a warp gathers ahead (registers permitting).
-template <class E> struct kLook { static constexpr int value = 3; };
-template <> struct kLook<cd> { static constexpr int value = 2; };
+// A row's descriptors (first gather stage): desc, dependency columns and
+// halo slots at level-order position p (p >= p1: inactive).
+struct RowIdx {
+    int4 d, c4, s4;
+};
+__device__ __forceinline__ void gather_idx(RowIdx& g, int32_t p, int32_t p1, int32_t base,
+                                           const int4* __restrict__ desc, const int4* __restrict__ dcol,
+                                           const int4* __restrict__ dslot) {
+    g.d = make_int4(-1, 0, 0, -1);
+    g.c4 = make_int4(-1, -1, -1, -1);
+    g.s4 = make_int4(-1, -1, -1, -1);
+    if (p < p1) {
+        g.d = desc[base + p];
+        g.c4 = dcol[base + p];
+        g.s4 = dslot[base + p];
+    }
+}
+
+// Second gather stage: resolve the dependency sources, load alpha b_i, the
+// diagonal and the dependency values.
+template <class E, bool UNIT>
+__device__ __forceinline__ void gather_val(RowData<E>& r, const RowIdx& g, int32_t base, int32_t m,
+                                           const E* __restrict__ val, E alpha, const E* __restrict__ b) {
+    constexpr int H = kHalo<E>::value;
+    const int4 d = g.d;
+    r.row = d.x;
+    r.e0 = d.y;
+    r.nd = d.z;
+    const int32_t c[kPre] = {g.c4.x, g.c4.y, g.c4.z, g.c4.w};
+    const int32_t sl[kPre] = {g.s4.x, g.s4.y, g.s4.z, g.s4.w};
+#pragma unroll
+    for (int k = 0; k < kPre; ++k) {
+        const int32_t jl = c[k] - base;
+        r.src[k] = (jl >= 0 && jl < m) ? jl : (sl[k] >= 0 && sl[k] < H ? -(sl[k] + 2) : -1);
+        r.v[k] = E{};
+    }
+    r.rhs = E{};
+    r.dg = E{};
+    if (d.x < 0) return;
+    r.rhs = scale(alpha, ldE(b, d.x));
+    if (!UNIT) r.dg = ldE(val, d.w);
+#pragma unroll
+    for (int k = 0; k < kPre; ++k)
+        if (k < d.z) r.v[k] = ldE(val, d.y + k);
+}
 
 template <class E, bool UNIT>
 __device__ __forceinline__ void gather_row(RowData<E>& r, int32_t p, int32_t p1, int32_t base, int32_t m,
                                            const int4* __restrict__ desc, const int4* __restrict__ dcol,
                                            const int4* __restrict__ dslot, const E* __restrict__ val, E alpha,
                                            const E* __restrict__ b) {
-    constexpr int H = kHalo<E>::value;
-    r.row = -1;
-    r.e0 = 0;
-    r.nd = 0;
-    r.rhs = E{};
-    r.dg = E{};
-#pragma unroll
-    for (int k = 0; k < kPre; ++k) {
-        r.src[k] = -1;
-        r.v[k] = E{};
-    }
-    if (p >= p1) return;
-    const int4 d = desc[base + p], c4 = dcol[base + p], s4 = dslot[base + p];
-    const int32_t c[kPre] = {c4.x, c4.y, c4.z, c4.w};
-    const int32_t sl[kPre] = {s4.x, s4.y, s4.z, s4.w};
-    r.row = d.x;
-    r.e0 = d.y;
-    r.nd = d.z;
-#pragma unroll
-    for (int k = 0; k < kPre; ++k) {
-        const int32_t jl = c[k] - base;
-        r.src[k] = (jl >= 0 && jl < m) ? jl : (sl[k] >= 0 && sl[k] < H ? -(sl[k] + 2) : -1);
-    }
-    r.rhs = scale(alpha, ldE(b, d.x));
-    if (!UNIT) r.dg = ldE(val, d.w);
-#pragma unroll
-    for (int k = 0; k < kPre; ++k)
-        if (k < d.z) r.v[k] = ldE(val, d.y + k);
+    RowIdx g;
+    gather_idx(g, p, p1, base, desc, dcol, dslot);
+    gather_val<E, UNIT>(r, g, base, m, val, alpha, b);
 }
 
 // Solve one gathered row; returns x_row.
@@ -599,7 +657,6 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int4* __r
        const int32_t* __restrict__ lvlptr, const int32_t* __restrict__ nlev, const int32_t* __restrict__ ci,
        const E* __restrict__ val, E alpha, const E* __restrict__ b, E* x, unsigned* ticket, int* err) {
     constexpr int H = kHalo<E>::value;
-    constexpr int D = kLook<E>::value;
     extern __shared__ __align__(16) unsigned char smraw[];
     E* xs = reinterpret_cast<E*>(smraw);
     E* halo = xs + kTriTile;
@@ -618,69 +675,92 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int4* __r
     constexpr int W = kSolveWarps;
 
     if (warp == W) {  // ---- receiver warp
+        // Lane k takes slots k, k + 32, k + 64, ... in order, kRecv of its
+        // own slots in flight at a time; lanes advance independently (no
+        // warp-wide window), so one late value holds back only its lane.
+        constexpr int K = kRecv;
         const int32_t h0 = hoff[t];
         const int32_t nsl = min(hoff[t + 1] - h0, H);
         const int32_t* hr = hrow + h0;
-        int32_t s0 = 0;
-        unsigned pend = 0xFu;  // bit j: slot s0 + lane + 32 j not yet delivered
-        int32_t row[4];
+        int32_t j0 = 0;  // own index of the window's first slot: slot = lane + 32 (j0 + k)
+        unsigned pend = 0;
+        int32_t row[K];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) row[j] = s0 + lane + 32 * j < nsl ? hr[s0 + lane + 32 * j] : 0;
+        for (int k = 0; k < K; ++k) {
+            const int32_t sl = lane + 32 * k;
+            row[k] = sl < nsl ? hr[sl] : 0;
+            if (sl < nsl) pend |= 1u << k;
+        }
         Waiter w;
-        while (s0 < nsl) {
-            E v[4];
+        while (pend != 0u) {
+            E v[K];
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (((pend >> j) & 1u) && s0 + lane + 32 * j < nsl) v[j] = Pub<E>::load(x, row[j]);
+            for (int k = 0; k < K; ++k)
+                if ((pend >> k) & 1u) v[k] = Pub<E>::load(x, row[k]);
+            bool got = false;
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int32_t sl = s0 + lane + 32 * j;
-                if (!((pend >> j) & 1u)) continue;
-                if (sl >= nsl) {
-                    pend &= ~(1u << j);
-                } else if (!Pub<E>::pending(v[j])) {
-                    vstore(halo + sl, v[j]);
-                    pend &= ~(1u << j);
+            for (int k = 0; k < K; ++k)
+                if (((pend >> k) & 1u) && !Pub<E>::pending(v[k])) {
+                    vstore(halo + lane + 32 * (j0 + k), v[k]);
+                    pend &= ~(1u << k);
+                    got = true;
                 }
+            // slide over the delivered front of the window
+            for (int g = 0; g < K && (pend & 1u) == 0u && lane + 32 * j0 < nsl; ++g) {
+                ++j0;
+                pend >>= 1;
+#pragma unroll
+                for (int k = 0; k + 1 < K; ++k) row[k] = row[k + 1];
+                const int32_t sl = lane + 32 * (j0 + K - 1);
+                row[K - 1] = sl < nsl ? hr[sl] : 0;
+                if (sl < nsl) pend |= 1u << (K - 1);
             }
-            if (__all_sync(0xffffffffu, (pend & 1u) == 0u)) {  // the window's first 32 slots are in: slide
-                s0 += 32;
-                pend = (pend >> 1) | 0x8u;
-                row[0] = row[1];
-                row[1] = row[2];
-                row[2] = row[3];
-                row[3] = s0 + lane + 96 < nsl ? hr[s0 + lane + 96] : 0;
+            if (got) {
                 w = Waiter();
             } else {
-                const bool stop = w.check(err, 15);  // every lane checks, the warp leaves together
-                if (__any_sync(0xffffffffu, stop)) break;
+                // nothing arrived in this pass: back off before polling the same
+                // lines again, so waiting receivers do not flood the L2 slices
+                // their producers store to
+                if (w.check(err, 15)) break;
+                __nanosleep(100);
             }
         }
         return;
     }
 
-    // ---- solve warps: levels round-robin.  A warp holds the gathered first
-    // chunk (32 rows) of its next D levels; within a level, the next chunk is
-    // gathered while the current one is solved.
+    // ---- solve warps: levels round-robin.  The first chunk (32 rows) of a
+    // warp's coming levels is gathered in a three-stage software pipeline
+    // across the warp's visits -- level bounds for level l + 3W, descriptors
+    // for l + 2W, values for l + W -- so each stage uses only registers that
+    // arrived during an earlier visit and a visit never stalls on a chain of
+    // dependent loads.  Within a level, the next chunk is gathered while the
+    // current one is solved.
     const int L = nlev[t];
     const int32_t* lp = lvlptr + size_t(t) * (kTriTile + 1);
-    RowData<E> ahead[D];
-#pragma unroll
-    for (int j = 0; j < D; ++j) {
-        const int lj = warp + j * W;
-        const int32_t a0 = lj < L ? lp[lj] : 0, a1 = lj < L ? lp[lj + 1] : 0;
-        gather_row<E, UNIT>(ahead[j], a0 + lane, a1, base, m, desc, dcol, dslot, val, alpha, b);
-    }
+    auto bounds = [&](int lj, int32_t& a0, int32_t& a1) {
+        a0 = lj < L ? lp[lj] : 0;
+        a1 = lj < L ? lp[lj + 1] : 0;
+    };
+    int32_t pa0, pa1;          // stage 1: bounds of level l + 2W (l + 3W after the shift below)
+    RowIdx gb;                 // stage 2: descriptors of level l + W (l + 2W after the shift)
+    int32_t gb0, gb1;
+    RowData<E> rc;             // stage 3: gathered rows of level l (l + W after the shift)
+    int32_t rc0, rc1;
+    bounds(warp, rc0, rc1);
+    gather_row<E, UNIT>(rc, rc0 + lane, rc1, base, m, desc, dcol, dslot, val, alpha, b);
+    bounds(warp + W, gb0, gb1);
+    gather_idx(gb, gb0 + lane, gb1, base, desc, dcol, dslot);
+    bounds(warp + 2 * W, pa0, pa1);
     for (int l = warp; l < L; l += W) {
-        const int32_t p0 = lp[l], p1 = lp[l + 1];
-        RowData<E> cur = ahead[0];
-#pragma unroll
-        for (int j = 0; j + 1 < D; ++j) ahead[j] = ahead[j + 1];
-        {
-            const int lj = l + D * W;
-            const int32_t a0 = lj < L ? lp[lj] : 0, a1 = lj < L ? lp[lj + 1] : 0;
-            gather_row<E, UNIT>(ahead[D - 1], a0 + lane, a1, base, m, desc, dcol, dslot, val, alpha, b);
-        }
+        const int32_t p0 = rc0, p1 = rc1;
+        RowData<E> cur = rc;
+        gather_val<E, UNIT>(rc, gb, base, m, val, alpha, b);        // level l + W
+        rc0 = gb0;
+        rc1 = gb1;
+        gather_idx(gb, pa0 + lane, pa1, base, desc, dcol, dslot);   // level l + 2W
+        gb0 = pa0;
+        gb1 = pa1;
+        bounds(l + 3 * W, pa0, pa1);                                 // level l + 3W
         int32_t pub_row = -1;
         E pub_val{};
         if (l > 0) level_sync(l - 1);  // levels < l of the tile are complete
@@ -819,11 +899,14 @@ int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* 
     P->ntiles = int32_t((int64_t(n) + kTriTile - 1) / kTriTile);
     cudaGetDevice(&P->device);
     cudaStream_t s = ctx->stream;
-    int32_t *beg = nullptr, *cnt = nullptr;
+    int32_t *beg = nullptr, *cnt = nullptr, *glev = nullptr;
+    unsigned* chain = nullptr;
     int* missing = nullptr;
     auto fail = [&](int status, const char* what) {
         cudaFree(beg);
         cudaFree(cnt);
+        cudaFree(glev);
+        cudaFree(chain);
         cudaFree(missing);
         release(P);
         return set_error(ctx, status, "hpb_csr_tri_create: %s", what);
@@ -837,7 +920,9 @@ int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* 
         cudaMalloc(&P->dpos, nn * sizeof(int32_t)) != cudaSuccess ||
         cudaMalloc(&P->flags, (nn + 1) * sizeof(unsigned)) != cudaSuccess ||
         cudaMalloc(&P->err, 2 * sizeof(int)) != cudaSuccess || cudaMalloc(&beg, nn * sizeof(int32_t)) != cudaSuccess ||
-        cudaMalloc(&cnt, nn * sizeof(int32_t)) != cudaSuccess || cudaMalloc(&missing, sizeof(int)) != cudaSuccess) {
+        cudaMalloc(&cnt, nn * sizeof(int32_t)) != cudaSuccess || cudaMalloc(&missing, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&glev, nn * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&chain, (size_t(P->ntiles) + 1) * sizeof(unsigned)) != cudaSuccess) {
         cudaGetLastError();
         return fail(HPB_ERROR_OUT_OF_MEMORY, "device allocation failed");
     }
@@ -846,15 +931,18 @@ int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* 
     cudaMemcpyAsync(P->err, init, sizeof(init), cudaMemcpyHostToDevice, s);
     cudaMemsetAsync(missing, 0, sizeof(int), s);
     k_tri_rows<<<(n + 255) / 256, 256, 0, s>>>(n, nnz, P->upper, rp, ci, beg, cnt, P->dpos, P->err, missing);
-    const size_t lv_smem = (2 * size_t(kTriTile) + 1) * sizeof(int);
+    const size_t lv_smem = size_t(kTriTile) * (sizeof(unsigned long long) + sizeof(int));
+    cudaMemsetAsync(chain, 0, (size_t(P->ntiles) + 1) * sizeof(unsigned), s);
     if (P->upper) {
         allow_smem(k_tri_levels<true>, lv_smem);
-        k_tri_levels<true><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, ci, beg, cnt, P->dpos, P->desc, P->dcol,
-                                                                   P->lvlptr, P->nlev, P->hoff);
+        k_tri_levels<true><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, P->ntiles, ci, beg, cnt, P->dpos, glev,
+                                                                   P->desc, P->dcol, P->lvlptr, P->nlev, P->hoff,
+                                                                   chain, P->err);
     } else {
         allow_smem(k_tri_levels<false>, lv_smem);
-        k_tri_levels<false><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, ci, beg, cnt, P->dpos, P->desc, P->dcol,
-                                                                    P->lvlptr, P->nlev, P->hoff);
+        k_tri_levels<false><<<P->ntiles, kLvThreads, lv_smem, s>>>(n, P->ntiles, ci, beg, cnt, P->dpos, glev,
+                                                                    P->desc, P->dcol, P->lvlptr, P->nlev, P->hoff,
+                                                                    chain, P->err);
     }
     count_launch(2);
     if (cudaGetLastError() != cudaSuccess) return fail(HPB_ERROR_CUDA, "analysis launch failed");
@@ -890,8 +978,11 @@ int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* 
         return fail(HPB_ERROR_CUDA, "analysis failed");
     cudaFree(beg);
     cudaFree(cnt);
+    cudaFree(glev);
+    cudaFree(chain);
     cudaFree(missing);
-    beg = cnt = nullptr;
+    beg = cnt = glev = nullptr;
+    chain = nullptr;
     missing = nullptr;
     if (host_err & kErrColumn) return fail(HPB_ERROR_INVALID_VALUE, "row pointer or column index out of range");
     if (host_err & kErrUnsorted)
