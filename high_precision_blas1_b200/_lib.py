@@ -126,6 +126,17 @@ for t in TYPES:
     _sig(f"hpb_csr_spmv_dot2_{t}", C.c_int, [P, I32, I32, I64, P, P, P, P, P, P, P])
     _sig(f"hpb_csr_diag_{t}", C.c_int, [P, I32, P, P, P, P])
     _sig(f"hpb_random_{t}", C.c_int, [P, I64, C.c_uint64, S, S, P])
+# Matrix Market reader (host)
+class hpb_mm_csr(C.Structure):
+    _fields_ = [("rows", C.c_int32), ("cols", C.c_int32), ("nnz", C.c_int64), ("is_complex", C.c_int),
+                ("symmetric", C.c_int), ("row_ptr", C.POINTER(C.c_int32)), ("col_ind", C.POINTER(C.c_int32)),
+                ("val", C.POINTER(C.c_double))]
+
+
+_sig("hpb_mm_read_csr", C.c_int, [C.c_char_p, C.POINTER(hpb_mm_csr)])
+_sig("hpb_mm_free", None, [C.POINTER(hpb_mm_csr)])
+_sig("hpb_mm_last_error", C.c_char_p, [])
+
 # sparse triangular solves and ILU(0)
 _sig("hpb_csr_tri_create", C.c_int, [P, C.c_int, I32, I64, P, P, C.POINTER(P)])
 _sig("hpb_csr_tri_destroy", C.c_int, [P])

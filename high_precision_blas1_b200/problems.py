@@ -185,3 +185,31 @@ def rhs_uniform(n: int, seed: int, complex_: bool = False) -> np.ndarray:
     if complex_:
         return rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)
     return rng.uniform(-1, 1, n)
+
+
+def read_matrix_market(path) -> CSR:
+    """A Matrix Market coordinate file as a CSR matrix (host arrays), read by
+    the library's parser (hpb_mm_read_csr: the reference's
+    csr::matrix_market_reader semantics -- symmetric files mirrored, entries
+    in stable (row, column) order, duplicates kept, pattern entries 1).
+    Raises ValueError with the parser's message on a rejected file."""
+    import ctypes as C
+    from . import _lib
+    m = _lib.hpb_mm_csr()
+    st = _lib.lib.hpb_mm_read_csr(str(path).encode(), C.byref(m))
+    if st != 0:
+        raise ValueError(_lib.lib.hpb_mm_last_error().decode())
+    try:
+        n, nnz = m.rows, m.nnz
+        rp = np.ctypeslib.as_array(m.row_ptr, shape=(n + 1,)).copy()
+        ci = np.ctypeslib.as_array(m.col_ind, shape=(max(nnz, 1),))[:nnz].copy()
+        if m.is_complex:
+            v = np.ctypeslib.as_array(m.val, shape=(max(2 * nnz, 2),))[:2 * nnz].copy()
+            val = v[0::2] + 1j * v[1::2]
+        else:
+            val = np.ctypeslib.as_array(m.val, shape=(max(nnz, 1),))[:nnz].copy()
+        if m.cols != m.rows:
+            raise ValueError(f"matrix is {m.rows} x {m.cols}; the CSR type here holds square operators")
+        return CSR(n, rp.astype(np.int32), ci.astype(np.int32), val)
+    finally:
+        _lib.lib.hpb_mm_free(C.byref(m))

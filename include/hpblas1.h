@@ -370,6 +370,32 @@ int hpb_csr_ilu0_c64(hpb_context* ctx, const hpb_csr_tri* lower, void* val);
 int hpb_csr_ilu0_c128(hpb_context* ctx, const hpb_csr_tri* lower, void* val);
 
 /* ---------------------------------------------------------------------- */
+/* Matrix Market file -> CSR in host memory (replaces csr::              */
+/* matrix_market_reader, common/csr/matrix_market_reader.h:48-673; the     */
+/* C++ drop-in common/csr/matrix_market_reader.h is built on this).        */
+/* Accepts "%%MatrixMarket matrix coordinate {real|integer|pattern|complex} */
+/* {general|symmetric}"; a symmetric file's off-diagonal entries are        */
+/* mirrored; hermitian / skew-symmetric and array storage are refused.      */
+/* 1-based indices are checked against the declared size; entries are      */
+/* stably sorted by (row, column), duplicates kept; pattern entries are 1.  */
+/* Host code only (no GPU needed).                                          */
+/* ---------------------------------------------------------------------- */
+typedef struct hpb_mm_csr {
+    int32_t rows, cols;
+    int64_t nnz;
+    int is_complex;         /* val holds (re, im) pairs */
+    int symmetric;          /* the file was symmetric (already mirrored) */
+    int32_t* row_ptr;       /* rows + 1, 0-based */
+    int32_t* col_ind;       /* nnz */
+    double* val;            /* nnz (real) or 2 nnz (complex) */
+} hpb_mm_csr;
+/* Returns 0 or a negative hpb_status (message: hpb_mm_last_error()); the
+ * arrays are allocated by the library and released by hpb_mm_free. */
+int hpb_mm_read_csr(const char* path, hpb_mm_csr* out);
+void hpb_mm_free(hpb_mm_csr* m);
+const char* hpb_mm_last_error(void);
+
+/* ---------------------------------------------------------------------- */
 /* Krylov solvers on a CSR matrix (the reference's bicgstabl.h, gmres.h,   */
 /* bicgstab.h over gpu_vector_operations + csr::gpu_matrix, as driven by   */
 /* test_csr_linear_solver.cpp:101-353), plain drop-in path: every          */

@@ -15,6 +15,7 @@ SRC = r'''
 #include <common/csr/linear_operator.h>
 #include <common/csr/preconditioner.h>
 #include <common/csr/gpu_ilu0_preconditioner.h>
+#include <common/csr/matrix_market_reader.h>
 #include <numerical_algos/lin_solvers/default_monitor.h>
 #include <numerical_algos/lin_solvers/bicgstabl.h>
 #include <numerical_algos/lin_solvers/bicgstab.h>
@@ -54,6 +55,14 @@ template <class T> int run(int n) {
     ok = ok && s4.solve(lin_op, b, x);
     mat.triangular_solve_lower(b, x);
     mat.triangular_solve_upper(x, b, T(2.0));
+    // Matrix Market reader (test_csr_matrix.cpp's use of csr::matrix_market_reader)
+    csr::matrix_market_reader<T> reader(true);
+    mat_t mm_mat(&cublas);
+    reader.read_file_2_csr_marix("m.mtx", &mm_mat);
+    int rp_n, ci_n, nnz, rows, cols; int *rp = nullptr, *ci = nullptr; T* val = nullptr;
+    reader.get_matrix_dim(rows, cols);
+    reader.allocate_set_csr_pointers(rp_n, ci_n, nnz, rp, ci, val);
+    free(rp); free(ci); free(val);
     vec_ops.free_vector(x); vec_ops.free_vector(b);
     return ok;
 }

@@ -169,3 +169,19 @@ def test_spmv_dot2_bad_args(gpu):
     assert f(ctx.h, A.n, A.n, A.nnz, p[0], p[1], p[2] + 4, p[3], p[4], p[5], out.data_ptr()) == -1
     # zero rows: out is the empty sum
     assert f(ctx.h, 0, 0, 0, p[0], None, None, None, None, None, out.data_ptr()) == 0
+
+
+@pytest.mark.parametrize("name,t", [("general_real", "f64"), ("symmetric_real", "f32"), ("complex_general", "c128")])
+def test_spmv_of_matrix_market_file(gpu, name, t):
+    """A Matrix Market file read by the library's parser, multiplied on the
+    GPU: equals scipy's product of scipy's own reading of the file."""
+    import scipy.io
+    from conftest import GOLDEN
+    ctx, torch = gpu
+    A = problems.read_matrix_market(GOLDEN / "mm" / f"{name}.mtx")
+    ref = scipy.io.mmread(str(GOLDEN / "mm" / f"{name}.mtx")).tocsr()
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(A.n) + (1j * rng.standard_normal(A.n) if t.startswith("c") else 0)
+    y = spmv(ctx, torch, t, A, 1.0, x, 0.0, np.zeros(A.n))
+    want = ref @ x.astype(WIDE[t])
+    assert np.allclose(y, want, rtol=4e-6 if t in ("f32", "c64") else 1e-14, atol=1e-6 if t == "f32" else 1e-14)
