@@ -147,6 +147,8 @@ for t in TYPES:
     _sig(f"hpb_csr_ilu0_{t}", C.c_int, [P, P, P])
 _sig("hpb_gendot_f64", C.c_int, [C.c_uint64, I64, C.c_double, P, P, C.POINTER(C.c_int64)])
 _sig("hpb_gendot_c128", C.c_int, [C.c_uint64, I64, C.c_double, P, P])
+_sig("hpb_gendot_f64_dev", C.c_int, [P, C.c_uint64, I64, C.c_double, P, P, C.POINTER(C.c_int64)])
+_sig("hpb_gendot_c128_dev", C.c_int, [P, C.c_uint64, I64, C.c_double, P, P])
 _sig("hpb_copy", C.c_int, [P, I64, C.c_size_t, P, P])
 _sig("hpb_swap", C.c_int, [P, I64, C.c_size_t, P, P])
 
@@ -254,4 +256,4 @@ def exported_symbols() -> list[str]:
     import re
     hdr = Path(__file__).resolve().parent.parent / "include" / "hpblas1.h"
     txt = hdr.read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|void\*|const char\*|uint64_t)\s+(hpb_\w+)\s*\(", txt, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void\*|void|const char\*|uint64_t)\s+(hpb_\w+)\s*\(", txt, re.M)))

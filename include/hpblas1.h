@@ -584,6 +584,20 @@ int hpb_gendot_f64(uint64_t seed, int64_t n, double cond, double* x, double* y, 
 /* Complex pair (interleaved): Re conj(x).y is ill-conditioned
  * (generate_vector_pair_complex.hpp:142-460 generates complex pairs). */
 int hpb_gendot_c128(uint64_t seed, int64_t n, double cond, double* x, double* y);
+/* The same scheme generated on the device into device arrays x, y (n
+ * elements; complex: n interleaved complex values), for accuracy sweeps at
+ * lengths where the host generator is the bottleneck (the reference's
+ * generate_vector_pair / generate_vector_pair_complex, common/
+ * generate_vector_pair.hpp:119-182, generate_vector_pair_complex.hpp:
+ * 142-460).  The random part comes from a counter-based hash of (seed,
+ * index), so the vectors depend only on (seed, n, cond), not on the host
+ * generator's sequence; the running dot of the tail step is the Dot2 of
+ * the head (a double-double), then a compensated sequential update.
+ * Stream-ordered on the context's stream; uses a stream-ordered allocation
+ * of N_fix + 4 doubles (complex: plus 2n doubles). */
+int hpb_gendot_f64_dev(hpb_context* ctx, uint64_t seed, int64_t n, double cond, double* x, double* y,
+                       int64_t* n_fixed_out);
+int hpb_gendot_c128_dev(hpb_context* ctx, uint64_t seed, int64_t n, double cond, void* x, void* y);
 
 #ifdef __cplusplus
 }

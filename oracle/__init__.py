@@ -59,6 +59,8 @@ def oro():
             getattr(lib, name).restype = D
         lib.oro_bound_dot2_block_real.argtypes = [D, D, D, D]
         lib.oro_bound_dot2_block_real.restype = D
+        lib.oro_gendot_dev_f64.argtypes = [C.c_uint64, I64, D, P, P]
+        lib.oro_gendot_dev_f64.restype = I64
         for suf in ("f32", "f64", "c64", "c128"):
             f = getattr(lib, "oro_csr_trsv_" + suf)
             f.argtypes = [C.c_int32, P, P, P, C.c_int, C.c_int, P, P, P]
@@ -289,3 +291,11 @@ def csr_ilu0(row_ptr: np.ndarray, col_ind: np.ndarray, val: np.ndarray):
     if r == -2:
         raise ValueError("a row stores no diagonal")
     return lu, int(r)
+
+
+def gendot_dev(seed: int, n: int, cond: float):
+    """The device GenDot generator restated on the CPU: (x, y, N_fix)."""
+    x = np.zeros(n)
+    y = np.zeros(n)
+    nfix = oro().oro_gendot_dev_f64(seed, n, cond, _ptr(x), _ptr(y))
+    return x, y, int(nfix)
