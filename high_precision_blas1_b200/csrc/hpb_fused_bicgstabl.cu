@@ -52,6 +52,20 @@ struct Report {
     int nonfinite;  // x held a non-finite entry
 };
 
+// The monitor of the device-side cycle loop (default_monitor semantics, one
+// test per cycle): the host sets tol / max_iters / iters once per solve and
+// chunk_left / hl before each launch of the loop graph.
+constexpr int kLoopChunk = 128;  // cycles one launch of the loop graph runs at most
+struct MonState {
+    double tol;
+    double rn;
+    int max_iters;
+    int iters;
+    int chunk_left;
+    int hl;          // history entries written in this launch
+    int finished, conv, valid, breakdown;
+};
+
 template <class E>
 struct Vecs {
     E* r[kMaxL + 1];
@@ -478,7 +492,43 @@ struct BcgPlan<E>::Impl {
     double* dnorm = nullptr;
     Report* hrep = nullptr;
     double* hnorm = nullptr;
+    MonState* mon = nullptr;    // device
+    double* dhist = nullptr;    // device: 2 kLoopChunk
+    MonState* hmon = nullptr;   // pinned
+    double* hhist = nullptr;    // pinned: 2 kLoopChunk
 };
+
+// End of a cycle inside the loop graph: the host loop's test, then the
+// loop's condition.  Every path reaches the one cudaGraphSetConditional
+// call, and the loop stops after chunk_left cycles whatever the test says,
+// so one launch of the graph always ends.
+__global__ void k_monitor(MonState* M, const Report* rep, double* hist, int L, cudaGraphConditionalHandle h) {
+    const int it = M->iters + L;
+    M->iters = it;
+    int fin;
+    if (rep->breakdown) {
+        M->breakdown = 1;
+        fin = 1;
+    } else {
+        const double rn = rep->rnorm;
+        const int valid = !rep->nonfinite && isfinite(rn);
+        const int conv = valid && rn <= M->tol;
+        M->rn = rn;
+        M->valid = valid;
+        M->conv = conv;
+        const int k = M->hl;
+        if (k < kLoopChunk) {
+            hist[2 * k] = double(it);
+            hist[2 * k + 1] = rn;
+            M->hl = k + 1;
+        }
+        fin = !valid || conv || it >= M->max_iters;
+    }
+    M->finished = fin;
+    const int left = M->chunk_left - 1;
+    M->chunk_left = left;
+    cudaGraphSetConditional(h, (fin || left <= 0) ? 0u : 1u);
+}
 
 template <class E>
 BcgPlan<E>::BcgPlan() = default;
@@ -526,7 +576,7 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     SolverWorkspace& ws = P.ws;
     Vecs<E>& V = P.V;
     const size_t vb = size_t(n) * sizeof(E);
-    int wst = ws.open(sizeof(Report) + 8 * sizeof(double));
+    int wst = ws.open(sizeof(Report) + 8 * sizeof(double) + sizeof(MonState) + 2 * kLoopChunk * sizeof(double));
     if (wst != HPB_SUCCESS) return wst;
     cudaStream_t s = ws.stream;
     // allocations and the diagonal run after the caller's work on the legacy default stream
@@ -554,6 +604,11 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
         return HPB_ERROR_OUT_OF_MEMORY;
     P.hrep = static_cast<Report*>(ws.pinned);
     P.hnorm = reinterpret_cast<double*>(static_cast<char*>(ws.pinned) + sizeof(Report));
+    P.hmon = reinterpret_cast<MonState*>(P.hnorm + 8);
+    P.hhist = reinterpret_cast<double*>(P.hmon + 1);
+    P.mon = static_cast<MonState*>(ws.alloc(sizeof(MonState)));
+    P.dhist = static_cast<double*>(ws.alloc(2 * kLoopChunk * sizeof(double)));
+    if (!P.mon || !P.dhist) return HPB_ERROR_OUT_OF_MEMORY;
     cudaMemsetAsync(P.ticket, 0, 64, s);
     cudaMemsetAsync(P.badflag, 0, 64, s);
     if (jac) {
@@ -572,7 +627,21 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     E* rt = P.rt;
     EpiArgs<S> none{st, drep, EPI_NONE, 0, 0, L};
     int kernels = 0;
-    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HPB_ERROR_CUDA;
+    // the loop graph: a WHILE node whose body is one cycle + the monitor
+    if (cudaGraphCreate(&ws.graph, 0) != cudaSuccess) return HPB_ERROR_CUDA;
+    cudaGraphConditionalHandle cond;
+    if (cudaGraphConditionalHandleCreate(&cond, ws.graph, 1u, cudaGraphCondAssignDefault) != cudaSuccess)
+        return HPB_ERROR_CUDA;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t loop_node;
+    if (cudaGraphAddNode(&loop_node, ws.graph, nullptr, 0, &cp) != cudaSuccess) return HPB_ERROR_CUDA;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return HPB_ERROR_CUDA;
     for (int j = 0; j < L; ++j) {
         k_upd_u<E><<<g_ew, kThreads, 0, s>>>(n, j, V, st);
         k_spmv_dot<E, true><<<g_spd, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt, partials,
@@ -593,9 +662,9 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     }
     launch_final<E>(L, g_red, s, n, 1, V, x, rt, st, partials, ticket, badflag,
                     EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L});
-    ++kernels;
-    cudaMemcpyAsync(P.hrep, drep, sizeof(Report), cudaMemcpyDeviceToHost, s);
-    if (cudaStreamEndCapture(s, &ws.graph) != cudaSuccess) return HPB_ERROR_CUDA;
+    k_monitor<<<1, 1, 0, s>>>(P.mon, drep, P.dhist, L, cond);
+    kernels += 2;
+    if (cudaStreamEndCapture(s, &body) != cudaSuccess) return HPB_ERROR_CUDA;
     if (cudaGraphInstantiate(&ws.exec, ws.graph, 0) != cudaSuccess) return HPB_ERROR_CUDA;
     P.kernels = kernels;
     return HPB_SUCCESS;
@@ -663,16 +732,43 @@ int BcgPlan<E>::run(const E* b, hpb_solver_report* rep, double* hist, int cap) {
         return !valid || conv || iters >= p->max_iters;
     };
     bool finished = record();
-    while (!finished) {
-        if (cudaGraphLaunch(P.ws.exec, s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
-            return HPB_ERROR_CUDA;
-        count_launch(uint64_t(P.kernels));
-        iters += L;
-        if (hrep->breakdown) {
-            breakdown = true;
-            break;
+    if (!finished) {
+        // the cycles run on the device: each launch of the loop graph runs
+        // cycles until the monitor stops (converged, non-finite, max_iters,
+        // breakdown) or kLoopChunk cycles have run; the host reads the
+        // monitor and the history once per launch
+        MonState* hm = P.hmon;
+        *hm = MonState{};
+        hm->tol = tol;
+        hm->max_iters = p->max_iters;
+        hm->iters = 0;
+        while (!finished) {
+            hm->chunk_left = kLoopChunk;
+            hm->hl = 0;
+            const int it0 = hm->iters;
+            if (cudaMemcpyAsync(P.mon, hm, sizeof(MonState), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+                cudaGraphLaunch(P.ws.exec, s) != cudaSuccess ||
+                cudaMemcpyAsync(hm, P.mon, sizeof(MonState), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                cudaMemcpyAsync(P.hhist, P.dhist, 2 * kLoopChunk * sizeof(double), cudaMemcpyDeviceToHost, s) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(s) != cudaSuccess)
+                return HPB_ERROR_CUDA;
+            count_launch(uint64_t(P.kernels) * uint64_t((hm->iters - it0) / L));
+            for (int k = 0; k < hm->hl && hl < cap; ++k, ++hl) {
+                hist[2 * hl] = P.hhist[2 * k];
+                hist[2 * hl + 1] = P.hhist[2 * k + 1];
+            }
+            iters = hm->iters;
+            if (hm->breakdown) {
+                breakdown = true;
+                break;
+            }
+            if (hm->iters == it0) return HPB_ERROR_CUDA;  // the loop made no progress: never expected
+            rn = hm->rn;
+            valid = hm->valid != 0;
+            conv = hm->conv != 0;
+            finished = hm->finished != 0;
         }
-        finished = record();
     }
     auto t1 = std::chrono::steady_clock::now();
 
