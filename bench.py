@@ -901,7 +901,8 @@ def main():
         A, _ = solver_problem(0)
         with Context(0, torch.cuda.current_stream().cuda_stream) as ctx:
             r = spmv_roofline(torch, _lib.lib, ctx, A, reps=args.profile_spmv_dot2)
-        print(f"profile spmv+dot2: {r['avg_launch_us']:.2f} us per launch")
+        print(f"profile spmv+dot2: {r['avg_launch_us']:.2f} us per launch ({r['frac']:.3f} of HBM); plain spmv "
+              f"{r['plain_spmv']['avg_launch_us']:.2f} us ({r['plain_spmv']['frac']:.3f})")
         return
     dist = None
     if ws > 1:
