@@ -588,6 +588,22 @@ def fused_solve(torch, A, b, method, basis, tol, precond="none", complex_=False,
     return t, st, rep, x
 
 
+def plain_solve(torch, A, b, method, basis, tol, precond="none", max_iters=20000):
+    """One solve on the plain drop-in path (f64, host-synchronised
+    reductions), timed, after an untimed one-cycle warm-up."""
+    from high_precision_blas1_b200 import _lib
+    d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (A.row_ptr, A.col_ind, A.val.astype(np.float64),
+                                                                    b.astype(np.float64), np.zeros(A.n))]
+    rep = _lib.hpb_solver_report()
+    f = _lib.lib.hpb_csr_solve_f64
+    pw = _lib.solver_params(method, basis=basis, rel_tol=tol, max_iters=basis, precond=precond)
+    f(C.byref(pw), A.n, A.nnz, *[a.data_ptr() for a in d], C.byref(rep), None, 0)
+    d[4].zero_()
+    p = _lib.solver_params(method, basis=basis, rel_tol=tol, max_iters=max_iters, precond=precond)
+    t, st = _timed(torch, lambda: f(C.byref(p), A.n, A.nnz, *[a.data_ptr() for a in d], C.byref(rep), None, 0))
+    return t, st, rep, d[4].cpu().numpy()
+
+
 def ir_solve(torch, A, b, inner, basis, precond="none", M=None, complex_=False, inner_tol=1e-5, max_iters=5000,
              max_refinements=40, warm=True):
     """One refinement solve, timed; with warm, an untimed single-refinement
@@ -665,6 +681,11 @@ def bench_forms(torch, log=lambda *a: None):
         tj64, stj64, rj64, xj64 = fused_solve(torch, A, b, "gmres", 30, SOLVER_TOL, precond="jacobi", max_iters=30000)
         res["fp64_gmres30_jacobi"] = {"s": tj64, "status": stj64, "iters": rj64.iters,
                                       "true_rel_residual": _rel(A, b, xj64)}
+        # the plain FP64 drop-in (the reference's path: every reduction returns
+        # to the host), GMRES(30) + Jacobi -- the comparison the target names
+        tpd, stpd, rpd, xpd = plain_solve(torch, A, b, "gmres", 30, SOLVER_TOL, precond="jacobi", max_iters=30000)
+        res["plain_dropin_fp64_gmres30_jacobi"] = {"s": tpd, "status": stpd, "iters": rpd.iters,
+                                                   "true_rel_residual": _rel(A, b, xpd)}
         for pc in ("none", "jacobi"):  # one binary32 GMRES(30) cycle per refinement, same 30000-iteration budget
             t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond=pc, inner_tol=0.0, max_iters=0,
                                    max_refinements=1000)
@@ -686,6 +707,7 @@ def bench_forms(torch, log=lambda *a: None):
                 # plain FP64 without a preconditioner may not converge within the budget: then no ratio
                 res["speedup_learned_vs_plain_fp64"] = t64 / (t + tb) if st64 == 0 else None
                 res["speedup_learned_vs_fp64_jacobi"] = tj64 / (t + tb) if stj64 == 0 else None
+                res["speedup_learned_vs_plain_dropin_fp64_jacobi"] = tpd / (t + tb) if stpd == 0 else None
         out["learned_pc_gmres30_lognormal96"] = res
     except Exception as e:
         out["learned_pc_gmres30_lognormal96"] = {"error": repr(e)}
@@ -786,7 +808,45 @@ def dot2_probe(torch, L, ctx, reps=200):
     gbs = 16.0 * n / (us * 1e-6) / 1e9
     return {"workload": "dot2 f64 GenDot n=1048576 cond~1e20, 16 pairs rotated (268 MB > L2)",
             "value": gbs, "unit": "GB/s", "us_per_call": us, "frac_of_hbm": gbs / hbm, "peak_source": src,
+            "graph_replay": dot2_graph_replay(torch, L, xs, ys, n),
             "by_n": dot2_by_n(torch, L, ctx)}
+
+
+def dot2_graph_replay(torch, L, xs, ys, n, calls=64, reps=10):
+    """The same Dot2 calls captured into a CUDA graph and replayed: the GPU
+    time per Dot2 without the host's per-call launch cost (at n = 2^20 a
+    call through the C ABI costs the host about as long as the kernel runs
+    on the device)."""
+    from high_precision_blas1_b200 import Context
+    R = len(xs)
+    side = torch.cuda.Stream()
+    out = torch.zeros(64, dtype=torch.float64, device="cuda")
+    with torch.cuda.stream(side):
+        ctx = Context(0, side.cuda_stream)
+        try:
+            for i in range(4):  # set-up outside the capture (context scratch, module load)
+                ctx.check(L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(), out.data_ptr()))
+            side.synchronize()
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=side):
+                for i in range(calls):
+                    ctx.check(L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(),
+                                             out.data_ptr()))
+            g.replay()
+            side.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(side)
+            for _ in range(reps):
+                g.replay()
+            e1.record(side)
+            side.synchronize()
+            us = e0.elapsed_time(e1) * 1e3 / (reps * calls)
+        finally:
+            ctx.close()
+    hbm, src = peaks()
+    gbs = 16.0 * n / (us * 1e-6) / 1e9
+    return {"us_per_call": us, "GB/s": gbs, "frac_of_hbm": gbs / hbm, "calls_per_graph": calls}
 
 
 def cpu_baseline_solver(t_gpu_iters):
