@@ -569,18 +569,21 @@ def _timed(torch, fn):
     return e0.elapsed_time(e1) * 1e-3, out
 
 
-def fused_solve(torch, A, b, method, basis, tol, precond="none", complex_=False, max_iters=20000, warm=True):
+def fused_solve(torch, A, b, method, basis, tol, precond="none", complex_=False, max_iters=20000, warm=True,
+                ilu_sweeps=0):
     """One fused solve, timed; with warm, an untimed solve of at most one
     cycle on the same system first (kernel modules load lazily on their
     first launch and the workspace pool grows on first use: one-time costs
     that are not the solve's)."""
     from high_precision_blas1_b200 import _lib
     if warm:
-        fused_solve(torch, A, b, method, basis, tol, precond, complex_, max_iters=max(basis, 1), warm=False)
+        fused_solve(torch, A, b, method, basis, tol, precond, complex_, max_iters=max(basis, 1), warm=False,
+                    ilu_sweeps=ilu_sweeps)
     dt = np.complex128 if complex_ else np.float64
     d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (A.row_ptr, A.col_ind, A.val.astype(dt),
                                                                     b.astype(dt), np.zeros(A.n, dtype=dt))]
-    p = _lib.solver_params(method, basis=basis, rel_tol=tol, max_iters=max_iters, precond=precond, fused=True)
+    p = _lib.solver_params(method, basis=basis, rel_tol=tol, max_iters=max_iters, precond=precond, fused=True,
+                           ilu_sweeps=ilu_sweeps)
     rep = _lib.hpb_solver_report()
     f = _lib.lib.hpb_csr_solve_c128 if complex_ else _lib.lib.hpb_csr_solve_f64
     t, st = _timed(torch, lambda: f(C.byref(p), A.n, A.nnz, *[a.data_ptr() for a in d], C.byref(rep), None, 0))
@@ -717,14 +720,17 @@ def bench_forms(torch, log=lambda *a: None):
         A = problems.convdiff2d(1024)
         b = problems.rhs_uniform(A.n, 606)
         res = {"kernels": ilu0_probe(torch, A)}
-        for pc in ("none", "jacobi", "ilu0"):
-            t, st, r, x = fused_solve(torch, A, b, "gmres", 30, SOLVER_TOL, precond=pc, max_iters=30000)
-            res[f"fp64_gmres30_{pc}"] = {"s": t, "status": st, "iters": r.iters, "true_rel_residual": _rel(A, b, x)}
+        for pc, sw in (("none", 0), ("jacobi", 0), ("ilu0", 0), ("ilu0", 2)):
+            t, st, r, x = fused_solve(torch, A, b, "gmres", 30, SOLVER_TOL, precond=pc, max_iters=30000, ilu_sweeps=sw)
+            res[f"fp64_gmres30_{pc}" + (f"_sweeps{sw}" if sw else "")] = {
+                "s": t, "status": st, "iters": r.iters, "true_rel_residual": _rel(A, b, x)}
         A5 = spai.family(96, seed=424242)
         b5 = problems.rhs_uniform(A5.n, 505)
-        t, st, r, x = fused_solve(torch, A5, b5, "gmres", 30, SOLVER_TOL, precond="ilu0", max_iters=30000)
-        res["lognormal96_fp64_gmres30_ilu0"] = {"s": t, "status": st, "iters": r.iters,
-                                                "true_rel_residual": _rel(A5, b5, x)}
+        for sw in (0, 2):
+            t, st, r, x = fused_solve(torch, A5, b5, "gmres", 30, SOLVER_TOL, precond="ilu0", max_iters=30000,
+                                      ilu_sweeps=sw)
+            res["lognormal96_fp64_gmres30_ilu0" + (f"_sweeps{sw}" if sw else "")] = {
+                "s": t, "status": st, "iters": r.iters, "true_rel_residual": _rel(A5, b5, x)}
         out["ilu0_convdiff1024"] = res
     except Exception as e:
         out["ilu0_convdiff1024"] = {"error": repr(e)}

@@ -145,6 +145,7 @@ _sig("hpb_csr_tri_check", C.c_int, [P, P])
 for t in TYPES:
     _sig(f"hpb_csr_trsv_{t}", C.c_int, [P, P, C.c_int, P, SCALAR[t], P, P])
     _sig(f"hpb_csr_ilu0_{t}", C.c_int, [P, P, P])
+    _sig(f"hpb_csr_trsv_sweeps_{t}", C.c_int, [P, P, C.c_int, P, SCALAR[t], P, P, C.c_int])
 _sig("hpb_gendot_f64", C.c_int, [C.c_uint64, I64, C.c_double, P, P, C.POINTER(C.c_int64)])
 _sig("hpb_gendot_c128", C.c_int, [C.c_uint64, I64, C.c_double, P, P])
 _sig("hpb_gendot_f64_dev", C.c_int, [P, C.c_uint64, I64, C.c_double, P, P, C.POINTER(C.c_int64)])
@@ -157,7 +158,7 @@ class hpb_solver_params(C.Structure):
     _fields_ = [("method", C.c_int), ("basis", C.c_int), ("rel_tol", C.c_double), ("abs_tol", C.c_double),
                 ("max_iters", C.c_int), ("precond", C.c_int), ("high_precision", C.c_int),
                 ("resid_recalc_freq", C.c_int), ("early_exit", C.c_int), ("reorthogonalize", C.c_int),
-                ("fused", C.c_int)]
+                ("fused", C.c_int), ("ilu_sweeps", C.c_int)]
 
 
 class hpb_solver_report(C.Structure):
@@ -226,7 +227,8 @@ def ir_params(inner="gmres", basis=50, inner_rel_tol=1e-5, inner_max_iters=5000,
 
 
 def solver_params(method="bicgstabl", basis=2, rel_tol=1e-10, abs_tol=0.0, max_iters=10000, precond="none",
-                  high_precision=True, resid_recalc_freq=0, early_exit=False, reorthogonalize=False, fused=False):
+                  high_precision=True, resid_recalc_freq=0, early_exit=False, reorthogonalize=False, fused=False,
+                  ilu_sweeps=0):
     p = hpb_solver_params()
     lib.hpb_solver_params_default(C.byref(p))
     p.method = SOLVER[method]
@@ -240,6 +242,7 @@ def solver_params(method="bicgstabl", basis=2, rel_tol=1e-10, abs_tol=0.0, max_i
     p.early_exit = 1 if early_exit else 0
     p.reorthogonalize = 1 if reorthogonalize else 0
     p.fused = 1 if fused else 0
+    p.ilu_sweeps = ilu_sweeps
     return p
 
 

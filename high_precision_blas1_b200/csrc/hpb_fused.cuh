@@ -334,6 +334,7 @@ struct RightPrec {
     const E* val = nullptr;                 // kind 2: M; kind 3: L\U on A's pattern
     const hpb_csr_tri* lower = nullptr;     // kind 3: analyses of A's triangles
     const hpb_csr_tri* upper = nullptr;
+    int sweeps = 0;                         // kind 3: 0 exact triangular solves, k > 0 Jacobi sweeps
 };
 
 // Device-resident GMRES(m) (hpb_fused_gmres.cu); E in {float, double, cf, cd}.

@@ -403,7 +403,7 @@ struct GmPlan<E>::Impl {
     E* x = nullptr;
     int g_ew = 1, g_md = 1, g_sp = 1, kernels = 0;
     SolverWorkspace ws;
-    E *V = nullptr, *W = nullptr, *Z = nullptr, *R = nullptr, *diag = nullptr;
+    E *V = nullptr, *W = nullptr, *Z = nullptr, *R = nullptr, *diag = nullptr, *T = nullptr;
     GmState<S>* st = nullptr;
     A* partials = nullptr;
     unsigned int* ticket = nullptr;
@@ -468,6 +468,8 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     E* Z = P.Z = M.kind ? static_cast<E*>(ws.alloc(vb)) : nullptr;
     E* R = P.R = static_cast<E*>(ws.alloc(vb));
     E* diag = P.diag = M.kind == 1 ? static_cast<E*>(ws.alloc(vb)) : nullptr;
+    P.T = (M.kind == 3 && M.sweeps > 0) ? static_cast<E*>(ws.alloc(vb)) : nullptr;
+    if (M.kind == 3 && M.sweeps > 0 && !P.T) return HPB_ERROR_OUT_OF_MEMORY;
     auto* st = P.st = static_cast<GmState<S>*>(ws.alloc(sizeof(GmState<S>)));
     const size_t np = std::max<size_t>(size_t(m + 1) * g_md, std::max<size_t>(g_ew, g_sp));
     auto* partials = P.partials = static_cast<A*>(ws.alloc(np * sizeof(A)));
@@ -503,11 +505,16 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
             k_gm_spmv<E><<<(M.rows + kGmThreads - 1) / kGmThreads, kGmThreads, 0, s>>>(M.rows, M.rp, M.ci, M.val, vi, Z);
             src = Z;
             ++kernels;
-        } else if (M.kind == 3) {  // z = U^-1 L^-1 v_i (R is free inside the cycle)
+        } else if (M.kind == 3 && M.sweeps == 0) {  // z = U^-1 L^-1 v_i (R is free inside the cycle)
             tri::launch_trsv<E>(M.lower->plan, 1, M.val, unit_of<E>(), vi, R, s);
             tri::launch_trsv<E>(M.upper->plan, 0, M.val, unit_of<E>(), R, Z, s);
             src = Z;
             kernels += 4;
+        } else if (M.kind == 3) {  // the same with Jacobi sweeps (T: ping-pong buffer)
+            tri::launch_trsv_sweeps<E>(M.lower->plan, 1, M.val, unit_of<E>(), vi, R, P.T, M.sweeps, s);
+            tri::launch_trsv_sweeps<E>(M.upper->plan, 0, M.val, unit_of<E>(), R, Z, P.T, M.sweeps, s);
+            src = Z;
+            kernels += 2 * (M.sweeps + 1);
         }
         k_gm_spmv<E><<<g_sp, kGmThreads, 0, s>>>(rows, rp, ci, val, src, W);
         k_multidot<E><<<g_md, kGmThreads, 0, s>>>(n, i + 1, V, W, partials);
@@ -536,10 +543,14 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
             k_gm_jacobi<E><<<g_ew, kGmThreads, 0, s>>>(n, W, diag, Z);
         } else if (M.kind == 2) {
             k_gm_spmv<E><<<(M.rows + kGmThreads - 1) / kGmThreads, kGmThreads, 0, s>>>(M.rows, M.rp, M.ci, M.val, W, Z);
-        } else {
+        } else if (M.sweeps == 0) {
             tri::launch_trsv<E>(M.lower->plan, 1, M.val, unit_of<E>(), W, R, s);
             tri::launch_trsv<E>(M.upper->plan, 0, M.val, unit_of<E>(), R, Z, s);
             kernels += 3;
+        } else {
+            tri::launch_trsv_sweeps<E>(M.lower->plan, 1, M.val, unit_of<E>(), W, R, P.T, M.sweeps, s);
+            tri::launch_trsv_sweeps<E>(M.upper->plan, 0, M.val, unit_of<E>(), R, Z, P.T, M.sweeps, s);
+            kernels += 2 * (M.sweeps + 1) - 1;
         }
         k_gm_axpy<E><<<g_ew, kGmThreads, 0, s>>>(n, x, Z);
         kernels += 3;

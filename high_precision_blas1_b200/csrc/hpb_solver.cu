@@ -138,6 +138,7 @@ int solve_device(const hpb_solver_params* p, int32_t rows, int64_t nnz, const in
                 M.val = F.lu;
                 M.lower = F.lower;
                 M.upper = F.upper;
+                M.sweeps = p->ilu_sweeps;
             } else if (p->precond != HPB_PRECOND_NONE) {
                 return HPB_ERROR_NOT_SUPPORTED;
             }
@@ -163,6 +164,7 @@ int solve_device(const hpb_solver_params* p, int32_t rows, int64_t nnz, const in
             jac->jac.reset(new typename S::PJ(&ops));
             jac->jac->set_matrix(&A);
         } else if (p->precond == HPB_PRECOND_ILU0) {
+            if (p->ilu_sweeps != 0) return HPB_ERROR_NOT_SUPPORTED;  // the drop-in applies the factors exactly
             jac.reset(new AnyPrec<S>);
             jac->ilu.reset(new typename S::PI(&ops));
             jac->ilu->set_matrix(A);

@@ -790,6 +790,44 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int4* __r
     if (L > 0 && warp == L % W) level_sync(L - 1);
 }
 
+// ---- approximate solves: Jacobi sweeps ------------------------------------
+// x_{k+1} = D^-1 (alpha b - (T - D) x_k), x_0 = 0 (so the first pass forms
+// D^-1 alpha b; D = I for a unit diagonal): one pass per kernel, one thread
+// per row over the row's triangle in index order.  Bandwidth-bound passes
+// instead of the exact solve's chain of levels; the result approaches
+// T^-1 alpha b as the sweeps grow (exact after as many sweeps as the
+// triangle's depth).
+template <class E, bool UPPER, bool UNIT, bool FIRST>
+__global__ void __launch_bounds__(256)
+k_tri_sweep(int32_t n, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
+            const int32_t* __restrict__ dpos, const E* __restrict__ val, E alpha, const E* __restrict__ b,
+            const E* __restrict__ xin, E* __restrict__ xout) {
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        E acc = scale(alpha, ldE(b, i));
+        const int32_t dp = __ldg(dpos + i);
+        if (!FIRST) {
+            const int32_t b0 = __ldg(rp + i), b1 = __ldg(rp + i + 1);
+            int32_t e0, e1;
+            if (dp >= 0) {
+                e0 = UPPER ? dp + 1 : b0;
+                e1 = UPPER ? b1 : dp;
+            } else {  // no stored diagonal (unit solves only): locate the triangle by column
+                e0 = b0;
+                while (e0 < b1 && __ldg(ci + e0) < i) ++e0;
+                if (UPPER) {
+                    e1 = b1;
+                } else {
+                    e1 = e0;
+                    e0 = b0;
+                }
+            }
+            for (int32_t e = e0; e < e1; ++e) acc = fms(acc, ldE(val, e), ldE(xin, __ldg(ci + e)));
+        }
+        if (!UNIT) acc = quot(acc, ldE(val, dp));
+        stE(xout, i, acc);
+    }
+}
+
 // ---- ILU(0) ---------------------------------------------------------------
 // Row i, for each strictly lower entry k (ascending): l_ik = a_ik / u_kk,
 // then a_ij -= l_ik u_kj for every j > k present in both rows (the IKJ
@@ -1037,6 +1075,29 @@ cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E*
     return cudaGetLastError();
 }
 
+template <class E, bool UPPER, bool UNIT>
+cudaError_t sweeps_t(const Plan& P, const E* val, E alpha, const E* b, E* x, E* tmp, int sweeps, cudaStream_t s) {
+    const int grid = int(std::min<int64_t>((int64_t(P.n) + 255) / 256, 148 * 8));
+    const int K = sweeps + 1;  // kernels; the last one writes x
+    auto dst = [&](int t) { return ((K - 1 - t) % 2 == 0) ? x : tmp; };
+    k_tri_sweep<E, UPPER, UNIT, true><<<grid, 256, 0, s>>>(P.n, P.rp, P.ci, P.dpos, val, alpha, b, nullptr, dst(0));
+    for (int t = 1; t < K; ++t)
+        k_tri_sweep<E, UPPER, UNIT, false><<<grid, 256, 0, s>>>(P.n, P.rp, P.ci, P.dpos, val, alpha, b, dst(t - 1),
+                                                                dst(t));
+    count_launch(uint64_t(K));
+    return cudaGetLastError();
+}
+
+template <class E>
+cudaError_t launch_trsv_sweeps(const Plan& P, int unit, const E* val, E alpha, const E* b, E* x, E* tmp, int sweeps,
+                               cudaStream_t s) {
+    if (P.n == 0) return cudaSuccess;
+    if (P.upper) return unit ? sweeps_t<E, true, true>(P, val, alpha, b, x, tmp, sweeps, s)
+                             : sweeps_t<E, true, false>(P, val, alpha, b, x, tmp, sweeps, s);
+    return unit ? sweeps_t<E, false, true>(P, val, alpha, b, x, tmp, sweeps, s)
+                : sweeps_t<E, false, false>(P, val, alpha, b, x, tmp, sweeps, s);
+}
+
 template <class E>
 cudaError_t launch_ilu0(const Plan& P, E* val, cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
@@ -1053,6 +1114,12 @@ template cudaError_t launch_trsv<double>(const Plan&, int, const double*, double
                                          cudaStream_t);
 template cudaError_t launch_trsv<cf>(const Plan&, int, const cf*, cf, const cf*, cf*, cudaStream_t);
 template cudaError_t launch_trsv<cd>(const Plan&, int, const cd*, cd, const cd*, cd*, cudaStream_t);
+template cudaError_t launch_trsv_sweeps<float>(const Plan&, int, const float*, float, const float*, float*, float*,
+                                               int, cudaStream_t);
+template cudaError_t launch_trsv_sweeps<double>(const Plan&, int, const double*, double, const double*, double*,
+                                                double*, int, cudaStream_t);
+template cudaError_t launch_trsv_sweeps<cf>(const Plan&, int, const cf*, cf, const cf*, cf*, cf*, int, cudaStream_t);
+template cudaError_t launch_trsv_sweeps<cd>(const Plan&, int, const cd*, cd, const cd*, cd*, cd*, int, cudaStream_t);
 template cudaError_t launch_ilu0<float>(const Plan&, float*, cudaStream_t);
 template cudaError_t launch_ilu0<double>(const Plan&, double*, cudaStream_t);
 template cudaError_t launch_ilu0<cf>(const Plan&, cf*, cudaStream_t);
@@ -1096,6 +1163,37 @@ int trsv_impl(hpb_context* ctx, const hpb_csr_tri* tri, int unit, const E* val, 
         return HPB_SUCCESS;
     }
     HPB_CUDA_TRY(ctx, tri::launch_trsv<E>(P, unit, val, alpha, b, x, ctx->stream));
+    return HPB_SUCCESS;
+}
+
+template <class E>
+int sweeps_impl(hpb_context* ctx, const hpb_csr_tri* tri, int unit, const E* val, E alpha, const E* b, E* x,
+                int sweeps, const char* name) {
+    HPB_CHECK_CTX(ctx);
+    if (tri == nullptr) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null analysis", name);
+    const tri::Plan& P = tri->plan;
+    if (sweeps < 0) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: negative sweep count", name);
+    if (P.n == 0) return HPB_SUCCESS;
+    if (val == nullptr || b == nullptr || x == nullptr)
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null pointer", name);
+    constexpr size_t kA = sizeof(typename real_of<E>::type);
+    if (!aligned(val, kA) || !aligned(b, kA) || !aligned(x, kA))
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: pointer not aligned to its element type", name);
+    if (!unit && !P.all_diag)
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: a row stores no diagonal entry (structural zero)", name);
+    const size_t bytes = size_t(P.n) * sizeof(E);
+    const char* bb = reinterpret_cast<const char*>(b);
+    const char* xb = reinterpret_cast<const char*>(x);
+    if (bb < xb + bytes && xb < bb + bytes)
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: b and x must not overlap", name);
+    tri::Plan& Pm = const_cast<tri::Plan&>(P);
+    if (Pm.scratch == nullptr && cudaMalloc(&Pm.scratch, size_t(P.n) * 16) != cudaSuccess) {
+        cudaGetLastError();
+        Pm.scratch = nullptr;
+        return set_error(ctx, HPB_ERROR_OUT_OF_MEMORY, "%s: scratch allocation failed", name);
+    }
+    HPB_CUDA_TRY(ctx, tri::launch_trsv_sweeps<E>(P, unit, val, alpha, b, x, static_cast<E*>(Pm.scratch), sweeps,
+                                                 ctx->stream));
     return HPB_SUCCESS;
 }
 
@@ -1204,6 +1302,25 @@ int hpb_csr_trsv_c128(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, c
                       const void* b, void* x) {
     return hpb::trsv_impl<cd>(ctx, tri, unit_diag, static_cast<const cd*>(val), cd{alpha.re, alpha.im},
                               static_cast<const cd*>(b), static_cast<cd*>(x), "hpb_csr_trsv_c128");
+}
+
+int hpb_csr_trsv_sweeps_f32(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const float* val, float alpha,
+                            const float* b, float* x, int sweeps) {
+    return hpb::sweeps_impl<float>(ctx, tri, unit_diag, val, alpha, b, x, sweeps, "hpb_csr_trsv_sweeps_f32");
+}
+int hpb_csr_trsv_sweeps_f64(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const double* val,
+                            double alpha, const double* b, double* x, int sweeps) {
+    return hpb::sweeps_impl<double>(ctx, tri, unit_diag, val, alpha, b, x, sweeps, "hpb_csr_trsv_sweeps_f64");
+}
+int hpb_csr_trsv_sweeps_c64(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const void* val, hpb_c64 alpha,
+                            const void* b, void* x, int sweeps) {
+    return hpb::sweeps_impl<cf>(ctx, tri, unit_diag, static_cast<const cf*>(val), cf{alpha.re, alpha.im},
+                                static_cast<const cf*>(b), static_cast<cf*>(x), sweeps, "hpb_csr_trsv_sweeps_c64");
+}
+int hpb_csr_trsv_sweeps_c128(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const void* val,
+                             hpb_c128 alpha, const void* b, void* x, int sweeps) {
+    return hpb::sweeps_impl<cd>(ctx, tri, unit_diag, static_cast<const cd*>(val), cd{alpha.re, alpha.im},
+                                static_cast<const cd*>(b), static_cast<cd*>(x), sweeps, "hpb_csr_trsv_sweeps_c128");
 }
 
 int hpb_csr_ilu0_f32(hpb_context* ctx, const hpb_csr_tri* lower, float* val) {

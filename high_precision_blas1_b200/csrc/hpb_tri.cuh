@@ -71,6 +71,13 @@ void release(Plan* P);
 template <class E>
 cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E* b, E* x, cudaStream_t s);
 
+// Approximate x ~ T^-1 (alpha b) by Jacobi sweeps (x_0 = 0, then `sweeps`
+// passes x_{k+1} = D^-1 (alpha b - (T - D) x_k)); tmp: n elements; b must
+// not overlap x or tmp.  sweeps + 1 launches, graph-capturable.
+template <class E>
+cudaError_t launch_trsv_sweeps(const Plan& P, int unit, const E* val, E alpha, const E* b, E* x, E* tmp, int sweeps,
+                               cudaStream_t s);
+
 // ILU(0) in place on val (lower plan): val := L\U with L unit lower
 // (strictly lower entries stored) and U upper (diagonal included).
 template <class E>

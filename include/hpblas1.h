@@ -355,6 +355,20 @@ int hpb_csr_trsv_c64(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, co
                      const void* b, void* x);
 int hpb_csr_trsv_c128(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const void* val, hpb_c128 alpha,
                       const void* b, void* x);
+/* Approximate solve by Jacobi sweeps (no counterpart in the reference):
+ * x_0 = 0, then `sweeps` passes x_{k+1} = D^-1 (alpha b - (T - D) x_k)
+ * (D = I for a unit diagonal) -- bandwidth-bound row passes instead of the
+ * exact solve's chain of dependent levels; approaches T^-1 (alpha b) as the
+ * sweeps grow.  b must not overlap x; the analysis allocates an n-element
+ * scratch on the first call. */
+int hpb_csr_trsv_sweeps_f32(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const float* val, float alpha,
+                            const float* b, float* x, int sweeps);
+int hpb_csr_trsv_sweeps_f64(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const double* val,
+                            double alpha, const double* b, double* x, int sweeps);
+int hpb_csr_trsv_sweeps_c64(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const void* val, hpb_c64 alpha,
+                            const void* b, void* x, int sweeps);
+int hpb_csr_trsv_sweeps_c128(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const void* val,
+                             hpb_c128 alpha, const void* b, void* x, int sweeps);
 /* Blocking: HPB_ERROR_TIMEOUT if a bounded device-side wait of an earlier
  * solve with this analysis gave up (cannot happen for a valid analysis). */
 int hpb_csr_tri_check(hpb_context* ctx, const hpb_csr_tri* tri);
@@ -433,6 +447,10 @@ typedef struct hpb_solver_params {
                                on the GPU, right Jacobi or none; the monitor tests the
                                compensated true residual once per restart).
                                0: the drop-in path. */
+    int ilu_sweeps;         /* HPB_PRECOND_ILU0 in the fused GMRES: 0 applies the factors
+                               by exact triangular solves (csrsv2's result); k > 0 by k
+                               Jacobi sweeps per factor (approximate, bandwidth-bound;
+                               see hpb_csr_trsv_sweeps_*).  The drop-in path supports 0. */
 } hpb_solver_params;
 
 typedef struct hpb_solver_report {

@@ -68,6 +68,9 @@ def oro():
             f = getattr(lib, "oro_csr_ilu0_" + suf)
             f.argtypes = [C.c_int32, P, P, P]
             f.restype = C.c_int32
+            f = getattr(lib, "oro_csr_trsv_sweeps_" + suf)
+            f.argtypes = [C.c_int32, P, P, P, C.c_int, C.c_int, P, P, C.c_int, P, P]
+            f.restype = C.c_int
         _ORO = lib
     return _ORO
 
@@ -299,3 +302,20 @@ def gendot_dev(seed: int, n: int, cond: float):
     y = np.zeros(n)
     nfix = oro().oro_gendot_dev_f64(seed, n, cond, _ptr(x), _ptr(y))
     return x, y, int(nfix)
+
+
+def csr_trsv_sweeps(row_ptr, col_ind, val, b, upper: bool, unit: bool, sweeps: int, alpha=1.0) -> np.ndarray:
+    """Jacobi-sweep approximation of T^-1 (alpha b) (oracle/tri.c)."""
+    suf = _TRI_SUFFIX[val.dtype]
+    rp = np.ascontiguousarray(row_ptr, dtype=np.int32)
+    ci = np.ascontiguousarray(col_ind, dtype=np.int32)
+    v = np.ascontiguousarray(val)
+    bb = np.ascontiguousarray(b, dtype=val.dtype)
+    x = np.zeros_like(bb)
+    tmp = np.zeros_like(bb)
+    a = np.array([alpha], dtype=val.dtype)
+    st = getattr(oro(), "oro_csr_trsv_sweeps_" + suf)(len(rp) - 1, _ptr(rp), _ptr(ci), _ptr(v), int(upper),
+                                                      int(unit), _ptr(a), _ptr(bb), int(sweeps), _ptr(x), _ptr(tmp))
+    if st != 0:
+        raise ValueError("a row stores no diagonal")
+    return x

@@ -107,6 +107,30 @@ static int32_t diag_pos(const int32_t *rp, const int32_t *ci, int32_t i) {
         }                                                                                                \
         return 0;                                                                                        \
     }                                                                                                    \
+    /* Jacobi sweeps: x_0 = 0, x_{k+1} = D^-1 (alpha b - (T - D) x_k), each row over its triangle   \
+     * in index order; xprev: n scratch elements.  Returns 0, or -1 for a missing diagonal. */       \
+    int oro_csr_trsv_sweeps_##SUF(int32_t n, const int32_t *rp, const int32_t *ci, const T *val,       \
+                                  int upper, int unit, const T *alpha, const T *b, int sweeps, T *x,   \
+                                  T *xprev) {                                                          \
+        for (int k = 0; k <= sweeps; ++k) {                                                             \
+            for (int32_t i = 0; i < n; ++i) xprev[i] = x[i];                                           \
+            for (int32_t i = 0; i < n; ++i) {                                                          \
+                T acc = MUL(*alpha, b[i]);                                                              \
+                int32_t dp = -1;                                                                        \
+                for (int32_t e = rp[i]; e < rp[i + 1]; ++e) {                                           \
+                    const int32_t j = ci[e];                                                            \
+                    if (j == i) dp = e;                                                                 \
+                    if (k > 0 && (upper ? j > i : j < i)) acc = FMS(acc, val[e], xprev[j]);             \
+                }                                                                                       \
+                if (!unit) {                                                                            \
+                    if (dp < 0) return -1;                                                              \
+                    acc = DIV(acc, val[dp]);                                                            \
+                }                                                                                       \
+                x[i] = acc;                                                                             \
+            }                                                                                           \
+        }                                                                                               \
+        return 0;                                                                                       \
+    }                                                                                                   \
     int32_t oro_csr_ilu0_##SUF(int32_t n, const int32_t *rp, const int32_t *ci, T *val) {                \
         int32_t first_zero = -1;                                                                         \
         for (int32_t i = 0; i < n; ++i)                                                                  \

@@ -180,3 +180,25 @@ def test_fused_gmres_ilu0(gpu, t):
         assert true_rel(A, b, x) <= (1.05 if tol == 1e-10 else 20) * tol
         its[precond] = rep.iters
     assert its["ilu0"] < its["jacobi"], its
+
+
+@pytest.mark.parametrize("t", ["f64", "f32"])
+def test_fused_gmres_ilu0_sweeps(gpu, t):
+    """ILU(0) factors applied by Jacobi sweeps (ilu_sweeps = 2) inside the
+    fused GMRES: converges on the true residual, with fewer iterations than
+    Jacobi; the drop-in path refuses the option (it applies factors exactly)."""
+    ctx, torch = gpu
+    A = problems.convdiff2d(96)
+    b = problems.rhs_uniform(A.n, 8)
+    tol = 1e-10 if t == "f64" else 1e-6
+    pj = _lib.solver_params("gmres", basis=30, rel_tol=tol, max_iters=100000, precond="jacobi", fused=True)
+    st, rj, x, _ = solve(torch, t, A, b, pj)
+    assert st == 0
+    ps = _lib.solver_params("gmres", basis=30, rel_tol=tol, max_iters=100000, precond="ilu0", fused=True,
+                            ilu_sweeps=2)
+    st, rs, x, _ = solve(torch, t, A, b, ps)
+    assert st == 0 and rs.iters < rj.iters, (rs.iters, rj.iters)
+    assert true_rel(A, b, x) <= (1.05 if tol == 1e-10 else 20) * tol
+    pd = _lib.solver_params("gmres", basis=30, rel_tol=tol, max_iters=100, precond="ilu0", ilu_sweeps=2)
+    st, _, _, _ = solve(torch, t, A, b, pd)
+    assert st == -4

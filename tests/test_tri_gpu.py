@@ -244,3 +244,52 @@ def test_errors(gpu):
     e = C.c_void_p()
     assert _lib.lib.hpb_csr_tri_create(ctx.h, 0, 0, 0, None, None, C.byref(e)) == 0
     assert _lib.lib.hpb_csr_tri_destroy(e) == 0
+
+
+def sweeps(ctx, torch, tri, t, val_d, b, unit, k, alpha=1.0):
+    bd = dev(torch, b.astype(DT[t]))
+    xd = torch.zeros_like(bd)
+    st = getattr(_lib.lib, f"hpb_csr_trsv_sweeps_{t}")(ctx.h, tri.h, int(unit), val_d.data_ptr(),
+                                                       _lib.scalar(t, alpha), bd.data_ptr(), xd.data_ptr(), k)
+    ctx.check(st, "trsv_sweeps")
+    torch.cuda.synchronize()
+    return host(xd)
+
+
+@pytest.mark.parametrize("name", ["convdiff64", "poisson3d_32", "banded_ragged", "diag_only"])
+@pytest.mark.parametrize("t", ["f64", "f32", "c128", "c64"])
+def test_sweeps_bitwise(gpu, name, t):
+    """Jacobi-sweep approximation of the triangular solves: bit for bit the
+    CPU restatement for 0, 1 and 3 sweeps, both triangles, unit and not."""
+    ctx, torch = gpu
+    rng = np.random.default_rng(21)
+    A, val = typed(problem(name, rng), t, rng)
+    vd = dev(torch, val)
+    b = (rng.standard_normal(A.n) + (1j * rng.standard_normal(A.n) if t.startswith("c") else 0)).astype(DT[t])
+    for upper in (False, True):
+        tri = Tri(ctx, torch, A, upper)
+        try:
+            for unit in (True, False):
+                for k in (0, 1, 3):
+                    got = sweeps(ctx, torch, tri, t, vd, b, unit, k, alpha=-0.5)
+                    want = oracle.csr_trsv_sweeps(A.row_ptr, A.col_ind, val, b, upper, unit, k, alpha=-0.5)
+                    assert np.array_equal(got, want), (name, t, upper, unit, k)
+        finally:
+            tri.close()
+
+
+def test_sweeps_reach_the_exact_solve(gpu):
+    """A triangle's Jacobi iteration is exact after as many sweeps as its
+    longest dependency chain: then every row is formed from exact values in
+    the same order as forward / backward substitution, bit for bit."""
+    ctx, torch = gpu
+    rng = np.random.default_rng(2)
+    A, val = typed(problems.convdiff2d(8), "f64", rng)  # longest chain: 14 steps
+    vd = dev(torch, val)
+    b = rng.standard_normal(A.n)
+    for upper in (False, True):
+        tri = Tri(ctx, torch, A, upper)
+        exact = trsv(ctx, torch, tri, "f64", vd, b, unit=not upper)
+        assert not np.array_equal(sweeps(ctx, torch, tri, "f64", vd, b, not upper, 3), exact)
+        assert np.array_equal(sweeps(ctx, torch, tri, "f64", vd, b, not upper, 15), exact)
+        tri.close()
