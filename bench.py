@@ -608,17 +608,18 @@ def plain_solve(torch, A, b, method, basis, tol, precond="none", max_iters=20000
 
 
 def ir_solve(torch, A, b, inner, basis, precond="none", M=None, complex_=False, inner_tol=1e-5, max_iters=5000,
-             max_refinements=40, warm=True):
+             max_refinements=40, warm=True, ilu_sweeps=0):
     """One refinement solve, timed; with warm, an untimed single-refinement
     run on the same system first (as in fused_solve)."""
     from high_precision_blas1_b200 import _lib
     if warm:
-        ir_solve(torch, A, b, inner, basis, precond, M, complex_, inner_tol, max_iters, max_refinements=1, warm=False)
+        ir_solve(torch, A, b, inner, basis, precond, M, complex_, inner_tol, max_iters, max_refinements=1, warm=False,
+                 ilu_sweeps=ilu_sweeps)
     dt = np.complex128 if complex_ else np.float64
     d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (A.row_ptr, A.col_ind, A.val.astype(dt),
                                                                     b.astype(dt), np.zeros(A.n, dtype=dt))]
     p = _lib.ir_params(inner, basis=basis, inner_rel_tol=inner_tol, inner_max_iters=max_iters, precond=precond,
-                       rel_tol=SOLVER_TOL, max_refinements=max_refinements)
+                       rel_tol=SOLVER_TOL, max_refinements=max_refinements, ilu_sweeps=ilu_sweeps)
     rep = _lib.hpb_ir_report()
     mp = [None, None, None, 0] if M is None else [d[0].data_ptr(), d[1].data_ptr(), M.data_ptr(), A.nnz]
     f = _lib.lib.hpb_ir_solve_c128 if complex_ else _lib.lib.hpb_ir_solve_f64
@@ -689,11 +690,13 @@ def bench_forms(torch, log=lambda *a: None):
         tpd, stpd, rpd, xpd = plain_solve(torch, A, b, "gmres", 30, SOLVER_TOL, precond="jacobi", max_iters=30000)
         res["plain_dropin_fp64_gmres30_jacobi"] = {"s": tpd, "status": stpd, "iters": rpd.iters,
                                                    "true_rel_residual": _rel(A, b, xpd)}
-        for pc in ("none", "jacobi"):  # one binary32 GMRES(30) cycle per refinement, same 30000-iteration budget
+        # one binary32 GMRES(30) cycle per refinement, same 30000-iteration budget
+        for pc, sw in (("none", 0), ("jacobi", 0), ("ilu0", 2)):
             t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond=pc, inner_tol=0.0, max_iters=0,
-                                   max_refinements=1000)
-            res[f"fp32_dot2_gmres30_refined_{pc}"] = {"s": t, "status": st, "inner_iters": r.inner_iters,
-                                                      "refinements": r.refinements, "true_rel_residual": _rel(A, b, x)}
+                                   max_refinements=1000, ilu_sweeps=sw)
+            res[f"fp32_dot2_gmres30_refined_{pc}" + (f"_sweeps{sw}" if sw else "")] = {
+                "s": t, "status": st, "inner_iters": r.inner_iters, "refinements": r.refinements,
+                "true_rel_residual": _rel(A, b, x)}
         wfile = spai.WEIGHTS_FILE
         if wfile.exists():
             offs, dslot = spai.stencil7(96)

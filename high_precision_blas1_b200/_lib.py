@@ -174,7 +174,7 @@ PRECOND = {"none": 0, "jacobi": 1, "matrix": 2, "ilu0": 3}
 class hpb_ir_params(C.Structure):
     _fields_ = [("inner_method", C.c_int), ("inner_basis", C.c_int), ("inner_rel_tol", C.c_double),
                 ("inner_max_iters", C.c_int), ("precond", C.c_int), ("rel_tol", C.c_double),
-                ("max_refinements", C.c_int)]
+                ("max_refinements", C.c_int), ("ilu_sweeps", C.c_int)]
 
 
 class hpb_ir_report(C.Structure):
@@ -213,7 +213,7 @@ _sig("hpb_spai_adam", C.c_int, [P, C.c_float, C.c_float])
 
 
 def ir_params(inner="gmres", basis=50, inner_rel_tol=1e-5, inner_max_iters=5000, precond="none", rel_tol=1e-10,
-              max_refinements=30):
+              max_refinements=30, ilu_sweeps=0):
     p = hpb_ir_params()
     lib.hpb_ir_params_default(C.byref(p))
     p.inner_method = SOLVER[inner]
@@ -223,6 +223,7 @@ def ir_params(inner="gmres", basis=50, inner_rel_tol=1e-5, inner_max_iters=5000,
     p.precond = PRECOND[precond]
     p.rel_tol = rel_tol
     p.max_refinements = max_refinements
+    p.ilu_sweeps = ilu_sweeps
     return p
 
 

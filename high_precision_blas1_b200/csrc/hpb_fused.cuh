@@ -14,6 +14,7 @@
 #include "hpb_tri.cuh"
 
 #include <memory>
+#include <type_traits>
 #include <vector>
 
 namespace hpb {
@@ -375,6 +376,46 @@ struct BcgPlan {
 template <class E>
 int solve_bicgstabl(const hpb_solver_params* p, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
                     const E* val, const E* b, E* x, hpb_solver_report* rep, double* hist, int cap);
+
+// ILU(0) factors of A for the fused GMRES (and the binary32 inner GMRES of
+// iterative refinement): a copy of the values (from the
+// solvers' memory pool) factored in place, and the analyses of both
+// triangles; released when the solve returns.
+template <class E>
+struct IluFactors {
+    hpb_context* ctx = nullptr;
+    hpb_csr_tri* lower = nullptr;
+    hpb_csr_tri* upper = nullptr;
+    E* lu = nullptr;
+    int build(int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci, const E* val) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || hpb_create(&ctx, dev, nullptr) != HPB_SUCCESS)
+            return HPB_ERROR_CUDA;
+        lu = static_cast<E*>(pool_alloc(size_t(nnz ? nnz : 1) * sizeof(E), nullptr));
+        if (lu == nullptr) return HPB_ERROR_OUT_OF_MEMORY;
+        if (cudaMemcpyAsync(lu, val, size_t(nnz) * sizeof(E), cudaMemcpyDeviceToDevice, nullptr) != cudaSuccess)
+            return HPB_ERROR_CUDA;
+        int st = hpb_csr_tri_create(ctx, 0, rows, nnz, rp, ci, &lower);
+        if (st == HPB_SUCCESS) st = hpb_csr_tri_create(ctx, 1, rows, nnz, rp, ci, &upper);
+        if (st != HPB_SUCCESS) return st;
+        if (std::is_same<E, float>::value)
+            st = hpb_csr_ilu0_f32(ctx, lower, reinterpret_cast<float*>(lu));
+        else if (std::is_same<E, double>::value)
+            st = hpb_csr_ilu0_f64(ctx, lower, reinterpret_cast<double*>(lu));
+        else if (std::is_same<E, cf>::value)
+            st = hpb_csr_ilu0_c64(ctx, lower, lu);
+        else
+            st = hpb_csr_ilu0_c128(ctx, lower, lu);
+        return st;
+    }
+    ~IluFactors() {
+        hpb_csr_tri_destroy(lower);
+        hpb_csr_tri_destroy(upper);
+        if (lu) pool_free(lu, nullptr);
+        if (ctx) hpb_destroy(ctx);
+        cudaStreamSynchronize(nullptr);
+    }
+};
 
 }  // namespace fused
 }  // namespace hpb

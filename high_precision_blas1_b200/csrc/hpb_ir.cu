@@ -101,7 +101,8 @@ int ir_solve(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* r
         return HPB_SUCCESS;
     }
     if (p->precond == HPB_PRECOND_MATRIX && (!m_rp || !m_ci || !m_val)) return HPB_ERROR_INVALID_VALUE;
-    if (p->precond == HPB_PRECOND_MATRIX && p->inner_method != HPB_SOLVER_GMRES) return HPB_ERROR_NOT_SUPPORTED;
+    if ((p->precond == HPB_PRECOND_MATRIX || p->precond == HPB_PRECOND_ILU0) && p->inner_method != HPB_SOLVER_GMRES)
+        return HPB_ERROR_NOT_SUPPORTED;
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
@@ -164,7 +165,17 @@ int ir_solve(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* r
     ip.high_precision = 1;
     ip.fused = 1;
     RightPrec<L> M;
+    IluFactors<L> F;  // ILU(0) of the binary32 matrix, for HPB_PRECOND_ILU0
     if (p->precond == HPB_PRECOND_JACOBI) M.kind = 1;
+    if (p->precond == HPB_PRECOND_ILU0) {
+        const int fst = F.build(rows, nnz, rp, ci, vlo);
+        if (fst != HPB_SUCCESS) return fst;
+        M.kind = 3;
+        M.val = F.lu;
+        M.lower = F.lower;
+        M.upper = F.upper;
+        M.sweeps = p->ilu_sweeps;
+    }
     if (p->precond == HPB_PRECOND_MATRIX) {
         M.kind = 2;
         M.rows = rows;

@@ -521,9 +521,11 @@ typedef struct hpb_ir_params {
     int inner_basis;        /* m of GMRES(m) / l of BiCGStab(l) */
     double inner_rel_tol;   /* residual reduction asked of each inner solve */
     int inner_max_iters;    /* per inner solve; 0: one GMRES cycle / 10000 */
-    int precond;            /* none, Jacobi, or HPB_PRECOND_MATRIX (GMRES only) */
+    int precond;            /* none, Jacobi, HPB_PRECOND_MATRIX or HPB_PRECOND_ILU0 (GMRES
+                               only; ILU(0) of the binary32 matrix) */
     double rel_tol;         /* stop when ||b - A x|| <= rel_tol ||b|| (compensated) */
     int max_refinements;
+    int ilu_sweeps;         /* HPB_PRECOND_ILU0: 0 exact triangular solves, k > 0 Jacobi sweeps */
 } hpb_ir_params;
 
 typedef struct hpb_ir_report {
