@@ -10,6 +10,7 @@
 // computed by one thread, over its entries in index order, whatever the
 // schedule.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <mutex>
 #include <vector>
@@ -1060,13 +1061,19 @@ cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E*
     const int fill_grid = int(std::min<int64_t>((int64_t(P.n) + 255) / 256, 148 * 8));
     k_tri_fill<E><<<fill_grid, 256, 0, s>>>(P.n, x, P.flags + P.n);
     constexpr size_t sm = trsv_smem<E>();
-    static std::once_flag once;
-    std::call_once(once, [&] {
+    // the shared-memory limit is a per-device function attribute: raise it
+    // once for every device this process launches on
+    static std::atomic<uint64_t> done_mask{0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return cudaErrorInvalidDevice;
+    const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
+    if (bit == 0 || !(done_mask.load(std::memory_order_acquire) & bit)) {
         allow_smem(k_trsv<E, false, false>, sm);
         allow_smem(k_trsv<E, false, true>, sm);
         allow_smem(k_trsv<E, true, false>, sm);
         allow_smem(k_trsv<E, true, true>, sm);
-    });
+        done_mask.fetch_or(bit, std::memory_order_release);
+    }
     auto k = P.upper ? (unit ? k_trsv<E, true, true> : k_trsv<E, true, false>)
                      : (unit ? k_trsv<E, false, true> : k_trsv<E, false, false>);
     k<<<P.ntiles, kTriThreads, sm, s>>>(P.n, P.ntiles, P.desc, P.dcol, P.dslot, P.hoff, P.hrow, P.lvlptr,
