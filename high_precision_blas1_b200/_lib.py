@@ -137,6 +137,10 @@ _sig("hpb_mm_read_csr", C.c_int, [C.c_char_p, C.POINTER(hpb_mm_csr)])
 _sig("hpb_mm_free", None, [C.POINTER(hpb_mm_csr)])
 _sig("hpb_mm_last_error", C.c_char_p, [])
 
+_sig("hpb_csr_transpose_pattern", C.c_int, [P, I32, I32, I64, P, P, P, P, P])
+for t in TYPES:
+    _sig(f"hpb_gather_{t}", C.c_int, [P, I64, P, P, P])
+
 # sparse triangular solves and ILU(0)
 _sig("hpb_csr_tri_create", C.c_int, [P, C.c_int, I32, I64, P, P, C.POINTER(P)])
 _sig("hpb_csr_tri_destroy", C.c_int, [P])

@@ -169,6 +169,172 @@ int diag_impl(hpb_context* ctx, int32_t rows, const int32_t* rp, const int32_t* 
     return check_launch(ctx, name);
 }
 
+// ------------------------------------------------------------- transpose
+// Pattern of A^T from A's CSR, deterministic: column counts (atomics on
+// integers), an exclusive scan, a scatter with per-column cursors, then each
+// row of A^T sorted by the entries' positions in A (unique keys, so the
+// order is the stable order: rows of A increasing, duplicates in their
+// order in A).  perm[k] = position in A of the k-th entry of A^T.
+// Entries with a column outside [0, cols) or rows whose pointers leave
+// [0, nnz] are skipped and reported through *bad (the caller gets an error).
+__global__ void k_tr_count(int32_t rows, int32_t cols, int64_t nnz, const int32_t* __restrict__ rp,
+                           const int32_t* __restrict__ ci, int32_t* __restrict__ cnt, int* bad) {
+    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        const int32_t b = rp[r], e = rp[r + 1];
+        if (b < 0 || e < b || int64_t(e) > nnz) {
+            atomicOr(bad, 1);
+            continue;
+        }
+        for (int32_t k = b; k < e; ++k) {
+            const int32_t c = ci[k];
+            if (c < 0 || c >= cols) {
+                atomicOr(bad, 1);
+                continue;
+            }
+            atomicAdd(cnt + c, 1);
+        }
+    }
+}
+
+// exclusive scan of cnt[0, m) into out[0, m], out[m] = total: per-block
+// scans of 1024 entries, block totals scanned by one block, offsets added
+constexpr int kScanBlock = 1024;
+__global__ void __launch_bounds__(kScanBlock)
+k_scan_local(int32_t m, const int32_t* __restrict__ cnt, int32_t* __restrict__ out, int32_t* __restrict__ bsum) {
+    __shared__ int32_t sh[kScanBlock];
+    const int32_t i = blockIdx.x * kScanBlock + threadIdx.x;
+    const int32_t v = i < m ? cnt[i] : 0;
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int d = 1; d < kScanBlock; d <<= 1) {  // inclusive Hillis-Steele scan
+        const int32_t t = threadIdx.x >= d ? sh[threadIdx.x - d] : 0;
+        __syncthreads();
+        sh[threadIdx.x] += t;
+        __syncthreads();
+    }
+    if (i < m) out[i] = sh[threadIdx.x] - v;
+    if (threadIdx.x == kScanBlock - 1) bsum[blockIdx.x] = sh[threadIdx.x];
+}
+__global__ void __launch_bounds__(kScanBlock) k_scan_sums(int32_t nb, int32_t* __restrict__ bsum, int32_t* total) {
+    if (threadIdx.x != 0) return;
+    int32_t acc = 0;
+    for (int32_t b = 0; b < nb; ++b) {
+        const int32_t v = bsum[b];
+        bsum[b] = acc;
+        acc += v;
+    }
+    *total = acc;
+}
+__global__ void k_scan_add(int32_t m, int32_t* __restrict__ out, const int32_t* __restrict__ bsum) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) out[i] += bsum[i / kScanBlock];
+}
+__global__ void k_tr_fill(int32_t rows, int32_t cols, int64_t nnz, const int32_t* __restrict__ rp,
+                          const int32_t* __restrict__ ci, int32_t* __restrict__ cursor, int32_t* __restrict__ ci_t,
+                          int32_t* __restrict__ perm) {
+    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        const int32_t b = rp[r], e = rp[r + 1];
+        if (b < 0 || e < b || int64_t(e) > nnz) continue;
+        for (int32_t k = b; k < e; ++k) {
+            const int32_t c = ci[k];
+            if (c < 0 || c >= cols) continue;
+            const int32_t pos = atomicAdd(cursor + c, 1);
+            ci_t[pos] = r;
+            perm[pos] = k;
+        }
+    }
+}
+// heap sort of one row of A^T by perm (keys unique), carrying ci_t
+__device__ void sift(int32_t* key, int32_t* val, int32_t root, int32_t len) {
+    for (;;) {
+        int32_t c = 2 * root + 1;
+        if (c >= len) return;
+        if (c + 1 < len && key[c + 1] > key[c]) ++c;
+        if (key[root] >= key[c]) return;
+        const int32_t tk = key[root], tv = val[root];
+        key[root] = key[c];
+        val[root] = val[c];
+        key[c] = tk;
+        val[c] = tv;
+        root = c;
+    }
+}
+__global__ void k_tr_sort(int32_t cols, const int32_t* __restrict__ rp_t, int32_t* __restrict__ ci_t,
+                          int32_t* __restrict__ perm) {
+    for (int32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cols; c += gridDim.x * blockDim.x) {
+        int32_t* key = perm + rp_t[c];
+        int32_t* val = ci_t + rp_t[c];
+        const int32_t len = rp_t[c + 1] - rp_t[c];
+        for (int32_t i = len / 2 - 1; i >= 0; --i) sift(key, val, i, len);
+        for (int32_t end = len - 1; end > 0; --end) {
+            const int32_t tk = key[0], tv = val[0];
+            key[0] = key[end];
+            val[0] = val[end];
+            key[end] = tk;
+            val[end] = tv;
+            sift(key, val, 0, end);
+        }
+    }
+}
+
+template <class E>
+__global__ void k_gather(int64_t n, const int32_t* __restrict__ idx, const E* __restrict__ src, E* __restrict__ dst) {
+    for (int64_t k = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; k < n; k += int64_t(gridDim.x) * blockDim.x)
+        stE(dst, k, ldE(src, idx[k]));
+}
+
+int transpose_pattern(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz, const int32_t* rp, const int32_t* ci,
+                      int32_t* rp_t, int32_t* ci_t, int32_t* perm) {
+    const char* name = "hpb_csr_transpose_pattern";
+    HPB_CHECK_CTX(ctx);
+    if (rows < 0 || cols < 0 || nnz < 0 || nnz > INT32_MAX)
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: invalid dimensions", name);
+    if (rp_t == nullptr || (rows > 0 && rp == nullptr) ||
+        (nnz > 0 && (ci == nullptr || ci_t == nullptr || perm == nullptr)))
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null pointer", name);
+    cudaStream_t s = ctx->stream;
+    const int32_t nb = (cols + kScanBlock - 1) / kScanBlock;
+    int32_t* work = nullptr;  // counts / cursors (cols), block sums (nb + 1), the error flag
+    HPB_CUDA_TRY(ctx, cudaMallocAsync(&work, (size_t(cols) + size_t(nb) + 3) * sizeof(int32_t), s));
+    int32_t* cnt = work;
+    int32_t* bsum = work + cols;
+    int* bad = reinterpret_cast<int*>(work + cols + nb + 2);
+    cudaMemsetAsync(cnt, 0, size_t(cols) * sizeof(int32_t), s);
+    cudaMemsetAsync(bad, 0, sizeof(int), s);
+    if (rows > 0) k_tr_count<<<grid_for(ctx, rows, 256, 8), 256, 0, s>>>(rows, cols, nnz, rp, ci, cnt, bad);
+    if (cols > 0) {
+        k_scan_local<<<nb, kScanBlock, 0, s>>>(cols, cnt, rp_t, bsum);
+        k_scan_sums<<<1, kScanBlock, 0, s>>>(nb, bsum, rp_t + cols);
+        k_scan_add<<<(cols + 255) / 256, 256, 0, s>>>(cols, rp_t, bsum);
+        cudaMemcpyAsync(cnt, rp_t, size_t(cols) * sizeof(int32_t), cudaMemcpyDeviceToDevice, s);  // cursors
+    } else {
+        cudaMemsetAsync(rp_t, 0, sizeof(int32_t), s);
+    }
+    if (rows > 0 && nnz > 0) {
+        k_tr_fill<<<grid_for(ctx, rows, 256, 8), 256, 0, s>>>(rows, cols, nnz, rp, ci, cnt, ci_t, perm);
+        if (cols > 0) k_tr_sort<<<grid_for(ctx, cols, 256, 8), 256, 0, s>>>(cols, rp_t, ci_t, perm);
+    }
+    count_launch(6);
+    int hbad = 0;
+    cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaFreeAsync(work, s);
+    HPB_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    if (hbad) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: row pointer or column index out of range", name);
+    return check_launch(ctx, name);
+}
+
+template <class E>
+int gather_impl(hpb_context* ctx, int64_t n, const int32_t* idx, const E* src, E* dst, const char* name) {
+    HPB_CHECK_CTX(ctx);
+    if (n < 0) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: negative n", name);
+    if (n == 0) return HPB_SUCCESS;
+    if (idx == nullptr || src == nullptr || dst == nullptr)
+        return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null pointer", name);
+    k_gather<E><<<grid_for(ctx, n, 256, 8), 256, 0, ctx->stream>>>(n, idx, src, dst);
+    count_launch();
+    return check_launch(ctx, name);
+}
+
 }  // namespace hpb
 
 using hpb::cd;
@@ -224,6 +390,23 @@ int hpb_csr_spmv_dot2_c128(hpb_context* ctx, int32_t rows, int32_t cols, int64_t
     return hpb::spmv_dot2_impl<cd>(ctx, rows, cols, nnz, row_ptr, col_ind, static_cast<const cd*>(val),
                                    static_cast<const cd*>(x), static_cast<cd*>(y), static_cast<const cd*>(w), out,
                                    "hpb_csr_spmv_dot2_c128");
+}
+
+int hpb_csr_transpose_pattern(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz, const int32_t* row_ptr,
+                              const int32_t* col_ind, int32_t* row_ptr_t, int32_t* col_ind_t, int32_t* perm) {
+    return hpb::transpose_pattern(ctx, rows, cols, nnz, row_ptr, col_ind, row_ptr_t, col_ind_t, perm);
+}
+int hpb_gather_f32(hpb_context* ctx, int64_t n, const int32_t* idx, const float* src, float* dst) {
+    return hpb::gather_impl<float>(ctx, n, idx, src, dst, "hpb_gather_f32");
+}
+int hpb_gather_f64(hpb_context* ctx, int64_t n, const int32_t* idx, const double* src, double* dst) {
+    return hpb::gather_impl<double>(ctx, n, idx, src, dst, "hpb_gather_f64");
+}
+int hpb_gather_c64(hpb_context* ctx, int64_t n, const int32_t* idx, const void* src, void* dst) {
+    return hpb::gather_impl<cf>(ctx, n, idx, static_cast<const cf*>(src), static_cast<cf*>(dst), "hpb_gather_c64");
+}
+int hpb_gather_c128(hpb_context* ctx, int64_t n, const int32_t* idx, const void* src, void* dst) {
+    return hpb::gather_impl<cd>(ctx, n, idx, static_cast<const cd*>(src), static_cast<cd*>(dst), "hpb_gather_c128");
 }
 
 int hpb_csr_diag_f32(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,

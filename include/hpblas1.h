@@ -305,6 +305,23 @@ int hpb_csr_spmv_dot2_c128(hpb_context* ctx, int32_t rows, int32_t cols, int64_t
                            const int32_t* row_ptr, const int32_t* col_ind, const void* val,
                            const void* x, void* y, const void* w, double* out);
 
+/* Pattern of A^T (cols x rows) from A's CSR (rows x cols), on the device,
+ * deterministic: row_ptr_t[cols + 1], col_ind_t[nnz] (row indices of A,
+ * increasing within each row of A^T; repeated (row, column) pairs in their
+ * order in A), perm[nnz] = position in A of each entry of A^T, so the
+ * values of A^T are val[perm[k]] (hpb_gather_*).  Blocking (one sync);
+ * HPB_ERROR_INVALID_VALUE if a row pointer or column index is out of range.
+ * With the gather, csr::gpu_matrix::axpy and the triangular solves take
+ * their transposed forms (the reference's transpose_ = true,
+ * common/csr/gpu_matrix.h:150-375, CUSPARSE_OPERATION_TRANSPOSE). */
+int hpb_csr_transpose_pattern(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz, const int32_t* row_ptr,
+                              const int32_t* col_ind, int32_t* row_ptr_t, int32_t* col_ind_t, int32_t* perm);
+/* dst[k] := src[idx[k]], k < n (stream-ordered). */
+int hpb_gather_f32(hpb_context* ctx, int64_t n, const int32_t* idx, const float* src, float* dst);
+int hpb_gather_f64(hpb_context* ctx, int64_t n, const int32_t* idx, const double* src, double* dst);
+int hpb_gather_c64(hpb_context* ctx, int64_t n, const int32_t* idx, const void* src, void* dst);
+int hpb_gather_c128(hpb_context* ctx, int64_t n, const int32_t* idx, const void* src, void* dst);
+
 /* diag[r] := A(r, r) (0 if row r stores no diagonal entry); used by the
  * Jacobi preconditioner (the diagonal scaling of linear_operator.hpp:59-91). */
 int hpb_csr_diag_f32(hpb_context* ctx, int32_t rows, const int32_t* row_ptr, const int32_t* col_ind,

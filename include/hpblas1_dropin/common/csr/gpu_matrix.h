@@ -16,8 +16,11 @@
 // 142-311, there cuSPARSE csrsv2 with an analysis and a cudaMalloc'd buffer
 // per call) run the library's level-scheduled kernel (hpb_csr_trsv_*); the
 // analysis of each triangle is made on the first solve and kept until the
-// matrix is set again or destroyed.  Transposed solves and the transposed
-// product report "not supported".
+// matrix is set again or destroyed.  The transposed product and solves
+// (transpose_ = true) run on A^T's pattern, built on the device once
+// (hpb_csr_transpose_pattern) and kept like the analyses; A^T's values are
+// gathered from A's on every transposed call, so in-place value changes are
+// seen.
 #ifndef __CSR__GPU_MATRIX_H__
 #define __CSR__GPU_MATRIX_H__
 
@@ -111,12 +114,18 @@ public:
         set(data_, col_ind_, row_ptr_);
     }
 
-    // y := alpha*A*x + beta*y
+    // y := alpha*op(A)*x + beta*y, op(A) = A or A^T
     void axpy(const T& alpha_, const T_vec& x_, const T& beta_, T_vec& y_, bool transpose_ = false) const {
-        if (transpose_) throw std::logic_error("csr::gpu_matrix::axpy: transposed product is not supported");
         if (!initialized) throw std::runtime_error("csr::gpu_matrix::axpy: matrix not set");
         dimensions_t d = get_dim();
         using A = hpb_dropin::abi<T>;
+        if (transpose_) {
+            const Transposed& t = transposed();
+            hpb_dropin::check(A::spmv(ctx, d.columns, d.rows, nnz, t.rp, t.ci, t.val, A::s(alpha_), x_, A::s(beta_),
+                                      y_),
+                              ctx, "csr::gpu_matrix::axpy");
+            return;
+        }
         hpb_dropin::check(A::spmv(ctx, d.rows, d.columns, nnz, row_ptr, col_ind, data, A::s(alpha_), x_, A::s(beta_),
                                   y_),
                           ctx, "csr::gpu_matrix::axpy");
@@ -182,12 +191,46 @@ private:
     hpb_context* ctx = nullptr;
     bool owns_ = true;
     mutable hpb_csr_tri* tri_[2] = {nullptr, nullptr};  // analyses of the lower / upper triangle
+    struct Transposed {
+        int32_t* rp = nullptr;    // pattern of A^T
+        int32_t* ci = nullptr;
+        int32_t* perm = nullptr;  // position in A of each entry of A^T
+        T* val = nullptr;         // values of A^T, gathered per transposed call
+        hpb_csr_tri* tri[2] = {nullptr, nullptr};
+    };
+    mutable Transposed tr_;
 
     void drop_analyses() {
         for (auto& t : tri_) {
             hpb_csr_tri_destroy(t);
             t = nullptr;
         }
+        for (auto& t : tr_.tri) {
+            hpb_csr_tri_destroy(t);
+            t = nullptr;
+        }
+        cudaFree(tr_.rp);
+        cudaFree(tr_.ci);
+        cudaFree(tr_.perm);
+        cudaFree(tr_.val);
+        tr_.rp = tr_.ci = tr_.perm = nullptr;
+        tr_.val = nullptr;
+    }
+    // A^T's pattern (built once) with A's current values gathered into it
+    const Transposed& transposed() const {
+        using A = hpb_dropin::abi<T>;
+        dimensions_t d = get_dim();
+        if (tr_.rp == nullptr) {
+            tr_.rp = static_cast<int32_t*>(dalloc(size_t(d.columns + 1) * sizeof(int32_t)));
+            tr_.ci = static_cast<int32_t*>(dalloc(size_t(nnz) * sizeof(int32_t)));
+            tr_.perm = static_cast<int32_t*>(dalloc(size_t(nnz) * sizeof(int32_t)));
+            tr_.val = static_cast<T*>(dalloc(size_t(nnz) * sizeof(T)));
+            hpb_dropin::check(hpb_csr_transpose_pattern(ctx, d.rows, d.columns, nnz, row_ptr, col_ind, tr_.rp, tr_.ci,
+                                                        tr_.perm),
+                              ctx, "csr::gpu_matrix: transpose");
+        }
+        hpb_dropin::check(A::gather(ctx, nnz, tr_.perm, data, tr_.val), ctx, "csr::gpu_matrix: transpose");
+        return tr_;
     }
     hpb_csr_tri* analysis(bool upper) const {
         hpb_csr_tri*& t = tri_[upper ? 1 : 0];
@@ -198,11 +241,22 @@ private:
     }
     void tri_solve(bool upper, bool unit, const T_vec& b_, T_vec& x_, const T& alpha_, bool transpose_,
                    const char* what) const {
-        if (transpose_) throw std::logic_error(std::string(what) + ": transposed solve is not supported");
         if (!initialized) throw std::runtime_error(std::string(what) + ": matrix not set");
         using A = hpb_dropin::abi<T>;
-        hpb_csr_tri* t = analysis(upper);
-        hpb_dropin::check(A::trsv(ctx, t, unit ? 1 : 0, data, A::s(alpha_), b_, x_), ctx, what);
+        hpb_csr_tri* t = nullptr;
+        const T* vals = data;
+        if (transpose_) {  // the transpose of a lower triangle is the upper triangle of A^T and vice versa
+            const Transposed& tt = transposed();
+            hpb_csr_tri*& slot = tr_.tri[upper ? 0 : 1];
+            if (slot == nullptr)
+                hpb_dropin::check(hpb_csr_tri_create(ctx, upper ? 0 : 1, get_dim().columns, nnz, tt.rp, tt.ci, &slot),
+                                  ctx, "csr::gpu_matrix: triangular analysis");
+            t = slot;
+            vals = tt.val;
+        } else {
+            t = analysis(upper);
+        }
+        hpb_dropin::check(A::trsv(ctx, t, unit ? 1 : 0, vals, A::s(alpha_), b_, x_), ctx, what);
         // blocking, like the reference's call (its cudaFree of the work buffer
         // synchronises); also reports a solve whose bounded waits gave up
         hpb_dropin::check(hpb_csr_tri_check(ctx, t), ctx, what);

@@ -134,6 +134,9 @@ template <class T> struct abi;
             return hpb_csr_trsv_##SUF(c, t, unit, v, a, b, x);                                            \
         }                                                                                                 \
         static int ilu0(hpb_context* c, const hpb_csr_tri* t, T* v) { return hpb_csr_ilu0_##SUF(c, t, v); } \
+        static int gather(hpb_context* c, int64_t n, const int32_t* idx, const T* src, T* dst) {          \
+            return hpb_gather_##SUF(c, n, idx, src, dst);                                                 \
+        }                                                                                                 \
     };
 
 HPB_DROPIN_ABI(float, f32, float, v)

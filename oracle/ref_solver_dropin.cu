@@ -86,6 +86,22 @@ int ref_dropin_solve_prec_f64(int method, int precond, int rows, int64_t nnz, co
     return run_solver(prec, vec_ops, lin_op, method, b, x, basis, rel_tol, max_iters, iters_out, resid_out);
 }
 
+// The drop-in's transposed operations on one matrix (device arrays):
+// y = A^T x (csr::gpu_matrix::axpy with transpose_ = true), z solves
+// L^T z = x with L the unit lower triangle, w solves U^T w = x with U the
+// upper triangle with its diagonal.  Returns 1.
+int ref_dropin_transposed_ops_f64(int rows, int64_t nnz, const int* rp, const int* ci, const double* val,
+                                  double* x, double* y, double* z, double* w) {
+    cublas_wrap cublas(false);
+    mat_t mat(&cublas);
+    mat.attach(rows, rows, int(nnz), rp, ci, val);
+    mat.axpy(1.0, x, 0.0, y, true);
+    mat.triangular_solve_lower(x, z, 1.0, true);
+    mat.triangular_solve_upper(x, w, 1.0, true);
+    cudaDeviceSynchronize();
+    return 1;
+}
+
 int ref_dropin_solve_f64(int method, int rows, int64_t nnz, const int* rp, const int* ci, const double* val,
                          double* b, double* x, int basis, double rel_tol, int max_iters, int high_prec,
                          int* iters_out, double* resid_out) {

@@ -55,6 +55,9 @@ template <class T> int run(int n) {
     ok = ok && s4.solve(lin_op, b, x);
     mat.triangular_solve_lower(b, x);
     mat.triangular_solve_upper(x, b, T(2.0));
+    mat.axpy(T(1.0), x, T(0.0), b, true);
+    mat.triangular_solve_lower(b, x, T(1.0), true);
+    mat.triangular_solve_upper(x, b, T(1.0), true);
     // Matrix Market reader (test_csr_matrix.cpp's use of csr::matrix_market_reader)
     csr::matrix_market_reader<T> reader(true);
     mat_t mm_mat(&cublas);

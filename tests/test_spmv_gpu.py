@@ -185,3 +185,68 @@ def test_spmv_of_matrix_market_file(gpu, name, t):
     y = spmv(ctx, torch, t, A, 1.0, x, 0.0, np.zeros(A.n))
     want = ref @ x.astype(WIDE[t])
     assert np.allclose(y, want, rtol=4e-6 if t in ("f32", "c64") else 1e-14, atol=1e-6 if t == "f32" else 1e-14)
+
+
+@pytest.mark.parametrize("shape", [(300, 200), (200, 300), (1024, 1024)])
+def test_transpose_pattern_matches_scipy(gpu, shape):
+    """hpb_csr_transpose_pattern: A^T's row pointers and column indices equal
+    scipy's transpose (sorted indices), and the gathered values
+    (hpb_gather_f64 with perm) equal its values; rectangular and square."""
+    import scipy.sparse as sp
+    ctx, torch = gpu
+    rows, cols = shape
+    A = sp.random(rows, cols, density=0.02, random_state=rows + cols, format="csr")
+    A.sort_indices()
+    T = sp.csr_matrix(A.T)
+    T.sort_indices()
+    d = [dev(torch, a) for a in (A.indptr.astype(np.int32), A.indices.astype(np.int32), A.data)]
+    rp_t = torch.zeros(cols + 1, dtype=torch.int32, device="cuda")
+    ci_t = torch.zeros(max(A.nnz, 1), dtype=torch.int32, device="cuda")
+    perm = torch.zeros(max(A.nnz, 1), dtype=torch.int32, device="cuda")
+    ctx.check(_lib.lib.hpb_csr_transpose_pattern(ctx.h, rows, cols, A.nnz, d[0].data_ptr(), d[1].data_ptr(),
+                                                 rp_t.data_ptr(), ci_t.data_ptr(), perm.data_ptr()), "transpose")
+    vt = torch.zeros(max(A.nnz, 1), dtype=torch.float64, device="cuda")
+    ctx.check(_lib.lib.hpb_gather_f64(ctx.h, A.nnz, perm.data_ptr(), d[2].data_ptr(), vt.data_ptr()), "gather")
+    torch.cuda.synchronize()
+    assert np.array_equal(host(rp_t), T.indptr) and np.array_equal(host(ci_t)[:A.nnz], T.indices)
+    assert np.array_equal(host(vt)[:A.nnz], T.data)
+
+
+def test_transpose_pattern_rejects_bad_columns(gpu):
+    ctx, torch = gpu
+    rp = dev(torch, np.array([0, 2], np.int32))
+    ci = dev(torch, np.array([0, 7], np.int32))
+    out = [torch.zeros(4, dtype=torch.int32, device="cuda") for _ in range(3)]
+    st = _lib.lib.hpb_csr_transpose_pattern(ctx.h, 1, 3, 2, rp.data_ptr(), ci.data_ptr(), *[o.data_ptr() for o in out])
+    assert st == -1
+
+
+def test_dropin_transposed_operations(gpu):
+    """csr::gpu_matrix with transpose_ = true (compiled into the drop-in test
+    library): A^T x against scipy, L^T and U^T solves bit for bit against
+    substitution on scipy's transpose (oracle/tri.c)."""
+    import ctypes as C
+    import oracle
+    import scipy.sparse as sp
+    ctx, torch = gpu
+    so = oracle.HERE / "_ref" / "libhpb_ref_dropin.so"
+    if not so.exists():
+        pytest.skip("oracle/_ref/libhpb_ref_dropin.so not built")
+    lib = C.CDLL(str(so))
+    lib.ref_dropin_transposed_ops_f64.argtypes = [C.c_int, C.c_int64] + [C.c_void_p] * 7
+    A = problems.convdiff2d(48)
+    rows = np.repeat(np.arange(A.n), np.diff(A.row_ptr))
+    diag = A.val[A.col_ind == rows]
+    A = problems.CSR(A.n, A.row_ptr, A.col_ind, A.val / diag[rows])  # row-scaled: bounded unit solves
+    rng = np.random.default_rng(4)
+    x = rng.standard_normal(A.n)
+    d = [dev(torch, a) for a in (A.row_ptr, A.col_ind, A.val, x, np.zeros(A.n), np.zeros(A.n), np.zeros(A.n))]
+    assert lib.ref_dropin_transposed_ops_f64(A.n, A.nnz, *[a.data_ptr() for a in d]) == 1
+    torch.cuda.synchronize()
+    M = sp.csr_matrix((A.val, A.col_ind, A.row_ptr), shape=(A.n, A.n))
+    T = sp.csr_matrix(M.T)
+    T.sort_indices()
+    assert np.allclose(host(d[4]), T @ x, rtol=1e-14, atol=1e-14 * np.abs(T).dot(np.abs(x)).max())
+    z = oracle.csr_trsv(T.indptr, T.indices, T.data, x, upper=True, unit=True)    # (L)^T = unit upper of A^T
+    w = oracle.csr_trsv(T.indptr, T.indices, T.data, x, upper=False, unit=False)  # (U)^T = lower of A^T
+    assert np.array_equal(host(d[5]), z) and np.array_equal(host(d[6]), w)
