@@ -293,3 +293,38 @@ def test_sweeps_reach_the_exact_solve(gpu):
         assert not np.array_equal(sweeps(ctx, torch, tri, "f64", vd, b, not upper, 3), exact)
         assert np.array_equal(sweeps(ctx, torch, tri, "f64", vd, b, not upper, 15), exact)
         tri.close()
+
+
+def random_long_range(rng, n, deps):
+    """Each row depends on `deps` random earlier (lower) rows anywhere above
+    it, plus a dominant diagonal and as many random later columns: most
+    dependencies cross tiles, more of them than a tile's halo holds (so the
+    solve's direct polling path runs too)."""
+    rp, ci, va = [0], [], []
+    for r in range(n):
+        lo = rng.choice(r, size=min(deps, r), replace=False) if r else np.zeros(0, np.int64)
+        hi = rng.choice(np.arange(r + 1, n), size=min(deps, n - r - 1), replace=False) if r + 1 < n else \
+            np.zeros(0, np.int64)
+        cols = np.sort(np.concatenate([lo, [r], hi]).astype(np.int64))
+        ci.extend(cols.tolist())
+        va.extend(float(2 * deps + 1) if c == r else rng.standard_normal() for c in cols)
+        rp.append(len(ci))
+    return problems.CSR(n, np.array(rp, np.int32), np.array(ci, np.int32), np.array(va))
+
+
+@pytest.mark.parametrize("t", ["f64", "c128"])
+def test_trsv_long_range_dependencies(gpu, t):
+    ctx, torch = gpu
+    rng = np.random.default_rng(31)
+    A, val = typed(random_long_range(rng, 3 * TILE + 100, 3), t, rng)
+    vd = dev(torch, val)
+    b = (rng.standard_normal(A.n) + (1j * rng.standard_normal(A.n) if t.startswith("c") else 0)).astype(DT[t])
+    for upper in (False, True):
+        tri = Tri(ctx, torch, A, upper)
+        try:
+            for unit in (True, False):
+                got = trsv(ctx, torch, tri, t, vd, b, unit)
+                want = oracle.csr_trsv(A.row_ptr, A.col_ind, val, b, upper, unit)
+                assert np.array_equal(got, want), (t, upper, unit)
+        finally:
+            tri.close()
