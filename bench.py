@@ -936,6 +936,9 @@ def main():
     ap.add_argument("--profile-solve", type=int, default=0, metavar="K",
                     help="profiling aid: run one fused solve of the solver workload capped at K iterations, "
                          "print its report and exit (no bench line)")
+    ap.add_argument("--profile-ir", type=int, default=0, metavar="K",
+                    help="K binary64 refinements of the config-3 system, each one binary32 GMRES(50) cycle (a short "
+                         "run of the precision form for ncu)")
     ap.add_argument("--profile-trsv", type=int, default=0, metavar="K",
                     help="ILU(0) of the config-2 matrix, then K lower and K upper triangular solves (a short run of "
                          "the triangular-solve kernel for ncu)")
@@ -959,6 +962,14 @@ def main():
     import torch
     if args.profile_solve > 0:
         profile_solve(torch, args.profile_solve, args.profile_method)
+        return
+    if args.profile_ir > 0:
+        from high_precision_blas1_b200 import problems
+        A = problems.poisson3d_aniso(128, eps=(1.0, 1e-2, 1e-4))
+        b = problems.rhs_uniform(A.n, 303)
+        t, st, r, _ = ir_solve(torch, A, b, "gmres", 50, inner_tol=0.0, max_iters=0,
+                               max_refinements=args.profile_ir, warm=False)
+        print(f"profile ir: status {st}, refinements {r.refinements}, inner iterations {r.inner_iters}, {t:.4f} s")
         return
     if args.profile_trsv > 0:
         from high_precision_blas1_b200 import problems

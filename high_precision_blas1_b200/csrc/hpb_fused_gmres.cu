@@ -20,6 +20,7 @@
 #include <cmath>
 #include <memory>
 #include <new>
+#include <type_traits>
 #include <vector>
 
 #include "hpb_fused.cuh"
@@ -118,9 +119,35 @@ k_multidot(int64_t n, int K, const E* __restrict__ V, const E* __restrict__ w,
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     using PA = typename pacc_of<E>::type;
     constexpr int kMdTile = md_tile<E>::value;
+    // binary32: four consecutive rows per thread with 16-byte loads (scalar
+    // 4-byte loads leave HBM well short of its bandwidth); the vectors start
+    // 16-byte aligned when n % 4 == 0 and V, w are
+    bool vec4 = false;
+    if constexpr (std::is_same<E, float>::value)
+        vec4 = n % 4 == 0 && ((reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(w)) & 15) == 0;
     for (int kb = 0; kb < K; kb += kMdTile) {
         PA pacc[kMdTile];
-        for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+        if constexpr (std::is_same<E, float>::value) {
+            if (vec4) {
+                const float4* w4 = reinterpret_cast<const float4*>(w);
+                for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 4; q += stride) {
+                    const float4 wq = w4[q];
+                    float4 vk[kMdTile];
+#pragma unroll
+                    for (int t = 0; t < kMdTile; ++t)
+                        if (kb + t < K) vk[t] = __ldg(reinterpret_cast<const float4*>(V + size_t(kb + t) * n) + q);
+#pragma unroll
+                    for (int t = 0; t < kMdTile; ++t)
+                        if (kb + t < K) {
+                            pdot_add(pacc[t], vk[t].x, wq.x);
+                            pdot_add(pacc[t], vk[t].y, wq.y);
+                            pdot_add(pacc[t], vk[t].z, wq.z);
+                            pdot_add(pacc[t], vk[t].w, wq.w);
+                        }
+                }
+            }
+        }
+        for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; !vec4 && q < n; q += stride) {
             const E wq = ldE(w, q);
             E vk[kMdTile];
 #pragma unroll
@@ -172,7 +199,40 @@ k_gs_update(int64_t n, int K, const E* __restrict__ V, const E* win, E* wout,
     typename pacc_of<E>::type pacc;
     bool bad = false;
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
+    // binary32: four consecutive rows per thread with 16-byte loads and
+    // stores (each row's FMA chain unchanged); win may equal wout, and each
+    // thread reads its rows before writing them
+    bool vec4 = false;
+    if constexpr (std::is_same<E, float>::value) {
+        vec4 = n % 4 == 0 && ((reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(win) |
+                               reinterpret_cast<uintptr_t>(wout)) & 15) == 0;
+        if (vec4) {
+            for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 4; q += stride) {
+                const float4 wi = reinterpret_cast<const float4*>(win)[q];
+                // the scalar type of binary32 storage: each row accumulates in
+                // S and rounds to binary32 once, as in the scalar loop below
+                S v0 = to_s(wi.x), v1 = to_s(wi.y), v2 = to_s(wi.z), v3 = to_s(wi.w);
+                for (int k = 0; k < K; ++k) {
+                    const float4 vk = __ldg(reinterpret_cast<const float4*>(V + size_t(k) * n) + q);
+                    v0 = s_fma(sc[k], to_s(vk.x), v0);
+                    v1 = s_fma(sc[k], to_s(vk.y), v1);
+                    v2 = s_fma(sc[k], to_s(vk.z), v2);
+                    v3 = s_fma(sc[k], to_s(vk.w), v3);
+                }
+                const float4 v = make_float4(from_s<float>(v0), from_s<float>(v1), from_s<float>(v2),
+                                             from_s<float>(v3));
+                reinterpret_cast<float4*>(wout)[q] = v;
+                if (NORM) {
+                    pdot_add(pacc, v.x, v.x);
+                    pdot_add(pacc, v.y, v.y);
+                    pdot_add(pacc, v.z, v.z);
+                    pdot_add(pacc, v.w, v.w);
+                    bad |= !finite_e(v.x) || !finite_e(v.y) || !finite_e(v.z) || !finite_e(v.w);
+                }
+            }
+        }
+    }
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; !vec4 && q < n; q += stride) {
         S v = to_s(ldE(win, q));
         for (int k = 0; k < K; ++k) v = s_fma(sc[k], to_s(ldE(V + size_t(k) * n, q)), v);
         E ve = from_s<E>(v);
