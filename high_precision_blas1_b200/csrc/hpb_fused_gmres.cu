@@ -147,7 +147,28 @@ k_multidot(int64_t n, int K, const E* __restrict__ V, const E* __restrict__ w,
                 }
             }
         }
-        for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; !vec4 && q < n; q += stride) {
+        bool vec2 = false;
+        if constexpr (std::is_same<E, double>::value) {
+            // binary64: two consecutive rows per thread with 16-byte loads
+            vec2 = n % 2 == 0 && ((reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(w)) & 15) == 0;
+            if (vec2) {
+                const double2* w2 = reinterpret_cast<const double2*>(w);
+                for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 2; q += stride) {
+                    const double2 wq = w2[q];
+                    double2 vk[kMdTile];
+#pragma unroll
+                    for (int t = 0; t < kMdTile; ++t)
+                        if (kb + t < K) vk[t] = __ldg(reinterpret_cast<const double2*>(V + size_t(kb + t) * n) + q);
+#pragma unroll
+                    for (int t = 0; t < kMdTile; ++t)
+                        if (kb + t < K) {
+                            pdot_add(pacc[t], vk[t].x, wq.x);
+                            pdot_add(pacc[t], vk[t].y, wq.y);
+                        }
+                }
+            }
+        }
+        for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; !vec4 && !vec2 && q < n; q += stride) {
             const E wq = ldE(w, q);
             E vk[kMdTile];
 #pragma unroll
@@ -232,7 +253,30 @@ k_gs_update(int64_t n, int K, const E* __restrict__ V, const E* win, E* wout,
             }
         }
     }
-    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; !vec4 && q < n; q += stride) {
+    bool vec2 = false;
+    if constexpr (std::is_same<E, double>::value) {
+        // binary64: two consecutive rows per thread with 16-byte loads and stores
+        vec2 = n % 2 == 0 && ((reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(win) |
+                               reinterpret_cast<uintptr_t>(wout)) & 15) == 0;
+        if (vec2) {
+            for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 2; q += stride) {
+                const double2 wi = reinterpret_cast<const double2*>(win)[q];
+                S v0 = wi.x, v1 = wi.y;
+                for (int k = 0; k < K; ++k) {
+                    const double2 vk = __ldg(reinterpret_cast<const double2*>(V + size_t(k) * n) + q);
+                    v0 = s_fma(sc[k], vk.x, v0);
+                    v1 = s_fma(sc[k], vk.y, v1);
+                }
+                reinterpret_cast<double2*>(wout)[q] = make_double2(v0, v1);
+                if (NORM) {
+                    pdot_add(pacc, v0, v0);
+                    pdot_add(pacc, v1, v1);
+                    bad |= !finite_e(v0) || !finite_e(v1);
+                }
+            }
+        }
+    }
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; !vec4 && !vec2 && q < n; q += stride) {
         S v = to_s(ldE(win, q));
         for (int k = 0; k < K; ++k) v = s_fma(sc[k], to_s(ldE(V + size_t(k) * n, q)), v);
         E ve = from_s<E>(v);
