@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <type_traits>
 #include <memory>
 #include <new>
 #include <vector>
@@ -169,6 +170,22 @@ __global__ void __launch_bounds__(kThreads) k_upd_u(int64_t n, int j, Vecs<E> V,
     using S = typename scalar_of<E>::type;
     const S nb = s_neg(st->beta);
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    if constexpr (std::is_same<E, double>::value) {
+        // binary64: two rows per thread with 16-byte loads and stores (the
+        // same FMA per element)
+        bool vec = n % 2 == 0;
+        for (int i = 0; i <= j; ++i)
+            vec = vec && ((reinterpret_cast<uintptr_t>(V.u[i]) | reinterpret_cast<uintptr_t>(V.r[i])) & 15) == 0;
+        if (vec) {
+            for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 2; q += stride)
+                for (int i = 0; i <= j; ++i) {
+                    const double2 ui = reinterpret_cast<const double2*>(V.u[i])[q];
+                    const double2 ri = reinterpret_cast<const double2*>(V.r[i])[q];
+                    reinterpret_cast<double2*>(V.u[i])[q] = make_double2(fma(nb, ui.x, ri.x), fma(nb, ui.y, ri.y));
+                }
+            return;
+        }
+    }
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
         for (int i = 0; i <= j; ++i) {
             S ui = to_s(ldE(V.u[i], q));
@@ -184,6 +201,25 @@ __global__ void __launch_bounds__(kThreads) k_upd_rx(int64_t n, int j, Vecs<E> V
     using S = typename scalar_of<E>::type;
     const S al = st->alpha, nal = s_neg(st->alpha);
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    if constexpr (std::is_same<E, double>::value) {
+        // binary64: two rows per thread with 16-byte loads and stores
+        bool vec = n % 2 == 0 && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(V.u[0])) & 15) == 0;
+        for (int i = 0; i <= j; ++i)
+            vec = vec && ((reinterpret_cast<uintptr_t>(V.u[i + 1]) | reinterpret_cast<uintptr_t>(V.r[i])) & 15) == 0;
+        if (vec) {
+            for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 2; q += stride) {
+                for (int i = 0; i <= j; ++i) {
+                    const double2 u = reinterpret_cast<const double2*>(V.u[i + 1])[q];
+                    const double2 r = reinterpret_cast<const double2*>(V.r[i])[q];
+                    reinterpret_cast<double2*>(V.r[i])[q] = make_double2(fma(nal, u.x, r.x), fma(nal, u.y, r.y));
+                }
+                const double2 u0 = reinterpret_cast<const double2*>(V.u[0])[q];
+                const double2 xq = reinterpret_cast<const double2*>(x)[q];
+                reinterpret_cast<double2*>(x)[q] = make_double2(fma(al, u0.x, xq.x), fma(al, u0.y, xq.y));
+            }
+            return;
+        }
+    }
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
         for (int i = 0; i <= j; ++i)
             stE(V.r[i], q, from_s<E>(s_fma(nal, to_s(ldE(V.u[i + 1], q)), to_s(ldE(V.r[i], q)))));
