@@ -93,6 +93,8 @@ _sig("hpb_status_string", C.c_char_p, [C.c_int])
 _sig("hpb_last_error", C.c_char_p, [P])
 _sig("hpb_version", C.c_int, [C.POINTER(C.c_int)] * 3)
 _sig("hpb_launch_count", C.c_uint64, [])
+_sig("hpb_shard_merge", C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p])
+_sig("hpb_shard_merge_cpu", C.c_int, [C.c_int, C.c_int, C.c_void_p, C.c_void_p])
 
 # reductions
 for t in TYPES:

@@ -1,0 +1,167 @@
+"""Compensated reductions over a vector sharded across GPUs (one process
+per GPU, ``torch.distributed`` over NCCL).
+
+The vector of global length n is split in contiguous slices, rank r owning
+``partition(n, world, r)``.  Element-wise operations need no exchange: each
+rank runs the single-GPU kernels on its slice.  A reduction takes one
+exchange step:
+
+1. the rank reduces its slice with the single-GPU kernel (``hpb_dot2_*``,
+   ``hpb_sum2_*``, ``hpb_asum2_*``), leaving one (hi, lo) result -- 2
+   doubles, 4 for a complex result -- in device memory;
+2. ``all_gather_into_tensor`` collects the world's results (16 or 32 bytes
+   per rank over NVLink) on every rank, in rank order;
+3. ``hpb_shard_merge`` merges them in rank order with the compensated
+   recurrence of the reference's second reduction pass, one device thread,
+   on the same stream.
+
+Every rank ends with the same bits, whatever order the ranks finish in;
+the result stays within the Ogita-Rump-Oishi bound of the whole-vector Dot2
+(the merge adds world-1 compensated additions to the single-GPU combine).
+An all-reduce(sum) would drop the error terms and has no specified order.
+
+The reference runs on one GPU and has no sharded reductions; the
+single-GPU entry points replaced are ``gpu_reduction_ogita<T>::dot / sum /
+asum / norm`` (common/ogita/gpu_reduction_ogita.h:74-96).
+
+There is no CPU compute path: the reductions and the merge run in
+libhpblas1.so on the GPU.  ``merge_gathered_cpu`` (the host build of the
+same merge, ``hpb_shard_merge_cpu``) serves callers whose exchange gathers
+to host memory, e.g. a gloo process group.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import Context, load
+
+_RED = {  # (name, complex result)
+    ("dot", "f32"): ("hpb_dot2_f32", False), ("dot", "f64"): ("hpb_dot2_f64", False),
+    ("dot", "c64"): ("hpb_dot2_c64", True), ("dot", "c128"): ("hpb_dot2_c128", True),
+    ("sum", "f32"): ("hpb_sum2_f32", False), ("sum", "f64"): ("hpb_sum2_f64", False),
+    ("sum", "c64"): ("hpb_sum2_c64", True), ("sum", "c128"): ("hpb_sum2_c128", True),
+    ("asum", "f32"): ("hpb_asum2_f32", False), ("asum", "f64"): ("hpb_asum2_f64", False),
+    ("asum", "c64"): ("hpb_asum2_c64", False), ("asum", "c128"): ("hpb_asum2_c128", False),
+}
+
+
+def partition(n: int, world: int, rank: int) -> tuple[int, int]:
+    """[lo, hi) of rank's contiguous slice: the first n % world ranks hold
+    one element more than the others."""
+    if n < 0 or world < 1 or not 0 <= rank < world:
+        raise ValueError("partition: need n >= 0, world >= 1, 0 <= rank < world")
+    q, r = divmod(n, world)
+    lo = rank * q + min(rank, r)
+    return lo, lo + q + (1 if rank < r else 0)
+
+
+def merge_gathered_cpu(parts: np.ndarray, is_complex: bool) -> np.ndarray:
+    """Merge gathered results (count x 2, or count x 4 complex, float64, in
+    rank order) on the host with hpb_shard_merge_cpu."""
+    L = load().lib
+    comps = 2 if is_complex else 1
+    a = np.ascontiguousarray(parts, dtype=np.float64).reshape(-1)
+    if a.size == 0 or a.size % (2 * comps):
+        raise ValueError("merge_gathered_cpu: need count >= 1 results of 2 (real) or 4 (complex) doubles")
+    out = np.empty(2 * comps)
+    st = L.hpb_shard_merge_cpu(a.size // (2 * comps), int(is_complex), a.ctypes.data, out.ctypes.data)
+    if st != 0:
+        raise load().HpbError(st, "hpb_shard_merge_cpu")
+    return out
+
+
+def value_of(res, is_complex: bool):
+    """hi of a merged result (the rounded compensated value, as the
+    reference's reductions return it)."""
+    r = [float(v) for v in res]
+    return complex(r[0], r[1]) if is_complex else r[0]
+
+
+class ShardedReductions:
+    """Dot2 / Sum2 / asum2 / norm of vectors sharded over the ranks of
+    ``group`` (NCCL), one GPU per rank.  ``x`` and ``y`` are this rank's
+    slices: CUDA tensors of the element type (float32, float64, complex64,
+    complex128), contiguous, on this rank's device.  Calls are ordered on
+    torch's current stream and return host scalars (like the reference's
+    by-value reductions, gpu_vector_operations.h:257-340)."""
+
+    def __init__(self, device: int, group=None):
+        import torch
+        import torch.distributed as dist
+        self._torch, self._dist = torch, dist
+        self.group = group
+        self.world = dist.get_world_size(group) if dist.is_initialized() else 1
+        self.rank = dist.get_rank(group) if dist.is_initialized() else 0
+        self.device = torch.device("cuda", device)
+        self.stream = torch.cuda.current_stream(self.device)
+        self.ctx = Context(device, self.stream.cuda_stream)
+        self.L = load().lib
+        self._local = torch.zeros(4, dtype=torch.float64, device=self.device)
+        self._gathered = torch.zeros(4 * self.world, dtype=torch.float64, device=self.device)
+        self._out = torch.zeros(4, dtype=torch.float64, device=self.device)
+
+    @staticmethod
+    def _type(t) -> str:
+        import torch
+        m = {torch.float32: "f32", torch.float64: "f64", torch.complex64: "c64", torch.complex128: "c128"}
+        if t.dtype not in m:
+            raise TypeError(f"unsupported element type {t.dtype}")
+        return m[t.dtype]
+
+    def _check(self, *ts):
+        for t in ts:
+            if not t.is_cuda or t.device != self.device or not t.is_contiguous():
+                raise ValueError("sharded reductions take contiguous CUDA tensors on this rank's device")
+        if len(ts) == 2 and (ts[0].numel() != ts[1].numel() or ts[0].dtype != ts[1].dtype):
+            raise ValueError("x and y differ in length or element type")
+
+    def _reduce(self, op: str, x, y=None):
+        self._check(*((x,) if y is None else (x, y)))
+        t = self._type(x)
+        name, cplx = _RED[(op, t)]
+        width = 4 if cplx else 2
+        f = getattr(self.L, name)
+        if torch_stream_changed(self):
+            raise RuntimeError("torch's current stream changed since this object was made")
+        args = (self.ctx.h, x.numel(), x.data_ptr()) + (() if y is None else (y.data_ptr(),))
+        self.ctx.check(f(*args, self._local.data_ptr()), name)
+        local = self._local[:width]
+        gathered = self._gathered[:width * self.world]
+        if self._dist.is_initialized():
+            self._dist.all_gather_into_tensor(gathered, local, group=self.group)
+        else:
+            gathered.copy_(local)
+        self.ctx.check(self.L.hpb_shard_merge(self.ctx.h, self.world, int(cplx), gathered.data_ptr(),
+                                              self._out.data_ptr()), "hpb_shard_merge")
+        return self._out[:width].cpu().numpy(), cplx
+
+    def dot(self, x, y):
+        """sum_i conj(x_i) y_i over the whole vector (Dot2)."""
+        res, cplx = self._reduce("dot", x, y)
+        return value_of(res, cplx)
+
+    def sum(self, x):
+        """sum_i x_i (Sum2)."""
+        res, cplx = self._reduce("sum", x)
+        return value_of(res, cplx)
+
+    def asum(self, x):
+        """sum_i |x_i| (real), sum_i |re_i| + |im_i| (complex), compensated."""
+        res, cplx = self._reduce("asum", x)
+        return value_of(res, cplx)
+
+    def norm(self, x):
+        """sqrt(Re Dot2(x, x)) over the whole vector."""
+        res, cplx = self._reduce("dot", x, x)
+        return float(np.sqrt(res[0]))
+
+    def result(self, op: str, x, y=None) -> np.ndarray:
+        """The merged (hi, lo) result itself (2 doubles; 4 for complex)."""
+        return self._reduce(op, x, y)[0]
+
+    def close(self):
+        self.ctx.close()
+
+
+def torch_stream_changed(obj: ShardedReductions) -> bool:
+    return obj._torch.cuda.current_stream(obj.device).cuda_stream != obj.stream.cuda_stream

@@ -134,6 +134,19 @@ int hpb_nrm2_c128(hpb_context* ctx, int64_t n, const void* x, double* out);
 #define HPB_DOT2_NOALLOC_MAX_N 16777216
 int hpb_dot2_f64_noalloc(int64_t n, const double* x, const double* y, double* out, void* stream);
 
+/* Sharded reductions: merge `count` reduction results (one per rank of a
+ * vector split in contiguous slices, in rank order, each in the layout
+ * above: 2 doubles real, 4 complex) into one result of the same layout.
+ * Per real component, in rank order: s = TwoSum(s, hi_k, t),
+ * c = c + (t + lo_k); then (hi, lo) = TwoSum(s, c) -- the recurrence the
+ * reference uses on (value, error) partials
+ * (common/ogita/gpu_reduction_ogita_impl.cuh:274-276).  No counterpart in
+ * the reference, which runs on one GPU.  hpb_shard_merge: device buffers,
+ * stream-ordered on the context's stream; hpb_shard_merge_cpu: host
+ * buffers, the same additions on the host, same bits. */
+int hpb_shard_merge(hpb_context* ctx, int count, int is_complex, const double* parts, double* out);
+int hpb_shard_merge_cpu(int count, int is_complex, const double* parts, double* out);
+
 /* Plain ("standard precision") reductions: one FMA per term, plain tree,
  * same output layout with lo = 0.  Replace the cuBLAS ?dot/?dotc, ?asum and
  * ?nrm2 calls of the standard path (external_libraries/cublas_wrap.h:520-590). */

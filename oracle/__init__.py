@@ -319,3 +319,31 @@ def csr_trsv_sweeps(row_ptr, col_ind, val, b, upper: bool, unit: bool, sweeps: i
     if st != 0:
         raise ValueError("a row stores no diagonal")
     return x
+
+
+def shard_merge(parts, is_complex: bool) -> np.ndarray:
+    """Merge of per-rank (hi, lo) reduction results in rank order (the
+    sharded reductions' combine), restated in plain Python binary64: per
+    real component s = TwoSum(s, hi_k, t), c = c + (t + lo_k), then
+    (hi, lo) = TwoSum(s, c) -- the (value, error) recurrence of the
+    reference's compensated pass, common/ogita/gpu_reduction_ogita_impl.cuh:
+    274-276.  parts: count x 2 (real) or count x 4 (complex: hi.re, hi.im,
+    lo.re, lo.im)."""
+    comps = 2 if is_complex else 1
+    a = [float(v) for v in np.asarray(parts, dtype=np.float64).reshape(-1)]
+
+    def two_sum(x, y):
+        s = x + y
+        bv = s - x
+        av = s - bv
+        return s, (y - bv) + (x - av)
+
+    out = np.zeros(2 * comps)
+    for q in range(comps):
+        s = c = 0.0
+        for k in range(len(a) // (2 * comps)):
+            s, t = two_sum(s, a[k * 2 * comps + q])
+            c = c + (t + a[k * 2 * comps + comps + q])
+        hi, lo = two_sum(s, c)
+        out[q], out[comps + q] = hi, lo
+    return out

@@ -1,0 +1,135 @@
+"""Host logic of the sharded reductions (high_precision_blas1_b200/sharded.py):
+the contiguous partition, the rank-ordered merge of per-rank (hi, lo)
+results (the library's host build, hpb_shard_merge_cpu, against the
+oracle's plain-Python restatement, bit for bit), and the exchange itself
+with 2 and 3 gloo ranks on CPU: every rank ends with the same bits, equal
+to the oracle's merge of the ranks' results and within the Dot2 bound of
+the exact dot product.  Each rank's local Dot2 here comes from the oracle
+(no GPU in these tests); on a GPU it is hpb_dot2_* (tests/test_sharded_gpu.py)."""
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import oracle
+from high_precision_blas1_b200 import sharded
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def two_sum(a, b):
+    s = a + b
+    bv = s - a
+    av = s - bv
+    return s, (b - bv) + (a - av)
+
+
+def local_result(x, y):
+    """(hi, lo) of the reference's sequential Dot2 of one slice."""
+    out = np.zeros(3)
+    oracle.oro().oro_dot2_seq_f64(x.shape[0], oracle._ptr(x), oracle._ptr(y), oracle._ptr(out))
+    return np.array(two_sum(out[1], out[2]))
+
+
+@pytest.mark.parametrize("n", [0, 1, 7, 64, 1000003])
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_partition_covers_contiguously(n, world):
+    parts = [sharded.partition(n, world, r) for r in range(world)]
+    assert parts[0][0] == 0 and parts[-1][1] == n
+    for (a, b), (c, _) in zip(parts, parts[1:]):
+        assert b == c
+    sizes = [b - a for a, b in parts]
+    assert max(sizes) - min(sizes) <= 1 and sizes == sorted(sizes, reverse=True)
+
+
+def test_partition_rejects_bad_arguments():
+    for args in [(-1, 2, 0), (4, 0, 0), (4, 2, 2), (4, 2, -1)]:
+        with pytest.raises(ValueError):
+            sharded.partition(*args)
+
+
+@pytest.mark.parametrize("is_complex", [False, True])
+def test_merge_cpu_matches_oracle_bitwise(is_complex):
+    rng = np.random.default_rng(5)
+    comps = 2 if is_complex else 1
+    for count in range(1, 10):
+        for trial in range(20):
+            hi = rng.standard_normal((count, comps)) * 10.0 ** rng.integers(-20, 20, (count, comps))
+            err = rng.standard_normal((count, comps)) * 10.0 ** rng.integers(-20, 20, (count, comps))
+            pairs = np.zeros((count, 2 * comps))
+            for k in range(count):
+                for q in range(comps):
+                    pairs[k, q], pairs[k, comps + q] = two_sum(hi[k, q], err[k, q])
+            got = sharded.merge_gathered_cpu(pairs, is_complex)
+            want = oracle.shard_merge(pairs, is_complex)
+            assert got.tobytes() == want.tobytes()
+            if count == 1:  # one result merges to itself
+                assert got.tobytes() == pairs[0].tobytes()
+
+
+def test_merge_cpu_cancellation_keeps_the_error_terms():
+    """hi terms that cancel exactly leave the lo terms: the merged value is
+    their sum, which a plain sum of the his would lose."""
+    pairs = np.array([[1.0e16, 1.0], [-1.0e16, 0.5]])
+    got = sharded.merge_gathered_cpu(pairs, False)
+    assert got[0] == 1.5 and got[1] == 0.0
+
+
+def test_merge_cpu_rejects_bad_shapes():
+    with pytest.raises(ValueError):
+        sharded.merge_gathered_cpu(np.zeros(3), False)
+    with pytest.raises(ValueError):
+        sharded.merge_gathered_cpu(np.zeros(0), False)
+    with pytest.raises(ValueError):
+        sharded.merge_gathered_cpu(np.zeros(2), True)
+
+
+def _worker(rank, world, port, n, cond, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, str(ROOT))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        x, y, _ = oracle.gendot_dev(1234, n, cond)  # the same pair on every rank (seeded)
+        lo, hi = sharded.partition(n, world, rank)
+        local = torch.from_numpy(local_result(x[lo:hi].copy(), y[lo:hi].copy()))
+        gathered = torch.zeros(2 * world, dtype=torch.float64)
+        dist.all_gather_into_tensor(gathered, local)
+        merged = sharded.merge_gathered_cpu(gathered.numpy(), False)
+        q.put((rank, gathered.numpy().tobytes(), merged.tobytes()))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_sharded_dot2(world):
+    n, cond = 50_001, 1e12
+    port = 29700 + world * 10 + (os.getpid() % 500)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, n, cond, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    gathered = {g for _, g, _ in out}
+    merged = {m for _, _, m in out}
+    assert len(gathered) == 1 and len(merged) == 1  # every rank holds the same bits
+    x, y, _ = oracle.gendot_dev(1234, n, cond)
+    parts = np.frombuffer(out[0][1], dtype=np.float64).reshape(world, 2)
+    for r in range(world):
+        lo, hi = sharded.partition(n, world, r)
+        assert parts[r].tobytes() == local_result(x[lo:hi].copy(), y[lo:hi].copy()).tobytes()
+    got = np.frombuffer(out[0][2], dtype=np.float64)
+    assert got.tobytes() == oracle.shard_merge(parts, False).tobytes()
+    ex_hi, ex_lo = oracle.exact_dot(x, y)
+    exact = ex_hi + ex_lo
+    c = oracle.condition_dot(x, y)
+    assert abs(got[0] - exact) <= oracle.bound_dot2(n, c) * abs(exact) + 2.0 ** -53 * abs(exact)
