@@ -101,13 +101,15 @@ __device__ __forceinline__ double s_abs(cd v) { return cabs_(v); }
 //                   order.
 // (A warp-per-basis-vector layout left 12 warps per SM resident and the
 // Arnoldi step latency-bound.)
-// basis vectors per pass: binary64 storage 4 (its binary64 Dot2 arithmetic
-// needs registers; 48 per thread keeps 5 blocks per SM), binary32 storage 8
-// (binary32 arithmetic, w loaded half as often) -- the faster of 4 and 8 for
-// each on B200 (GMRES(30)/(50) solves of configs 3 and 5)
-template <class E> struct md_tile { static constexpr int value = 8; };
-template <> struct md_tile<double> { static constexpr int value = 4; };
-template <> struct md_tile<cd> { static constexpr int value = 4; };
+// basis vectors per pass: 4 for every storage type.  binary64: its Dot2
+// arithmetic needs registers (48 per thread keeps 5 blocks per SM).
+// binary32: measured on B200, binary32 GMRES(50) in binary64 refinement on
+// the 128^3 anisotropic Poisson system took 0.360 s with 4 vectors per pass
+// (64 registers, 4 blocks per SM), 0.364 s with 6 (capped at 80 registers,
+// 3 blocks per SM) and 0.382 s with 8 (103 registers, 2 blocks per SM: w is
+// loaded less often, but fewer loads are in flight); on the lognormal 96^3
+// system with Jacobi the time per iteration was within 3 % across the three.
+template <class E> struct md_tile { static constexpr int value = 4; };
 
 template <class E>
 __global__ void __launch_bounds__(kGmThreads)
