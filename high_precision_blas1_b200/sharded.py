@@ -165,3 +165,152 @@ class ShardedReductions:
 
 def torch_stream_changed(obj: ShardedReductions) -> bool:
     return obj._torch.cuda.current_stream(obj.device).cuda_stream != obj.stream.cuda_stream
+
+
+# --------------------------------------------------------------- sparse operator
+def owner_of(cols: np.ndarray, n: int, world: int) -> np.ndarray:
+    """Rank owning each global index under partition(n, world, .)."""
+    starts = np.array([partition(n, world, r)[0] for r in range(world)] + [n], dtype=np.int64)
+    return np.searchsorted(starts, np.asarray(cols, dtype=np.int64), side="right") - 1
+
+
+class HaloPlan:
+    """Row block of a square CSR operator split like the vectors: rank r owns
+    rows and x entries partition(n, world, r).  Each stored column index is
+    renumbered into this rank's extended vector x_ext = [own slice | halo]:
+    an own column c becomes c - lo, a column owned by another rank becomes
+    n_own + its position in ``halo`` (the needed remote indices, sorted by
+    owner and then by index, so each owner's entries arrive as one
+    contiguous segment).  Entries keep their order inside a row, so the
+    row sums run in the same order as on one GPU.
+
+    ``send_index`` / ``send_counts`` say which own entries (local indices,
+    grouped by destination rank in rank order) this rank sends to the others
+    at every product; they are known once every rank's ``requests`` have been
+    exchanged (``finish``)."""
+
+    def __init__(self, row_ptr, col_ind, n: int, world: int, rank: int):
+        self.n, self.world, self.rank = n, world, rank
+        self.lo, self.hi = partition(n, world, rank)
+        self.rows = self.hi - self.lo
+        rp = np.asarray(row_ptr, dtype=np.int64)
+        ci = np.asarray(col_ind, dtype=np.int64)
+        if rp.shape[0] != self.rows + 1 or rp[0] != 0 or rp[-1] != ci.shape[0]:
+            raise ValueError("HaloPlan: row_ptr must hold this rank's rows, starting at 0")
+        if ci.size and (ci.min() < 0 or ci.max() >= n):
+            raise ValueError("HaloPlan: column index out of range")
+        own = (ci >= self.lo) & (ci < self.hi)
+        remote = np.unique(ci[~own])  # sorted by index, hence by owner
+        self.halo = remote
+        self.recv_counts = np.bincount(owner_of(remote, n, world), minlength=world).astype(np.int64) \
+            if remote.size else np.zeros(world, dtype=np.int64)
+        loc = np.empty_like(ci)
+        loc[own] = ci[own] - self.lo
+        loc[~own] = self.rows + np.searchsorted(remote, ci[~own])
+        self.row_ptr = rp.astype(np.int32)
+        self.col_ind = loc.astype(np.int32)
+        self.cols = self.rows + int(remote.size)
+        owners = owner_of(remote, n, world) if remote.size else np.zeros(0, dtype=np.int64)
+        # requests[s]: the global indices this rank needs from rank s
+        self.requests = [remote[owners == s] for s in range(world)]
+        self.send_index = None
+        self.send_counts = None
+
+    def finish(self, requests_to_me):
+        """requests_to_me[s]: the global indices rank s needs from this rank."""
+        parts = []
+        for s, req in enumerate(requests_to_me):
+            req = np.asarray(req, dtype=np.int64)
+            if req.size and (req.min() < self.lo or req.max() >= self.hi):
+                raise ValueError(f"HaloPlan: rank {s} requests indices this rank does not own")
+            if s == self.rank and req.size:
+                raise ValueError("HaloPlan: a rank requested its own entries")
+            parts.append(req - self.lo)
+        self.send_counts = np.array([p.size for p in parts], dtype=np.int64)
+        self.send_index = (np.concatenate(parts) if parts else np.zeros(0, dtype=np.int64)).astype(np.int32)
+        return self
+
+    def exchange_requests(self, group=None):
+        """All ranks' requests through torch.distributed (once per operator)."""
+        import torch.distributed as dist
+        everyone = [None] * self.world
+        dist.all_gather_object(everyone, [r.tolist() for r in self.requests], group=group)
+        return self.finish([everyone[s][self.rank] for s in range(self.world)])
+
+
+class ShardedCSR:
+    """y = A x for a square CSR operator whose rows and vectors are split
+    over the ranks (one GPU each) as ``partition`` says.  Per product: the
+    entries other ranks need are gathered on the device (hpb_gather_*), one
+    ``all_to_all_single`` over NCCL moves them into the halo of the extended
+    vector, the own slice is copied in front of the halo (hpb_copy), and the
+    row block's SpMV (hpb_csr_spmv_*) runs on the extended vector.  The
+    result equals the single-GPU SpMV's rows bit for bit.
+
+    The reference has no sharded operator; the single-GPU operator replaced
+    is csr::gpu_matrix::axpy (common/csr/gpu_matrix.h:322-375)."""
+
+    _T = {"float32": "f32", "float64": "f64", "complex64": "c64", "complex128": "c128"}
+
+    def __init__(self, device: int, row_ptr, col_ind, val, n: int, group=None, plan: HaloPlan | None = None):
+        import torch
+        import torch.distributed as dist
+        self._torch, self._dist, self.group = torch, dist, group
+        world = dist.get_world_size(group) if dist.is_initialized() else 1
+        rank = dist.get_rank(group) if dist.is_initialized() else 0
+        if plan is None:
+            plan = HaloPlan(row_ptr, col_ind, n, world, rank)
+            plan = plan.exchange_requests(group) if world > 1 else plan.finish([np.zeros(0)] * world)
+        self.plan = plan
+        self.device = torch.device("cuda", device)
+        self.stream = torch.cuda.current_stream(self.device)
+        self.ctx = Context(device, self.stream.cuda_stream)
+        self.L = load().lib
+        v = np.ascontiguousarray(val)
+        self.t = self._T[str(v.dtype)]
+        self.elem = v.dtype.itemsize
+        d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+        self.rp, self.ci, self.val = d(plan.row_ptr), d(plan.col_ind), d(v)
+        self.send_index = d(plan.send_index)
+        tdt = getattr(torch, str(v.dtype))
+        self.send_buf = torch.zeros(max(1, int(plan.send_counts.sum())), dtype=tdt, device=self.device)
+        self.x_ext = torch.zeros(max(1, plan.cols), dtype=tdt, device=self.device)
+        self._one = load().scalar(self.t, 1.0)
+        self._zero = load().scalar(self.t, 0.0)
+
+    def gather_send(self, x_local):
+        n_send = int(self.plan.send_counts.sum())
+        if n_send:
+            f = getattr(self.L, f"hpb_gather_{self.t}")
+            self.ctx.check(f(self.ctx.h, n_send, self.send_index.data_ptr(), x_local.data_ptr(),
+                             self.send_buf.data_ptr()), "hpb_gather")
+
+    def exchange(self):
+        p = self.plan
+        if p.world > 1:
+            self._dist.all_to_all_single(self.x_ext[p.rows:p.cols], self.send_buf[:int(p.send_counts.sum())],
+                                         output_split_sizes=p.recv_counts.tolist(),
+                                         input_split_sizes=p.send_counts.tolist(), group=self.group)
+
+    def local_spmv(self, x_local, y_local):
+        p = self.plan
+        if p.rows:
+            self.ctx.check(self.L.hpb_copy(self.ctx.h, p.rows, self.elem, x_local.data_ptr(), self.x_ext.data_ptr()),
+                           "hpb_copy")
+        f = getattr(self.L, f"hpb_csr_spmv_{self.t}")
+        self.ctx.check(f(self.ctx.h, p.rows, p.cols, int(p.col_ind.size), self.rp.data_ptr(), self.ci.data_ptr(),
+                         self.val.data_ptr(), self._one, self.x_ext.data_ptr(), self._zero, y_local.data_ptr()),
+                       "hpb_csr_spmv")
+
+    def apply(self, x_local, y_local):
+        """y_local = (A x) on this rank's rows; x_local, y_local: this rank's
+        slices (contiguous CUDA tensors of the operator's element type)."""
+        for t in (x_local, y_local):
+            if not t.is_cuda or t.device != self.device or not t.is_contiguous() or t.numel() != self.plan.rows:
+                raise ValueError("ShardedCSR.apply takes this rank's contiguous slices on its device")
+        self.gather_send(x_local)
+        self.exchange()
+        self.local_spmv(x_local, y_local)
+
+    def close(self):
+        self.ctx.close()

@@ -1,11 +1,16 @@
-"""Host logic of the sharded reductions (high_precision_blas1_b200/sharded.py):
+"""Host logic of the sharded reductions and the sharded SpMV
+(high_precision_blas1_b200/sharded.py):
 the contiguous partition, the rank-ordered merge of per-rank (hi, lo)
 results (the library's host build, hpb_shard_merge_cpu, against the
 oracle's plain-Python restatement, bit for bit), and the exchange itself
 with 2 and 3 gloo ranks on CPU: every rank ends with the same bits, equal
 to the oracle's merge of the ranks' results and within the Dot2 bound of
 the exact dot product.  Each rank's local Dot2 here comes from the oracle
-(no GPU in these tests); on a GPU it is hpb_dot2_* (tests/test_sharded_gpu.py)."""
+(no GPU in these tests); on a GPU it is hpb_dot2_* (tests/test_sharded_gpu.py).
+The SpMV's halo plan (column renumbering, requests, send lists) is checked
+by emulating the exchange in one process and with gloo ranks running the
+all-to-all: the row blocks' products (scipy here, hpb_csr_spmv_* on a GPU)
+equal the whole product bit for bit."""
 import os
 import sys
 from pathlib import Path
@@ -16,8 +21,10 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
+import scipy.sparse as sp
+
 import oracle
-from high_precision_blas1_b200 import sharded
+from high_precision_blas1_b200 import problems, sharded
 
 ROOT = Path(__file__).resolve().parent.parent
 
@@ -133,3 +140,123 @@ def test_gloo_ranks_sharded_dot2(world):
     exact = ex_hi + ex_lo
     c = oracle.condition_dot(x, y)
     assert abs(got[0] - exact) <= oracle.bound_dot2(n, c) * abs(exact) + 2.0 ** -53 * abs(exact)
+
+
+# ------------------------------------------------------------ sharded SpMV
+
+
+def _matrices():
+    A = problems.convdiff2d(24)
+    yield sp.csr_matrix((A.val, A.col_ind, A.row_ptr), shape=(A.n, A.n))
+    R = sp.random(500, 500, density=0.02, random_state=9, format="csr") + sp.eye(500)
+    R.sort_indices()
+    yield R.tocsr()
+
+
+def _rows(M, lo, hi):
+    rp = M.indptr[lo:hi + 1].astype(np.int64)
+    return rp - rp[0], M.indices[rp[0]:rp[-1]].copy(), M.data[rp[0]:rp[-1]].copy()
+
+
+def _plans(M, world):
+    n = M.shape[0]
+    plans = []
+    for r in range(world):
+        lo, hi = sharded.partition(n, world, r)
+        rp, ci, _ = _rows(M, lo, hi)
+        plans.append(sharded.HaloPlan(rp, ci, n, world, r))
+    for r, p in enumerate(plans):
+        p.finish([plans[s].requests[r] for s in range(world)])
+    return plans
+
+
+def _emulated_product(M, plans, x):
+    """Each rank's send buffer, the all-to-all done by hand, the local products."""
+    world, n = len(plans), M.shape[0]
+    send = [x[p.lo:p.hi][p.send_index] for p in plans]
+    y = np.zeros(n)
+    for r, p in enumerate(plans):
+        segs = []
+        for s, q in enumerate(plans):
+            off = int(q.send_counts[:r].sum())
+            segs.append(send[s][off:off + int(q.send_counts[r])])
+        x_ext = np.concatenate([x[p.lo:p.hi]] + segs)
+        assert x_ext.size == p.cols
+        _, _, val = _rows(M, p.lo, p.hi)
+        L = sp.csr_matrix((val, p.col_ind, p.row_ptr), shape=(p.rows, p.cols))
+        y[p.lo:p.hi] = L @ x_ext
+    return y
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 4, 7])
+def test_halo_plan_reproduces_the_product_bitwise(world):
+    rng = np.random.default_rng(world)
+    for M in _matrices():
+        n = M.shape[0]
+        plans = _plans(M, world)
+        for r, p in enumerate(plans):
+            assert p.recv_counts[r] == 0 and p.send_counts[r] == 0
+            for s in range(world):  # what s asks of r is owned by r, and r sends exactly that
+                assert np.all(sharded.owner_of(plans[s].requests[r], n, world) == r)
+                assert p.send_counts[s] == plans[s].recv_counts[r]
+            assert p.col_ind.size == 0 or (p.col_ind.min() >= 0 and p.col_ind.max() < p.cols)
+        x = rng.standard_normal(n)
+        assert _emulated_product(M, plans, x).tobytes() == (M @ x).tobytes()
+
+
+def test_halo_plan_rejects_bad_input():
+    with pytest.raises(ValueError):  # column out of range
+        sharded.HaloPlan(np.array([0, 1]), np.array([5]), 4, 2, 0)
+    with pytest.raises(ValueError):  # row_ptr does not hold this rank's 2 rows
+        sharded.HaloPlan(np.array([0, 1, 2, 3]), np.array([0, 1, 2]), 4, 2, 0)
+    p = sharded.HaloPlan(np.array([0, 1, 2]), np.array([0, 3]), 4, 2, 0)  # rank 0 owns 0, 1
+    assert [r.tolist() for r in p.requests] == [[], [3]] and p.cols == 3
+    with pytest.raises(ValueError):  # rank 1 asks rank 0 for index 3, which rank 1 owns
+        p.finish([np.array([], np.int64), np.array([3])])
+    with pytest.raises(ValueError):  # a rank asking itself
+        p.finish([np.array([1]), np.array([], np.int64)])
+
+
+def _spmv_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, str(ROOT))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        A = problems.convdiff2d(32)
+        M = sp.csr_matrix((A.val, A.col_ind, A.row_ptr), shape=(A.n, A.n))
+        lo, hi = sharded.partition(A.n, world, rank)
+        rp, ci, val = _rows(M, lo, hi)
+        plan = sharded.HaloPlan(rp, ci, A.n, world, rank).exchange_requests()
+        x = np.random.default_rng(3).standard_normal(A.n)  # the same x on every rank (seeded)
+        xl = torch.from_numpy(x[lo:hi].copy())
+        send = xl[torch.from_numpy(plan.send_index.astype(np.int64))]
+        halo = torch.zeros(plan.cols - plan.rows, dtype=torch.float64)
+        dist.all_to_all_single(halo, send, output_split_sizes=plan.recv_counts.tolist(),
+                               input_split_sizes=plan.send_counts.tolist())
+        x_ext = np.concatenate([xl.numpy(), halo.numpy()])
+        y = sp.csr_matrix((val, plan.col_ind, plan.row_ptr), shape=(plan.rows, plan.cols)) @ x_ext
+        q.put((rank, lo, hi, y.tobytes()))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_sharded_spmv(world):
+    """The halo plan's request exchange and the per-product all-to-all over
+    gloo ranks; the row blocks' products equal the whole product bit for bit."""
+    port = 29300 + world * 10 + (os.getpid() % 500)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_spmv_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=300) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    A = problems.convdiff2d(32)
+    M = sp.csr_matrix((A.val, A.col_ind, A.row_ptr), shape=(A.n, A.n))
+    want = M @ np.random.default_rng(3).standard_normal(A.n)
+    for rank, lo, hi, yb in out:
+        assert np.frombuffer(yb, dtype=np.float64).tobytes() == want[lo:hi].tobytes()

@@ -9,7 +9,10 @@ hpb_shard_merge):
     to 8 slices;
   * ShardedReductions on one rank -- without a process group, and over a
     one-rank NCCL group (the all-gather runs) -- returns the single-GPU
-    reduction's bits (one result merges to itself)."""
+    reduction's bits (one result merges to itself);
+  * ShardedCSR: 1-4 emulated ranks in one process (device gathers and
+    row-block SpMVs, the all-to-all replaced by copies) and one rank over
+    NCCL give the single-GPU SpMV's bits."""
 import os
 
 import numpy as np
@@ -134,6 +137,87 @@ def test_one_rank_nccl_group(gpu):
             _check_one_rank(ctx, torch, S)
         finally:
             S.close()
+    finally:
+        torch.cuda.synchronize()
+        dist.destroy_process_group()
+
+
+# ------------------------------------------------------------ sharded SpMV
+def _global_spmv(ctx, torch, A, x):
+    d = [dev(torch, a) for a in (A.row_ptr, A.col_ind, A.val)]
+    y = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+    ctx.check(_lib.lib.hpb_csr_spmv_f64(ctx.h, A.n, A.n, A.nnz, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(),
+                                        1.0, x.data_ptr(), 0.0, y.data_ptr()))
+    return y.cpu().numpy()
+
+
+def _rank_rows(A, lo, hi):
+    rp = A.row_ptr[lo:hi + 1].astype(np.int64)
+    return rp - rp[0], A.col_ind[rp[0]:rp[-1]].copy(), A.val[rp[0]:rp[-1]].copy()
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 4])
+def test_sharded_spmv_emulated_ranks(gpu, world):
+    """Every rank's ShardedCSR in one process on one GPU: the device gathers
+    of the send lists and the row-block SpMVs run through the library; only
+    the all-to-all is replaced by copies between the ranks' buffers (nothing
+    waits on anything).  The row blocks equal the whole SpMV bit for bit."""
+    ctx, torch = gpu
+    from high_precision_blas1_b200 import problems
+    A = problems.convdiff2d(200)
+    x = np.random.default_rng(8).standard_normal(A.n)
+    want = _global_spmv(ctx, torch, A, dev(torch, x))
+    plans, ops = [], []
+    for r in range(world):
+        lo, hi = sharded.partition(A.n, world, r)
+        rp, ci, _ = _rank_rows(A, lo, hi)
+        plans.append(sharded.HaloPlan(rp, ci, A.n, world, r))
+    for r, p in enumerate(plans):
+        p.finish([plans[s].requests[r] for s in range(world)])
+    for r, p in enumerate(plans):
+        rp, ci, val = _rank_rows(A, p.lo, p.hi)
+        ops.append(sharded.ShardedCSR(0, rp, ci, val, A.n, plan=p))
+    xs = [dev(torch, x[p.lo:p.hi]) for p in plans]
+    ys = [torch.zeros(p.rows, dtype=torch.float64, device="cuda") for p in plans]
+    try:
+        for op, xl in zip(ops, xs):
+            op.gather_send(xl)
+        for r, (op, p) in enumerate(zip(ops, plans)):  # the all-to-all, by hand
+            at = p.rows
+            for s, q in enumerate(plans):
+                off, cnt = int(q.send_counts[:r].sum()), int(q.send_counts[r])
+                assert cnt == int(p.recv_counts[s])
+                op.x_ext[at:at + cnt].copy_(ops[s].send_buf[off:off + cnt])
+                at += cnt
+            assert at == p.cols
+        for op, xl, yl in zip(ops, xs, ys):
+            op.local_spmv(xl, yl)
+        got = np.concatenate([y.cpu().numpy() for y in ys])
+        assert got.tobytes() == want.tobytes()
+    finally:
+        for op in ops:
+            op.close()
+
+
+def test_sharded_spmv_one_rank_nccl_group(gpu):
+    ctx, torch = gpu
+    import torch.distributed as dist
+    from high_precision_blas1_b200 import problems
+    A = problems.convdiff2d(128)
+    x = np.random.default_rng(9).standard_normal(A.n)
+    want = _global_spmv(ctx, torch, A, dev(torch, x))
+    port = 29400 + os.getpid() % 500
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            device_id=torch.device("cuda", 0))
+    try:
+        op = sharded.ShardedCSR(0, A.row_ptr, A.col_ind, A.val, A.n)
+        try:
+            y = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+            op.apply(dev(torch, x), y)
+            assert y.cpu().numpy().tobytes() == want.tobytes()
+            assert op.plan.cols == A.n and int(op.plan.send_counts.sum()) == 0
+        finally:
+            op.close()
     finally:
         torch.cuda.synchronize()
         dist.destroy_process_group()
