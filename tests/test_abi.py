@@ -67,3 +67,65 @@ def test_generator_is_seeded_and_reaches_condition():
     assert np.array_equal(a, c) and np.array_equal(b, d)
     cond = oracle.condition_dot(a, b)
     assert 1e18 < cond < 1e24
+
+
+def _header_prototypes():
+    h = (ROOT / "include" / "hpblas1.h").read_text()
+    h = re.sub(r"/\*.*?\*/", " ", h, flags=re.S)
+    h = re.sub(r"//[^\n]*", " ", h)
+    h = re.sub(r"#[^\n]*", " ", h)
+    h = re.sub(r"\s+", " ", h)
+    out = {}
+    for ret, name, args in re.findall(r"([A-Za-z_][\w\s\*]*?)\s*\b(hpb_\w+)\s*\(([^)]*)\)\s*;", h):
+        ts = []
+        for a in args.split(","):
+            a = a.strip()
+            if not a or a == "void":
+                continue
+            t = a if a.endswith("*") else re.sub(r"\b\w+$", "", a)
+            ts.append(re.sub(r"\bconst\b", "", t).replace(" ", ""))
+        out[name] = (re.sub(r"\bconst\b", "", ret).replace(" ", ""), ts)
+    return out
+
+
+def _c_kind(t: str):
+    """(kind, bytes) of a C parameter or return type of the header."""
+    if t.endswith("*"):
+        return ("ptr", 8)
+    return {"int": ("int", 4), "int32_t": ("int", 4), "int64_t": ("int", 8), "uint64_t": ("uint", 8),
+            "size_t": ("uint", 8), "double": ("float", 8), "float": ("float", 4), "void": ("void", 0),
+            "hpb_c64": ("struct", 8), "hpb_c128": ("struct", 16)}[t]
+
+
+def _ctypes_kind(ct):
+    if ct is None:
+        return ("void", 0)
+    if isinstance(ct, type) and issubclass(ct, (C._Pointer, C.c_void_p, C.c_char_p)):
+        return ("ptr", 8)
+    if isinstance(ct, type) and issubclass(ct, C.Structure):
+        return ("struct", C.sizeof(ct))
+    code = getattr(ct, "_type_", None)
+    kinds = {"i": "int", "l": "int", "q": "int", "I": "uint", "L": "uint", "Q": "uint", "d": "float", "f": "float",
+             "P": "ptr", "z": "ptr"}
+    return (kinds[code], C.sizeof(ct))
+
+
+def test_ctypes_declarations_match_the_header():
+    """Every ctypes declaration in _lib.py has the prototype's arity and, per
+    argument, its kind and width (a 32-bit int where the C side takes a
+    64-bit pointer or size would corrupt the call)."""
+    from high_precision_blas1_b200 import _lib
+    protos = _header_prototypes()
+    assert set(protos) == set(_lib.exported_symbols())
+    bad = []
+    for name, (ret, args) in protos.items():
+        f = _lib.lib.__dict__.get(name)
+        assert f is not None, name
+        got = [_ctypes_kind(a) for a in (f.argtypes or [])]
+        want = [_c_kind(a) for a in args]
+        if got != want:
+            bad.append((name, want, got))
+        if _ctypes_kind(f.restype) != _c_kind(ret) and not (ret in ("char*", "void*") and
+                                                             _ctypes_kind(f.restype)[0] == "ptr"):
+            bad.append((name, "restype", ret, f.restype))
+    assert not bad, bad[:5]
