@@ -314,3 +314,116 @@ class ShardedCSR:
 
     def close(self):
         self.ctx.close()
+
+
+# ----------------------------------------------------------------- solver
+class ShardedVectorOps:
+    """Vector operations on this rank's float64 slices for ``bicgstabl``:
+    element-wise work in the library's kernels (hpb_axpby_f64, hpb_copy,
+    hpb_fill_f64), dot products and norms through ``ShardedReductions``
+    (identical on every rank).  The operations mirror the reference's
+    vector-operations concept (add_mul, assign, assign_scalar, scalar_prod,
+    norm; common/gpu_vector_operations.h:257-462)."""
+
+    def __init__(self, reductions: ShardedReductions, n_local: int):
+        self.red, self.n = reductions, n_local
+        self.ctx, self.L = reductions.ctx, reductions.L
+        self._torch = reductions._torch
+
+    def new(self):
+        return self._torch.zeros(self.n, dtype=self._torch.float64, device=self.red.device)
+
+    def dot(self, x, y) -> float:
+        return self.red.dot(x, y)
+
+    def norm(self, x) -> float:
+        return self.red.norm(x)
+
+    def axpby(self, a: float, x, b: float, y):
+        """y := a x + b y"""
+        self.ctx.check(self.L.hpb_axpby_f64(self.ctx.h, self.n, a, x.data_ptr(), b, y.data_ptr()), "hpb_axpby_f64")
+
+    def copy(self, x, y):
+        self.ctx.check(self.L.hpb_copy(self.ctx.h, self.n, 8, x.data_ptr(), y.data_ptr()), "hpb_copy")
+
+    def fill(self, y, v: float):
+        self.ctx.check(self.L.hpb_fill_f64(self.ctx.h, self.n, v, y.data_ptr()), "hpb_fill_f64")
+
+
+def bicgstabl(ops, A, b, x, L: int = 2, rel_tol: float = 1e-10, max_iters: int = 10000):
+    """BiCGStab(l) on vectors split across ranks: the Sleijpen-Fokkema
+    recurrences of the reference's numerical_algos/lin_solvers/bicgstabl.h
+    (cycle :196-265: BiCG part :198-222, MR part with modified Gram-Schmidt
+    :223-258) with
+    its monitor's test ||r_0|| <= rel_tol ||b|| once per cycle
+    (default_monitor.h:202-226), unpreconditioned.  ``ops`` supplies new,
+    dot, norm, axpby (y := a x + b y), copy and fill on this rank's slices;
+    ``A.apply(x, y)`` the row block of y = A x.  Every scalar comes from a
+    reduction that every rank holds bit for bit, so all ranks take the same
+    branches.  x holds the initial guess and receives the solution.
+    Returns (converged, iterations, ||r_0|| / ||b||)."""
+    if L < 1:
+        raise ValueError("bicgstabl: basis size must be >= 1")
+    r = [ops.new() for _ in range(L + 1)]
+    u = [ops.new() for _ in range(L + 1)]
+    rt = ops.new()
+    bnorm = ops.norm(b)
+    A.apply(x, r[0])
+    ops.axpby(1.0, b, -1.0, r[0])  # r_0 = b - A x
+    ops.copy(r[0], rt)
+    ops.axpby(0.0, r[0], 1.0 / ops.norm(rt), rt)  # rt = r_0 / ||r_0||
+    ops.fill(u[0], 0.0)
+    sigma, gam, gam1, gam2 = ([0.0] * (L + 1) for _ in range(4))
+    tau = [[0.0] * (L + 1) for _ in range(L + 1)]
+    rho, alpha, omega = 1.0, 0.0, 1.0
+    it = 0
+    rnorm = ops.norm(r[0])
+    while True:
+        if not np.isfinite(rnorm):
+            return False, it, float("nan")
+        if rnorm <= rel_tol * bnorm:
+            return True, it, rnorm / bnorm
+        if it >= max_iters:
+            return False, it, rnorm / bnorm
+        rho = -omega * rho
+        for j in range(L):
+            if rho == 0.0:
+                return False, it, rnorm / bnorm  # breakdown
+            rho1 = ops.dot(rt, r[j])
+            beta = alpha * rho1 / rho
+            rho = rho1
+            for i in range(j + 1):
+                ops.axpby(1.0, r[i], -beta, u[i])  # u_i = r_i - beta u_i
+            A.apply(u[j], u[j + 1])
+            alpha = rho / ops.dot(rt, u[j + 1])
+            for i in range(j + 1):
+                ops.axpby(-alpha, u[i + 1], 1.0, r[i])  # r_i -= alpha u_{i+1}
+            A.apply(r[j], r[j + 1])
+            ops.axpby(alpha, u[0], 1.0, x)
+        for j in range(1, L + 1):
+            for i in range(1, j):
+                tau[i][j] = ops.dot(r[i], r[j]) / sigma[i]
+                ops.axpby(-tau[i][j], r[i], 1.0, r[j])
+            sigma[j] = ops.dot(r[j], r[j])
+            gam1[j] = ops.dot(r[j], r[0]) / sigma[j]
+        gam[L] = gam1[L]
+        omega = gam[L]
+        for j in range(L - 1, 0, -1):
+            g = gam1[j]
+            for i in range(j + 1, L + 1):
+                g -= tau[j][i] * gam[i]
+            gam[j] = g
+        for j in range(1, L):
+            g = gam[j + 1]
+            for i in range(j + 1, L):
+                g += tau[j][i] * gam[i + 1]
+            gam2[j] = g
+        ops.axpby(gam[1], r[0], 1.0, x)
+        ops.axpby(-gam1[L], r[L], 1.0, r[0])
+        ops.axpby(-gam[L], u[L], 1.0, u[0])
+        for j in range(1, L):
+            ops.axpby(gam2[j], r[j], 1.0, x)
+            ops.axpby(-gam1[j], r[j], 1.0, r[0])
+            ops.axpby(-gam[j], u[j], 1.0, u[0])
+        it += L
+        rnorm = ops.norm(r[0])

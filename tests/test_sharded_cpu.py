@@ -260,3 +260,108 @@ def test_gloo_ranks_sharded_spmv(world):
     want = M @ np.random.default_rng(3).standard_normal(A.n)
     for rank, lo, hi, yb in out:
         assert np.frombuffer(yb, dtype=np.float64).tobytes() == want[lo:hi].tobytes()
+
+
+# ------------------------------------------------------------ sharded solver
+class _HostOps:
+    """The sharded solver's vector operations on host slices for these CPU
+    tests: element-wise work in numpy, each rank's Dot2 from the oracle,
+    the (hi, lo) results exchanged over gloo and merged with the library's
+    host merge (one rank: no exchange)."""
+
+    def __init__(self, n_local, world):
+        self.n, self.world = n_local, world
+
+    def new(self):
+        return np.zeros(self.n)
+
+    def dot(self, x, y):
+        local = torch.from_numpy(local_result(x, y))
+        if self.world == 1:
+            return float(local[0])
+        gathered = torch.zeros(2 * self.world, dtype=torch.float64)
+        dist.all_gather_into_tensor(gathered, local)
+        return float(sharded.merge_gathered_cpu(gathered.numpy(), False)[0])
+
+    def norm(self, x):
+        return float(np.sqrt(self.dot(x, x)))
+
+    def axpby(self, a, x, b, y):
+        y[:] = a * x + b * y
+
+    def copy(self, x, y):
+        y[:] = x
+
+    def fill(self, y, v):
+        y[:] = v
+
+
+class _HostCSR:
+    def __init__(self, plan, val):
+        self.plan = plan
+        self.M = sp.csr_matrix((val, plan.col_ind, plan.row_ptr), shape=(plan.rows, plan.cols))
+
+    def apply(self, x, y):
+        p = self.plan
+        halo = torch.zeros(p.cols - p.rows, dtype=torch.float64)
+        if p.world > 1:
+            send = torch.from_numpy(x[p.send_index.astype(np.int64)].copy())
+            dist.all_to_all_single(halo, send, output_split_sizes=p.recv_counts.tolist(),
+                                   input_split_sizes=p.send_counts.tolist())
+        y[:] = self.M @ np.concatenate([x, halo.numpy()])
+
+
+def _solve_rows(world, rank):
+    A = problems.convdiff2d(24)
+    M = sp.csr_matrix((A.val, A.col_ind, A.row_ptr), shape=(A.n, A.n))
+    b = problems.rhs_uniform(A.n, 11)
+    lo, hi = sharded.partition(A.n, world, rank)
+    rp, ci, val = _rows(M, lo, hi)
+    plan = sharded.HaloPlan(rp, ci, A.n, world, rank)
+    plan = plan.exchange_requests() if world > 1 else plan.finish([np.zeros(0)])
+    x = np.zeros(hi - lo)
+    ok, it, rel = sharded.bicgstabl(_HostOps(hi - lo, world), _HostCSR(plan, val), b[lo:hi].copy(), x, L=2,
+                                    rel_tol=1e-10, max_iters=2000)
+    return ok, it, rel, lo, hi, x
+
+
+def _solver_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, str(ROOT))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        ok, it, rel, lo, hi, x = _solve_rows(world, rank)
+        q.put((rank, ok, it, rel, lo, hi, x.tobytes()))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_sharded_bicgstabl(world):
+    """BiCGStab(2) on row blocks of a 24 x 24 convection-diffusion system
+    across gloo ranks: every rank stops after the same iteration with the
+    same residual ratio (the merged reductions are identical on every rank),
+    the assembled solution meets the tolerance in a binary64 residual, and
+    the iteration count is the one-rank solve's to within a cycle."""
+    port = 29600 + world * 10 + (os.getpid() % 300)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_solver_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = sorted(q.get(timeout=300) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(o[1] for o in out)
+    assert len({(o[2], o[3]) for o in out}) == 1
+    A = problems.convdiff2d(24)
+    b = problems.rhs_uniform(A.n, 11)
+    x = np.zeros(A.n)
+    for _, _, _, _, lo, hi, xb in out:
+        x[lo:hi] = np.frombuffer(xb, dtype=np.float64)
+    assert np.linalg.norm(b - A.matvec(x)) <= 1.5e-10 * np.linalg.norm(b)
+    ok1, it1, _, _, _, x1 = _solve_rows(1, 0)
+    assert ok1 and abs(out[0][2] - it1) <= 2
+    assert np.abs(x - x1).max() <= 1e-8 * np.abs(x1).max()

@@ -221,3 +221,32 @@ def test_sharded_spmv_one_rank_nccl_group(gpu):
     finally:
         torch.cuda.synchronize()
         dist.destroy_process_group()
+
+
+def test_sharded_bicgstabl_one_rank(gpu):
+    """The sharded BiCGStab(4) driver on one rank (library kernels for the
+    element-wise work, the reductions and the row-block SpMV): it meets the
+    tolerance in a binary64 residual and takes the library's plain
+    BiCGStab(4) iteration count to within a cycle (the same recurrences)."""
+    ctx, torch = gpu
+    import ctypes as C
+    from high_precision_blas1_b200 import problems
+    A = problems.convdiff2d(64)
+    b = problems.rhs_uniform(A.n, 12)
+    R = sharded.ShardedReductions(0)
+    op = sharded.ShardedCSR(0, A.row_ptr, A.col_ind, A.val, A.n)
+    try:
+        x = torch.zeros(A.n, dtype=torch.float64, device="cuda")
+        ok, it, rel = sharded.bicgstabl(sharded.ShardedVectorOps(R, A.n), op, dev(torch, b), x, L=4, rel_tol=1e-10,
+                                        max_iters=4000)
+        xs = x.cpu().numpy()
+        assert ok and rel <= 1e-10
+        assert np.linalg.norm(b - A.matvec(xs)) <= 1.5e-10 * np.linalg.norm(b)
+        d = [dev(torch, a) for a in (A.row_ptr, A.col_ind, A.val, b, np.zeros(A.n))]
+        p = _lib.solver_params("bicgstabl", basis=4, rel_tol=1e-10, max_iters=4000)
+        rep = _lib.hpb_solver_report()
+        st = _lib.lib.hpb_csr_solve_f64(C.byref(p), A.n, A.nnz, *[a.data_ptr() for a in d], C.byref(rep), None, 0)
+        assert st == 0 and abs(rep.iters - it) <= 4, (rep.iters, it)
+    finally:
+        op.close()
+        R.close()
