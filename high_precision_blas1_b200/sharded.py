@@ -427,3 +427,90 @@ def bicgstabl(ops, A, b, x, L: int = 2, rel_tol: float = 1e-10, max_iters: int =
             ops.axpby(-gam[j], u[j], 1.0, u[0])
         it += L
         rnorm = ops.norm(r[0])
+
+
+def _make_rotation(dx: float, dy: float):
+    if dy == 0.0:
+        return 1.0, 0.0
+    if abs(dy) > abs(dx):
+        t = dx / dy
+        sn = 1.0 / np.sqrt(1.0 + t * t)
+        return t * sn, sn
+    t = dy / dx
+    cs = 1.0 / np.sqrt(1.0 + t * t)
+    return cs, t * cs
+
+
+def _rotate(dx: float, dy: float, cs: float, sn: float):
+    return cs * dx + sn * dy, -sn * dx + cs * dy
+
+
+def gmres(ops, A, b, x, m: int = 30, rel_tol: float = 1e-10, max_iters: int = 10000, reorthogonalize: bool = False):
+    """Restarted GMRES(m) on vectors split across ranks, real binary64: the
+    reference's numerical_algos/lin_solvers/gmres.h (restart loop :412-484;
+    modified Gram-Schmidt with optional reorthogonalisation :426-452; Givens
+    rotations :224-273, applied on the host to the rank-identical Hessenberg
+    entries), unpreconditioned, with the monitor's test
+    ||b - A x|| <= rel_tol ||b|| at every restart (default_monitor.h:202-226).
+    ``ops`` and ``A`` as for ``bicgstabl``.  Returns (converged, iterations,
+    ||b - A x|| / ||b||)."""
+    if m < 1:
+        raise ValueError("gmres: basis size must be >= 1")
+    V = [ops.new() for _ in range(m + 1)]
+    r = ops.new()
+    bnorm = ops.norm(b)
+
+    def residual():
+        A.apply(x, r)
+        ops.axpby(1.0, b, -1.0, r)  # r = b - A x
+        return ops.norm(r)
+
+    it = 0
+    rnorm = residual()
+    while True:
+        if not np.isfinite(rnorm):
+            return False, it, float("nan")
+        if rnorm <= rel_tol * bnorm:
+            return True, it, rnorm / bnorm
+        if it >= max_iters:
+            return False, it, rnorm / bnorm
+        ops.copy(r, V[0])
+        ops.axpby(0.0, r, 1.0 / rnorm, V[0])  # V_0 = r / ||r||
+        H = np.zeros((m + 1, m))
+        s = np.zeros(m + 1)
+        cs = np.zeros(m)
+        sn = np.zeros(m)
+        s[0] = rnorm
+        i = -1
+        while i + 1 < m:
+            i += 1
+            it += 1
+            A.apply(V[i], V[i + 1])
+            for k in range(i + 1):  # modified Gram-Schmidt
+                a = ops.dot(V[k], V[i + 1])
+                ops.axpby(-a, V[k], 1.0, V[i + 1])
+                if reorthogonalize:
+                    c = ops.dot(V[k], V[i + 1])
+                    ops.axpby(-c, V[k], 1.0, V[i + 1])
+                    a += c
+                H[k, i] = a
+            hn = ops.norm(V[i + 1])
+            H[i + 1, i] = hn
+            if hn > 0.0:
+                ops.axpby(0.0, V[i + 1], 1.0 / hn, V[i + 1])
+            for k in range(i):
+                H[k, i], H[k + 1, i] = _rotate(H[k, i], H[k + 1, i], cs[k], sn[k])
+            cs[i], sn[i] = _make_rotation(H[i, i], H[i + 1, i])
+            H[i, i], H[i + 1, i] = _rotate(H[i, i], H[i + 1, i], cs[i], sn[i])
+            H[i + 1, i] = 0.0
+            s[i], s[i + 1] = _rotate(s[i], s[i + 1], cs[i], sn[i])
+            if hn == 0.0:  # happy breakdown: the Krylov space is invariant
+                break
+        y = s.copy()
+        for j in range(i, -1, -1):
+            y[j] /= H[j, j]
+            for k in range(j - 1, -1, -1):
+                y[k] -= H[k, j] * y[j]
+        for j in range(i + 1):
+            ops.axpby(float(y[j]), V[j], 1.0, x)
+        rnorm = residual()

@@ -311,7 +311,7 @@ class _HostCSR:
         y[:] = self.M @ np.concatenate([x, halo.numpy()])
 
 
-def _solve_rows(world, rank):
+def _solve_rows(world, rank, method="bicgstabl"):
     A = problems.convdiff2d(24)
     M = sp.csr_matrix((A.val, A.col_ind, A.row_ptr), shape=(A.n, A.n))
     b = problems.rhs_uniform(A.n, 11)
@@ -320,34 +320,40 @@ def _solve_rows(world, rank):
     plan = sharded.HaloPlan(rp, ci, A.n, world, rank)
     plan = plan.exchange_requests() if world > 1 else plan.finish([np.zeros(0)])
     x = np.zeros(hi - lo)
-    ok, it, rel = sharded.bicgstabl(_HostOps(hi - lo, world), _HostCSR(plan, val), b[lo:hi].copy(), x, L=2,
-                                    rel_tol=1e-10, max_iters=2000)
+    ops, op = _HostOps(hi - lo, world), _HostCSR(plan, val)
+    if method == "bicgstabl":
+        ok, it, rel = sharded.bicgstabl(ops, op, b[lo:hi].copy(), x, L=2, rel_tol=1e-10, max_iters=2000)
+    else:
+        ok, it, rel = sharded.gmres(ops, op, b[lo:hi].copy(), x, m=20, rel_tol=1e-10, max_iters=2000,
+                                    reorthogonalize=(method == "gmres_reorth"))
     return ok, it, rel, lo, hi, x
 
 
-def _solver_worker(rank, world, port, q):
+def _solver_worker(rank, world, port, method, q):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     sys.path.insert(0, str(ROOT))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        ok, it, rel, lo, hi, x = _solve_rows(world, rank)
+        ok, it, rel, lo, hi, x = _solve_rows(world, rank, method)
         q.put((rank, ok, it, rel, lo, hi, x.tobytes()))
         dist.barrier()
     finally:
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("method", ["bicgstabl", "gmres", "gmres_reorth"])
 @pytest.mark.parametrize("world", [2, 3])
-def test_gloo_ranks_sharded_bicgstabl(world):
-    """BiCGStab(2) on row blocks of a 24 x 24 convection-diffusion system
-    across gloo ranks: every rank stops after the same iteration with the
-    same residual ratio (the merged reductions are identical on every rank),
-    the assembled solution meets the tolerance in a binary64 residual, and
-    the iteration count is the one-rank solve's to within a cycle."""
-    port = 29600 + world * 10 + (os.getpid() % 300)
+def test_gloo_ranks_sharded_solvers(world, method):
+    """BiCGStab(2) and GMRES(20) on row blocks of a 24 x 24
+    convection-diffusion system across gloo ranks: every rank stops after
+    the same iteration with the same residual ratio (the merged reductions
+    are identical on every rank), the assembled solution meets the
+    tolerance in a binary64 residual, and the iteration count is the
+    one-rank solve's to within a cycle."""
+    port = 29600 + world * 40 + ["bicgstabl", "gmres", "gmres_reorth"].index(method) * 10 + (os.getpid() % 300)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
-    procs = [ctx.Process(target=_solver_worker, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_solver_worker, args=(r, world, port, method, q)) for r in range(world)]
     for p in procs:
         p.start()
     out = sorted(q.get(timeout=300) for _ in range(world))
@@ -362,6 +368,6 @@ def test_gloo_ranks_sharded_bicgstabl(world):
     for _, _, _, _, lo, hi, xb in out:
         x[lo:hi] = np.frombuffer(xb, dtype=np.float64)
     assert np.linalg.norm(b - A.matvec(x)) <= 1.5e-10 * np.linalg.norm(b)
-    ok1, it1, _, _, _, x1 = _solve_rows(1, 0)
-    assert ok1 and abs(out[0][2] - it1) <= 2
+    ok1, it1, _, _, _, x1 = _solve_rows(1, 0, method)
+    assert ok1 and abs(out[0][2] - it1) <= (2 if method == "bicgstabl" else 20)
     assert np.abs(x - x1).max() <= 1e-8 * np.abs(x1).max()
