@@ -358,7 +358,13 @@ def bicgstabl(ops, A, b, x, L: int = 2, rel_tol: float = 1e-10, max_iters: int =
     its monitor's test ||r_0|| <= rel_tol ||b|| once per cycle
     (default_monitor.h:202-226), unpreconditioned.  ``ops`` supplies new,
     dot, norm, axpby (y := a x + b y), copy and fill on this rank's slices;
-    ``A.apply(x, y)`` the row block of y = A x.  Every scalar comes from a
+    ``A.apply(x, y)`` the row block of y = A x.  With complex vectors
+    ops.dot(x, y) = sum conj(x_i) y_i, and every inner product puts the
+    conjugated vector on the left (rho = (rt, r_j), (rt, u_{j+1}),
+    tau = (r_i, r_j), gamma' = (r_j, r_0)), as the library's solvers do:
+    the reference's order (bicgstabl.h:207, :216, :226, :230) conjugates
+    these scalars, which breaks the complex iteration; on real data both
+    orders give the same bits.  Every scalar comes from a
     reduction that every rank holds bit for bit, so all ranks take the same
     branches.  x holds the initial guess and receives the solution.
     Returns (converged, iterations, ||r_0|| / ||b||)."""

@@ -263,28 +263,42 @@ def test_gloo_ranks_sharded_spmv(world):
 
 
 # ------------------------------------------------------------ sharded solver
+def local_result_c128(x, y):
+    """(hi.re, hi.im, lo.re, lo.im) of the reference's sequential complex
+    Dot2, sum conj(x_i) y_i, of one slice."""
+    out = np.zeros(6)
+    oracle.oro().oro_dot2_seq_c128(x.shape[0], oracle._ptr(x), oracle._ptr(y), oracle._ptr(out))
+    hr, lr = two_sum(out[2], out[4])
+    hi, li = two_sum(out[3], out[5])
+    return np.array([hr, hi, lr, li])
+
+
 class _HostOps:
     """The sharded solver's vector operations on host slices for these CPU
     tests: element-wise work in numpy, each rank's Dot2 from the oracle,
     the (hi, lo) results exchanged over gloo and merged with the library's
     host merge (one rank: no exchange)."""
 
-    def __init__(self, n_local, world):
-        self.n, self.world = n_local, world
+    def __init__(self, n_local, world, dtype=np.float64):
+        self.n, self.world, self.dtype = n_local, world, np.dtype(dtype)
+        self.cplx = self.dtype == np.complex128
 
     def new(self):
-        return np.zeros(self.n)
+        return np.zeros(self.n, dtype=self.dtype)
 
     def dot(self, x, y):
-        local = torch.from_numpy(local_result(x, y))
+        local = torch.from_numpy(local_result_c128(x, y) if self.cplx else local_result(x, y))
+        w = local.numel()
         if self.world == 1:
-            return float(local[0])
-        gathered = torch.zeros(2 * self.world, dtype=torch.float64)
-        dist.all_gather_into_tensor(gathered, local)
-        return float(sharded.merge_gathered_cpu(gathered.numpy(), False)[0])
+            merged = local.numpy()
+        else:
+            gathered = torch.zeros(w * self.world, dtype=torch.float64)
+            dist.all_gather_into_tensor(gathered, local)
+            merged = sharded.merge_gathered_cpu(gathered.numpy(), self.cplx)
+        return complex(merged[0], merged[1]) if self.cplx else float(merged[0])
 
     def norm(self, x):
-        return float(np.sqrt(self.dot(x, x)))
+        return float(np.sqrt(self.dot(x, x).real))
 
     def axpby(self, a, x, b, y):
         y[:] = a * x + b * y
@@ -303,7 +317,8 @@ class _HostCSR:
 
     def apply(self, x, y):
         p = self.plan
-        halo = torch.zeros(p.cols - p.rows, dtype=torch.float64)
+        tdt = torch.complex128 if np.iscomplexobj(x) else torch.float64
+        halo = torch.zeros(p.cols - p.rows, dtype=tdt)
         if p.world > 1:
             send = torch.from_numpy(x[p.send_index.astype(np.int64)].copy())
             dist.all_to_all_single(halo, send, output_split_sizes=p.recv_counts.tolist(),
@@ -311,17 +326,24 @@ class _HostCSR:
         y[:] = self.M @ np.concatenate([x, halo.numpy()])
 
 
-def _solve_rows(world, rank, method="bicgstabl"):
+def _system(method):
+    if method == "bicgstabl_c128":
+        A = problems.helmholtz2d(24, ppw=10.0, damping=0.5)
+        return A, problems.rhs_uniform(A.n, 13, complex_=True)
     A = problems.convdiff2d(24)
+    return A, problems.rhs_uniform(A.n, 11)
+
+
+def _solve_rows(world, rank, method="bicgstabl"):
+    A, b = _system(method)
     M = sp.csr_matrix((A.val, A.col_ind, A.row_ptr), shape=(A.n, A.n))
-    b = problems.rhs_uniform(A.n, 11)
     lo, hi = sharded.partition(A.n, world, rank)
     rp, ci, val = _rows(M, lo, hi)
     plan = sharded.HaloPlan(rp, ci, A.n, world, rank)
     plan = plan.exchange_requests() if world > 1 else plan.finish([np.zeros(0)])
-    x = np.zeros(hi - lo)
-    ops, op = _HostOps(hi - lo, world), _HostCSR(plan, val)
-    if method == "bicgstabl":
+    x = np.zeros(hi - lo, dtype=b.dtype)
+    ops, op = _HostOps(hi - lo, world, b.dtype), _HostCSR(plan, val)
+    if method.startswith("bicgstabl"):
         ok, it, rel = sharded.bicgstabl(ops, op, b[lo:hi].copy(), x, L=2, rel_tol=1e-10, max_iters=2000)
     else:
         ok, it, rel = sharded.gmres(ops, op, b[lo:hi].copy(), x, m=20, rel_tol=1e-10, max_iters=2000,
@@ -335,22 +357,27 @@ def _solver_worker(rank, world, port, method, q):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         ok, it, rel, lo, hi, x = _solve_rows(world, rank, method)
-        q.put((rank, ok, it, rel, lo, hi, x.tobytes()))
+        q.put((rank, ok, it, rel, lo, hi, x.tobytes(), str(x.dtype)))
         dist.barrier()
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("method", ["bicgstabl", "gmres", "gmres_reorth"])
+METHODS = ["bicgstabl", "gmres", "gmres_reorth", "bicgstabl_c128"]
+
+
+@pytest.mark.parametrize("method", METHODS)
 @pytest.mark.parametrize("world", [2, 3])
 def test_gloo_ranks_sharded_solvers(world, method):
     """BiCGStab(2) and GMRES(20) on row blocks of a 24 x 24
-    convection-diffusion system across gloo ranks: every rank stops after
+    convection-diffusion system, and complex BiCGStab(2) on a 24 x 24
+    damped Helmholtz system (conj-linear inner products in the reference's
+    argument order), across gloo ranks: every rank stops after
     the same iteration with the same residual ratio (the merged reductions
     are identical on every rank), the assembled solution meets the
     tolerance in a binary64 residual, and the iteration count is the
     one-rank solve's to within a cycle."""
-    port = 29600 + world * 40 + ["bicgstabl", "gmres", "gmres_reorth"].index(method) * 10 + (os.getpid() % 300)
+    port = 29600 + world * 50 + METHODS.index(method) * 10 + (os.getpid() % 300)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_solver_worker, args=(r, world, port, method, q)) for r in range(world)]
@@ -362,12 +389,11 @@ def test_gloo_ranks_sharded_solvers(world, method):
         assert p.exitcode == 0
     assert all(o[1] for o in out)
     assert len({(o[2], o[3]) for o in out}) == 1
-    A = problems.convdiff2d(24)
-    b = problems.rhs_uniform(A.n, 11)
-    x = np.zeros(A.n)
-    for _, _, _, _, lo, hi, xb in out:
-        x[lo:hi] = np.frombuffer(xb, dtype=np.float64)
+    A, b = _system(method)
+    x = np.zeros(A.n, dtype=b.dtype)
+    for _, _, _, _, lo, hi, xb, dt in out:
+        x[lo:hi] = np.frombuffer(xb, dtype=dt)
     assert np.linalg.norm(b - A.matvec(x)) <= 1.5e-10 * np.linalg.norm(b)
     ok1, it1, _, _, _, x1 = _solve_rows(1, 0, method)
-    assert ok1 and abs(out[0][2] - it1) <= (2 if method == "bicgstabl" else 20)
+    assert ok1 and abs(out[0][2] - it1) <= (2 if method.startswith("bicgstabl") else 20)
     assert np.abs(x - x1).max() <= 1e-8 * np.abs(x1).max()
