@@ -29,6 +29,14 @@ from high_precision_blas1_b200 import problems, sharded
 ROOT = Path(__file__).resolve().parent.parent
 
 
+def _free_port() -> int:
+    """A TCP port on 127.0.0.1 that nothing listens on right now."""
+    import socket
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
 def two_sum(a, b):
     s = a + b
     bv = s - a
@@ -116,7 +124,7 @@ def _worker(rank, world, port, n, cond, q):
 @pytest.mark.parametrize("world", [2, 3])
 def test_gloo_ranks_sharded_dot2(world):
     n, cond = 50_001, 1e12
-    port = 29700 + world * 10 + (os.getpid() % 500)
+    port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_worker, args=(r, world, port, n, cond, q)) for r in range(world)]
@@ -245,7 +253,7 @@ def _spmv_worker(rank, world, port, q):
 def test_gloo_ranks_sharded_spmv(world):
     """The halo plan's request exchange and the per-product all-to-all over
     gloo ranks; the row blocks' products equal the whole product bit for bit."""
-    port = 29300 + world * 10 + (os.getpid() % 500)
+    port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_spmv_worker, args=(r, world, port, q)) for r in range(world)]
@@ -377,7 +385,7 @@ def test_gloo_ranks_sharded_solvers(world, method):
     are identical on every rank), the assembled solution meets the
     tolerance in a binary64 residual, and the iteration count is the
     one-rank solve's to within a cycle."""
-    port = 29600 + world * 50 + METHODS.index(method) * 10 + (os.getpid() % 300)
+    port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_solver_worker, args=(r, world, port, method, q)) for r in range(world)]
