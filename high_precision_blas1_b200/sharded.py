@@ -248,7 +248,11 @@ class ShardedCSR:
     result equals the single-GPU SpMV's rows bit for bit.
 
     The reference has no sharded operator; the single-GPU operator replaced
-    is csr::gpu_matrix::axpy (common/csr/gpu_matrix.h:322-375)."""
+    is csr::gpu_matrix::axpy (common/csr/gpu_matrix.h:322-375).
+
+    Construction without a ``plan`` exchanges the halo requests with
+    ``all_gather_object``, which NCCL runs on the current CUDA device: call
+    ``torch.cuda.set_device(device)`` on every rank first."""
 
     _T = {"float32": "f32", "float64": "f64", "complex64": "c64", "complex128": "c128"}
 
