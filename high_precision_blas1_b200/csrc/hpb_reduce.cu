@@ -21,6 +21,7 @@
 // reference's arithmetic) and are widened to binary64 before the warp tree,
 // so every combine of compensation terms runs in binary64.
 #include "hpb_common.cuh"
+#include "hpb_symbol_cache.h"
 
 #include <mutex>
 
@@ -489,39 +490,68 @@ HPB_RED_ALL(HPB_RED1, nrm2plain, OP_NRM2P)
 // kNoAllocMaxBlocks * 2048 = 16,777,216.  All calls share the array and it
 // keeps the last call's contents: the ticket is cleared before every launch,
 // and calls that overlap on the GPU (unordered streams) race.
-// The device address of the array is looked up once per device, with that
-// device current, by the first call on it.
+// The device address of the array is looked up once per CUDA context, with
+// that context current, by the first call in it (a new context -- after
+// cudaDeviceReset, or a caller's own driver context -- gets its own lookup).
 // ---------------------------------------------------------------------------
 namespace hpb {
 constexpr int kNoAllocMaxBlocks = 8192;
 constexpr int64_t kNoAllocElemsPerBlock = int64_t(kRedThreads) * kRedUnroll * 2;  // doubles per block
 constexpr size_t kNoAllocPartialBytes = size_t(kNoAllocMaxBlocks) * 2 * sizeof(double);
 constexpr size_t kNoAllocScratchBytes = kNoAllocPartialBytes + 256;  // + ticket, padded
-constexpr int kNoAllocMaxDevices = 64;
 static_assert(kNoAllocMaxBlocks * kNoAllocElemsPerBlock == HPB_DOT2_NOALLOC_MAX_N, "limit mismatch");
 }  // namespace hpb
 
 static __device__ __align__(256) unsigned char g_noalloc_dot2_scratch[hpb::kNoAllocScratchBytes];
 
 namespace {
-std::mutex g_noalloc_mutex;
-void* g_noalloc_addr[hpb::kNoAllocMaxDevices] = {};
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points (the
+// library links only the CUDA runtime).
+using CtxGetCurrentFn = int (*)(void** ctx);
+using CtxGetIdFn = int (*)(void* ctx, unsigned long long* id);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+std::once_flag g_ctx_fns_once;
 
-// Device address of the static scratch on the current device (set-up on
-// first use per device).  Host code only sees a host-side stand-in for the
-// array's name, so the address must come from cudaGetSymbolAddress.
-cudaError_t noalloc_scratch(int* device, unsigned char** ptr) {
-    cudaError_t e = cudaGetDevice(device);
-    if (e != cudaSuccess) return e;
-    if (*device < 0 || *device >= hpb::kNoAllocMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_addr[*device] == nullptr) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_dot2_scratch);
-        if (e != cudaSuccess) return e;
-        g_noalloc_addr[*device] = p;
+void load_ctx_fns() {
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    cudaDriverEntryPointQueryResult q1{}, q2{};
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess &&
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+        q2 == cudaDriverEntryPointSuccess) {
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+        g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f2);
     }
-    *ptr = static_cast<unsigned char*>(g_noalloc_addr[*device]);
+}
+
+hpb::SymbolAddressCache<64> g_noalloc_cache;
+
+// Device address of the static scratch in the current context.  Host code
+// only sees a host-side stand-in for the array's name, so the address must
+// come from cudaGetSymbolAddress.
+cudaError_t noalloc_scratch(unsigned char** ptr) {
+    void* p = nullptr;
+    std::call_once(g_ctx_fns_once, load_ctx_fns);
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (g_ctx_get_current == nullptr || g_ctx_get_current(&ctx) != 0 || ctx == nullptr ||
+        g_ctx_get_id(ctx, &id) != 0) {
+        // No context current yet (the runtime creates it on this lookup) or no
+        // driver entry points: look the symbol up without caching.
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_dot2_scratch);
+        if (e != cudaSuccess) return e;
+        *ptr = static_cast<unsigned char*>(p);
+        return cudaSuccess;
+    }
+    cudaError_t err = cudaSuccess;
+    const int st = g_noalloc_cache.get(id, &p, [&err](void** out) {
+        err = cudaGetSymbolAddress(out, g_noalloc_dot2_scratch);
+        return err == cudaSuccess ? 0 : 1;
+    });
+    if (st != 0) return err;
+    *ptr = static_cast<unsigned char*>(p);
     return cudaSuccess;
 }
 }  // namespace
@@ -532,19 +562,25 @@ extern "C" int hpb_dot2_f64_noalloc(int64_t n, const double* x, const double* y,
     if ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y) | reinterpret_cast<uintptr_t>(out)) %
             sizeof(double) != 0)
         return HPB_ERROR_INVALID_VALUE;
-    int device = 0;
     unsigned char* scratch = nullptr;
-    if (noalloc_scratch(&device, &scratch) != cudaSuccess) return HPB_ERROR_CUDA;
+    if (noalloc_scratch(&scratch) != cudaSuccess) return HPB_ERROR_CUDA;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     unsigned int* ticket = reinterpret_cast<unsigned int*>(scratch + hpb::kNoAllocPartialBytes);
     if (cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s) != cudaSuccess) return HPB_ERROR_CUDA;
     int64_t blocks = (n + hpb::kNoAllocElemsPerBlock - 1) / hpb::kNoAllocElemsPerBlock;
     const int grid = int(blocks < 1 ? 1 : blocks);
     const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
-    if (aligned)
-        hpb::reduce_kernel<double, hpb::OP_DOT2, true><<<grid, hpb::kRedThreads, 0, s>>>(n, x, y, scratch, ticket, out);
-    else
-        hpb::reduce_kernel<double, hpb::OP_DOT2, false><<<grid, hpb::kRedThreads, 0, s>>>(n, x, y, scratch, ticket, out);
+    // The launch's own status only: an error the caller left pending is
+    // neither reported as this call's nor cleared.
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(unsigned(grid));
+    cfg.blockDim = dim3(unsigned(hpb::kRedThreads));
+    cfg.stream = s;
+    void* vscratch = scratch;
+    cudaError_t e = aligned ? cudaLaunchKernelEx(&cfg, hpb::reduce_kernel<double, hpb::OP_DOT2, true>, n, x, y,
+                                                 vscratch, ticket, out)
+                            : cudaLaunchKernelEx(&cfg, hpb::reduce_kernel<double, hpb::OP_DOT2, false>, n, x, y,
+                                                 vscratch, ticket, out);
     hpb::count_launch();
-    return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
+    return e == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
 }

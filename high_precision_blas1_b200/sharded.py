@@ -121,8 +121,7 @@ class ShardedReductions:
         name, cplx = _RED[(op, t)]
         width = 4 if cplx else 2
         f = getattr(self.L, name)
-        if torch_stream_changed(self):
-            raise RuntimeError("torch's current stream changed since this object was made")
+        check_stream_and_device(self)
         args = (self.ctx.h, x.numel(), x.data_ptr()) + (() if y is None else (y.data_ptr(),))
         self.ctx.check(f(*args, self._local.data_ptr()), name)
         local = self._local[:width]
@@ -163,8 +162,18 @@ class ShardedReductions:
         self.ctx.close()
 
 
-def torch_stream_changed(obj: ShardedReductions) -> bool:
+def torch_stream_changed(obj) -> bool:
     return obj._torch.cuda.current_stream(obj.device).cuda_stream != obj.stream.cuda_stream
+
+
+def check_stream_and_device(obj) -> None:
+    """The library's kernels run on the stream saved at construction, and the
+    NCCL collectives on torch's current stream of the current device: the two
+    are ordered only while they are the same stream."""
+    if obj._torch.cuda.current_device() != obj.device.index:
+        raise RuntimeError("torch's current device differs from the one this object was made on")
+    if torch_stream_changed(obj):
+        raise RuntimeError("torch's current stream changed since this object was made")
 
 
 # --------------------------------------------------------------- sparse operator
@@ -291,6 +300,7 @@ class ShardedCSR:
 
     def exchange(self):
         p = self.plan
+        check_stream_and_device(self)
         if p.world > 1:
             self._dist.all_to_all_single(self.x_ext[p.rows:p.cols], self.send_buf[:int(p.send_counts.sum())],
                                          output_split_sizes=p.recv_counts.tolist(),
@@ -312,6 +322,7 @@ class ShardedCSR:
         for t in (x_local, y_local):
             if not t.is_cuda or t.device != self.device or not t.is_contiguous() or t.numel() != self.plan.rows:
                 raise ValueError("ShardedCSR.apply takes this rank's contiguous slices on its device")
+        check_stream_and_device(self)
         self.gather_send(x_local)
         self.exchange()
         self.local_spmv(x_local, y_local)
@@ -463,7 +474,14 @@ def gmres(ops, A, b, x, m: int = 30, rel_tol: float = 1e-10, max_iters: int = 10
     entries), unpreconditioned, with the monitor's test
     ||b - A x|| <= rel_tol ||b|| at every restart (default_monitor.h:202-226).
     ``ops`` and ``A`` as for ``bicgstabl``.  Returns (converged, iterations,
-    ||b - A x|| / ||b||)."""
+    ||b - A x|| / ||b||).
+
+    ``reorthogonalize`` applies ONE correction per basis vector (classical
+    "twice is enough" re-orthogonalisation).  The reference's loop
+    (gmres.h:431-447) repeats the correction while |alpha| > 1e-10 sqrt(N), up
+    to 11 times, but tests the accumulated coefficient alpha rather than the
+    correction c, so it runs all 11 corrections whenever the projection
+    itself is not tiny; the single pass is the intended method."""
     if m < 1:
         raise ValueError("gmres: basis size must be >= 1")
     V = [ops.new() for _ in range(m + 1)]

@@ -126,11 +126,16 @@ int hpb_nrm2_c128(hpb_context* ctx, int64_t n, const void* x, double* out);
  * library holds until the process exits.  out: device double[2] (hi, lo),
  * as hpb_dot2_f64; x, y, out: device pointers aligned to 8 bytes; stream: a
  * cudaStream_t or NULL.  n <= HPB_DOT2_NOALLOC_MAX_N, otherwise
- * HPB_ERROR_SIZE_LIMIT.  The first call on a device sets up (looks up the
- * array's device address with that device current); make that first call
- * before any stream capture.  All calls share the array and it keeps the last
- * call's contents; calls that overlap on the GPU (streams without an order
- * between them) race and give wrong results. */
+ * HPB_ERROR_SIZE_LIMIT.  The first call in each CUDA context sets up (looks
+ * up the array's device address in the current context and caches it under
+ * the context's id); make that first call before any stream capture.  A new
+ * context -- the primary context recreated after cudaDeviceReset, or a
+ * caller's own driver context -- gets its own lookup on its first call.  All
+ * calls share the array and it keeps the last call's contents; calls that
+ * overlap on the GPU (streams without an order between them) race and give
+ * wrong results.  Returns HPB_ERROR_CUDA when the launch itself fails; an
+ * error left pending by earlier work of the caller is neither reported nor
+ * cleared. */
 #define HPB_DOT2_NOALLOC_MAX_N 16777216
 int hpb_dot2_f64_noalloc(int64_t n, const double* x, const double* y, double* out, void* stream);
 

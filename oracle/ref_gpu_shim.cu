@@ -40,4 +40,19 @@ int ref_gpu_dot2_c128(int64_t n, const double* x, const double* y, double* out) 
     return 0;
 }
 
+// A reducer kept across calls, as gpu_vector_operations keeps its reducers
+// (common/gpu_vector_operations.h:129-141): constructed once for n, then dot()
+// per call.  Used to time the reference's GPU Dot2 per call.
+void* ref_gpu_reducer_f64_create(int64_t n) {
+    return new gpu_reduction_ogita<double, double*>(static_cast<size_t>(n));
+}
+
+int ref_gpu_reducer_f64_dot(void* h, const double* x, const double* y, double* out) {
+    auto* r = static_cast<gpu_reduction_ogita<double, double*>*>(h);
+    out[0] = r->dot(const_cast<double*>(x), const_cast<double*>(y));
+    return 0;
+}
+
+void ref_gpu_reducer_f64_destroy(void* h) { delete static_cast<gpu_reduction_ogita<double, double*>*>(h); }
+
 }  // extern "C"

@@ -1,13 +1,29 @@
 """CPU test: the reference's own solver headers compile unchanged against the
 C++ drop-in (include/hpblas1_dropin), for real and complex scalar types.
-Skipped where the reference sources are not present."""
+
+The reference's source tree comes from HPB_REF_SOURCE, else from the path the
+oracle build recorded in oracle/_ref/source_path; skipped where neither names
+an existing directory."""
+import os
 import subprocess
 from pathlib import Path
 
 import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
-REF = Path("/root/reference/source")
+
+
+def _ref_source() -> Path | None:
+    env = os.environ.get("HPB_REF_SOURCE")
+    if env:
+        return Path(env)
+    rec = ROOT / "oracle" / "_ref" / "source_path"
+    if rec.exists():
+        return Path(rec.read_text().strip())
+    return None
+
+
+REF = _ref_source()
 
 SRC = r'''
 #include <common/gpu_vector_operations.h>
@@ -73,7 +89,7 @@ int main() { return run<double>(10) + run<float>(10) + run<thrust::complex<doubl
 '''
 
 
-@pytest.mark.skipif(not REF.exists(), reason="reference sources not present")
+@pytest.mark.skipif(REF is None or not REF.is_dir(), reason="reference sources not present")
 def test_reference_solvers_compile_against_dropin(tmp_path):
     src = tmp_path / "dropin_driver.cu"
     src.write_text(SRC)

@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 import torch
 import torch.distributed as dist
-import torch.multiprocessing as mp
+import torch.multiprocessing as mp  # noqa: F401  (spawned ranks)
+from rank_utils import run_ranks
 
 ROOT = Path(__file__).resolve().parent.parent
 
@@ -47,15 +48,8 @@ def _worker(rank, world, port, q):
 def test_two_gloo_ranks_replica_logic():
     world = 2
     port = 29500 + (os.getpid() % 2000)
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
-    for p in procs:
-        p.start()
-    out = [q.get(timeout=300) for _ in range(world)]
-    for p in procs:
-        p.join(timeout=60)
-        assert p.exitcode == 0
+    out, codes = run_ranks(_worker, world, lambda r, q: (r, world, port, q))
+    assert codes == [0] * world
     for r, ws, t, same_op, own_rhs, printed in out:
         assert ws == world
         assert t == pytest.approx(1.0 + 2.0 * (world - 1))  # the slowest rank's time, on every rank

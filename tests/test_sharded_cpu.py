@@ -19,7 +19,8 @@ import numpy as np
 import pytest
 import torch
 import torch.distributed as dist
-import torch.multiprocessing as mp
+import torch.multiprocessing as mp  # noqa: F401  (spawned ranks)
+from rank_utils import run_ranks
 
 import scipy.sparse as sp
 
@@ -125,15 +126,8 @@ def _worker(rank, world, port, n, cond, q):
 def test_gloo_ranks_sharded_dot2(world):
     n, cond = 50_001, 1e12
     port = _free_port()
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, n, cond, q)) for r in range(world)]
-    for p in procs:
-        p.start()
-    out = [q.get(timeout=300) for _ in range(world)]
-    for p in procs:
-        p.join(timeout=60)
-        assert p.exitcode == 0
+    out, codes = run_ranks(_worker, world, lambda r, q: (r, world, port, n, cond, q))
+    assert codes == [0] * world
     gathered = {g for _, g, _ in out}
     merged = {m for _, _, m in out}
     assert len(gathered) == 1 and len(merged) == 1  # every rank holds the same bits
@@ -254,15 +248,8 @@ def test_gloo_ranks_sharded_spmv(world):
     """The halo plan's request exchange and the per-product all-to-all over
     gloo ranks; the row blocks' products equal the whole product bit for bit."""
     port = _free_port()
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    procs = [ctx.Process(target=_spmv_worker, args=(r, world, port, q)) for r in range(world)]
-    for p in procs:
-        p.start()
-    out = [q.get(timeout=300) for _ in range(world)]
-    for p in procs:
-        p.join(timeout=60)
-        assert p.exitcode == 0
+    out, codes = run_ranks(_spmv_worker, world, lambda r, q: (r, world, port, q))
+    assert codes == [0] * world
     A = problems.convdiff2d(32)
     M = sp.csr_matrix((A.val, A.col_ind, A.row_ptr), shape=(A.n, A.n))
     want = M @ np.random.default_rng(3).standard_normal(A.n)
@@ -386,15 +373,9 @@ def test_gloo_ranks_sharded_solvers(world, method):
     tolerance in a binary64 residual, and the iteration count is the
     one-rank solve's to within a cycle."""
     port = _free_port()
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    procs = [ctx.Process(target=_solver_worker, args=(r, world, port, method, q)) for r in range(world)]
-    for p in procs:
-        p.start()
-    out = sorted(q.get(timeout=300) for _ in range(world))
-    for p in procs:
-        p.join(timeout=60)
-        assert p.exitcode == 0
+    out, codes = run_ranks(_solver_worker, world, lambda r, q: (r, world, port, method, q))
+    assert codes == [0] * world
+    out = sorted(out)
     assert all(o[1] for o in out)
     assert len({(o[2], o[3]) for o in out}) == 1
     A, b = _system(method)
