@@ -201,10 +201,13 @@ def ref_cpu_cycles_sample(A, b, cycles, threads=-1):
 
 
 def ref_full_iters():
-    """Iterations the reference CPU BiCGStab(4) needs on this system (measured
-    once to convergence by tests/golden/make_solver_calibration.py)."""
+    """Iterations the reference CPU BiCGStab(4) needs on this system: the
+    median over its calibration runs (tests/golden/make_solver_calibration.py;
+    its threaded Dot2 merges thread results in completion order, so the count
+    varies from run to run)."""
     try:
-        return int(json.loads(REF_CAL.read_text())["iters"])
+        cal = json.loads(REF_CAL.read_text())
+        return int(cal.get("iters_median", cal["iters"]))
     except Exception:
         return None
 
@@ -434,14 +437,15 @@ def spmv_roofline(torch, L, ctx, A, reps=40):
 
 def bicgstabl_cycle_bytes(n, nnz, L, elem=8):
     """Algorithmic HBM bytes of one fused BiCGStab(L) cycle: 2L SpMVs (2L-1
-    with the Dot2 against rt), the u/r/x updates, the L modified Gram-Schmidt
+    with the Dot2 against rt; the L products of r_j - beta u_j gather both
+    vectors), one update pass per BiCG step, the L modified Gram-Schmidt
     sweeps and the closing update, each vector read or written once per
     kernel."""
     mat = (elem + 4.0) * nnz + 4.0 * (n + 1)
     spmv = mat + 2.0 * elem * n
     vec = elem * float(n)
-    passes = sum(3 * (j + 1) for j in range(L))            # u_i = r_i - beta u_i
-    passes += sum(3 * (j + 1) + 3 for j in range(L))       # r_i -= alpha u_{i+1}, x += alpha u_0
+    passes = L                                             # r_j gathered beside u_j by A (r_j - beta u_j)
+    passes += sum(4 * j + 7 for j in range(L))             # u_i = r_i - beta u_i, r_i -= alpha u_{i+1}, x += alpha u_0
     for k in range(1, L + 1):                              # right-looking MGS sweep k
         passes += (L + 1) if k == 1 else (L - k + 3) + (L - k + 1)
     passes += (2 + 2 * L + 2) + 3                          # closing update: reads, then x, r_0, u_0 written
@@ -607,6 +611,36 @@ def plain_solve(torch, A, b, method, basis, tol, precond="none", max_iters=20000
     return t, st, rep, d[4].cpu().numpy()
 
 
+def plain_solve_to_true_tol(torch, A, b, method, basis, tol, precond="none", max_iters=30000, max_rounds=6):
+    """The plain drop-in solve continued until the TRUE relative residual
+    ||b - A x|| / ||b|| (binary64, host) meets tol.  With left Jacobi the
+    monitor tests the preconditioned residual, which can stop well above tol
+    on a high-contrast operator; each further round restarts from the last
+    x with the monitor tolerance scaled down by the shortfall.  Returns the
+    summed time, the last status, the summed iterations, x and the rounds."""
+    from high_precision_blas1_b200 import _lib
+    plain_solve(torch, A, b, method, basis, tol, precond, max_iters=basis)  # warm-up
+    d = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (A.row_ptr, A.col_ind, A.val.astype(np.float64),
+                                                                    b.astype(np.float64), np.zeros(A.n))]
+    f = _lib.lib.hpb_csr_solve_f64
+    total, iters, mtol, st, rounds = 0.0, 0, tol, -1, 0
+    x = d[4].cpu().numpy()
+    while rounds < max_rounds:
+        rounds += 1
+        rep = _lib.hpb_solver_report()
+        p = _lib.solver_params(method, basis=basis, rel_tol=mtol, max_iters=max(basis, max_iters - iters),
+                               precond=precond)
+        t, st = _timed(torch, lambda: f(C.byref(p), A.n, A.nnz, *[a.data_ptr() for a in d], C.byref(rep), None, 0))
+        total += t
+        iters += rep.iters
+        x = d[4].cpu().numpy()
+        true = _rel(A, b, x)
+        if st != 0 or true <= tol or iters >= max_iters:
+            break
+        mtol *= 0.5 * tol / true
+    return total, st, iters, x, rounds
+
+
 def ir_solve(torch, A, b, inner, basis, precond="none", M=None, complex_=False, inner_tol=1e-5, max_iters=5000,
              max_refinements=40, warm=True, ilu_sweeps=0):
     """One refinement solve, timed; with warm, an untimed single-refinement
@@ -686,10 +720,19 @@ def bench_forms(torch, log=lambda *a: None):
         res["fp64_gmres30_jacobi"] = {"s": tj64, "status": stj64, "iters": rj64.iters,
                                       "true_rel_residual": _rel(A, b, xj64)}
         # the plain FP64 drop-in (the reference's path: every reduction returns
-        # to the host), GMRES(30) + Jacobi -- the comparison the target names
-        tpd, stpd, rpd, xpd = plain_solve(torch, A, b, "gmres", 30, SOLVER_TOL, precond="jacobi", max_iters=30000)
-        res["plain_dropin_fp64_gmres30_jacobi"] = {"s": tpd, "status": stpd, "iters": rpd.iters,
+        # to the host), GMRES(30) + Jacobi -- the comparison the target names,
+        # since unpreconditioned FP64 GMRES(30) does not reach 1e-10 on this
+        # family within the iteration budget.  Left Jacobi: its monitor tests
+        # the preconditioned residual, so the solve is continued until the
+        # true residual meets 1e-10.
+        tpd, stpd, ipd, xpd, rpd_rounds = plain_solve_to_true_tol(torch, A, b, "gmres", 30, SOLVER_TOL,
+                                                                  precond="jacobi", max_iters=30000)
+        res["plain_dropin_fp64_gmres30_jacobi"] = {"s": tpd, "status": stpd, "iters": ipd, "rounds": rpd_rounds,
                                                    "true_rel_residual": _rel(A, b, xpd)}
+        tp1 = plain_solve(torch, A, b, "gmres", 30, SOLVER_TOL, precond="jacobi", max_iters=30000)
+        res["plain_dropin_fp64_gmres30_jacobi_monitor_only"] = {
+            "s": tp1[0], "status": tp1[1], "iters": tp1[2].iters, "true_rel_residual": _rel(A, b, tp1[3]),
+            "note": "stops on the preconditioned residual; not a 1e-10 solve"}
         # one binary32 GMRES(30) cycle per refinement, same 30000-iteration budget
         for pc, sw in (("none", 0), ("jacobi", 0), ("ilu0", 2)):
             t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond=pc, inner_tol=0.0, max_iters=0,
@@ -713,7 +756,13 @@ def bench_forms(torch, log=lambda *a: None):
                 # plain FP64 without a preconditioner may not converge within the budget: then no ratio
                 res["speedup_learned_vs_plain_fp64"] = t64 / (t + tb) if st64 == 0 else None
                 res["speedup_learned_vs_fp64_jacobi"] = tj64 / (t + tb) if stj64 == 0 else None
-                res["speedup_learned_vs_plain_dropin_fp64_jacobi"] = tpd / (t + tb) if stpd == 0 else None
+                res["speedup_learned_vs_plain_dropin_fp64_jacobi"] = (
+                    tpd / (t + tb) if stpd == 0 and _rel(A, b, xpd) <= SOLVER_TOL else None)
+                # every form that reached a 1e-10 true residual, fastest first
+                cands = {k: v["s"] + v.get("build_s", 0.0) for k, v in res.items()
+                         if isinstance(v, dict) and v.get("status") == 0 and "s" in v
+                         and v.get("true_rel_residual", 1.0) <= 1.05 * SOLVER_TOL}
+                res["reached_1e-10_by_time"] = sorted(cands.items(), key=lambda kv: kv[1])
         out["learned_pc_gmres30_lognormal96"] = res
     except Exception as e:
         out["learned_pc_gmres30_lognormal96"] = {"error": repr(e)}

@@ -148,6 +148,8 @@ _sig("hpb_csr_tri_create", C.c_int, [P, C.c_int, I32, I64, P, P, C.POINTER(P)])
 _sig("hpb_csr_tri_destroy", C.c_int, [P])
 _sig("hpb_csr_tri_info", C.c_int, [P, C.POINTER(I32), C.POINTER(I32), C.POINTER(I64), C.POINTER(C.c_int)])
 _sig("hpb_csr_tri_check", C.c_int, [P, P])
+_sig("hpb_csr_tri_set_wait_limit", C.c_int, [P, C.c_uint64])
+_sig("hpb_csr_tri_test_withhold_row", C.c_int, [P, I32])
 for t in TYPES:
     _sig(f"hpb_csr_trsv_{t}", C.c_int, [P, P, C.c_int, P, SCALAR[t], P, P])
     _sig(f"hpb_csr_ilu0_{t}", C.c_int, [P, P, P])

@@ -11,13 +11,15 @@
 //   * each SpMV is fused with the Dot2 that consumes its output
 //     (u_{j+1} = A u_j with <rt, u_{j+1}>, r_{j+1} = A r_j with <rt, r_{j+1}>),
 //     and an optional Jacobi scaling (left preconditioning) is applied to
-//     the rows in the same kernel;
+//     the rows in the same kernel; the first of them also forms its operand
+//     u_j = r_j - beta u_j at each gathered column, and one pass after it
+//     stores the u updates and makes the r / x updates;
 //   * the MR part's modified Gram-Schmidt runs in l sweeps (right-looking:
 //     sweep k finishes r_k, projects r_{k-1} out of r_k..r_l and forms all
 //     inner products with r_k), each followed by a one-block combine;
 //   * the closing update of x, r_0, u_0 also produces ||r_0|| (the monitor's
 //     residual), <rt, r_0> (next cycle's rho) and the finiteness of x;
-//   * one cycle = 6l + 1 kernels, captured once into a CUDA graph
+//   * one cycle = 5l + 1 kernels, captured once into a CUDA graph
 //     and replayed; the host reads 16 bytes (||r_0||, breakdown, non-finite)
 //     per cycle to apply the monitor's test, as the reference does once per
 //     cycle (default_monitor.h:202-226).
@@ -132,12 +134,17 @@ __device__ void run_epi(const EpiArgs<S>& a, const S* v, bool bad) {
 
 // ------------------------------------------------------------ SpMV (+ Dot2)
 // y = D^{-1} (A x) (diag = D, may be null: no scaling), and <w, y> when DOT.
-template <class E, bool DOT>
+// UPD: the operand is the BiCG update u_j = r_j - beta u_j, formed at every
+// gathered column from x = u_j and xr = r_j as the update kernel forms it
+// (the same FMA, so the same bits); the updated u_j itself is stored by the
+// next kernel (k_upd_urx), which reads both vectors anyway.  This removes the
+// separate pass that wrote u_j to HBM only for this product to read it back.
+template <class E, bool DOT, bool UPD = false>
 __global__ void __launch_bounds__(kThreads)
 k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const E* __restrict__ val,
            const E* __restrict__ diag, const E* __restrict__ x, E* __restrict__ y, const E* __restrict__ w,
            typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
-           EpiArgs<typename scalar_of<E>::type> ea) {
+           EpiArgs<typename scalar_of<E>::type> ea, const E* __restrict__ xr = nullptr) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
     // rows in a grid-stride loop, consecutive threads on consecutive rows:
@@ -146,11 +153,21 @@ k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
     // 6 blocks per SM (B200, 1024^2: 20.5 us against 26.7 us for one row
     // per thread, whose 4096 blocks each hold their warps at the merge).
     typename pacc_of<E>::type pacc;
+    S nb = s_zero(S{});
+    if (UPD) nb = s_neg(ea.st->beta);
     const int32_t stride = gridDim.x * kThreads;
     for (int32_t r = blockIdx.x * kThreads + threadIdx.x; r < rows; r += stride) {
         const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
         S acc = s_zero(S{});
-        for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ldcsE(val, k)), to_s(ldgE(x, ldcsI(ci, k))), acc);
+        for (int32_t k = b; k < e; ++k) {
+            const int32_t c = ldcsI(ci, k);
+            S xv;
+            if (UPD)
+                xv = to_s(from_s<E>(s_fma(nb, to_s(ldgE(x, c)), to_s(ldgE(xr, c)))));
+            else
+                xv = to_s(ldgE(x, c));
+            acc = s_fma(to_s(ldcsE(val, k)), xv, acc);
+        }
         if (diag) acc = s_div(acc, to_s(ldE(diag, r)));
         E out = from_s<E>(acc);
         stE(y, r, out);
@@ -163,68 +180,76 @@ k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
 }
 
 // ------------------------------------------------------------ BiCG updates
-// u_i = r_i - beta u_i, i = 0..j
-template <class E>
-__global__ void __launch_bounds__(kThreads) k_upd_u(int64_t n, int j, Vecs<E> V,
-                                                    const BcgState<typename scalar_of<E>::type>* st) {
+// One pass per inner step j, after u_{j+1} = A (r_j - beta u_j):
+//   u_i = r_i - beta u_i          (i = 0..j; u_j's value equals the one the
+//                                  product gathered)
+//   r_i = r_i - alpha u_{i+1}     (i = 0..j, with the updated u_{i+1})
+//   x   = x + alpha u_0
+// The same FMAs, in the same order per element, as separate u and r/x
+// passes, so the same bits; every vector is read and written once.  J = j is
+// a template parameter so the row's values stay in registers.
+template <class E, int J>
+__global__ void __launch_bounds__(kThreads) k_upd_urx(int64_t n, Vecs<E> V, E* __restrict__ x,
+                                                      const BcgState<typename scalar_of<E>::type>* st) {
     using S = typename scalar_of<E>::type;
-    const S nb = s_neg(st->beta);
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    if constexpr (std::is_same<E, double>::value) {
-        // binary64: two rows per thread with 16-byte loads and stores (the
-        // same FMA per element)
-        bool vec = n % 2 == 0;
-        for (int i = 0; i <= j; ++i)
-            vec = vec && ((reinterpret_cast<uintptr_t>(V.u[i]) | reinterpret_cast<uintptr_t>(V.r[i])) & 15) == 0;
-        if (vec) {
-            for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 2; q += stride)
-                for (int i = 0; i <= j; ++i) {
-                    const double2 ui = reinterpret_cast<const double2*>(V.u[i])[q];
-                    const double2 ri = reinterpret_cast<const double2*>(V.r[i])[q];
-                    reinterpret_cast<double2*>(V.u[i])[q] = make_double2(fma(nb, ui.x, ri.x), fma(nb, ui.y, ri.y));
-                }
-            return;
-        }
-    }
-    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
-        for (int i = 0; i <= j; ++i) {
-            S ui = to_s(ldE(V.u[i], q));
-            stE(V.u[i], q, from_s<E>(s_fma(nb, ui, to_s(ldE(V.r[i], q)))));
-        }
-    }
-}
-
-// r_i = r_i - alpha u_{i+1}, i = 0..j ;  x = x + alpha u_0
-template <class E>
-__global__ void __launch_bounds__(kThreads) k_upd_rx(int64_t n, int j, Vecs<E> V, E* __restrict__ x,
-                                                     const BcgState<typename scalar_of<E>::type>* st) {
-    using S = typename scalar_of<E>::type;
-    const S al = st->alpha, nal = s_neg(st->alpha);
+    const S nb = s_neg(st->beta), al = st->alpha, nal = s_neg(st->alpha);
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     if constexpr (std::is_same<E, double>::value) {
         // binary64: two rows per thread with 16-byte loads and stores
-        bool vec = n % 2 == 0 && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(V.u[0])) & 15) == 0;
-        for (int i = 0; i <= j; ++i)
-            vec = vec && ((reinterpret_cast<uintptr_t>(V.u[i + 1]) | reinterpret_cast<uintptr_t>(V.r[i])) & 15) == 0;
+        bool vec = n % 2 == 0 && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(V.u[J + 1])) & 15) == 0;
+#pragma unroll
+        for (int i = 0; i <= J; ++i)
+            vec = vec && ((reinterpret_cast<uintptr_t>(V.u[i]) | reinterpret_cast<uintptr_t>(V.r[i])) & 15) == 0;
         if (vec) {
             for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 2; q += stride) {
-                for (int i = 0; i <= j; ++i) {
-                    const double2 u = reinterpret_cast<const double2*>(V.u[i + 1])[q];
-                    const double2 r = reinterpret_cast<const double2*>(V.r[i])[q];
-                    reinterpret_cast<double2*>(V.r[i])[q] = make_double2(fma(nal, u.x, r.x), fma(nal, u.y, r.y));
+                double2 u[J + 2], r[J + 1];
+#pragma unroll
+                for (int i = 0; i <= J; ++i) {
+                    u[i] = reinterpret_cast<const double2*>(V.u[i])[q];
+                    r[i] = reinterpret_cast<const double2*>(V.r[i])[q];
                 }
-                const double2 u0 = reinterpret_cast<const double2*>(V.u[0])[q];
+                u[J + 1] = reinterpret_cast<const double2*>(V.u[J + 1])[q];
                 const double2 xq = reinterpret_cast<const double2*>(x)[q];
-                reinterpret_cast<double2*>(x)[q] = make_double2(fma(al, u0.x, xq.x), fma(al, u0.y, xq.y));
+#pragma unroll
+                for (int i = 0; i <= J; ++i) {
+                    u[i] = make_double2(fma(nb, u[i].x, r[i].x), fma(nb, u[i].y, r[i].y));
+                    reinterpret_cast<double2*>(V.u[i])[q] = u[i];
+                }
+#pragma unroll
+                for (int i = 0; i <= J; ++i)
+                    reinterpret_cast<double2*>(V.r[i])[q] =
+                        make_double2(fma(nal, u[i + 1].x, r[i].x), fma(nal, u[i + 1].y, r[i].y));
+                reinterpret_cast<double2*>(x)[q] = make_double2(fma(al, u[0].x, xq.x), fma(al, u[0].y, xq.y));
             }
             return;
         }
     }
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
-        for (int i = 0; i <= j; ++i)
-            stE(V.r[i], q, from_s<E>(s_fma(nal, to_s(ldE(V.u[i + 1], q)), to_s(ldE(V.r[i], q)))));
-        stE(x, q, from_s<E>(s_fma(al, to_s(ldE(V.u[0], q)), to_s(ldE(x, q)))));
+        E u[J + 2];
+        S r[J + 1];
+#pragma unroll
+        for (int i = 0; i <= J; ++i) {
+            r[i] = to_s(ldE(V.r[i], q));
+            u[i] = from_s<E>(s_fma(nb, to_s(ldE(V.u[i], q)), r[i]));
+            stE(V.u[i], q, u[i]);
+        }
+        u[J + 1] = ldE(V.u[J + 1], q);
+#pragma unroll
+        for (int i = 0; i <= J; ++i) stE(V.r[i], q, from_s<E>(s_fma(nal, to_s(u[i + 1]), r[i])));
+        stE(x, q, from_s<E>(s_fma(al, to_s(u[0]), to_s(ldE(x, q)))));
     }
+}
+
+template <class E>
+void launch_upd_urx(int j, int grid, cudaStream_t s, int64_t n, const Vecs<E>& V, E* x,
+                    const BcgState<typename scalar_of<E>::type>* st) {
+#define HPB_URX(JJ) \
+    case JJ: k_upd_urx<E, JJ><<<grid, kThreads, 0, s>>>(n, V, x, st); break;
+    switch (j) {
+        HPB_URX(0) HPB_URX(1) HPB_URX(2) HPB_URX(3) HPB_URX(4) HPB_URX(5) HPB_URX(6) HPB_URX(7)
+        default: break;
+    }
+#undef HPB_URX
 }
 
 // ------------------------------------------------------------ MR part
@@ -448,10 +473,26 @@ inline int occupancy_of(const void* f) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, kThreads, 0) == cudaSuccess && o > 0 ? o : 1;
 }
 
+// blocks per SM of the BiCG update pass of step j (each step's own
+// occupancy: its register count grows with j)
+template <class E>
+int update_occupancy(int j) {
+    int occ = 1;
+#define HPB_OCC_U(JJ) \
+    case JJ: occ = occupancy_of(reinterpret_cast<const void*>(k_upd_urx<E, JJ>)); break;
+    switch (j) {
+        HPB_OCC_U(0) HPB_OCC_U(1) HPB_OCC_U(2) HPB_OCC_U(3) HPB_OCC_U(4) HPB_OCC_U(5) HPB_OCC_U(6) HPB_OCC_U(7)
+        default: break;
+    }
+#undef HPB_OCC_U
+    return occ;
+}
+
+// blocks per SM of the elementwise kernels outside the cycle
 template <class E>
 int light_occupancy() {
-    return std::min(occupancy_of(reinterpret_cast<const void*>(k_upd_u<E>)),
-                    occupancy_of(reinterpret_cast<const void*>(k_upd_rx<E>)));
+    return std::min(occupancy_of(reinterpret_cast<const void*>(k_residual_finish<E>)),
+                    occupancy_of(reinterpret_cast<const void*>(k_scale_by_inv_norm<E>)));
 }
 
 template <class E>
@@ -517,6 +558,7 @@ struct BcgPlan<E>::Impl {
     const E* val = nullptr;
     E* x = nullptr;
     int g_ew = 1, g_red = 1, g_sp = 1, g_spd = 1, g_nrm = 1, kernels = 0;
+    int g_upd[kMaxL] = {};
     SolverWorkspace ws;
     Vecs<E> V{};
     E *rt = nullptr, *tmp = nullptr, *diag = nullptr;
@@ -603,6 +645,9 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     const int64_t n = rows;
     const int64_t need = (n + kThreads - 1) / kThreads;
     P.g_ew = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * light_occupancy<E>())));
+    for (int j = 0; j < L; ++j)
+        P.g_upd[j] = int(std::max<int64_t>(1, std::min<int64_t>((n / 2 + kThreads - 1) / kThreads + 1,
+                                                                  int64_t(sms) * update_occupancy<E>(j))));
     P.g_red = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * reduction_occupancy<E>(L))));
     P.g_sp = int(std::max<int64_t>(1, need));
     P.g_spd = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * 6)));
@@ -679,10 +724,11 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     if (cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return HPB_ERROR_CUDA;
     for (int j = 0; j < L; ++j) {
-        k_upd_u<E><<<g_ew, kThreads, 0, s>>>(n, j, V, st);
-        k_spmv_dot<E, true><<<g_spd, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt, partials,
-                                                       ticket, badflag, EpiArgs<S>{st, drep, EPI_ALPHA, 0, j, L});
-        k_upd_rx<E><<<g_ew, kThreads, 0, s>>>(n, j, V, x, st);
+        // u_{j+1} = A (r_j - beta u_j) and alpha = rho / <rt, u_{j+1}>
+        k_spmv_dot<E, true, true><<<g_spd, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt,
+                                                             partials, ticket, badflag,
+                                                             EpiArgs<S>{st, drep, EPI_ALPHA, 0, j, L}, V.r[j]);
+        launch_upd_urx<E>(j, P.g_upd[j], s, n, V, x, st);
         if (j + 1 < L)
             k_spmv_dot<E, true><<<g_spd, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.r[j], V.r[j + 1], rt,
                                                            partials, ticket, badflag,
@@ -690,7 +736,7 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
         else
             k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.r[j], V.r[j + 1], nullptr,
                                                            partials, ticket, badflag, none);
-        kernels += 4;
+        kernels += 3;
     }
     for (int k = 1; k <= L; ++k) {
         launch_mgs_step<E>(L - k + 2, g_red, s, n, k, V, st, partials, EpiArgs<S>{st, drep, EPI_STEP, k, 0, L});

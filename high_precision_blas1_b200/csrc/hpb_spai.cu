@@ -123,52 +123,165 @@ __device__ __forceinline__ void load_weights(const __nv_bfloat16* __restrict__ w
     for (int k = threadIdx.x; k < kNumParams; k += blockDim.x) sw[k] = __bfloat162float(w[k]);
 }
 
-// out[i] = W3 relu(W2 relu(W1 x + b1) + b2) + b3 ; keeps h1, h2 (post-ReLU)
-__global__ void __launch_bounds__(kThreads)
+// ---------------------------------------------------------------- MLP on tensor cores
+// The per-row MLP as warp-level bf16 tensor-core products
+// (mma.sync.m16n8k16, binary32 accumulation): a warp owns 16 rows; the
+// accumulator fragment of one layer (16 rows x 8 outputs per n-tile) has
+// exactly the element layout of the next layer's A fragment (16 rows x 16
+// inputs per k-tile = two n-tiles), so activations stay in registers from
+// the features to the outputs.  Weights are bf16 (as stored); each binary32
+// activation x is carried as the bf16 pair hi = bf16(x), lo = bf16(x - hi)
+// and multiplied as two products, so a product keeps about 16 bits of x
+// (relative error ~2^-17 against binary32 activations) instead of bf16's 8.
+// The B fragments of all three layers are laid out once per block in shared
+// memory in fragment order (lane-contiguous 8-byte pairs: conflict-free).
+constexpr int kMmaWarps = 8;
+constexpr int kFragW1 = (kH / 8) * (kF / 16);   // n-tiles x k-tiles
+constexpr int kFragW2 = (kH / 8) * (kH / 16);
+constexpr int kFragW3 = (kO / 8) * (kH / 16);
+constexpr int kFragAll = kFragW1 + kFragW2 + kFragW3;  // 8 + 32 + 4 fragments x 32 lanes x 8 bytes
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo_k, float hi_k) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo_k, hi_k);  // .x (low half) = the lower k index
+    uint32_t r;
+    memcpy(&r, &v, 4);
+    return r;
+}
+// a = (hi, lo) bf16 pairs of two adjacent binary32 values
+__device__ __forceinline__ void split2(float v0, float v1, uint32_t& hi, uint32_t& lo) {
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(v0), h1 = __float2bfloat16_rn(v1);
+    __nv_bfloat162 h;
+    h.x = h0;
+    h.y = h1;
+    memcpy(&hi, &h, 4);
+    lo = pack_bf16(v0 - __bfloat162float(h0), v1 - __bfloat162float(h1));
+}
+
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint2 b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b.x), "r"(b.y));
+}
+
+// B fragment (k-tile kt, n-tile nt) of a K x N row-major bf16 weight matrix,
+// for lane (g = lane / 4, t = lane % 4): b0 = W[16kt + 2t .. +1][8nt + g],
+// b1 = W[16kt + 8 + 2t .. +1][8nt + g].
+__device__ __forceinline__ uint2 b_frag(const __nv_bfloat16* __restrict__ w, int N, int kt, int nt, int lane) {
+    const int g = lane >> 2, t = lane & 3, n = 8 * nt + g, k = 16 * kt + 2 * t;
+    auto at = [&](int kk) { return __bfloat162float(w[kk * N + n]); };
+    return make_uint2(pack_bf16(at(k), at(k + 1)), pack_bf16(at(k + 8), at(k + 9)));
+}
+
+// out[i] = W3 relu(W2 relu(W1 x + b1) + b2) + b3 ; keeps h1, h2 (post-ReLU,
+// binary32) for the backward pass when h1g / h2g are not null.
+__global__ void __launch_bounds__(kMmaWarps * 32)
 k_forward(int32_t rows, const float* __restrict__ feat, const __nv_bfloat16* __restrict__ w,
           float* __restrict__ h1g, float* __restrict__ h2g, float* __restrict__ out) {
-    extern __shared__ float smem[];
-    float* sw = smem;                        // kNumParams
-    float* sx = sw + kNumParams;             // kTile * kF
-    float* sh1 = sx + kTile * kF;            // kTile * kH
-    float* sh2 = sh1 + kTile * kH;           // kTile * kH
-    load_weights(w, sw);
-    const int ntiles = (rows + kTile - 1) / kTile;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int32_t r0 = t * kTile;
-        const int nr = min(kTile, rows - r0);
-        __syncthreads();
-        for (int k = threadIdx.x; k < kTile * kF; k += blockDim.x)
-            sx[k] = (k / kF) < nr ? feat[size_t(r0) * kF + k] : 0.f;
-        __syncthreads();
-        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x) {
-            const int r = k / kH, u = k % kH;
-            float z = sw[Params::B1 + u];
+    __shared__ uint2 sfrag[kFragAll * 32];
+    __shared__ float sbias[kH + kH + kO];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int f = warp; f < kFragAll; f += kMmaWarps) {
+        uint2 b;
+        if (f < kFragW1)
+            b = b_frag(w + Params::W1, kH, 0, f, lane);
+        else if (f < kFragW1 + kFragW2)
+            b = b_frag(w + Params::W2, kH, (f - kFragW1) % (kH / 16), (f - kFragW1) / (kH / 16), lane);
+        else
+            b = b_frag(w + Params::W3, kO, f - kFragW1 - kFragW2, 0, lane);
+        sfrag[f * 32 + lane] = b;
+    }
+    for (int k = threadIdx.x; k < kH; k += blockDim.x) {
+        sbias[k] = __bfloat162float(w[Params::B1 + k]);
+        sbias[kH + k] = __bfloat162float(w[Params::B2 + k]);
+    }
+    if (threadIdx.x < kO) sbias[2 * kH + threadIdx.x] = __bfloat162float(w[Params::B3 + threadIdx.x]);
+    __syncthreads();
+    const uint2* f1 = sfrag;                       // [nt]
+    const uint2* f2 = sfrag + kFragW1 * 32;        // [nt][kt]
+    const uint2* f3 = sfrag + (kFragW1 + kFragW2) * 32;  // [kt]
+    const int g = lane >> 2, t = lane & 3;
+    const int ntiles = (rows + 15) / 16;
+    for (int tile = blockIdx.x * kMmaWarps + warp; tile < ntiles; tile += gridDim.x * kMmaWarps) {
+        const int32_t ra = tile * 16 + g, rb = ra + 8;
+        const bool va = ra < rows, vb = rb < rows;
+        // ---- layer 1: A = features (16 rows x 16), one k-tile
+        float2 xa0 = va ? *reinterpret_cast<const float2*>(feat + size_t(ra) * kF + 2 * t) : make_float2(0.f, 0.f);
+        float2 xb0 = vb ? *reinterpret_cast<const float2*>(feat + size_t(rb) * kF + 2 * t) : make_float2(0.f, 0.f);
+        float2 xa1 = va ? *reinterpret_cast<const float2*>(feat + size_t(ra) * kF + 8 + 2 * t) : make_float2(0.f, 0.f);
+        float2 xb1 = vb ? *reinterpret_cast<const float2*>(feat + size_t(rb) * kF + 8 + 2 * t) : make_float2(0.f, 0.f);
+        uint32_t ah[4], al[4];
+        split2(xa0.x, xa0.y, ah[0], al[0]);
+        split2(xb0.x, xb0.y, ah[1], al[1]);
+        split2(xa1.x, xa1.y, ah[2], al[2]);
+        split2(xb1.x, xb1.y, ah[3], al[3]);
+        float h[kH / 8][4];
 #pragma unroll
-            for (int q = 0; q < kF; ++q) z = fmaf(sx[r * kF + q], sw[Params::W1 + q * kH + u], z);
-            sh1[k] = fmaxf(z, 0.f);
+        for (int nt = 0; nt < kH / 8; ++nt) {
+            const float b0 = sbias[8 * nt + 2 * t], b1 = sbias[8 * nt + 2 * t + 1];
+            h[nt][0] = b0; h[nt][1] = b1; h[nt][2] = b0; h[nt][3] = b1;
+            const uint2 bf = f1[nt * 32 + lane];
+            mma_bf16(h[nt], ah[0], ah[1], ah[2], ah[3], bf);
+            mma_bf16(h[nt], al[0], al[1], al[2], al[3], bf);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) h[nt][e] = fmaxf(h[nt][e], 0.f);
         }
-        __syncthreads();
-        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x) {
-            const int r = k / kH, u = k % kH;
-            float z = sw[Params::B2 + u];
-#pragma unroll 16
-            for (int q = 0; q < kH; ++q) z = fmaf(sh1[r * kH + q], sw[Params::W2 + q * kH + u], z);
-            sh2[k] = fmaxf(z, 0.f);
-        }
-        __syncthreads();
-        for (int k = threadIdx.x; k < kTile * kO; k += blockDim.x) {
-            const int r = k / kO, u = k % kO;
-            float z = sw[Params::B3 + u];
-#pragma unroll 16
-            for (int q = 0; q < kH; ++q) z = fmaf(sh2[r * kH + q], sw[Params::W3 + q * kO + u], z);
-            if (r < nr) out[size_t(r0 + r) * kO + u] = z;
-        }
-        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x)
-            if (k / kH < nr) {
-                if (h1g) h1g[size_t(r0) * kH + k] = sh1[k];
-                if (h2g) h2g[size_t(r0) * kH + k] = sh2[k];
+        if (h1g) {
+#pragma unroll
+            for (int nt = 0; nt < kH / 8; ++nt) {
+                if (va) *reinterpret_cast<float2*>(h1g + size_t(ra) * kH + 8 * nt + 2 * t) = make_float2(h[nt][0], h[nt][1]);
+                if (vb) *reinterpret_cast<float2*>(h1g + size_t(rb) * kH + 8 * nt + 2 * t) = make_float2(h[nt][2], h[nt][3]);
             }
+        }
+        // ---- layer 2: A = h1 (16 x 64), four k-tiles
+        uint32_t xh[kH / 16][4], xl[kH / 16][4];
+#pragma unroll
+        for (int kt = 0; kt < kH / 16; ++kt) {
+            split2(h[2 * kt][0], h[2 * kt][1], xh[kt][0], xl[kt][0]);
+            split2(h[2 * kt][2], h[2 * kt][3], xh[kt][1], xl[kt][1]);
+            split2(h[2 * kt + 1][0], h[2 * kt + 1][1], xh[kt][2], xl[kt][2]);
+            split2(h[2 * kt + 1][2], h[2 * kt + 1][3], xh[kt][3], xl[kt][3]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < kH / 8; ++nt) {
+            const float b0 = sbias[kH + 8 * nt + 2 * t], b1 = sbias[kH + 8 * nt + 2 * t + 1];
+            h[nt][0] = b0; h[nt][1] = b1; h[nt][2] = b0; h[nt][3] = b1;
+#pragma unroll
+            for (int kt = 0; kt < kH / 16; ++kt) {
+                const uint2 bf = f2[(nt * (kH / 16) + kt) * 32 + lane];
+                mma_bf16(h[nt], xh[kt][0], xh[kt][1], xh[kt][2], xh[kt][3], bf);
+                mma_bf16(h[nt], xl[kt][0], xl[kt][1], xl[kt][2], xl[kt][3], bf);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) h[nt][e] = fmaxf(h[nt][e], 0.f);
+        }
+        if (h2g) {
+#pragma unroll
+            for (int nt = 0; nt < kH / 8; ++nt) {
+                if (va) *reinterpret_cast<float2*>(h2g + size_t(ra) * kH + 8 * nt + 2 * t) = make_float2(h[nt][0], h[nt][1]);
+                if (vb) *reinterpret_cast<float2*>(h2g + size_t(rb) * kH + 8 * nt + 2 * t) = make_float2(h[nt][2], h[nt][3]);
+            }
+        }
+        // ---- layer 3: A = h2 (16 x 64), one n-tile of 8 outputs
+#pragma unroll
+        for (int kt = 0; kt < kH / 16; ++kt) {
+            split2(h[2 * kt][0], h[2 * kt][1], xh[kt][0], xl[kt][0]);
+            split2(h[2 * kt][2], h[2 * kt][3], xh[kt][1], xl[kt][1]);
+            split2(h[2 * kt + 1][0], h[2 * kt + 1][1], xh[kt][2], xl[kt][2]);
+            split2(h[2 * kt + 1][2], h[2 * kt + 1][3], xh[kt][3], xl[kt][3]);
+        }
+        float o[4];
+        o[0] = sbias[2 * kH + 2 * t]; o[1] = sbias[2 * kH + 2 * t + 1]; o[2] = o[0]; o[3] = o[1];
+#pragma unroll
+        for (int kt = 0; kt < kH / 16; ++kt) {
+            const uint2 bf = f3[kt * 32 + lane];
+            mma_bf16(o, xh[kt][0], xh[kt][1], xh[kt][2], xh[kt][3], bf);
+            mma_bf16(o, xl[kt][0], xl[kt][1], xl[kt][2], xl[kt][3], bf);
+        }
+        if (va) *reinterpret_cast<float2*>(out + size_t(ra) * kO + 2 * t) = make_float2(o[0], o[1]);
+        if (vb) *reinterpret_cast<float2*>(out + size_t(rb) * kO + 2 * t) = make_float2(o[2], o[3]);
     }
 }
 
@@ -495,10 +608,6 @@ int grow(hpb_spai* net, int32_t rows, int64_t nnz) {
     return HPB_SUCCESS;
 }
 
-size_t fwd_smem() {
-    using namespace hpb::spai;
-    return size_t(kNumParams + kTile * kF + 2 * kTile * kH) * sizeof(float);
-}
 size_t bwd_smem() {
     using namespace hpb::spai;
     return size_t(kNumParams + kTile * kF + 3 * kTile * kH + kTile * kO) * sizeof(float);
@@ -568,7 +677,15 @@ int forward_rows(hpb_spai* net, const hpb_spai_system& sys, float* diag, float* 
     int st = mean_log_diag(net, n, diag, scratch, &ml);
     if (st) return st;
     k_features<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, diag, float(ml), net->off, feat);
-    k_forward<<<kGridMlp, kThreads, fwd_smem()>>>(n, feat, net->wb, h1, h2, out);
+    {
+        int occ = 1, dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_forward, kMmaWarps * 32, 0);
+        const int need = (n + 16 * kMmaWarps - 1) / (16 * kMmaWarps);
+        const int grid = std::max(1, std::min(need, sms * std::max(occ, 1)));
+        k_forward<<<grid, kMmaWarps * 32>>>(n, feat, net->wb, h1, h2, out);
+    }
     hpb::count_launch(2);
     return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
 }
@@ -668,7 +785,6 @@ int hpb_spai_create(hpb_spai** out, int nslot, int dslot, const int* offsets, ui
         hpb_spai_destroy(net);
         return HPB_ERROR_CUDA;
     }
-    cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(fwd_smem()));
     cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bwd_smem()));
     *out = net;
     return HPB_SUCCESS;

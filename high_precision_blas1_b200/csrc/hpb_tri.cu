@@ -119,6 +119,9 @@ __device__ __forceinline__ unsigned long long gtimer() {
 struct Waiter {
     unsigned long long t0 = 0;
     long long it = 0;
+    unsigned long long limit = kWaitNs;
+    Waiter() = default;
+    __device__ __forceinline__ explicit Waiter(unsigned long long lim) : limit(lim) {}
     __device__ __forceinline__ bool check(int* err, int every_mask) {
         if ((++it & every_mask) != 0) return false;
         if (timed_out(err)) return true;
@@ -127,7 +130,7 @@ struct Waiter {
             t0 = now;
             return false;
         }
-        if (now - t0 > kWaitNs) {
+        if (now - t0 > limit) {
             atomicOr(err, kErrTimeout);
             return true;
         }
@@ -472,8 +475,8 @@ template <> struct Pub<cf> {
 
 // Wait (bounded) until x[j], as last loaded into v, is published.
 template <class E>
-__device__ __forceinline__ E await_value(const E* x, int32_t j, E v, int* err) {
-    Waiter w;
+__device__ __forceinline__ E await_value(const E* x, int32_t j, E v, int* err, unsigned long long lim) {
+    Waiter w(lim);
     while (Pub<E>::pending(v)) {
         if (w.check(err, 63)) break;
         v = Pub<E>::load(x, j);
@@ -617,7 +620,7 @@ __device__ __forceinline__ void gather_row(RowData<E>& r, int32_t p, int32_t p1,
 template <class E, bool UNIT>
 __device__ __forceinline__ E solve_row(const RowData<E>& r, int32_t base, int32_t m, const E* xs, const E* halo,
                                        const int32_t* __restrict__ ci, const E* __restrict__ val, const E* x,
-                                       int* err) {
+                                       int* err, unsigned long long lim) {
     E acc = r.rhs;
 #pragma unroll
     for (int k = 0; k < kPre; ++k)
@@ -630,7 +633,7 @@ __device__ __forceinline__ E solve_row(const RowData<E>& r, int32_t base, int32_
                 const E* slot = halo + (-sk - 2);
                 xj = vload(slot);
                 if (Pub<E>::pending(xj)) {
-                    Waiter w;
+                    Waiter w(lim);
                     do {
                         if (w.check(err, 255)) break;
                         xj = vload(slot);
@@ -638,13 +641,13 @@ __device__ __forceinline__ E solve_row(const RowData<E>& r, int32_t base, int32_
                 }
             } else {
                 const int32_t j = __ldg(ci + r.e0 + k);
-                xj = await_value(x, j, Pub<E>::load(x, j), err);
+                xj = await_value(x, j, Pub<E>::load(x, j), err, lim);
             }
             acc = fms(acc, r.v[k], xj);
         }
     for (int32_t e = r.e0 + kPre; e < r.e0 + r.nd; ++e) {
         const int32_t j = __ldg(ci + e), jl = j - base;
-        const E xj = (jl >= 0 && jl < m) ? xs[jl] : await_value(x, j, Pub<E>::load(x, j), err);
+        const E xj = (jl >= 0 && jl < m) ? xs[jl] : await_value(x, j, Pub<E>::load(x, j), err, lim);
         acc = fms(acc, ldE(val, e), xj);
     }
     if (!UNIT) acc = quot(acc, r.dg);
@@ -656,7 +659,8 @@ __global__ void __launch_bounds__(kTriThreads)
 k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int4* __restrict__ dcol,
        const int4* __restrict__ dslot, const int32_t* __restrict__ hoff, const int32_t* __restrict__ hrow,
        const int32_t* __restrict__ lvlptr, const int32_t* __restrict__ nlev, const int32_t* __restrict__ ci,
-       const E* __restrict__ val, E alpha, const E* __restrict__ b, E* x, unsigned* ticket, int* err) {
+       const E* __restrict__ val, E alpha, const E* __restrict__ b, E* x, unsigned* ticket, int* err,
+       unsigned long long lim, int32_t withhold) {
     constexpr int H = kHalo<E>::value;
     extern __shared__ __align__(16) unsigned char smraw[];
     E* xs = reinterpret_cast<E*>(smraw);
@@ -692,7 +696,7 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int4* __r
             row[k] = sl < nsl ? hr[sl] : 0;
             if (sl < nsl) pend |= 1u << k;
         }
-        Waiter w;
+        Waiter w(lim);
         while (pend != 0u) {
             E v[K];
 #pragma unroll
@@ -717,7 +721,7 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int4* __r
                 if (sl < nsl) pend |= 1u << (K - 1);
             }
             if (got) {
-                w = Waiter();
+                w = Waiter(lim);
             } else {
                 // nothing arrived in this pass: back off before polling the same
                 // lines again, so waiting receivers do not flood the L2 slices
@@ -770,10 +774,10 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int4* __r
             RowData<E> nxt;
             if (more) gather_row<E, UNIT>(nxt, q + 32 + lane, p1, base, m, desc, dcol, dslot, val, alpha, b);
             if (cur.row >= 0) {
-                const E acc = solve_row<E, UNIT>(cur, base, m, xs, halo, ci, val, x, err);
+                const E acc = solve_row<E, UNIT>(cur, base, m, xs, halo, ci, val, x, err, lim);
                 xs[cur.row - base] = acc;
                 if (more) {
-                    Pub<E>::store(x, cur.row, acc);  // more chunks follow in this level
+                    if (cur.row != withhold) Pub<E>::store(x, cur.row, acc);  // more chunks follow in this level
                 } else {
                     pub_row = cur.row;
                     pub_val = acc;
@@ -784,7 +788,7 @@ k_trsv(int32_t n, int32_t ntiles, const int4* __restrict__ desc, const int4* __r
         __syncwarp();
         level_arrive(l);
         // the global store after the in-tile announcement
-        if (pub_row >= 0) Pub<E>::store(x, pub_row, pub_val);
+        if (pub_row >= 0 && pub_row != withhold) Pub<E>::store(x, pub_row, pub_val);
     }
     // the warp that would take level L syncs on the last arrival, so that no
     // barrier is left half-arrived when the block ends
@@ -1077,7 +1081,8 @@ cudaError_t launch_trsv(const Plan& P, int unit, const E* val, E alpha, const E*
     auto k = P.upper ? (unit ? k_trsv<E, true, true> : k_trsv<E, true, false>)
                      : (unit ? k_trsv<E, false, true> : k_trsv<E, false, false>);
     k<<<P.ntiles, kTriThreads, sm, s>>>(P.n, P.ntiles, P.desc, P.dcol, P.dslot, P.hoff, P.hrow, P.lvlptr,
-                                             P.nlev, P.ci, val, alpha, b, x, P.flags + P.n, P.err);
+                                             P.nlev, P.ci, val, alpha, b, x, P.flags + P.n, P.err,
+                                             P.wait_ns ? P.wait_ns : kWaitNs, P.withhold_row);
     count_launch(2);
     return cudaGetLastError();
 }
@@ -1287,8 +1292,24 @@ int hpb_csr_tri_check(hpb_context* ctx, const hpb_csr_tri* tri) {
     int h = 0;
     HPB_CUDA_TRY(ctx, cudaMemcpyAsync(&h, tri->plan.err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     HPB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    if (h & hpb::tri::kErrTimeout)
+    if (h & hpb::tri::kErrTimeout) {
+        // reported once: the word is cleared for the solves that follow
+        HPB_CUDA_TRY(ctx, cudaMemsetAsync(tri->plan.err, 0, sizeof(int), ctx->stream));
+        HPB_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
         return hpb::set_error(ctx, HPB_ERROR_TIMEOUT, "hpb_csr_tri_check: a bounded device-side wait gave up");
+    }
+    return HPB_SUCCESS;
+}
+
+int hpb_csr_tri_set_wait_limit(hpb_csr_tri* tri, uint64_t ns) {
+    if (tri == nullptr) return HPB_ERROR_INVALID_VALUE;
+    tri->plan.wait_ns = ns;
+    return HPB_SUCCESS;
+}
+
+int hpb_csr_tri_test_withhold_row(hpb_csr_tri* tri, int32_t row) {
+    if (tri == nullptr || row < -1 || row >= tri->plan.n) return HPB_ERROR_INVALID_VALUE;
+    tri->plan.withhold_row = row;
     return HPB_SUCCESS;
 }
 

@@ -59,6 +59,8 @@ struct Plan {
     void* scratch = nullptr;        // n * 16 bytes, allocated on the first in-place solve
     int* err = nullptr;             // error bits
     int* err_row = nullptr;         // ILU(0): first row with a zero pivot
+    unsigned long long wait_ns = 0; // solve: limit of each bounded wait (0: the default, 4 s)
+    int32_t withhold_row = -1;      // solve, testing aid: this row's value is never published to x
 };
 
 int analyse(hpb_context* ctx, int upper, int32_t n, int64_t nnz, const int32_t* rp, const int32_t* ci, Plan* P);

@@ -405,8 +405,25 @@ int hpb_csr_trsv_sweeps_c64(hpb_context* ctx, const hpb_csr_tri* tri, int unit_d
 int hpb_csr_trsv_sweeps_c128(hpb_context* ctx, const hpb_csr_tri* tri, int unit_diag, const void* val,
                              hpb_c128 alpha, const void* b, void* x, int sweeps);
 /* Blocking: HPB_ERROR_TIMEOUT if a bounded device-side wait of an earlier
- * solve with this analysis gave up (cannot happen for a valid analysis). */
+ * solve with this analysis gave up (cannot happen for a valid analysis
+ * within the default limit); the condition is reported once and cleared, so
+ * later solves start clean.  Replaces the zero-pivot / structural check of
+ * csrsv2's info object (cusparseXcsrsv2_zeroPivot after the analysis and
+ * solve, common/csr/gpu_matrix.h:142-311). */
 int hpb_csr_tri_check(hpb_context* ctx, const hpb_csr_tri* tri);
+/* Limit, in ns of GPU time (%globaltimer), of each bounded wait of the
+ * solves with this analysis; 0 restores the default (4 s).  A solve whose
+ * wait runs out ends, leaves non-finite values where the missing
+ * dependencies were used, and hpb_csr_tri_check reports HPB_ERROR_TIMEOUT.
+ * No counterpart in the reference (csrsv2 has no device-side waits). */
+int hpb_csr_tri_set_wait_limit(hpb_csr_tri* tri, uint64_t ns);
+/* Testing aid for the timeout path: the solves with this analysis compute
+ * row `row` but never publish its value to x (-1: off), so the rows of
+ * other tiles that depend on it wait until the limit above and the solve
+ * reports HPB_ERROR_TIMEOUT.  No fault, no invalid address: the withheld
+ * value stays the sentinel the solve fills x with.  No counterpart in the
+ * reference. */
+int hpb_csr_tri_test_withhold_row(hpb_csr_tri* tri, int32_t row);
 /* ILU(0) in place (lower analysis of the pattern; every row must store its
  * diagonal): val := L\U, L unit lower (strictly lower entries stored), U
  * upper with its diagonal, the incomplete factors on A's pattern (IKJ

@@ -140,6 +140,11 @@ def ref_solver():
         lib.ref_cpu_solve_f64.argtypes = [C.c_int, C.c_int, P, P, P, P, P, C.c_int, D, C.c_int, C.c_int, C.c_int,
                                           C.POINTER(C.c_int), PD, PD]
         lib.ref_cpu_solve_f64.restype = C.c_int
+        if hasattr(lib, "ref_cpu_solve_hist_f64"):
+            lib.ref_cpu_solve_hist_f64.argtypes = [C.c_int, C.c_int, P, P, P, P, P, C.c_int, D, C.c_int, C.c_int,
+                                                   C.c_int, C.POINTER(C.c_int), PD, PD, P, C.c_int,
+                                                   C.POINTER(C.c_int)]
+            lib.ref_cpu_solve_hist_f64.restype = C.c_int
         _REF_SOLVER = lib
     return _REF_SOLVER
 
@@ -159,6 +164,28 @@ def ref_cpu_solve(method: int, A, b: np.ndarray, x0: np.ndarray, basis: int, rel
     ok = lib.ref_cpu_solve_f64(method, A.n, _ptr(A.row_ptr), _ptr(A.col_ind), _ptr(A.val), _ptr(bb), _ptr(x), basis,
                                rel_tol, max_iters, high_prec, threads, C.byref(it), C.byref(res), C.byref(sec))
     return bool(ok), it.value, res.value, sec.value, x
+
+
+def ref_cpu_solve_history(method: int, A, b: np.ndarray, x0: np.ndarray, basis: int, rel_tol: float,
+                          max_iters: int, high_prec: int = 1, threads: int = -1):
+    """As ref_cpu_solve, plus the reference monitor's convergence history:
+    returns (converged, iters, residual, seconds, x, history) with history an
+    (k, 2) array of (iteration, ||r||) pairs, one per monitor check."""
+    lib = ref_solver()
+    if lib is None or not hasattr(lib, "ref_cpu_solve_hist_f64"):
+        return None
+    x = np.ascontiguousarray(x0, dtype=np.float64).copy()
+    bb = np.ascontiguousarray(b, dtype=np.float64).copy()
+    it = C.c_int()
+    res = C.c_double()
+    sec = C.c_double()
+    cap = max_iters + 2
+    hist = np.zeros(2 * cap)
+    hl = C.c_int()
+    ok = lib.ref_cpu_solve_hist_f64(method, A.n, _ptr(A.row_ptr), _ptr(A.col_ind), _ptr(A.val), _ptr(bb), _ptr(x),
+                                    basis, rel_tol, max_iters, high_prec, threads, C.byref(it), C.byref(res),
+                                    C.byref(sec), _ptr(hist), cap, C.byref(hl))
+    return bool(ok), it.value, res.value, sec.value, x, hist[:2 * hl.value].reshape(-1, 2)
 
 
 # ----------------------------------------------------------------- helpers

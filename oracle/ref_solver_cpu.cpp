@@ -48,6 +48,16 @@ struct quiet_log : public utils::log_std {
 using vec_ops_t = cpu_vector_operations<double>;
 using mon_t = numerical_algos::lin_solvers::default_monitor<vec_ops_t, utils::log_std>;
 
+void copy_history(const std::vector<std::pair<int, double> >& h, double* out, int cap, int* len) {
+    if (out == nullptr) return;
+    int k = 0;
+    for (; k < int(h.size()) && k < cap; ++k) {
+        out[2 * k] = double(h[k].first);
+        out[2 * k + 1] = h[k].second;
+    }
+    if (len) *len = k;
+}
+
 }  // namespace
 
 extern "C" {
@@ -56,9 +66,23 @@ extern "C" {
 // monitor's iteration counter (BiCGStab(l) counts l per cycle).
 // threads: 0/1 -> sequential Dot2, >1 -> threaded_reduction with that many
 // threads (<0 -> hardware_concurrency).  Returns 1 if converged.
+// hist (optional, 2 * hist_cap doubles): the monitor's convergence history,
+// (iteration, ||r||) pairs as default_monitor records them
+// (default_monitor.h:206-212); *hist_len receives the number of pairs.
+int ref_cpu_solve_hist_f64(int method, int n, const int* rp, const int* ci, const double* v, double* b, double* x,
+                           int basis, double rel_tol, int max_iters, int high_prec, int threads, int* iters_out,
+                           double* resid_out, double* seconds_out, double* hist, int hist_cap, int* hist_len);
+
 int ref_cpu_solve_f64(int method, int n, const int* rp, const int* ci, const double* v, double* b, double* x,
                       int basis, double rel_tol, int max_iters, int high_prec, int threads, int* iters_out,
                       double* resid_out, double* seconds_out) {
+    return ref_cpu_solve_hist_f64(method, n, rp, ci, v, b, x, basis, rel_tol, max_iters, high_prec, threads,
+                                  iters_out, resid_out, seconds_out, nullptr, 0, nullptr);
+}
+
+int ref_cpu_solve_hist_f64(int method, int n, const int* rp, const int* ci, const double* v, double* b, double* x,
+                           int basis, double rel_tol, int max_iters, int high_prec, int threads, int* iters_out,
+                           double* resid_out, double* seconds_out, double* hist, int hist_cap, int* hist_len) {
     if (threads < 0) threads = int(std::thread::hardware_concurrency());
     vec_ops_t ops(size_t(n), high_prec, threads);
     if (high_prec)
@@ -76,18 +100,20 @@ int ref_cpu_solve_f64(int method, int n, const int* rp, const int* ci, const dou
     if (method == 0) {
         numerical_algos::lin_solvers::bicgstabl<csr_op, identity_prec, vec_ops_t, mon_t, utils::log_std> s(&ops, &log);
         s.set_basis_size(basis);
-        s.monitor().init(rel_tol, 0.0, max_iters);
+        s.monitor().init(rel_tol, 0.0, max_iters, 0, false, hist != nullptr);
         ok = s.solve(A, b, x);
         iters = s.monitor().iters_performed();
         resid = s.monitor().resid_norm();
+        copy_history(s.monitor().convergence_history(), hist, hist_cap, hist_len);
     } else {
         numerical_algos::lin_solvers::gmres<csr_op, identity_prec, vec_ops_t, mon_t, utils::log_std> s(&ops, &log);
         s.set_restarts(unsigned(basis));
         s.set_reorthogonalization(false);
-        s.monitor().init(rel_tol, 0.0, max_iters);
+        s.monitor().init(rel_tol, 0.0, max_iters, 0, false, hist != nullptr);
         ok = s.solve(A, b, x);
         iters = s.monitor().iters_performed();
         resid = s.monitor().resid_norm();
+        copy_history(s.monitor().convergence_history(), hist, hist_cap, hist_len);
     }
     if (seconds_out) *seconds_out = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (iters_out) *iters_out = iters;

@@ -13,6 +13,7 @@
 #include <common/csr/linear_operator.h>
 #include <common/csr/preconditioner.h>
 #include <common/gpu_vector_operations.h>
+#include <common/ogita/gpu_reduction_ogita.h>
 #include <numerical_algos/lin_solvers/bicgstabl.h>
 #include <numerical_algos/lin_solvers/default_monitor.h>
 #include <numerical_algos/lin_solvers/gmres.h>
@@ -110,3 +111,38 @@ int ref_dropin_solve_f64(int method, int rows, int64_t nnz, const int* rp, const
 }
 
 }  // extern "C"
+
+// The drop-in reducer class gpu_reduction_ogita<T, T*> (the reference's
+// common/ogita/gpu_reduction_ogita.h interface) on device vectors: what the
+// reference's own drivers call (test_vector_operations.cpp:100, :211, :304).
+// out: dot, sum (complex: re, im each), asum, norm -- 6 doubles.
+namespace {
+template <class T>
+void reducer_all(int64_t n, const void* x, const void* y, double* out) {
+    gpu_reduction_ogita<T, T*> r(static_cast<size_t>(n));
+    T* xp = static_cast<T*>(const_cast<void*>(x));
+    T* yp = static_cast<T*>(const_cast<void*>(y));
+    thrust::complex<double> d(r.dot(xp, yp)), s(r.sum(xp));
+    out[0] = d.real();
+    out[1] = d.imag();
+    out[2] = s.real();
+    out[3] = s.imag();
+    out[4] = double(r.asum(xp));
+    out[5] = double(r.norm(xp));
+}
+}  // namespace
+
+extern "C" int ref_dropin_reducer(int type, int64_t n, const void* x, const void* y, double* out) {
+    try {
+        switch (type) {
+            case 0: reducer_all<float>(n, x, y, out); break;
+            case 1: reducer_all<double>(n, x, y, out); break;
+            case 2: reducer_all<thrust::complex<float> >(n, x, y, out); break;
+            case 3: reducer_all<thrust::complex<double> >(n, x, y, out); break;
+            default: return -1;
+        }
+    } catch (...) {
+        return -2;
+    }
+    return 0;
+}

@@ -32,6 +32,7 @@ SRC = r'''
 #include <common/csr/preconditioner.h>
 #include <common/csr/gpu_ilu0_preconditioner.h>
 #include <common/csr/matrix_market_reader.h>
+#include <common/ogita/gpu_reduction_ogita.h>
 #include <numerical_algos/lin_solvers/default_monitor.h>
 #include <numerical_algos/lin_solvers/bicgstabl.h>
 #include <numerical_algos/lin_solvers/bicgstab.h>
@@ -82,6 +83,14 @@ template <class T> int run(int n) {
     reader.get_matrix_dim(rows, cols);
     reader.allocate_set_csr_pointers(rp_n, ci_n, nnz, rp, ci, val);
     free(rp); free(ci); free(val);
+    // the reducer class the reference's drivers instantiate directly
+    // (test_vector_operations.cpp:61, :100, :211, :304; obtain_condition_precision.cpp:81)
+    using gpu_reduction_ogita_t = gpu_reduction_ogita<T, T*>;
+    gpu_reduction_ogita_t reduciton_ogita(n);
+    T d = reduciton_ogita.dot(x, b);
+    T s = reduciton_ogita.sum(b);
+    typename gpu_reduction_ogita_type::type_complex_cast<T>::T a = reduciton_ogita.asum(b), nr = reduciton_ogita.norm(x);
+    ok = ok && (d == d) && (s == s) && (a == a) && (nr == nr);
     vec_ops.free_vector(x); vec_ops.free_vector(b);
     return ok;
 }

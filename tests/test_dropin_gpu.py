@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from gpu_utils import dev, host
+from gpu_utils import dev, host, red
 from high_precision_blas1_b200 import _lib, problems
 
 pytestmark = pytest.mark.gpu
@@ -100,3 +100,38 @@ def test_reference_solver_with_ilu0_matches_library_solver(gpu, method, basis, N
         assert np.allclose(host(x), host(x_ref), rtol=1e-12, atol=1e-14)
     # left preconditioning: the monitor tests the preconditioned residual
     assert rep.true_resid_norm <= 1e-6 * rep.true_rhs_norm
+
+
+@pytest.mark.parametrize("code,dtype,n", [(0, np.float32, 100_003), (1, np.float64, 1 << 20), (1, np.float64, 77),
+                                          (2, np.complex64, 50_001), (3, np.complex128, 65_537)])
+def test_dropin_reducer_class_returns_the_c_abi_bits(gpu, code, dtype, n):
+    """gpu_reduction_ogita<T, T*> from the drop-in headers (the class the
+    reference's drivers build directly, test_vector_operations.cpp:61/:100)
+    returns the C ABI's hi for dot / sum / asum / norm, bit for bit."""
+    ctx, torch = gpu
+    so = oracle.HERE / "_ref" / "libhpb_ref_dropin.so"
+    if not so.exists():
+        pytest.skip("oracle/_ref/libhpb_ref_dropin.so not built")
+    lib = C.CDLL(str(so))
+    lib.ref_dropin_reducer.argtypes = [C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(code * 1000 + n)
+    if np.issubdtype(dtype, np.complexfloating):
+        x = (rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)).astype(dtype)
+        y = (rng.uniform(-1, 1, n) + 1j * rng.uniform(-1, 1, n)).astype(dtype)
+    else:
+        x = rng.uniform(-1, 1, n).astype(dtype)
+        y = rng.uniform(-1, 1, n).astype(dtype)
+    dx, dy = dev(torch, x), dev(torch, y)
+    out = np.zeros(6)
+    torch.cuda.synchronize()
+    assert lib.ref_dropin_reducer(code, n, dx.data_ptr(), dy.data_ptr(), out.ctypes.data) == 0
+    real = np.float32 if dtype in (np.float32, np.complex64) else np.float64
+    cplx = np.issubdtype(dtype, np.complexfloating)
+    dot = red(ctx, "dot2", dx, dy)
+    s = red(ctx, "sum2", dx)
+    a = red(ctx, "asum2", dx)
+    nr = red(ctx, "nrm2", dx)
+    assert real(out[0]) == real(dot[0]) and real(out[2]) == real(s[0])
+    if cplx:
+        assert real(out[1]) == real(dot[1]) and real(out[3]) == real(s[1])
+    assert real(out[4]) == real(a[0]) and real(out[5]) == real(nr[0])

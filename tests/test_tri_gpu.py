@@ -328,3 +328,43 @@ def test_trsv_long_range_dependencies(gpu, t):
                 assert np.array_equal(got, want), (t, upper, unit)
         finally:
             tri.close()
+
+
+def test_trsv_bounded_wait_runs_out(gpu):
+    """The timeout path of the solve's bounded waits, without a fault: the
+    testing hook withholds the global publish of the first tile's last row,
+    so the second tile's rows that depend on it (row TILE + 127, through its
+    grid neighbour one line below) wait until the 1 ms
+    limit set on the analysis.  The launch ends, hpb_csr_tri_check reports
+    HPB_ERROR_TIMEOUT once, the first tile's other rows are exact, and the
+    next solve on the same analysis, hook off and default limit, is exact."""
+    import time
+    ctx, torch = gpu
+    L = _lib.lib
+    A = problems.convdiff2d(128)
+    rng = np.random.default_rng(3)
+    vd = dev(torch, A.val)
+    b = rng.standard_normal(A.n)
+    want = oracle.csr_trsv(A.row_ptr, A.col_ind, A.val, b, False, False, 1.0)
+    tri = Tri(ctx, torch, A, False)
+    try:
+        assert tri.info()[0] == 2
+        assert L.hpb_csr_tri_set_wait_limit(tri.h, 1_000_000) == 0
+        assert L.hpb_csr_tri_test_withhold_row(tri.h, TILE - 1) == 0
+        assert L.hpb_csr_tri_test_withhold_row(tri.h, A.n) != 0  # out of range refused
+        bd = dev(torch, b)
+        xd = torch.zeros_like(bd)
+        t0 = time.perf_counter()
+        ctx.check(L.hpb_csr_trsv_f64(ctx.h, tri.h, 0, vd.data_ptr(), 1.0, bd.data_ptr(), xd.data_ptr()), "trsv")
+        assert L.hpb_csr_tri_check(ctx.h, tri.h) == -9  # HPB_ERROR_TIMEOUT
+        assert time.perf_counter() - t0 < 2.0  # ended near the 1 ms limit, far below the 4 s default
+        x = host(xd)
+        assert np.array_equal(x[:TILE - 1], want[:TILE - 1])
+        assert not np.isfinite(x[TILE - 1]) and not np.isfinite(x[TILE + 127])
+        assert L.hpb_csr_tri_check(ctx.h, tri.h) == 0  # reported once
+        assert L.hpb_csr_tri_test_withhold_row(tri.h, -1) == 0
+        assert L.hpb_csr_tri_set_wait_limit(tri.h, 0) == 0
+        got = trsv(ctx, torch, tri, "f64", vd, b, False)
+        assert np.array_equal(got, want)
+    finally:
+        tri.close()
