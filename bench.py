@@ -745,7 +745,10 @@ def bench_forms(torch, log=lambda *a: None):
             offs, dslot = spai.stencil7(96)
             net = spai.SpaiNet(offs, dslot)
             net.set_weights(np.load(wfile))
-            tb, M = _timed(torch, lambda: net.assemble(torch, spai.DeviceCSR(torch, A)))
+            D5 = spai.DeviceCSR(torch, A)  # the matrix on the device before the timed build
+            net.assemble(torch, D5)  # warm-up (module load, workspace)
+            tb, M = _timed(torch, lambda: net.assemble(torch, D5))
+            res["spai_build"] = spai_build_roofline(A, tb)
             t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond="matrix", M=M, inner_tol=0.0, max_iters=0,
                                    max_refinements=1000)
             res["fp32_dot2_gmres30_refined_learned_spai"] = {
@@ -787,6 +790,19 @@ def bench_forms(torch, log=lambda *a: None):
     except Exception as e:
         out["ilu0_convdiff1024"] = {"error": repr(e)}
     return out
+
+
+def spai_build_roofline(A, t):
+    """Algorithmic HBM bytes of one learned-SPAI build (diagonal, features,
+    MLP, assembly) over the achieved time: A's pattern and values read by the
+    diagonal, feature and assembly passes (8 B per entry + 4 B per row
+    each), the 16 binary32 features written and read, the 8 binary32 outputs
+    written and read, M's values written."""
+    hbm, _ = peaks()
+    a_pass = 8.0 * A.nnz + 4.0 * (A.n + 1)
+    alg = 3 * a_pass + 2 * 64.0 * A.n + 2 * 32.0 * A.n + 4.0 * A.nnz
+    return {"s": t, "algorithmic_bytes": alg, "achieved_GBs": alg / t / 1e9, "frac_of_hbm": alg / t / 1e9 / hbm,
+            "mlp_gflop": 2.0 * A.n * (16 * 64 + 64 * 64 + 64 * 8) / 1e9}
 
 
 def ilu0_probe(torch, A, reps=10):
@@ -867,7 +883,98 @@ def dot2_probe(torch, L, ctx, reps=200):
     return {"workload": "dot2 f64 GenDot n=1048576 cond~1e20, 16 pairs rotated (268 MB > L2)",
             "value": gbs, "unit": "GB/s", "us_per_call": us, "frac_of_hbm": gbs / hbm, "peak_source": src,
             "graph_replay": dot2_graph_replay(torch, L, xs, ys, n),
-            "by_n": dot2_by_n(torch, L, ctx)}
+            "by_n": dot2_by_n(torch, L, ctx),
+            "same_box": dot2_same_box(torch, L, ctx),
+            "floors": dot2_floors(torch, L, ctx, xs, ys, n)}
+
+
+def _events_us(torch, fn, calls, rounds=5):
+    """Best-of-rounds CUDA-event time per call of `calls` back-to-back calls."""
+    stream = torch.cuda.current_stream()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    best = float("inf")
+    for _ in range(rounds):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for i in range(calls):
+            fn(i)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e3 / calls)
+    return best
+
+
+def dot2_same_box(torch, L, ctx, calls=200):
+    """The reference's own GPU Dot2 (gpu_reduction_ogita<double, double*>::dot,
+    its two-pass kernels built for sm_100a from its sources, oracle/_ref)
+    beside this library's, per call, on the same device data: both by value
+    (the reference's API returns the value to the host: two launches and two
+    blocking copies per call; here one launch and a result written to pinned
+    memory) and this library's device-resident call back to back.  Only
+    n <= 4,194,304: above it the reference's in-place second pass races."""
+    import oracle
+    lib = oracle.ref_gpu()
+    if lib is None or not hasattr(lib, "ref_gpu_reducer_f64_create"):
+        return {"unavailable": "oracle/_ref/libhpb_ref_gpu.so (the reference's GPU reductions) not built"}
+    lib.ref_gpu_reducer_f64_create.restype = C.c_void_p
+    lib.ref_gpu_reducer_f64_create.argtypes = [C.c_int64]
+    lib.ref_gpu_reducer_f64_dot.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ref_gpu_reducer_f64_destroy.argtypes = [C.c_void_p]
+    hbm, _ = peaks()
+    res = {}
+    for lg in (20, 22):
+        n = 1 << lg
+        R = max(2, int(np.ceil(2.0 * L2_BYTES / (16.0 * n))))
+        g = torch.Generator(device="cuda").manual_seed(100 + lg)
+        xs = [torch.rand(n, dtype=torch.float64, device="cuda", generator=g) - 0.5 for _ in range(R)]
+        ys = [torch.rand(n, dtype=torch.float64, device="cuda", generator=g) - 0.5 for _ in range(R)]
+        h = lib.ref_gpu_reducer_f64_create(n)
+        o_ref = np.zeros(2)
+        o_hpb = np.zeros(4)
+        od = torch.zeros(4, dtype=torch.float64, device="cuda")
+        try:
+            fr = lambda i: lib.ref_gpu_reducer_f64_dot(h, xs[i % R].data_ptr(), ys[i % R].data_ptr(),
+                                                       o_ref.ctypes.data)
+            fh = lambda i: L.hpb_dot2_f64_host(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(),
+                                               o_hpb.ctypes.data)
+            fd = lambda i: L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(), od.data_ptr())
+            for i in range(10):
+                fr(i), fh(i), fd(i)
+            t_ref = _events_us(torch, fr, calls)
+            t_hpb = _events_us(torch, fh, calls)
+            t_dev = _events_us(torch, fd, calls)
+        finally:
+            lib.ref_gpu_reducer_f64_destroy(h)
+        gb = lambda us: 16.0 * n / (us * 1e-6) / 1e9
+        res[f"n=2^{lg}"] = {
+            "reference_by_value_us": t_ref, "reference_GBs": gb(t_ref),
+            "hpb_by_value_us": t_hpb, "hpb_by_value_GBs": gb(t_hpb),
+            "hpb_device_us": t_dev, "hpb_device_GBs": gb(t_dev), "hpb_device_frac_of_hbm": gb(t_dev) / hbm,
+            "speedup_by_value": t_ref / t_hpb,
+            "same_value": bool(o_ref[0] == o_hpb[0])}
+        del xs, ys
+    return res
+
+
+def dot2_floors(torch, L, ctx, xs, ys, n, calls=200):
+    """What bounds one launch at 16.8 MB: back-to-back launches of a library
+    kernel with no work (hpb_fill_f64 of one element: the launch floor), the
+    plain FMA dot over the same pair (hpb_dot_f64: the same single-pass
+    combine without the error-free transformations), beside Dot2."""
+    R = len(xs)
+    one = torch.zeros(1, dtype=torch.float64, device="cuda")
+    od = torch.zeros(4, dtype=torch.float64, device="cuda")
+    t_launch = _events_us(torch, lambda i: L.hpb_fill_f64(ctx.h, 1, 0.0, one.data_ptr()), calls)
+    t_plain = _events_us(torch, lambda i: L.hpb_dot_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(),
+                                                        od.data_ptr()), calls)
+    t_dot2 = _events_us(torch, lambda i: L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(),
+                                                        od.data_ptr()), calls)
+    hbm, _ = peaks()
+    return {"launch_floor_us": t_launch, "plain_dot_us": t_plain, "dot2_us": t_dot2,
+            "transfer_at_peak_us": 16.0 * n / (hbm * 1e9) * 1e6,
+            "note": "one launch at 16.8 MB: launch floor + HBM transfer at the measured peak bound a single-pass "
+                    "reduction from below; the plain dot shows what the compensation itself costs"}
 
 
 def dot2_graph_replay(torch, L, xs, ys, n, calls=64, reps=10):
@@ -993,6 +1100,11 @@ def main():
                          "the triangular-solve kernel for ncu)")
     ap.add_argument("--profile-spmv-dot2", type=int, default=0, metavar="K",
                     help="profiling aid: K launches of hpb_csr_spmv_dot2_f64 on the config-2 matrix, then exit")
+    ap.add_argument("--profile-dot2", type=int, default=0, metavar="K",
+                    help="profiling aid: K back-to-back Dot2 calls at n = 2^20 over 16 rotated GenDot pairs, then exit")
+    ap.add_argument("--profile-spai", type=int, default=0, metavar="K",
+                    help="profiling aid: K learned-SPAI builds (features, MLP, assembly) on the config-5 96^3 "
+                         "system, then exit")
     ap.add_argument("--profile-method", choices=["bicgstabl", "gmres"], default="bicgstabl",
                     help="with --profile-solve: BiCGStab(4) on the config-2 system, or GMRES(30) + Jacobi on the "
                          "config-5 lognormal 96^3 system")
@@ -1024,6 +1136,34 @@ def main():
         from high_precision_blas1_b200 import problems
         r = ilu0_probe(torch, problems.convdiff2d(1024), reps=args.profile_trsv)
         print(f"profile trsv: lower {r['lower']['solve_us']:.1f} us, upper {r['upper']['solve_us']:.1f} us per solve")
+        return
+    if args.profile_dot2 > 0:
+        from high_precision_blas1_b200 import Context, _lib
+        n = 1 << 20
+        x = np.zeros(n)
+        y = np.zeros(n)
+        _lib.lib.hpb_gendot_f64(1, n, 1e20, x.ctypes.data, y.ctypes.data, None)
+        xs = [torch.from_numpy(x).cuda() for _ in range(16)]
+        ys = [torch.from_numpy(y).cuda() for _ in range(16)]
+        out = torch.zeros(4, dtype=torch.float64, device="cuda")
+        with Context(0, torch.cuda.current_stream().cuda_stream) as ctx:
+            us = _events_us(torch, lambda i: ctx.check(_lib.lib.hpb_dot2_f64(ctx.h, n, xs[i % 16].data_ptr(),
+                                                                              ys[i % 16].data_ptr(), out.data_ptr())),
+                            args.profile_dot2, rounds=1)
+        print(f"profile dot2: {us:.2f} us per call, result {float(out[0].item())!r}")
+        return
+    if args.profile_spai > 0:
+        from high_precision_blas1_b200 import spai
+        A = spai.family(96, seed=424242)
+        offs, dslot = spai.stencil7(96)
+        net = spai.SpaiNet(offs, dslot)
+        net.set_weights(np.load(spai.WEIGHTS_FILE))
+        D5 = spai.DeviceCSR(torch, A)
+        net.assemble(torch, D5)
+        t, _ = _timed(torch, lambda: [net.assemble(torch, D5) for _ in range(args.profile_spai)])
+        net.close()
+        r = spai_build_roofline(A, t / args.profile_spai)
+        print(f"profile spai: {r['s'] * 1e3:.3f} ms per build, {r['achieved_GBs']:.0f} GB/s algorithmic")
         return
     if args.profile_spmv_dot2 > 0:
         from high_precision_blas1_b200 import Context, _lib

@@ -29,8 +29,7 @@ struct hpb_context {
     double* result_slot = nullptr;   // device: 16 doubles for blocking calls
     double* host_slot = nullptr;     // pinned host: 16 doubles
     int* flag_dev = nullptr;         // device: flags for isfinite
-    unsigned int* red_sync = nullptr;  // device: reduction epoch [0], status [1], per-block flags [32, 32 + max_blocks)
-    unsigned int host_seq = 0;         // by-value reductions: sequence number of the last result delivered to host_slot
+    unsigned int* red_ticket = nullptr;  // device: the reductions' ticket counter (its own 128-byte line)
     char last_error[512] = {0};
 };
 

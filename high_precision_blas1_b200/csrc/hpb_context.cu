@@ -56,18 +56,18 @@ int hpb_create(hpb_context** out, int device, void* stream) {
         cudaMalloc(reinterpret_cast<void**>(&ctx->ticket), 64 * sizeof(unsigned int)) != cudaSuccess ||
         cudaMalloc(reinterpret_cast<void**>(&ctx->result_slot), 16 * sizeof(double)) != cudaSuccess ||
         cudaMalloc(reinterpret_cast<void**>(&ctx->flag_dev), 16 * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(reinterpret_cast<void**>(&ctx->red_sync), (32 + size_t(ctx->max_blocks)) * sizeof(unsigned int)) !=
-            cudaSuccess ||
+        cudaMalloc(reinterpret_cast<void**>(&ctx->red_ticket), 32 * sizeof(unsigned int)) != cudaSuccess ||
         cudaMallocHost(reinterpret_cast<void**>(&ctx->host_slot), 16 * sizeof(double)) != cudaSuccess) {
         hpb_destroy(ctx);
         cudaGetLastError();
         return HPB_ERROR_OUT_OF_MEMORY;
     }
+    memset(ctx->host_slot, 0, 16 * sizeof(double));  // by-value results: no stale sequence flag
     // The ticket counters start at zero; each reduction's last block resets
     // its counter, so no per-call memset is needed.
     if (cudaMemset(ctx->ticket, 0, 64 * sizeof(unsigned int)) != cudaSuccess ||
         cudaMemset(ctx->flag_dev, 0, 16 * sizeof(int)) != cudaSuccess ||
-        cudaMemset(ctx->red_sync, 0, (32 + size_t(ctx->max_blocks)) * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMemset(ctx->red_ticket, 0, 32 * sizeof(unsigned int)) != cudaSuccess ||
         cudaDeviceSynchronize() != cudaSuccess) {
         hpb_destroy(ctx);
         return HPB_ERROR_CUDA;
@@ -84,7 +84,7 @@ int hpb_destroy(hpb_context* ctx) {
     if (ctx->ticket) cudaFree(ctx->ticket);
     if (ctx->result_slot) cudaFree(ctx->result_slot);
     if (ctx->flag_dev) cudaFree(ctx->flag_dev);
-    if (ctx->red_sync) cudaFree(ctx->red_sync);
+    if (ctx->red_ticket) cudaFree(ctx->red_ticket);
     if (ctx->host_slot) cudaFreeHost(ctx->host_slot);
     delete ctx;
     return HPB_SUCCESS;

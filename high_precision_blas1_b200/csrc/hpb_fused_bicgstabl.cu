@@ -26,6 +26,7 @@
 // Storage E in {float, double, complex<float>, complex<double>}; scalars and
 // reductions in binary64 (complex<binary64>).
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <cmath>
 #include <type_traits>
@@ -574,7 +575,17 @@ struct BcgPlan<E>::Impl {
     double* dhist = nullptr;    // device: 2 kLoopChunk
     MonState* hmon = nullptr;   // pinned
     double* hhist = nullptr;    // pinned: 2 kLoopChunk
+    bool plain_graph = false;   // profiling aid: one plain graph per cycle, monitor on the host
 };
+
+// Profiling aid: with HPB_FUSED_PLAIN_GRAPH=1 in the environment the cycle is
+// captured as a plain CUDA graph launched once per cycle and the monitor's
+// test runs on the host (the same kernels and results; ncu lists kernels of
+// plain graphs but not those inside a conditional node's body).
+inline bool fused_plain_graph() {
+    const char* v = std::getenv("HPB_FUSED_PLAIN_GRAPH");
+    return v != nullptr && v[0] == '1';
+}
 
 // End of a cycle inside the loop graph: the host loop's test, then the
 // loop's condition.  Every path reaches the one cudaGraphSetConditional
@@ -708,21 +719,29 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     E* rt = P.rt;
     EpiArgs<S> none{st, drep, EPI_NONE, 0, 0, L};
     int kernels = 0;
+    P.plain_graph = fused_plain_graph();
     // the loop graph: a WHILE node whose body is one cycle + the monitor
-    if (cudaGraphCreate(&ws.graph, 0) != cudaSuccess) return HPB_ERROR_CUDA;
-    cudaGraphConditionalHandle cond;
-    if (cudaGraphConditionalHandleCreate(&cond, ws.graph, 1u, cudaGraphCondAssignDefault) != cudaSuccess)
-        return HPB_ERROR_CUDA;
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = cond;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    cudaGraphNode_t loop_node;
-    if (cudaGraphAddNode(&loop_node, ws.graph, nullptr, 0, &cp) != cudaSuccess) return HPB_ERROR_CUDA;
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    if (cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-        return HPB_ERROR_CUDA;
+    // (profiling aid: a plain graph of one cycle)
+    cudaGraphConditionalHandle cond{};
+    cudaGraph_t body = nullptr;
+    if (P.plain_graph) {
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HPB_ERROR_CUDA;
+    } else {
+        if (cudaGraphCreate(&ws.graph, 0) != cudaSuccess) return HPB_ERROR_CUDA;
+        if (cudaGraphConditionalHandleCreate(&cond, ws.graph, 1u, cudaGraphCondAssignDefault) != cudaSuccess)
+            return HPB_ERROR_CUDA;
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t loop_node;
+        if (cudaGraphAddNode(&loop_node, ws.graph, nullptr, 0, &cp) != cudaSuccess) return HPB_ERROR_CUDA;
+        body = cp.conditional.phGraph_out[0];
+        if (cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+            cudaSuccess)
+            return HPB_ERROR_CUDA;
+    }
     for (int j = 0; j < L; ++j) {
         // u_{j+1} = A (r_j - beta u_j) and alpha = rho / <rt, u_{j+1}>
         k_spmv_dot<E, true, true><<<g_spd, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt,
@@ -744,9 +763,14 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     }
     launch_final<E>(L, g_red, s, n, 1, V, x, rt, st, partials, ticket, badflag,
                     EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L});
-    k_monitor<<<1, 1, 0, s>>>(P.mon, drep, P.dhist, L, cond);
-    kernels += 2;
-    if (cudaStreamEndCapture(s, &body) != cudaSuccess) return HPB_ERROR_CUDA;
+    if (P.plain_graph) {
+        kernels += 1;
+        if (cudaStreamEndCapture(s, &ws.graph) != cudaSuccess) return HPB_ERROR_CUDA;
+    } else {
+        k_monitor<<<1, 1, 0, s>>>(P.mon, drep, P.dhist, L, cond);
+        kernels += 2;
+        if (cudaStreamEndCapture(s, &body) != cudaSuccess) return HPB_ERROR_CUDA;
+    }
     if (cudaGraphInstantiate(&ws.exec, ws.graph, 0) != cudaSuccess) return HPB_ERROR_CUDA;
     P.kernels = kernels;
     return HPB_SUCCESS;
@@ -814,6 +838,19 @@ int BcgPlan<E>::run(const E* b, hpb_solver_report* rep, double* hist, int cap) {
         return !valid || conv || iters >= p->max_iters;
     };
     bool finished = record();
+    while (!finished && P.plain_graph) {  // profiling aid: one graph launch and a host test per cycle
+        if (cudaGraphLaunch(P.ws.exec, s) != cudaSuccess ||
+            cudaMemcpyAsync(hrep, P.drep, sizeof(Report), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            return HPB_ERROR_CUDA;
+        count_launch(uint64_t(P.kernels));
+        iters += L;
+        if (hrep->breakdown) {
+            breakdown = true;
+            break;
+        }
+        finished = record();
+    }
     if (!finished) {
         // the cycles run on the device: each launch of the loop graph runs
         // cycles until the monitor stops (converged, non-finite, max_iters,

@@ -13,17 +13,16 @@
 //      (the tree rule of gpu_reduction_ogita_impl.cuh:527-600), then the
 //      block combines its warps the same way;
 //   3. each block stores its pair in the context's partials buffer and
-//      raises its flag (a release store of this launch's epoch); block 0's
-//      first warp, once its own share is done, merges the pairs as their
-//      flags come up -- lane l takes blocks l, l + 32, ... in order, then the
-//      lanes combine in a fixed tree -- and writes (hi, lo) = TwoSum(S, C).
+//      takes a ticket (an acquire-release atomic: no separate fence); the
+//      last block's first warp merges all partials -- lane l takes blocks
+//      l, l + 32, ... in order, all loads issued first, then the lanes
+//      combine in a fixed tree -- and writes (hi, lo) = TwoSum(S, C).
 //      Deterministic whatever order the blocks finish in; no host round
-//      trip, no second launch, no floating-point atomics.  The merge runs
-//      while the other blocks still stream, so after the last block's pair
-//      only one flag round trip and one warp tree remain (a last-block
-//      ticket put an atomic round trip, a partials round trip and a block
-//      tree after the last block: 2.3 us of 7.3 us at 16.8 MB on B200).
-//      The allocation-free entry point keeps the ticket form.
+//      trip, no second launch, no floating-point atomics.  (A combiner warp
+//      that merged each block's pair as its flag came up measured slower on
+//      B200: each lane's flag and partial loads form a chain of L2 round
+//      trips for the blocks that finish last.)  The allocation-free entry
+//      point keeps the older fence + ticket and block-wide merge.
 // float and complex<float> inputs accumulate per thread in binary32 (the
 // reference's arithmetic) and are widened to binary64 before the warp tree,
 // so every combine of compensation terms runs in binary64.
@@ -262,26 +261,16 @@ __device__ __forceinline__ Pack<E> ld16(const E* p, int64_t vi) {
 
 // ------------------------------------------------------------------ kernel
 constexpr int kRedThreads = 256;    // ticket form (allocation-free entry point)
-constexpr int kCombThreads = 512;   // combiner form (context entry points)
+constexpr int kCombThreads = 512;   // context entry points
 constexpr int kRedUnroll = 4;
-enum Tail { TAIL_TICKET = 0, TAIL_COMBINER = 1 };
-// Limit of the combiner's wait for one block's pair (GPU time): a block that
-// has not reported after this long means a broken launch; the result is
-// then NaN and bit 0 of the status word is set.
-constexpr unsigned long long kCombWaitNs = 1000000000ull;
+// TAIL_TICKET: fence + ticket, block-wide final merge (allocation-free entry
+// point); TAIL_WARP: acquire-release ticket, one-warp final merge.
+enum Tail { TAIL_TICKET = 0, TAIL_WARP = 1 };
 
-__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned int* p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_release_u32(unsigned int* p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned int* p, unsigned v) {
+    unsigned r;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(r) : "l"(p), "r"(v) : "memory");
+    return r;
 }
 
 template <class W>
@@ -308,8 +297,8 @@ __device__ __forceinline__ void write_result(double* o, W S, W C, int op) {
     }
 }
 
-// sync: TAIL_TICKET -- the ticket counter; TAIL_COMBINER -- the context's
-// red_sync words (epoch [0], status [1], block flags from [32]).
+// sync: the ticket counter.  host_flag (by-value calls): after the result,
+// the last block raises this pinned host word to host_seq.
 template <class E, int OP, bool VEC, int THREADS = kRedThreads, int TAIL = TAIL_TICKET>
 __global__ void __launch_bounds__(THREADS)
 reduce_kernel(int64_t n, const E* __restrict__ x, const E* __restrict__ y, void* __restrict__ partials,
@@ -321,9 +310,7 @@ reduce_kernel(int64_t n, const E* __restrict__ x, const E* __restrict__ y, void*
     constexpr bool COMP = op_is_comp(OP);
     constexpr int K = VEC ? VecOf<E>::k : 1;
     unsigned int* const ticket = sync;
-    pdl_enter();  // inputs and the sync words are read only after the previous kernel on the stream completed
-    // this launch's epoch: the previous launch's combiner stored it before that grid completed
-    const unsigned epoch = TAIL == TAIL_COMBINER ? __ldcg(sync) + 1u : 0u;
+    pdl_enter();  // inputs and the ticket are read only after the previous kernel on the stream completed
 
     Acc s{}, c{};
     const int64_t gtid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -371,44 +358,35 @@ reduce_kernel(int64_t n, const E* __restrict__ x, const E* __restrict__ y, void*
     block_combine<COMP>(ws, wc, sh);
 
     W* part = reinterpret_cast<W*>(partials);
-    if constexpr (TAIL == TAIL_COMBINER) {
-        unsigned int* flags = sync + 32;
+    if constexpr (TAIL == TAIL_WARP) {
         if (threadIdx.x == 0) {
             part[2 * blockIdx.x] = ws;
             part[2 * blockIdx.x + 1] = wc;
-            st_release_u32(flags + blockIdx.x, epoch);
+            // release: this thread's partial store is visible to the block
+            // that draws the last ticket; acquire: that block sees them all
+            am_last = atom_add_acq_rel(ticket, 1u) == gridDim.x - 1;
         }
-        if (blockIdx.x != 0 || threadIdx.x >= 32) return;
-        // block 0, warp 0: lane l merges the pairs of blocks l, l + 32, ...
-        // in order, each as soon as its flag carries this epoch
-        const int lane = threadIdx.x;
+        __syncthreads();
+        if (!am_last || threadIdx.x >= 32) return;
+        // last block, warp 0: lane l merges blocks l, l + 32, ... in order
+        const int lane = threadIdx.x, nb = int(gridDim.x);
         W S = wzero<W>(), C = wzero<W>();
-        bool bad = false;
-        for (int b = lane; b < int(gridDim.x) && !bad; b += 32) {
-            unsigned long long t0 = 0;
-            for (int it = 1; ld_acquire_u32(flags + b) != epoch; ++it) {
-                if ((it & 63) == 0) {
-                    const unsigned long long now = global_ns();
-                    if (t0 == 0) {
-                        t0 = now;
-                    } else if (now - t0 > kCombWaitNs) {
-                        bad = true;
-                        break;
-                    }
-                }
+        int b = lane;
+        for (; b + 96 < nb; b += 128) {
+            W sv[4], cv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                sv[u] = ldcg_w(part + 2 * (b + 32 * u));
+                cv[u] = ldcg_w(part + 2 * (b + 32 * u) + 1);
             }
-            if (!bad) merge<COMP>(S, C, ldcg_w(part + 2 * b), ldcg_w(part + 2 * b + 1));
+#pragma unroll
+            for (int u = 0; u < 4; ++u) merge<COMP>(S, C, sv[u], cv[u]);
         }
-        bad = __any_sync(0xffffffffu, bad);
+        for (; b < nb; b += 32) merge<COMP>(S, C, ldcg_w(part + 2 * b), ldcg_w(part + 2 * b + 1));
         warp_combine<COMP>(S, C);
         if (lane == 0) {
             write_result<W>(out, S, C, OP);
-            if (bad) {
-                const double qnan = __longlong_as_double(0x7ff8000000000000ll);
-                for (int k = 0; k < 4; ++k) out[k] = qnan;
-                atomicOr(sync + 1, 1u);
-            }
-            __stcg(sync, epoch);  // the next launch's blocks read it after this grid completed
+            *ticket = 0u;  // ready for the next launch on this stream (it starts after this grid completes)
             if (host_flag != nullptr) {
                 // by-value call: out is pinned host memory; the host polls the
                 // flag for this call's sequence number and then reads out
@@ -466,7 +444,7 @@ int max_blocks_for(const hpb_context* ctx) {
     if (per_sm == 0) {
         int b = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-                &b, reduce_kernel<E, OP, VEC, kCombThreads, TAIL_COMBINER>, kCombThreads, 0) != cudaSuccess ||
+                &b, reduce_kernel<E, OP, VEC, kCombThreads, TAIL_WARP>, kCombThreads, 0) != cudaSuccess ||
             b <= 0)
             b = 1;
         per_sm = b;
@@ -489,20 +467,19 @@ int launch_reduce(hpb_context* ctx, int64_t n, const E* x, const E* y, double* o
     const bool aligned = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(op_has_y(OP) ? y : x)) & 15) == 0;
     const int K = aligned ? VecOf<E>::k : 1;
     const int64_t work = (n / K + kRedUnroll - 1) / kRedUnroll;
-    // one resident wave at most: every block is running before the combiner
-    // waits (the grid is capped at the occupancy, which also bounds the flags)
+    // one resident wave at most (grid capped at the occupancy)
     if (aligned) {
         int grid = grid_for(ctx, work, kCombThreads, 1 << 20);
         int cap = max_blocks_for<E, OP, true>(ctx);
         if (grid > cap) grid = cap;
-        launch_pdl(ctx->stream, grid, kCombThreads, reduce_kernel<E, OP, true, kCombThreads, TAIL_COMBINER>, n, x, y,
-                   ctx->partials, ctx->red_sync, out, host_flag, host_seq);
+        launch_pdl(ctx->stream, grid, kCombThreads, reduce_kernel<E, OP, true, kCombThreads, TAIL_WARP>, n, x, y,
+                   ctx->partials, ctx->red_ticket, out, host_flag, host_seq);
     } else {
         int grid = grid_for(ctx, work, kCombThreads, 1 << 20);
         int cap = max_blocks_for<E, OP, false>(ctx);
         if (grid > cap) grid = cap;
-        launch_pdl(ctx->stream, grid, kCombThreads, reduce_kernel<E, OP, false, kCombThreads, TAIL_COMBINER>, n, x,
-                   y, ctx->partials, ctx->red_sync, out, host_flag, host_seq);
+        launch_pdl(ctx->stream, grid, kCombThreads, reduce_kernel<E, OP, false, kCombThreads, TAIL_WARP>, n, x,
+                   y, ctx->partials, ctx->red_ticket, out, host_flag, host_seq);
     }
     count_launch();
     return check_launch(ctx, name);
@@ -520,7 +497,12 @@ int launch_reduce_host(hpb_context* ctx, int64_t n, const E* x, const E* y, doub
     if (out_host == nullptr) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null output", name);
     double* hres = ctx->host_slot + 8;
     unsigned int* hflag = reinterpret_cast<unsigned int*>(ctx->host_slot + 12);
-    const unsigned seq = ++ctx->host_seq;
+    // Sequence numbers are unique across the process, not per context: a
+    // pinned slot recycled from a destroyed context may still hold one of
+    // that context's numbers, which a fresh per-context count would repeat.
+    static std::atomic<unsigned> g_host_seq{0};
+    unsigned seq = g_host_seq.fetch_add(1u, std::memory_order_relaxed) + 1u;
+    if (seq == 0u) seq = g_host_seq.fetch_add(1u, std::memory_order_relaxed) + 1u;
     int st = launch_reduce<E, OP>(ctx, n, x, y, hres, name, hflag, seq);
     if (st != HPB_SUCCESS) return st;
     const volatile unsigned int* f = hflag;
