@@ -259,7 +259,7 @@ __device__ __forceinline__ void block_merge(A (&acc)[ND], A* sh /* [ND][32] */) 
 }
 
 // Cross-block finish: block partials -> ticket -> the last block merges all
-// partials in block order and runs `epi(tot, bad)` on thread 0, where tot[d]
+// partials in a fixed order and runs `epi(tot, bad)` on thread 0, where tot[d]
 // is the merged (s, c) accumulator of dot d and bad = any block reported a
 // non-finite entry.
 template <int ND, class A, class Epi>
@@ -273,12 +273,15 @@ __device__ __forceinline__ void grid_finish_acc(A (&acc)[ND], bool bad, A* parti
 #pragma unroll
         for (int d = 0; d < ND; ++d) partials[size_t(d) * gridDim.x + blockIdx.x] = acc[d];
         if (any_bad) atomicOr(badflag, 1);
-        __threadfence();
-        am_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+        // acquire-release ticket: releases this thread's partial and flag
+        // stores to the block that draws the last ticket, which acquires
+        // all of them (the barrier below extends that to its other threads)
+        unsigned t;
+        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(t) : "l"(ticket) : "memory");
+        am_last = t == gridDim.x - 1;
     }
     __syncthreads();
     if (!am_last) return;
-    __threadfence();
     A tot[ND > 0 ? ND : 1];
 #pragma unroll
     for (int d = 0; d < ND; ++d) tot[d] = merge_partials<A>(partials + size_t(d) * gridDim.x, int(gridDim.x));

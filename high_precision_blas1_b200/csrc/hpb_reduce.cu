@@ -485,7 +485,13 @@ int launch_reduce(hpb_context* ctx, int64_t n, const E* x, const E* y, double* o
     return check_launch(ctx, name);
 }
 
-// By value: the kernel's combiner writes the result straight into the
+// Sequence numbers of by-value results: one counter for the whole process
+// (not per context or per kernel type), so a flag word left by any earlier
+// call -- of another reduction, or of a destroyed context whose pinned slot
+// was recycled -- never equals the number a new call waits for.
+std::atomic<unsigned> g_host_seq{0};
+
+// By value: the kernel's last block writes the result straight into the
 // context's pinned host slot and then raises a sequence flag there (system
 // scope); the host spins on the flag instead of a device-to-host copy plus a
 // stream synchronisation, so a call costs one launch and one write across
@@ -497,10 +503,6 @@ int launch_reduce_host(hpb_context* ctx, int64_t n, const E* x, const E* y, doub
     if (out_host == nullptr) return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: null output", name);
     double* hres = ctx->host_slot + 8;
     unsigned int* hflag = reinterpret_cast<unsigned int*>(ctx->host_slot + 12);
-    // Sequence numbers are unique across the process, not per context: a
-    // pinned slot recycled from a destroyed context may still hold one of
-    // that context's numbers, which a fresh per-context count would repeat.
-    static std::atomic<unsigned> g_host_seq{0};
     unsigned seq = g_host_seq.fetch_add(1u, std::memory_order_relaxed) + 1u;
     if (seq == 0u) seq = g_host_seq.fetch_add(1u, std::memory_order_relaxed) + 1u;
     int st = launch_reduce<E, OP>(ctx, n, x, y, hres, name, hflag, seq);

@@ -104,8 +104,10 @@ __global__ void k_features(int32_t rows, const int32_t* __restrict__ rp, const i
         }
     f[2 * (o.nslot - 1)] = logf(fabsf(dii)) - mean_log_diag;
     f[2 * (o.nslot - 1) + 1] = 1.f;
+    // the row's 64 bytes as four 16-byte stores (rows are 64-byte aligned)
+    float4* dst = reinterpret_cast<float4*>(feat + size_t(i) * kF);
 #pragma unroll
-    for (int k = 0; k < kF; ++k) feat[size_t(i) * kF + k] = f[k];
+    for (int k = 0; k < kF / 4; ++k) dst[k] = make_float4(f[4 * k], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]);
 }
 
 // Ah values on A's pattern
@@ -177,7 +179,7 @@ __device__ __forceinline__ uint2 b_frag(const __nv_bfloat16* __restrict__ w, int
 
 // out[i] = W3 relu(W2 relu(W1 x + b1) + b2) + b3 ; keeps h1, h2 (post-ReLU,
 // binary32) for the backward pass when h1g / h2g are not null.
-__global__ void __launch_bounds__(kMmaWarps * 32)
+__global__ void __launch_bounds__(kMmaWarps * 32, 3)
 k_forward(int32_t rows, const float* __restrict__ feat, const __nv_bfloat16* __restrict__ w,
           float* __restrict__ h1g, float* __restrict__ h2g, float* __restrict__ out) {
     __shared__ uint2 sfrag[kFragAll * 32];

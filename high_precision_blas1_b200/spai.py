@@ -170,6 +170,7 @@ def train(torch, n_systems=2000, N=24, epochs=3, batch=8, lr=3e-3, w_frob=1.0, w
         log(f"untrained (Jacobi): held-out loss {best:.5f}")
         rng = np.random.default_rng(seed)
         for ep in range(epochs):
+            te = time.time()
             order = rng.permutation(n_systems)
             tot = 0.0
             for b0 in range(0, n_systems, batch):
@@ -182,8 +183,8 @@ def train(torch, n_systems=2000, N=24, epochs=3, batch=8, lr=3e-3, w_frob=1.0, w
             vl = val_loss()
             if vl < best or not val:
                 best, best_w = vl, net.weights()
-            log(f"epoch {ep}: mean training loss {tot / n_systems:.5f}, held-out {vl:.5f} "
-                f"({time.time() - t0:.1f}s)")
+            log(f"epoch {ep}: mean training loss {tot / n_systems:.5f}, held-out {vl:.5f}, "
+                f"epoch {time.time() - te:.1f}s ({time.time() - t0:.1f}s total)")
     net.close()
     return best_w, hist
 
