@@ -261,7 +261,7 @@ void launch_upd_urx(int j, int grid, cudaStream_t s, int64_t n, const Vecs<E>& V
 // ...), so the results are the same; the L(L+1)/2 passes become L sweeps.
 //   k_mgs_step:   r_j -= tau[k-1][j] r_{k-1} for j = k..L (k > 1), then block
 //                 partials of <r_k, r_k>, <r_k, r_0>, <r_k, r_j> (j > k);
-//   k_mgs_finish: one block merges the partials in block order and sets
+//   k_mgs_finish: one block merges the partials in a fixed order and sets
 //                 sigma[k], gamma'_k, tau[k][j > k] (and, at k = L, gamma
 //                 and gamma'').
 // The combine is a separate launch (no ticket): the single-launch form with
@@ -310,8 +310,12 @@ k_mgs_step(int64_t n, int k, Vecs<E> V, const BcgState<typename scalar_of<E>::ty
         for (int d = 0; d < ND; ++d) partials[size_t(d) * gridDim.x + blockIdx.x] = acc[d];
 }
 
+// One block of 1024 threads: the ND x nb partials are one load round per
+// thread at the configured sizes (nb = one resident wave of the sweep).
+constexpr int kFinThreads = 1024;
+
 template <class S, int ND>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kFinThreads)
 k_mgs_finish(int nb, const typename acc_of<S>::type* __restrict__ partials, EpiArgs<S> ea) {
     using A = typename acc_of<S>::type;
     __shared__ A sh[ND * 32];
@@ -537,7 +541,7 @@ void launch_mgs_step(int nd, int grid, cudaStream_t s, int64_t n, int k, const V
 #define HPB_STEP(ND)                                                                         \
     case ND:                                                                                 \
         k_mgs_step<E, ND><<<grid, kThreads, 0, s>>>(n, k, V, st, partials);                  \
-        k_mgs_finish<S, ND><<<1, kThreads, 0, s>>>(grid, partials, ea);                      \
+        k_mgs_finish<S, ND><<<1, kFinThreads, 0, s>>>(grid, partials, ea);                   \
         break;
     switch (nd) {
         HPB_STEP(2) HPB_STEP(3) HPB_STEP(4) HPB_STEP(5) HPB_STEP(6) HPB_STEP(7) HPB_STEP(8) HPB_STEP(9)

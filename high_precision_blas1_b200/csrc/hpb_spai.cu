@@ -1,7 +1,9 @@
 // Learned sparse approximate inverse (SPAI) with A's sparsity pattern.
 //
 // A per-row MLP (16 -> 64 -> 64 -> 8, ReLU; weights held in bfloat16,
-// every product accumulated in binary32) reads local features of row i of
+// every product accumulated in binary32 on the tensor cores: warp-level
+// mma.sync bf16 tiles of 16 rows, forward and backward) reads local
+// features of row i of
 // the diagonally scaled matrix Ah = D^{-1/2} A D^{-1/2} (D = diag(A)) and
 // emits raw outputs o_{i,s}, one per stencil slot.  They define a symmetric,
 // diagonally dominant (hence positive definite) Mh on A's pattern:
@@ -45,7 +47,6 @@ namespace spai {
 
 constexpr int kF = 16, kH = 64, kO = 8, kMaxSlot = 8, kMaxSq = 64;
 constexpr int kNumParams = kF * kH + kH + kH * kH + kH + kH * kO + kO;  // 5768
-constexpr int kTile = 64;                                                // rows per tile
 constexpr int kThreads = 256;
 
 struct Offsets {
@@ -287,96 +288,212 @@ k_forward(int32_t rows, const float* __restrict__ feat, const __nv_bfloat16* __r
     }
 }
 
-// Weight gradients of one block (summed over its tiles) into part[block][:].
-__global__ void __launch_bounds__(kThreads)
+// Backward pass on tensor cores.  A block of kMmaWarps warps takes chunks
+// of 16 * kMmaWarps rows:
+//   phase 1, per warp and its 16 rows, in registers:
+//     dh2 = (dout W3^T) o [h2 > 0]   (K = 8 outputs, padded to one k-tile)
+//     dh1 = (dh2 W2^T) o [h1 > 0]
+//   then x, h1, h2, dout, dh2, dh1 of the chunk go to shared memory;
+//   phase 2, block-wide: the weight gradients as products over the chunk's
+//     rows, dW1 += x^T dh1 (16 x 64), dW2 += h1^T dh2 (64 x 64),
+//     dW3 += h2^T dout (64 x 8): 44 output tiles of 16 x 8 spread over the
+//     warps, accumulated in registers across the block's chunks; the bias
+//     gradients are column sums in a fixed order.
+// Operands are binary32 activations carried as bf16 pairs: phase 1 (bf16
+// weights on one side) takes hi and lo products; phase 2 (two activation
+// operands) takes hi*hi + hi*lo + lo*hi.  Every sum runs in a fixed order,
+// so the block partials -- and after k_reduce_grad the gradient -- are
+// deterministic.
+constexpr int kBwdRows = 16 * kMmaWarps;           // rows per chunk
+constexpr int kSX = kF + 4, kSH = kH + 4, kSO = kO + 4;  // padded row strides (floats): conflict-free column reads
+constexpr int kBwdTiles = (kF / 16) * (kH / 8) + (kH / 16) * (kH / 8) + (kH / 16) * (kO / 8);  // 8 + 32 + 4
+constexpr int kBwdTilesPerWarp = (kBwdTiles + kMmaWarps - 1) / kMmaWarps;
+constexpr int kFragW3T = (kH / 8);                 // W3^T: one k-tile (8 outputs padded), 8 n-tiles
+constexpr int kFragW2T = (kH / 8) * (kH / 16);     // W2^T: 4 k-tiles x 8 n-tiles
+
+size_t bwd_tc_smem() {
+    return size_t(kBwdRows) * (kSX + 4 * kSH + kSO) * sizeof(float) +
+           size_t(kFragW3T + kFragW2T) * 32 * sizeof(uint2);
+}
+
+// B fragment (k-tile kt, n-tile nt) of W^T for W stored row-major q x ld
+// (B'[k][n] = W[n][k]); k >= kreal reads as 0.
+__device__ __forceinline__ uint2 bt_frag(const __nv_bfloat16* __restrict__ w, int ld, int kreal, int kt, int nt,
+                                         int lane) {
+    const int g = lane >> 2, t = lane & 3, n = 8 * nt + g, k = 16 * kt + 2 * t;
+    auto at = [&](int kk) { return kk < kreal ? __bfloat162float(w[n * ld + kk]) : 0.f; };
+    return make_uint2(pack_bf16(at(k), at(k + 1)), pack_bf16(at(k + 8), at(k + 9)));
+}
+
+// two adjacent rows' values of one column of a padded shared array, as a
+// bf16 (hi, lo) pair for the lower (first) and upper k index
+__device__ __forceinline__ void col_pair(const float* a, int stride, int r, int c, uint32_t& hi, uint32_t& lo) {
+    split2(a[r * stride + c], a[(r + 1) * stride + c], hi, lo);
+}
+
+__global__ void __launch_bounds__(kMmaWarps * 32, 1)
 k_backward(int32_t rows, const float* __restrict__ feat, const __nv_bfloat16* __restrict__ w,
            const float* __restrict__ h1g, const float* __restrict__ h2g, const float* __restrict__ dout,
            float* __restrict__ part) {
-    extern __shared__ float smem[];
-    float* sw = smem;                    // kNumParams
-    float* sx = sw + kNumParams;         // kTile * kF
-    float* sh1 = sx + kTile * kF;        // kTile * kH  (h1, then dh1 in place)
-    float* sh2 = sh1 + kTile * kH;       // kTile * kH  (h2)
-    float* sd2 = sh2 + kTile * kH;       // kTile * kH  (dh2)
-    float* sdo = sd2 + kTile * kH;       // kTile * kO
-    load_weights(w, sw);
-    float acc[(kNumParams + kThreads - 1) / kThreads];
-    constexpr int kPer = (kNumParams + kThreads - 1) / kThreads;
-#pragma unroll
-    for (int k = 0; k < kPer; ++k) acc[k] = 0.f;
-    const int ntiles = (rows + kTile - 1) / kTile;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const int32_t r0 = t * kTile;
-        const int nr = min(kTile, rows - r0);
-        __syncthreads();
-        for (int k = threadIdx.x; k < kTile * kF; k += blockDim.x)
-            sx[k] = (k / kF) < nr ? feat[size_t(r0) * kF + k] : 0.f;
-        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x) {
-            const bool in = (k / kH) < nr;
-            sh1[k] = in ? h1g[size_t(r0) * kH + k] : 0.f;
-            sh2[k] = in ? h2g[size_t(r0) * kH + k] : 0.f;
-        }
-        for (int k = threadIdx.x; k < kTile * kO; k += blockDim.x)
-            sdo[k] = (k / kO) < nr ? dout[size_t(r0) * kO + k] : 0.f;
-        __syncthreads();
-        // dh2 = (dout W3^T) * [h2 > 0]
-        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x) {
-            const int r = k / kH, u = k % kH;
-            float g = 0.f;
-#pragma unroll
-            for (int q = 0; q < kO; ++q) g = fmaf(sdo[r * kO + q], sw[Params::W3 + u * kO + q], g);
-            sd2[k] = sh2[k] > 0.f ? g : 0.f;
-        }
-        __syncthreads();
-        // weight gradients that need h1/h2 before dh1 overwrites h1
-        for (int j = 0; j < kPer; ++j) {
-            const int pidx = threadIdx.x + j * kThreads;
-            if (pidx >= kNumParams) break;
-            float g = 0.f;
-            if (pidx >= Params::W3 && pidx < Params::B3) {  // dW3[q][u] = sum_r h2[r][q] dout[r][u]
-                const int q = (pidx - Params::W3) / kO, u = (pidx - Params::W3) % kO;
-                for (int r = 0; r < kTile; ++r) g = fmaf(sh2[r * kH + q], sdo[r * kO + u], g);
-            } else if (pidx >= Params::B3) {
-                const int u = pidx - Params::B3;
-                for (int r = 0; r < kTile; ++r) g += sdo[r * kO + u];
-            } else if (pidx >= Params::W2 && pidx < Params::B2) {  // dW2[q][u] = sum_r h1[r][q] dh2[r][u]
-                const int q = (pidx - Params::W2) / kH, u = (pidx - Params::W2) % kH;
-                for (int r = 0; r < kTile; ++r) g = fmaf(sh1[r * kH + q], sd2[r * kH + u], g);
-            } else if (pidx >= Params::B2 && pidx < Params::W3) {
-                const int u = pidx - Params::B2;
-                for (int r = 0; r < kTile; ++r) g += sd2[r * kH + u];
-            }
-            acc[j] += g;
-        }
-        __syncthreads();
-        // dh1 = (dh2 W2^T) * [h1 > 0], in place of h1
-        for (int k = threadIdx.x; k < kTile * kH; k += blockDim.x) {
-            const int r = k / kH, u = k % kH;
-            float g = 0.f;
-#pragma unroll 16
-            for (int q = 0; q < kH; ++q) g = fmaf(sd2[r * kH + q], sw[Params::W2 + u * kH + q], g);
-            sh2[k] = sh1[k] > 0.f ? g : 0.f;  // dh1 into sh2 (h2 no longer needed)
-        }
-        __syncthreads();
-        for (int j = 0; j < kPer; ++j) {
-            const int pidx = threadIdx.x + j * kThreads;
-            if (pidx >= Params::W2) break;
-            float g = 0.f;
-            if (pidx < Params::B1) {  // dW1[q][u] = sum_r x[r][q] dh1[r][u]
-                const int q = pidx / kH, u = pidx % kH;
-                for (int r = 0; r < kTile; ++r) g = fmaf(sx[r * kF + q], sh2[r * kH + u], g);
-            } else {
-                const int u = pidx - Params::B1;
-                for (int r = 0; r < kTile; ++r) g += sh2[r * kH + u];
-            }
-            acc[j] += g;
-        }
+    extern __shared__ __align__(16) unsigned char smraw[];
+    float* sX = reinterpret_cast<float*>(smraw);   // kBwdRows x kSX
+    float* sH1 = sX + kBwdRows * kSX;              // kBwdRows x kSH
+    float* sH2 = sH1 + kBwdRows * kSH;
+    float* sD2 = sH2 + kBwdRows * kSH;
+    float* sD1 = sD2 + kBwdRows * kSH;
+    float* sDO = sD1 + kBwdRows * kSH;             // kBwdRows x kSO
+    uint2* fW3 = reinterpret_cast<uint2*>(sDO + kBwdRows * kSO);  // [nt]
+    uint2* fW2 = fW3 + kFragW3T * 32;                              // [nt][kt]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    for (int f = warp; f < kFragW3T + kFragW2T; f += kMmaWarps) {
+        uint2 b;
+        if (f < kFragW3T)
+            b = bt_frag(w + Params::W3, kO, kO, 0, f, lane);
+        else
+            b = bt_frag(w + Params::W2, kH, kH, (f - kFragW3T) % (kH / 16), (f - kFragW3T) / (kH / 16), lane);
+        (f < kFragW3T ? fW3 : fW2)[(f < kFragW3T ? f : f - kFragW3T) * 32 + lane] = b;
     }
+    float acc[kBwdTilesPerWarp][4];
 #pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-        const int pidx = threadIdx.x + j * kThreads;
-        if (pidx < kNumParams) part[size_t(blockIdx.x) * kNumParams + pidx] = acc[j];
+    for (int i = 0; i < kBwdTilesPerWarp; ++i) acc[i][0] = acc[i][1] = acc[i][2] = acc[i][3] = 0.f;
+    float bsum = 0.f;  // bias gradient of parameter column threadIdx.x (< 2 kH + kO)
+    __syncthreads();
+    const int nchunks = (rows + kBwdRows - 1) / kBwdRows;
+    for (int ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+        // ---------------- phase 1: this warp's 16 rows
+        const int la = 16 * warp + g, lb = la + 8;  // rows within the chunk
+        const int32_t ra = ch * kBwdRows + la, rb = ch * kBwdRows + lb;
+        const bool va = ra < rows, vb = rb < rows;
+        auto ld2 = [](const float* p, bool v) { return v ? *reinterpret_cast<const float2*>(p) : make_float2(0.f, 0.f); };
+        const float2 oa = ld2(dout + size_t(ra) * kO + 2 * t, va), ob = ld2(dout + size_t(rb) * kO + 2 * t, vb);
+        uint32_t ah[4], al[4];
+        split2(oa.x, oa.y, ah[0], al[0]);
+        split2(ob.x, ob.y, ah[1], al[1]);
+        ah[2] = ah[3] = al[2] = al[3] = 0u;  // outputs 8..15: padding
+        float d[kH / 8][4];
+#pragma unroll
+        for (int nt = 0; nt < kH / 8; ++nt) {
+            d[nt][0] = d[nt][1] = d[nt][2] = d[nt][3] = 0.f;
+            const uint2 bf = fW3[nt * 32 + lane];
+            mma_bf16(d[nt], ah[0], ah[1], ah[2], ah[3], bf);
+            mma_bf16(d[nt], al[0], al[1], al[2], al[3], bf);
+            const float2 ha = ld2(h2g + size_t(ra) * kH + 8 * nt + 2 * t, va);
+            const float2 hb = ld2(h2g + size_t(rb) * kH + 8 * nt + 2 * t, vb);
+            if (!(ha.x > 0.f)) d[nt][0] = 0.f;
+            if (!(ha.y > 0.f)) d[nt][1] = 0.f;
+            if (!(hb.x > 0.f)) d[nt][2] = 0.f;
+            if (!(hb.y > 0.f)) d[nt][3] = 0.f;
+            *reinterpret_cast<float2*>(sH2 + la * kSH + 8 * nt + 2 * t) = ha;
+            *reinterpret_cast<float2*>(sH2 + lb * kSH + 8 * nt + 2 * t) = hb;
+            *reinterpret_cast<float2*>(sD2 + la * kSH + 8 * nt + 2 * t) = make_float2(d[nt][0], d[nt][1]);
+            *reinterpret_cast<float2*>(sD2 + lb * kSH + 8 * nt + 2 * t) = make_float2(d[nt][2], d[nt][3]);
+        }
+        *reinterpret_cast<float2*>(sDO + la * kSO + 2 * t) = oa;
+        *reinterpret_cast<float2*>(sDO + lb * kSO + 2 * t) = ob;
+        {
+            const float2 xa0 = ld2(feat + size_t(ra) * kF + 2 * t, va), xb0 = ld2(feat + size_t(rb) * kF + 2 * t, vb);
+            const float2 xa1 = ld2(feat + size_t(ra) * kF + 8 + 2 * t, va);
+            const float2 xb1 = ld2(feat + size_t(rb) * kF + 8 + 2 * t, vb);
+            *reinterpret_cast<float2*>(sX + la * kSX + 2 * t) = xa0;
+            *reinterpret_cast<float2*>(sX + lb * kSX + 2 * t) = xb0;
+            *reinterpret_cast<float2*>(sX + la * kSX + 8 + 2 * t) = xa1;
+            *reinterpret_cast<float2*>(sX + lb * kSX + 8 + 2 * t) = xb1;
+        }
+        uint32_t xh[kH / 16][4], xl[kH / 16][4];
+#pragma unroll
+        for (int kt = 0; kt < kH / 16; ++kt) {
+            split2(d[2 * kt][0], d[2 * kt][1], xh[kt][0], xl[kt][0]);
+            split2(d[2 * kt][2], d[2 * kt][3], xh[kt][1], xl[kt][1]);
+            split2(d[2 * kt + 1][0], d[2 * kt + 1][1], xh[kt][2], xl[kt][2]);
+            split2(d[2 * kt + 1][2], d[2 * kt + 1][3], xh[kt][3], xl[kt][3]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < kH / 8; ++nt) {
+            float e[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int kt = 0; kt < kH / 16; ++kt) {
+                const uint2 bf = fW2[(nt * (kH / 16) + kt) * 32 + lane];
+                mma_bf16(e, xh[kt][0], xh[kt][1], xh[kt][2], xh[kt][3], bf);
+                mma_bf16(e, xl[kt][0], xl[kt][1], xl[kt][2], xl[kt][3], bf);
+            }
+            const float2 ha = ld2(h1g + size_t(ra) * kH + 8 * nt + 2 * t, va);
+            const float2 hb = ld2(h1g + size_t(rb) * kH + 8 * nt + 2 * t, vb);
+            if (!(ha.x > 0.f)) e[0] = 0.f;
+            if (!(ha.y > 0.f)) e[1] = 0.f;
+            if (!(hb.x > 0.f)) e[2] = 0.f;
+            if (!(hb.y > 0.f)) e[3] = 0.f;
+            *reinterpret_cast<float2*>(sH1 + la * kSH + 8 * nt + 2 * t) = ha;
+            *reinterpret_cast<float2*>(sH1 + lb * kSH + 8 * nt + 2 * t) = hb;
+            *reinterpret_cast<float2*>(sD1 + la * kSH + 8 * nt + 2 * t) = make_float2(e[0], e[1]);
+            *reinterpret_cast<float2*>(sD1 + lb * kSH + 8 * nt + 2 * t) = make_float2(e[2], e[3]);
+        }
+        __syncthreads();
+        // ---------------- phase 2: weight gradients over the chunk's rows
+#pragma unroll
+        for (int i = 0; i < kBwdTilesPerWarp; ++i) {
+            const int tile = warp + kMmaWarps * i;
+            if (tile >= kBwdTiles) break;
+            const float *A, *B;
+            int sa, sb, mt, nt;
+            if (tile < 8) {  // dW1 = x^T dh1
+                A = sX; sa = kSX; B = sD1; sb = kSH; mt = 0; nt = tile;
+            } else if (tile < 40) {  // dW2 = h1^T dh2
+                A = sH1; sa = kSH; B = sD2; sb = kSH; mt = (tile - 8) / 8; nt = (tile - 8) % 8;
+            } else {  // dW3 = h2^T dout
+                A = sH2; sa = kSH; B = sDO; sb = kSO; mt = tile - 40; nt = 0;
+            }
+            const int q0 = 16 * mt + g, u0 = 8 * nt + g;
+#pragma unroll 2
+            for (int r0 = 0; r0 < kBwdRows; r0 += 16) {
+                uint32_t Ah[4], Al[4], Bh[2], Bl[2];
+                col_pair(A, sa, r0 + 2 * t, q0, Ah[0], Al[0]);
+                col_pair(A, sa, r0 + 2 * t, q0 + 8, Ah[1], Al[1]);
+                col_pair(A, sa, r0 + 8 + 2 * t, q0, Ah[2], Al[2]);
+                col_pair(A, sa, r0 + 8 + 2 * t, q0 + 8, Ah[3], Al[3]);
+                col_pair(B, sb, r0 + 2 * t, u0, Bh[0], Bl[0]);
+                col_pair(B, sb, r0 + 8 + 2 * t, u0, Bh[1], Bl[1]);
+                mma_bf16(acc[i], Ah[0], Ah[1], Ah[2], Ah[3], make_uint2(Bh[0], Bh[1]));
+                mma_bf16(acc[i], Ah[0], Ah[1], Ah[2], Ah[3], make_uint2(Bl[0], Bl[1]));
+                mma_bf16(acc[i], Al[0], Al[1], Al[2], Al[3], make_uint2(Bh[0], Bh[1]));
+            }
+        }
+        {
+            const int c = threadIdx.x;
+            const float* col = c < kH ? sD1 + c : (c < 2 * kH ? sD2 + (c - kH) : sDO + (c - 2 * kH));
+            const int st = c < 2 * kH ? kSH : kSO;
+            if (c < 2 * kH + kO)
+                for (int r = 0; r < kBwdRows; ++r) bsum += col[r * st];
+        }
+        __syncthreads();  // the next chunk overwrites the shared arrays
     }
+    // ---------------- block partials
+    float* pb = part + size_t(blockIdx.x) * kNumParams;
+#pragma unroll
+    for (int i = 0; i < kBwdTilesPerWarp; ++i) {
+        const int tile = warp + kMmaWarps * i;
+        if (tile >= kBwdTiles) break;
+        int base, ld, mt, nt;
+        if (tile < 8) {
+            base = Params::W1; ld = kH; mt = 0; nt = tile;
+        } else if (tile < 40) {
+            base = Params::W2; ld = kH; mt = (tile - 8) / 8; nt = (tile - 8) % 8;
+        } else {
+            base = Params::W3; ld = kO; mt = tile - 40; nt = 0;
+        }
+        const int q = 16 * mt + g, u = 8 * nt + 2 * t;
+        pb[base + q * ld + u] = acc[i][0];
+        pb[base + q * ld + u + 1] = acc[i][1];
+        pb[base + (q + 8) * ld + u] = acc[i][2];
+        pb[base + (q + 8) * ld + u + 1] = acc[i][3];
+    }
+    const int c = threadIdx.x;
+    if (c < kH)
+        pb[Params::B1 + c] = bsum;
+    else if (c < 2 * kH)
+        pb[Params::B2 + c - kH] = bsum;
+    else if (c < 2 * kH + kO)
+        pb[Params::B3 + c - 2 * kH] = bsum;
 }
 
 // g = sum_b part[b][p] (fixed order: deterministic); gsys[p] = g, gacc[p] += g
@@ -610,10 +727,6 @@ int grow(hpb_spai* net, int32_t rows, int64_t nnz) {
     return HPB_SUCCESS;
 }
 
-size_t bwd_smem() {
-    using namespace hpb::spai;
-    return size_t(kNumParams + kTile * kF + 3 * kTile * kH + kTile * kO) * sizeof(float);
-}
 
 // diag of a binary32 CSR
 __global__ void k_fdiag(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
@@ -787,7 +900,7 @@ int hpb_spai_create(hpb_spai** out, int nslot, int dslot, const int* offsets, ui
         hpb_spai_destroy(net);
         return HPB_ERROR_CUDA;
     }
-    cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bwd_smem()));
+    cudaFuncSetAttribute(k_backward, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bwd_tc_smem()));
     *out = net;
     return HPB_SUCCESS;
 }
@@ -902,9 +1015,13 @@ int loss_impl(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_r
     }
     if (grad) {
         k_dout<<<gb, 256>>>(n, sys->row_ptr, sys->col_ind, net->out, net->dm, net->off, net->dout);
-        const int ntiles = (n + kTile - 1) / kTile;
-        const int grid = std::min(kGridMlp, ntiles);
-        k_backward<<<grid, kThreads, bwd_smem()>>>(n, net->feat, net->wb, net->h1, net->h2, net->dout, net->part);
+        const int nchunks = (n + kBwdRows - 1) / kBwdRows;
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int grid = std::max(1, std::min(std::min(kGridMlp, sms), nchunks));
+        k_backward<<<grid, kMmaWarps * 32, bwd_tc_smem()>>>(n, net->feat, net->wb, net->h1, net->h2, net->dout,
+                                                            net->part);
         k_reduce_grad<<<(kNumParams + 255) / 256, 256>>>(grid, net->part, net->gtmp, net->grad);
         hpb::count_launch(3);
         if (grad_host && cudaMemcpy(grad_host, net->gtmp, kNumParams * 4, cudaMemcpyDeviceToHost) != cudaSuccess)

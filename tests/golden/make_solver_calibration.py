@@ -11,7 +11,7 @@ tol 1e-10) and record:
   thread's (s, c) pair into shared accumulators under a mutex in the order
   the threads finish, so with more than one thread the last bits of every
   inner product, and with them the iterates, change from run to run;
-* runs with 2, 4, 8 and 16 Dot2 threads (two or three each): their iteration counts
+* runs with 2, 4, 8 and 16 Dot2 threads (four each): their iteration counts
   (iters_by_run) and how far their residual histories drift from the
   one-thread history -- the reference's own run-to-run spread under
   last-bit changes of its reductions.  The drift is measured on the running
@@ -21,7 +21,7 @@ tol 1e-10) and record:
   |log10(env_run / env_1)| over the cycles where both exceed 1e-8.
 
 The benchmark's CPU baseline times a few reference cycles on the GPU box's
-host and scales by iters_median.  Takes about ten minutes on 8 cores.
+host and scales by iters_median.  Takes about twenty minutes on 8 cores.
 
     python tests/golden/make_solver_calibration.py
 """
@@ -40,7 +40,7 @@ sys.path.insert(0, str(HERE.parent.parent))
 import oracle  # noqa: E402
 from high_precision_blas1_b200 import problems  # noqa: E402
 
-RUNS = (("2a", 2), ("2b", 2), ("4a", 4), ("4b", 4), ("8a", 8), ("8b", 8), ("8c", 8), ("16a", 16), ("16b", 16))
+RUNS = tuple((f"{t}{c}", t) for t in (2, 4, 8, 16) for c in "abcd")
 FLOOR = 1e-8
 
 
