@@ -310,9 +310,9 @@ k_mgs_step(int64_t n, int k, Vecs<E> V, const BcgState<typename scalar_of<E>::ty
         for (int d = 0; d < ND; ++d) partials[size_t(d) * gridDim.x + blockIdx.x] = acc[d];
 }
 
-// One block of 1024 threads: the ND x nb partials are one load round per
+// One block of 512 threads: the ND x nb partials are about one load round per
 // thread at the configured sizes (nb = one resident wave of the sweep).
-constexpr int kFinThreads = 1024;
+constexpr int kFinThreads = 512;
 
 template <class S, int ND>
 __global__ void __launch_bounds__(kFinThreads)
