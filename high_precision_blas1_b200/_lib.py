@@ -209,6 +209,8 @@ class hpb_spai_system(C.Structure):
                 ("nres", C.c_int), ("residuals", P)]
 
 
+_sig("hpb_spai_ls_f32", C.c_int, [P, I32, I64, P, P, P, P])
+_sig("hpb_spai_ls_f64", C.c_int, [P, I32, I64, P, P, P, P])
 _sig("hpb_spai_create", C.c_int, [C.POINTER(P), C.c_int, C.c_int, C.POINTER(C.c_int), C.c_uint64])
 _sig("hpb_spai_destroy", C.c_int, [P])
 _sig("hpb_spai_num_params", C.c_int, [])

@@ -629,6 +629,20 @@ typedef struct hpb_spai_system {
 
 /* offsets[nslot]: the stencil's column offsets col - row (e.g. -N^2, -N, -1,
  * 0, 1, N, N^2); dslot: index of 0.  The untrained network is Jacobi. */
+/* Least-squares sparse approximate inverse on A's pattern (the classical
+ * fixed-pattern SPAI): the right preconditioner M, nonzero where A is, that
+ * minimises ||A M - I||_F; column j is the exact least-squares solution over
+ * the rows A's column j reaches (normal equations from the columns of A,
+ * Cholesky in binary64, one thread per column).  m_val receives M's values
+ * in A's CSR order, for HPB_PRECOND_MATRIX / hpb_ir_solve_*'s M.  Columns
+ * of A may hold at most 8 entries (HPB_ERROR_NOT_SUPPORTED otherwise).
+ * Blocking.  No counterpart in the reference (its preconditioners are the
+ * identity and csrsv2 triangular solves). */
+int hpb_spai_ls_f32(hpb_context* ctx, int32_t rows, int64_t nnz, const int32_t* row_ptr, const int32_t* col_ind,
+                    const float* val, float* m_val);
+int hpb_spai_ls_f64(hpb_context* ctx, int32_t rows, int64_t nnz, const int32_t* row_ptr, const int32_t* col_ind,
+                    const double* val, double* m_val);
+
 int hpb_spai_create(hpb_spai** net, int nslot, int dslot, const int* offsets, uint64_t seed);
 int hpb_spai_destroy(hpb_spai* net);
 int hpb_spai_num_params(void);
