@@ -981,19 +981,24 @@ def dot2_same_box(torch, L, ctx, calls=200):
 
 def dot2_floors(torch, L, ctx, xs, ys, n, calls=200):
     """What bounds one launch at 16.8 MB: back-to-back launches of a library
-    kernel with no work (hpb_fill_f64 of one element: the launch floor), the
-    plain FMA dot over the same pair (hpb_dot_f64: the same single-pass
-    combine without the error-free transformations), beside Dot2."""
+    kernel with no work (hpb_fill_f64 of one element, an ordinary launch),
+    the Dot2 kernel itself with n = 0 (a programmatic launch and the
+    combine, nothing to read), the plain FMA dot over the same pair
+    (hpb_dot_f64: the same single-pass combine without the error-free
+    transformations), beside Dot2."""
     R = len(xs)
     one = torch.zeros(1, dtype=torch.float64, device="cuda")
     od = torch.zeros(4, dtype=torch.float64, device="cuda")
     t_launch = _events_us(torch, lambda i: L.hpb_fill_f64(ctx.h, 1, 0.0, one.data_ptr()), calls)
+    # the same Dot2 kernel with nothing to read: launch (programmatic, as every Dot2) + one block's combine
+    t_empty = _events_us(torch, lambda i: L.hpb_dot2_f64(ctx.h, 0, xs[0].data_ptr(), ys[0].data_ptr(),
+                                                         od.data_ptr()), calls)
     t_plain = _events_us(torch, lambda i: L.hpb_dot_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(),
                                                         od.data_ptr()), calls)
     t_dot2 = _events_us(torch, lambda i: L.hpb_dot2_f64(ctx.h, n, xs[i % R].data_ptr(), ys[i % R].data_ptr(),
                                                         od.data_ptr()), calls)
     hbm, _ = peaks()
-    return {"launch_floor_us": t_launch, "plain_dot_us": t_plain, "dot2_us": t_dot2,
+    return {"launch_floor_us": t_launch, "dot2_n0_us": t_empty, "plain_dot_us": t_plain, "dot2_us": t_dot2,
             "transfer_at_peak_us": 16.0 * n / (hbm * 1e9) * 1e6,
             "note": "one launch at 16.8 MB: launch floor + HBM transfer at the measured peak bound a single-pass "
                     "reduction from below; the plain dot shows what the compensation itself costs"}

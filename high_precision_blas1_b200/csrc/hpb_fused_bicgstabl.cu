@@ -150,9 +150,10 @@ k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
     using A = typename acc_of<S>::type;
     // rows in a grid-stride loop, consecutive threads on consecutive rows:
     // streaming loads of the values and indices, x through the read-only
-    // path.  Launched with one row per thread without the dot; with it, on
-    // 6 blocks per SM (B200, 1024^2: 20.5 us against 26.7 us for one row
-    // per thread, whose 4096 blocks each hold their warps at the merge).
+    // path.  Without the dot on 8 blocks per SM (14.7 us against 16.4 us
+    // for one row per thread); with it on 6 blocks per SM (B200, 1024^2:
+    // 19.7-20.6 us against 26.7-28.8 us for one row per thread, whose 4096
+    // blocks each hold their warps at the merge).
     typename pacc_of<E>::type pacc;
     S nb = s_zero(S{});
     if (UPD) nb = s_neg(ea.st->beta);
@@ -664,7 +665,7 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
         P.g_upd[j] = int(std::max<int64_t>(1, std::min<int64_t>((n / 2 + kThreads - 1) / kThreads + 1,
                                                                   int64_t(sms) * update_occupancy<E>(j))));
     P.g_red = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * reduction_occupancy<E>(L))));
-    P.g_sp = int(std::max<int64_t>(1, need));
+    P.g_sp = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * 8)));  // grid-stride rows, 8 blocks per SM
     P.g_spd = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * 6)));
     P.g_nrm = int(std::max<int64_t>(
         1, std::min<int64_t>(need, int64_t(sms) * occupancy_of(reinterpret_cast<const void*>(k_norm<E>)))));

