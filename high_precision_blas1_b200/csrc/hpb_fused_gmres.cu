@@ -375,7 +375,7 @@ k_gm_jacobi(int64_t n, const E* __restrict__ x, const E* __restrict__ d, E* __re
         stE(y, q, from_s<E>(s_div(to_s(ldE(x, q)), to_s(ldE(d, q)))));
 }
 
-// plain CSR product y = A x (row per thread; x gathered through L1/L2)
+// plain CSR product y = A x (grid-stride rows; x gathered through L1/L2)
 template <class E>
 __global__ void __launch_bounds__(kGmThreads)
 k_gm_spmv(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const E* __restrict__ val,
@@ -507,7 +507,7 @@ struct GmPlan<E>::Impl {
     const E* val = nullptr;
     const E* b = nullptr;
     E* x = nullptr;
-    int g_ew = 1, g_md = 1, g_sp = 1, kernels = 0;
+    int g_ew = 1, g_md = 1, g_sp = 1, g_rc = 1, kernels = 0;
     SolverWorkspace ws;
     E *V = nullptr, *W = nullptr, *Z = nullptr, *R = nullptr, *diag = nullptr, *T = nullptr;
     GmState<S>* st = nullptr;
@@ -562,6 +562,8 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
         std::max<int64_t>(1, std::min<int64_t>((n + kGmThreads - 1) / kGmThreads, int64_t(sms) * occ_md)));
     const int g_sp = P.g_sp =
         int(std::max<int64_t>(1, std::min<int64_t>((int64_t(rows) + kGmThreads - 1) / kGmThreads, int64_t(sms) * 8)));
+    // the compensated residual (k_resid_comp) takes one row per thread
+    const int g_rc = P.g_rc = int(std::max<int64_t>(1, (int64_t(rows) + kGmThreads - 1) / kGmThreads));
     SolverWorkspace& ws = P.ws;
     const size_t vb = size_t(n) * sizeof(E);
     int wst = ws.open(sizeof(GmHostView));
@@ -578,7 +580,7 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     P.T = (M.kind == 3 && M.sweeps > 0) ? static_cast<E*>(ws.alloc(vb)) : nullptr;
     if (M.kind == 3 && M.sweeps > 0 && !P.T) return HPB_ERROR_OUT_OF_MEMORY;
     auto* st = P.st = static_cast<GmState<S>*>(ws.alloc(sizeof(GmState<S>)));
-    const size_t np = std::max<size_t>(size_t(m + 1) * g_md, std::max<size_t>(g_ew, g_sp));
+    const size_t np = std::max<size_t>(size_t(m + 1) * g_md, std::max<size_t>(g_ew, std::max(g_sp, g_rc)));
     auto* partials = P.partials = static_cast<A*>(ws.alloc(np * sizeof(A)));
     auto* ticket = P.ticket = static_cast<unsigned int*>(ws.alloc(64));
     auto* badflag = P.badflag = static_cast<int*>(ws.alloc(64));
@@ -662,7 +664,7 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
         k_gm_axpy<E><<<g_ew, kGmThreads, 0, s>>>(n, x, Z);
         kernels += 3;
     }
-    k_resid_comp<E, E><<<g_sp, kGmThreads, 0, s>>>(rows, rp, ci, val, x, b, R, st, partials, ticket, badflag);
+    k_resid_comp<E, E><<<g_rc, kGmThreads, 0, s>>>(rows, rp, ci, val, x, b, R, st, partials, ticket, badflag);
     ++kernels;
     cudaMemcpyAsync(&hv->rnorm, &st->rnorm, sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&hv->est, &st->est, sizeof(double), cudaMemcpyDeviceToHost, s);
@@ -690,7 +692,7 @@ int GmPlan<E>::run(hpb_solver_report* rep, double* hist, int cap) {
     auto t0 = std::chrono::steady_clock::now();
     cudaMemsetAsync(st, 0, sizeof(GmState<S>), s);
     k_gm_norm<E><<<P.g_ew, kGmThreads, 0, s>>>(P.n, P.b, P.dnorm, P.partials, P.ticket, P.badflag);
-    k_resid_comp<E, E><<<P.g_sp, kGmThreads, 0, s>>>(P.rows, P.rp, P.ci, P.val, P.x, P.b, P.R, st, P.partials,
+    k_resid_comp<E, E><<<P.g_rc, kGmThreads, 0, s>>>(P.rows, P.rp, P.ci, P.val, P.x, P.b, P.R, st, P.partials,
                                                      P.ticket, P.badflag);
     cudaMemcpyAsync(&hv->rnorm, &st->rnorm, sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&hv->est, &st->est, sizeof(double), cudaMemcpyDeviceToHost, s);
