@@ -235,6 +235,146 @@ __device__ __forceinline__ AccC widen_acc(const AccCf& a) {
 }
 __device__ __forceinline__ Acc2 widen_acc(const Acc2& a) { return a; }
 __device__ __forceinline__ AccC widen_acc(const AccC& a) { return a; }
+// merge and shuffle of the binary32 accumulators (the same compensated merge
+// as merge2, in binary32)
+__device__ __forceinline__ void merge(Acc2f& a, const Acc2f& b) {
+    float e;
+    a.s = two_sum(a.s, b.s, e);
+    a.c = add_rn(a.c, add_rn(e, b.c));
+}
+__device__ __forceinline__ void merge(AccCf& a, const AccCf& b) {
+    float e;
+    a.s.re = two_sum(a.s.re, b.s.re, e);
+    a.c.re = add_rn(a.c.re, add_rn(e, b.c.re));
+    a.s.im = two_sum(a.s.im, b.s.im, e);
+    a.c.im = add_rn(a.c.im, add_rn(e, b.c.im));
+}
+__device__ __forceinline__ Acc2f shfl_acc(const Acc2f& a, int off) {
+    Acc2f r;
+    r.s = __shfl_xor_sync(0xffffffffu, a.s, off);
+    r.c = __shfl_xor_sync(0xffffffffu, a.c, off);
+    return r;
+}
+__device__ __forceinline__ AccCf shfl_acc(const AccCf& a, int off) {
+    AccCf r;
+    r.s.re = __shfl_xor_sync(0xffffffffu, a.s.re, off);
+    r.s.im = __shfl_xor_sync(0xffffffffu, a.s.im, off);
+    r.c.re = __shfl_xor_sync(0xffffffffu, a.c.re, off);
+    r.c.im = __shfl_xor_sync(0xffffffffu, a.c.im, off);
+    return r;
+}
+
+// Two binary32 Dot2 accumulations in lockstep on packed pairs (the
+// .f32x2 forms of add / sub / mul / fma, sm_100): lane 0 and lane 1 of each
+// 64-bit register are two independent accumulators, each updated with
+// exactly the operations of pdot_add(Acc2f&, x, y) -- one instruction per
+// operation for both, half the issue slots of two scalar updates.
+using f32x2 = unsigned long long;
+__device__ __forceinline__ f32x2 pack2(float lo, float hi) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void unpack2(f32x2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+struct Acc2x2 {
+    f32x2 s = 0ull, c = 0ull;  // (s, c) of the two accumulations
+};
+// a += conj(x) * y lane-wise, with ny = -y (loop-invariant operands are
+// negated once by the caller): p = x y, -t = fma(x, -y, p) = p - x y exactly
+// (the negated TwoProd error), TwoSum(s, p) as two_sum, c += t + e.
+__device__ __forceinline__ void pdot_add2(Acc2x2& a, f32x2 x, f32x2 y, f32x2 ny) {
+    const f32x2 p = mul2(x, y);
+    const f32x2 nt = fma2(x, ny, p);
+    const f32x2 s = add2(a.s, p);
+    const f32x2 bv = sub2(s, a.s);
+    const f32x2 av = sub2(s, bv);
+    const f32x2 e = add2(sub2(p, bv), sub2(a.s, av));
+    a.c = add2(a.c, sub2(e, nt));
+    a.s = s;
+}
+__device__ __forceinline__ void split2(const Acc2x2& a, Acc2f& lo, Acc2f& hi) {
+    unpack2(a.s, lo.s, hi.s);
+    unpack2(a.c, lo.c, hi.c);
+}
+// lane-wise merge(Acc2f&, const Acc2f&) of two packed pairs
+__device__ __forceinline__ void merge(Acc2x2& a, const Acc2x2& b) {
+    const f32x2 s = add2(a.s, b.s);
+    const f32x2 bv = sub2(s, a.s);
+    const f32x2 av = sub2(s, bv);
+    const f32x2 e = add2(sub2(b.s, bv), sub2(a.s, av));
+    a.c = add2(a.c, add2(e, b.c));
+    a.s = s;
+}
+__device__ __forceinline__ Acc2x2 shfl_acc(const Acc2x2& a, int off) {
+    Acc2x2 r;
+    r.s = __shfl_xor_sync(0xffffffffu, a.s, off);
+    r.c = __shfl_xor_sync(0xffffffffu, a.c, off);
+    return r;
+}
+// the two lanes' accumulations as one: each widened to binary64, then merged
+__device__ __forceinline__ Acc2 widen_lanes(const Acc2x2& a) {
+    Acc2f lo, hi;
+    split2(a, lo, hi);
+    Acc2 r = widen_acc(lo);
+    merge(r, widen_acc(hi));
+    return r;
+}
+__device__ __forceinline__ f32x2 neg2(f32x2 v) { return v ^ 0x8000000080000000ull; }
+
+// Reduce-scatter of P = 2^p accumulators across the 32 lanes of a warp: at
+// each of the first p butterfly levels a lane keeps half of its values and
+// merges its partner's copy of them, the remaining levels merge one value.
+// Afterwards value j's warp total is in lane (j << (5 - p)) (and its
+// partners of the last levels); P + 5 - p merges per lane instead of the
+// 5 P of one butterfly per value, in a fixed order.  The levels are
+// unrolled at compile time so the values stay in registers.
+template <int COUNT, int O, class PA, int P>
+__device__ __forceinline__ void reduce_scatter_level(PA (&v)[P], int lane) {
+    if constexpr (O >= 1) {
+        if constexpr (COUNT > 1) {
+            constexpr int HALF = COUNT / 2;
+            const bool upper = (lane & O) != 0;
+#pragma unroll
+            for (int j = 0; j < HALF; ++j) {
+                PA send = upper ? v[j] : v[j + HALF];
+                PA keep = upper ? v[j + HALF] : v[j];
+                merge(keep, shfl_acc(send, O));
+                v[j] = keep;
+            }
+            reduce_scatter_level<HALF, O / 2>(v, lane);
+        } else {
+            merge(v[0], shfl_acc(v[0], O));
+            reduce_scatter_level<1, O / 2>(v, lane);
+        }
+    }
+}
+template <int P, class PA>
+__device__ __forceinline__ void warp_reduce_scatter(PA (&v)[P]) {
+    static_assert(P >= 1 && P <= 32 && (P & (P - 1)) == 0, "P a power of two up to 32");
+    reduce_scatter_level<P, 16>(v, int(threadIdx.x & 31));
+}
 
 // Block-wide merge of ND accumulators (result valid in thread 0).
 template <int ND, class A>

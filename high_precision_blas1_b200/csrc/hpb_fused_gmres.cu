@@ -3,18 +3,17 @@
 // preconditioning, and the binary64 iterative-refinement driver of the
 // precision form.
 //
-// Arnoldi orthogonalisation is classical Gram-Schmidt with one
-// re-orthogonalisation (CGS2): per step two batched multi-dot passes
-// h = V^T w and two batched updates w -= V h, instead of the reference's
-// (i+1) sequential modified-Gram-Schmidt dot/axpy pairs (gmres.h:426-452).
-// The multi-dot gives each warp a set of basis vectors and each block a
-// contiguous chunk of rows, so every basis vector is read once per pass and
-// w stays in L1.  The norm of the new vector is fused into the second
-// update; the last block of that kernel appends the Hessenberg column,
-// applies the previous Givens rotations, generates the new one, rotates the
-// right-hand side and records the residual estimate |s_{i+1}| -- all in
-// binary64 on the GPU.  One restart cycle (m steps, 6 kernels each, plus
-// the solution update and the true residual) is one CUDA graph.
+// Arnoldi orthogonalisation is classical Gram-Schmidt with a delayed
+// re-orthogonalisation (DCGS2, below): per step one pass over the basis
+// for all inner products (Dot2) and one pass that writes the finished
+// vector q_i and the next one, instead of the reference's (i+1) sequential
+// modified-Gram-Schmidt dot/axpy pairs (gmres.h:426-452).  The step's
+// scalar work -- the re-orthogonalisation of the previous column, the new
+// Hessenberg column, the Givens rotations, the right-hand side and the
+// residual estimate |s_{i+1}| -- runs in binary64 in the last block of the
+// reduction kernel.  One restart cycle (m steps of 4 kernels plus the
+// preconditioner, the closing reduction, the solution update and the true
+// residual) is one CUDA graph.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -33,17 +32,22 @@ constexpr int kGmMaxM = 64;  // basis size limit of the fused GMRES
 
 template <class S>
 struct GmState {
-    S H[(kGmMaxM + 1) * kGmMaxM];  // column-major: H[col * (m+1) + row]
+    S H[(kGmMaxM + 1) * kGmMaxM];   // rotated (the triangle R), column-major: H[col * (m+1) + row]
+    S Hr[(kGmMaxM + 1) * kGmMaxM];  // the Hessenberg matrix itself, same layout
     S cs[kGmMaxM], sn[kGmMaxM];
     S s[kGmMaxM + 1];
-    S h1[kGmMaxM + 1], h2[kGmMaxM + 1];
+    S dots[2 * kGmMaxM + 3];  // the step's inner products (see k_dcgs_dots)
+    S na[kGmMaxM];            // -a_k of the step's update
+    S nt[kGmMaxM + 1];        // -t_k of the step's update
     S y[kGmMaxM];
     S neg_y[kGmMaxM];
-    double inv_h;    // 1 / h_{i+1,i}
+    double inv_nu;   // 1 / nu of the step
+    double f;        // 1 / (nu alpha') of the step
+    double alpha;    // the scale of the vector in the next slot
     double beta;     // ||r|| at the cycle start
-    double est;      // |s_{i+1}| after the last step
+    double est;      // |s_{i+1}| after the last completed column
     double rnorm;    // true residual norm at the cycle end
-    int nsteps;      // Arnoldi steps without breakdown in this cycle
+    int nsteps;      // completed Arnoldi columns in this cycle
     int broken;
     int nonfinite;
 };
@@ -92,135 +96,559 @@ __device__ __forceinline__ void giv_apply(cd& dx, cd& dy, cd c, cd s) {
 __device__ __forceinline__ double s_abs(double v) { return fabs(v); }
 __device__ __forceinline__ double s_abs(cd v) { return cabs_(v); }
 
-// ------------------------------------------------------------ multi-dot
-// out[k] = <V_k, w> for k < K (Dot2), in two launches:
-//   k_multidot:     threads stream rows in a grid-stride loop; each pass
-//                   takes md_tile basis vectors, so w[q] is loaded once per
-//                   pass and every V_k once; block partials per k;
-//   k_mdot_finish:  one block per k merges its block partials in block
-//                   order.
-// (A warp-per-basis-vector layout left 12 warps per SM resident and the
-// Arnoldi step latency-bound.)
-// basis vectors per pass: 4 for every storage type.  binary64: its Dot2
-// arithmetic needs registers (48 per thread keeps 5 blocks per SM).
-// binary32: measured on B200, binary32 GMRES(50) in binary64 refinement on
-// the 128^3 anisotropic Poisson system took 0.360 s with 4 vectors per pass
-// (64 registers, 4 blocks per SM), 0.364 s with 6 (capped at 80 registers,
-// 3 blocks per SM) and 0.382 s with 8 (103 registers, 2 blocks per SM: w is
-// loaded less often, but fewer loads are in flight); on the lognormal 96^3
-// system with Jacobi the time per iteration was within 3 % across the three.
-template <class E> struct md_tile { static constexpr int value = 4; };
+// ------------------------------------------------------------ 16-byte packs
+// VW consecutive elements q*VW .. q*VW + VW - 1 of a vector moved as one
+// 16-byte access (VEC: VW * sizeof(E) == 16 and the vector 16-byte
+// aligned), or one element through ldE / stE (VW == 1).
+template <class E> struct pack_of { static constexpr int value = 16 / int(sizeof(E)); };
 
-template <class E>
-__global__ void __launch_bounds__(kGmThreads)
-k_multidot(int64_t n, int K, const E* __restrict__ V, const E* __restrict__ w,
-           typename acc_of<typename scalar_of<E>::type>::type* partials) {
-    using S = typename scalar_of<E>::type;
-    using A = typename acc_of<S>::type;
-    __shared__ A sh[md_tile<E>::value * 32];
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+template <class E, int VW, bool VEC, bool RO>
+__device__ __forceinline__ void ld_pack(const E* p, int64_t q, E (&o)[VW]) {
+    if constexpr (VEC) {
+        static_assert(VW * sizeof(E) == 16, "one 16-byte pack");
+        const uint4* a = reinterpret_cast<const uint4*>(p) + q;
+        const uint4 t = RO ? __ldg(a) : *a;
+        memcpy(&o[0], &t, 16);
+    } else {
+        static_assert(VW == 1, "one element");
+        o[0] = RO ? ldgE(p, q) : ldE(p, q);
+    }
+}
+template <class E, int VW, bool VEC>
+__device__ __forceinline__ void st_pack(E* p, int64_t q, const E (&v)[VW]) {
+    if constexpr (VEC) {
+        uint4 t;
+        memcpy(&t, &v[0], 16);
+        reinterpret_cast<uint4*>(p)[q] = t;
+    } else {
+        stE(p, q, v[0]);
+    }
+}
+
+// ------------------------------------------------------------ DCGS2 step
+// Arnoldi by classical Gram-Schmidt with a delayed re-orthogonalisation
+// (DCGS2).  At step i the slot V_i holds u: the previous step's vector after
+// its first projection, divided by a scale alpha (at i = 0, r / beta).  One
+// pass over the basis (k_dcgs_dots) gives every inner product of the step,
+// with w = A M u:
+//     a_k = <V_k, u>,  b_k = <V_k, w>  (k < i),   <u, u>,  <u, w>,  <w, w>.
+// From them one block (k_dcgs_finish, binary64) takes
+//     nu  = sqrt(<u, u> - |a|^2)                u's norm after its second projection
+//     q_i = (u - Q_i a) / nu                    the final basis vector
+//     H(0:i, i-1) += alpha a,  H(i, i-1) = alpha nu      column i-1 completed
+//     t   = Q_{i+1}^H w:  t_k = b_k,  t_i = (<u, w> - a^H b) / nu
+//     H(0:i+1, i) = (t - H(0:i+1, 0:i) a) / nu            column i, first projection
+//     alpha' = ||w - Q_{i+1} t|| / nu by Pythagoras (a scale only: the next
+//              step measures the vector it is given)
+// (A M q_i = (w - A M Q_i a) / nu = (w - Q_{i+1} H a) / nu), applies the
+// Givens rotations to column i-1, and one pass (k_dcgs_update) writes
+//     V_i = q_i,   V_{i+1} = (w - Q_i t - t_i q_i) / (nu alpha').
+// In exact arithmetic this is CGS2's basis and Hessenberg matrix; each step
+// reads the basis twice instead of four times and takes four kernels with
+// the product instead of seven.  After step m-1 a closing reduction
+// (<V_k, V_m>, <V_m, V_m>) completes column m-1.
+
+// Shape of k_dcgs_dots per storage type: T basis vectors per pass (two
+// accumulators each, <V_k, u> and <V_k, w>) and R 16-byte packs per thread.
+// With the three norms of the first pass, 2T + 3 accumulators per thread go
+// through one warp reduce-scatter per pass (padded to a power of two: 16 for
+// binary32, 8 for the others); more rows per thread share that cost.
+template <class E> struct dots_shape { static constexpr int T = 2, R = 1; };
+template <> struct dots_shape<float> { static constexpr int T = 5, R = 1; };
+template <> struct dots_shape<double> { static constexpr int T = 2, R = 1; };
+template <> struct dots_shape<cd> { static constexpr int T = 1, R = 1; };
+constexpr int kDotsBlocksPerSm = 3;
+constexpr int kDotsWarps = kGmThreads / 32;
+constexpr int kDotsSlots = 2 * kGmMaxM + 3;
+
+__host__ __device__ constexpr int pow2_at_least(int v) { return v <= 1 ? 1 : 2 * pow2_at_least((v + 1) / 2); }
+__host__ __device__ constexpr int log2_of(int v) { return v <= 1 ? 0 : 1 + log2_of(v / 2); }
+
+// Block partials of the step's inner products: dot d of block b at
+// partials[d * gridDim.x + b] with d = k (a_k), K + k (b_k), 2K (<u, u>),
+// 2K + 1 (<u, w>), 2K + 2 (<w, w>); without w only a_k and <u, u>.  Each
+// block takes R * blockDim.x consecutive packs (the grid covers the vector
+// once) and keeps its u and w packs in registers across the passes over the
+// basis, so u and w are read once per step.  Each pass ends with a warp
+// reduce-scatter; the owner lanes store their warp totals (widened to
+// binary64) in the warp's shared slots, and the block merges the warps'
+// slots in warp order once, at the end.
+template <class E, bool HAS_W, int VW, bool VEC>
+__device__ __forceinline__ void dots_body(int64_t n, int K, const E* __restrict__ V, const E* __restrict__ u,
+                                          const E* __restrict__ w,
+                                          typename acc_of<typename scalar_of<E>::type>::type* partials,
+                                          typename acc_of<typename scalar_of<E>::type>::type* sacc) {
+    using A = typename acc_of<typename scalar_of<E>::type>::type;
     using PA = typename pacc_of<E>::type;
-    constexpr int kMdTile = md_tile<E>::value;
-    // binary32: four consecutive rows per thread with 16-byte loads (scalar
-    // 4-byte loads leave HBM well short of its bandwidth); the vectors start
-    // 16-byte aligned when n % 4 == 0 and V, w are
-    bool vec4 = false;
-    if constexpr (std::is_same<E, float>::value)
-        vec4 = n % 4 == 0 && ((reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(w)) & 15) == 0;
-    for (int kb = 0; kb < K; kb += kMdTile) {
-        PA pacc[kMdTile];
-        if constexpr (std::is_same<E, float>::value) {
-            if (vec4) {
-                const float4* w4 = reinterpret_cast<const float4*>(w);
-                for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 4; q += stride) {
-                    const float4 wq = w4[q];
-                    float4 vk[kMdTile];
+    constexpr int T = dots_shape<E>::T, R = dots_shape<E>::R;
+    constexpr int X = HAS_W ? 2 * T : T;  // first of <u, u>, <u, w>, <w, w>
+    constexpr int ND = HAS_W ? X + 3 : X + 1;
+    constexpr int P = pow2_at_least(ND), LP = log2_of(P);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t nq = VEC ? n / VW : n;
+    const int64_t base = int64_t(blockIdx.x) * blockDim.x * R + threadIdx.x;
+    E uq[R][VW], wq[R][VW];
+    bool in[R];
 #pragma unroll
-                    for (int t = 0; t < kMdTile; ++t)
-                        if (kb + t < K) vk[t] = __ldg(reinterpret_cast<const float4*>(V + size_t(kb + t) * n) + q);
+    for (int r = 0; r < R; ++r) {
+        const int64_t q = base + int64_t(r) * blockDim.x;
+        in[r] = q < nq;
+        if (in[r]) {
+            ld_pack<E, VW, VEC, true>(u, q, uq[r]);
+            if (HAS_W) ld_pack<E, VW, VEC, true>(w, q, wq[r]);
+        }
+    }
+    A* mine = sacc + warp * kDotsSlots;
+    // the pass with kb = 0 also takes <u, u>, <u, w>, <w, w>; K = 0 makes it
+    // the only pass
+    for (int kb = 0; kb < (K > 0 ? K : 1); kb += T) {
+        PA p[P];  // p[t] <V_kb+t, u>, p[T + t] <V_kb+t, w>, p[X..] the three above, then padding
+        {
 #pragma unroll
-                    for (int t = 0; t < kMdTile; ++t)
-                        if (kb + t < K) {
-                            pdot_add(pacc[t], vk[t].x, wq.x);
-                            pdot_add(pacc[t], vk[t].y, wq.y);
-                            pdot_add(pacc[t], vk[t].z, wq.z);
-                            pdot_add(pacc[t], vk[t].w, wq.w);
+            for (int r = 0; r < R; ++r) {
+                if (!in[r]) continue;
+                const int64_t q = base + int64_t(r) * blockDim.x;
+                E vk[T][VW];
+#pragma unroll
+                for (int t = 0; t < T; ++t)
+                    if (kb + t < K) ld_pack<E, VW, VEC, true>(V + size_t(kb + t) * n, q, vk[t]);
+#pragma unroll
+                for (int t = 0; t < T; ++t)
+                    if (kb + t < K)
+#pragma unroll
+                        for (int j = 0; j < VW; ++j) {
+                            pdot_add(p[t], vk[t][j], uq[r][j]);
+                            if (HAS_W) pdot_add(p[T + t], vk[t][j], wq[r][j]);
                         }
-                }
+                if (kb == 0)
+#pragma unroll
+                    for (int j = 0; j < VW; ++j) {
+                        pdot_add(p[X], uq[r][j], uq[r][j]);
+                        if (HAS_W) {
+                            pdot_add(p[X + 1], uq[r][j], wq[r][j]);
+                            pdot_add(p[X + 2], wq[r][j], wq[r][j]);
+                        }
+                    }
             }
         }
-        bool vec2 = false;
-        if constexpr (std::is_same<E, double>::value) {
-            // binary64: two consecutive rows per thread with 16-byte loads
-            vec2 = n % 2 == 0 && ((reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(w)) & 15) == 0;
-            if (vec2) {
-                const double2* w2 = reinterpret_cast<const double2*>(w);
-                for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 2; q += stride) {
-                    const double2 wq = w2[q];
-                    double2 vk[kMdTile];
-#pragma unroll
-                    for (int t = 0; t < kMdTile; ++t)
-                        if (kb + t < K) vk[t] = __ldg(reinterpret_cast<const double2*>(V + size_t(kb + t) * n) + q);
-#pragma unroll
-                    for (int t = 0; t < kMdTile; ++t)
-                        if (kb + t < K) {
-                            pdot_add(pacc[t], vk[t].x, wq.x);
-                            pdot_add(pacc[t], vk[t].y, wq.y);
-                        }
-                }
+        warp_reduce_scatter<P>(p);
+        if ((lane & ((32 >> LP) - 1)) == 0) {
+            const int j = lane >> (5 - LP);
+            int d = -1;
+            if (j < T) {
+                if (kb + j < K) d = kb + j;
+            } else if (j < X) {
+                if (kb + j - T < K) d = K + kb + j - T;
+            } else if (j < ND) {
+                if (kb == 0) d = 2 * K + j - X;
             }
+            if (d >= 0) mine[d] = widen_acc(p[0]);
         }
-        for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; !vec4 && !vec2 && q < n; q += stride) {
-            const E wq = ldE(w, q);
-            E vk[kMdTile];
+    }
+    __syncthreads();
+    // block total of each dot: the warps' slots in warp order
+    const int nd = HAS_W ? 2 * K + 3 : K + 1;
+    for (int t = threadIdx.x; t < nd; t += blockDim.x) {
+        const int d = (HAS_W || t < K) ? t : 2 * K;
+        A a = sacc[d];
 #pragma unroll
-            for (int t = 0; t < kMdTile; ++t)
-                if (kb + t < K) vk[t] = ldE(V + size_t(kb + t) * n, q);
+        for (int wi = 1; wi < kDotsWarps; ++wi) merge(a, sacc[wi * kDotsSlots + d]);
+        partials[size_t(d) * gridDim.x + blockIdx.x] = a;
+    }
+}
+
+template <class E, bool HAS_W>
+__global__ void __launch_bounds__(kGmThreads, kDotsBlocksPerSm)
+k_dcgs_dots(int64_t n, int K, int vec, const E* __restrict__ V, const E* __restrict__ w,
+            typename acc_of<typename scalar_of<E>::type>::type* partials) {
+    using A = typename acc_of<typename scalar_of<E>::type>::type;
+    __shared__ A sacc[kDotsWarps * kDotsSlots];
+    const E* u = V + size_t(K) * n;
+    if (vec)
+        dots_body<E, HAS_W, pack_of<E>::value, true>(n, K, V, u, w, partials, sacc);
+    else
+        dots_body<E, HAS_W, 1, false>(n, K, V, u, w, partials, sacc);
+}
+
+// The binary32 steps (w present, 16-byte packs): each pack's element pairs
+// (x, y) and (z, w) go through the packed Dot2 (pdot_add2: the two lanes
+// accumulate the even and the odd elements), so one instruction serves two
+// elements.  Each thread takes R packs per pass, their u and w staged once
+// in its own shared-memory slots; the basis packs stream through a
+// per-thread two-stage ring of shared memory filled by cp.async one
+// (pass, pack) step ahead, across pass boundaries, so the next step's loads
+// are in flight while the current one is computed.  One reduce-scatter of
+// the 2T packed accumulators per pass merges the warp.  R is set per launch
+// so the grid is about one resident wave.
+constexpr int kF32T = 4;       // basis vectors per pass
+constexpr int kF32MaxR = 2;    // packs per thread per pass, at most
+constexpr int kF32BlocksPerSm = 3;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned a = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_none() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+__global__ void __launch_bounds__(kGmThreads, kF32BlocksPerSm)
+k_dcgs_dots_f32(int64_t n, int K, int R, const float* __restrict__ V, const float* __restrict__ w,
+                Acc2* partials) {
+    // dynamic: ring [2][kF32T][blockDim.x], then u / w [2 R][blockDim.x]
+    extern __shared__ uint4 dyn[];
+    __shared__ Acc2 sacc[kDotsWarps * kDotsSlots];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nt = int(blockDim.x);
+    uint4* ring = dyn;
+    uint4* suw = dyn + 2 * kF32T * nt;
+    const int64_t nq = n / 4;
+    const int64_t base = int64_t(blockIdx.x) * nt * R + threadIdx.x;
+    const uint4* V4 = reinterpret_cast<const uint4*>(V);
+    const uint4* u4 = V4 + size_t(K) * size_t(nq);
+    const uint4* w4 = reinterpret_cast<const uint4*>(w);
+    Acc2* mine = sacc + warp * kDotsSlots;
+    // the basis packs of pass kb, pack r into ring slot b
+    auto issue = [&](int kb, int r, int b) {
+        const int64_t q = base + int64_t(r) * nt;
+        if (kb < K && q < nq) {
+            uint4* slot = ring + b * kF32T * nt + threadIdx.x;
 #pragma unroll
-            for (int t = 0; t < kMdTile; ++t)
-                if (kb + t < K) pdot_add(pacc[t], vk[t], wq);
+            for (int t = 0; t < kF32T; ++t)
+                if (kb + t < K) cp_async16(slot + t * nt, V4 + size_t(kb + t) * size_t(nq) + q);
         }
-        A acc[kMdTile];
+        cp_async_commit();
+    };
+    issue(0, 0, 0);
+    // stage u and w; <u, u>, <u, w>, <w, w> on the way
+    Acc2x2 ex[4];
+    for (int r = 0; r < R; ++r) {
+        const int64_t q = base + int64_t(r) * nt;
+        if (q >= nq) break;
+        const uint4 ua = __ldg(u4 + q), wa = __ldg(w4 + q);
+        suw[(2 * r) * nt + threadIdx.x] = ua;
+        suw[(2 * r + 1) * nt + threadIdx.x] = wa;
+        f32x2 U[2], W[2];
+        memcpy(U, &ua, 16);
+        memcpy(W, &wa, 16);
 #pragma unroll
-        for (int t = 0; t < kMdTile; ++t) acc[t] = widen_acc(pacc[t]);
-        __syncthreads();  // sh is reused across passes
-        block_merge<kMdTile>(acc, sh);
-        if (threadIdx.x == 0)
+        for (int h = 0; h < 2; ++h) {
+            pdot_add2(ex[0], U[h], U[h], neg2(U[h]));
+            pdot_add2(ex[1], U[h], W[h], neg2(W[h]));
+            pdot_add2(ex[2], W[h], W[h], neg2(W[h]));
+        }
+    }
+    warp_reduce_scatter<4>(ex);
+    if ((lane & 7) == 0 && (lane >> 3) < 3) mine[2 * K + (lane >> 3)] = widen_lanes(ex[0]);
+    // the passes over the basis (own shared slots only: no barrier)
+    int b = 0;
+    for (int kb = 0; kb < K; kb += kF32T) {
+        Acc2x2 p[2 * kF32T];  // p[t] <V_kb+t, u>, p[T + t] <V_kb+t, w>
+        for (int r = 0; r < R; ++r) {
+            cp_async_wait_none();  // this step's packs have landed
+            // the next step's packs into the other slot (read in the previous step)
+            if (r + 1 < R)
+                issue(kb, r + 1, b ^ 1);
+            else
+                issue(kb + kF32T, 0, b ^ 1);
+            const int64_t q = base + int64_t(r) * nt;
+            if (q < nq) {
+                const uint4* slot = ring + b * kF32T * nt + threadIdx.x;
+                const uint4 ua = suw[(2 * r) * nt + threadIdx.x], wa = suw[(2 * r + 1) * nt + threadIdx.x];
+                f32x2 U[2], W[2], NU[2], NW[2];
+                memcpy(U, &ua, 16);
+                memcpy(W, &wa, 16);
 #pragma unroll
-            for (int t = 0; t < kMdTile; ++t)
-                if (kb + t < K) partials[size_t(kb + t) * gridDim.x + blockIdx.x] = acc[t];
+                for (int h = 0; h < 2; ++h) {
+                    NU[h] = neg2(U[h]);
+                    NW[h] = neg2(W[h]);
+                }
+#pragma unroll
+                for (int t = 0; t < kF32T; ++t)
+                    if (kb + t < K) {
+                        const uint4 vk = slot[t * nt];
+                        f32x2 X[2];
+                        memcpy(X, &vk, 16);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            pdot_add2(p[t], X[h], U[h], NU[h]);
+                            pdot_add2(p[kF32T + t], X[h], W[h], NW[h]);
+                        }
+                    }
+            }
+            b ^= 1;
+        }
+        warp_reduce_scatter<2 * kF32T>(p);
+        if ((lane & 3) == 0) {
+            const int j = lane >> 2;
+            const int k = kb + (j < kF32T ? j : j - kF32T);
+            if (k < K) mine[j < kF32T ? k : K + k] = widen_lanes(p[0]);
+        }
+    }
+    cp_async_wait_none();
+    __syncthreads();
+    // block total of each dot: the warps' slots in warp order
+    for (int d = threadIdx.x; d < 2 * K + 3; d += nt) {
+        Acc2 a = sacc[d];
+#pragma unroll
+        for (int wi = 1; wi < kDotsWarps; ++wi) merge(a, sacc[wi * kDotsSlots + d]);
+        partials[size_t(d) * gridDim.x + blockIdx.x] = a;
     }
 }
 
 template <class S>
+__device__ __forceinline__ S ldcg_s(const S* p);
+template <>
+__device__ __forceinline__ double ldcg_s<double>(const double* p) { return __ldcg(p); }
+template <>
+__device__ __forceinline__ cd ldcg_s<cd>(const cd* p) {
+    const double* q = reinterpret_cast<const double*>(p);
+    return cd{__ldcg(q), __ldcg(q + 1)};
+}
+__device__ __forceinline__ double abs2(double v) { return v * v; }
+__device__ __forceinline__ double abs2(cd v) { return v.re * v.re + v.im * v.im; }
+
+// Block d merges dot d's block partials (in block order) into st->dots[d];
+// the block that draws the last ticket then runs the step's scalar work
+// (see the DCGS2 comment above).  K = i, the step; last: the closing
+// reduction of the cycle (no w; K + 1 blocks: a_k and <u, u>).  The last
+// block first stages what its serial parts read -- a, b, the Givens
+// rotations and the band of H's columns 0..i-1 (rows 0..k+1 of column k,
+// packed at band_off(k)) -- in shared memory with parallel loads.
+__host__ __device__ constexpr int band_off(int k) { return k * (k + 3) / 2; }
+
+template <class S>
 __global__ void __launch_bounds__(kGmThreads)
-k_mdot_finish(int nb, const typename acc_of<S>::type* __restrict__ partials, S* __restrict__ out) {
+k_dcgs_finish(int nb, int K, int last, const typename acc_of<S>::type* __restrict__ partials, GmState<S>* st, int m,
+              unsigned int* ticket) {
     using A = typename acc_of<S>::type;
     __shared__ A sh[32];
-    const int k = blockIdx.x;
+    __shared__ bool am_last;
+    __shared__ S sa[kGmMaxM], sb[kGmMaxM], stt[kGmMaxM + 1], scol[kGmMaxM + 1];
+    __shared__ S scs[kGmMaxM], ssn[kGmMaxM];
+    __shared__ S shr[band_off(kGmMaxM)];
+    __shared__ double s_nu;
+    __shared__ int s_go;
+    const int tid = threadIdx.x;
+    const int d = (last && int(blockIdx.x) == K) ? 2 * K : int(blockIdx.x);
     A t[1];
-    t[0] = merge_partials<A>(partials + size_t(k) * nb, nb);
+    t[0] = merge_partials<A>(partials + size_t(d) * nb, nb);
     block_merge<1>(t, sh);
-    if (threadIdx.x == 0) out[k] = acc_value(t[0]);
+    if (tid == 0) {
+        st->dots[d] = acc_value(t[0]);
+        // acquire-release ticket: releases this block's dot to the block that
+        // draws the last ticket (the barrier below extends it to its threads)
+        unsigned tk;
+        asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(tk) : "l"(ticket) : "memory");
+        am_last = tk == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!am_last) return;
+    GmState<S>& g = *st;
+    const int i = K, ld = m + 1;
+    if (tid < i) {
+        sa[tid] = ldcg_s(g.dots + tid);
+        if (!last) sb[tid] = ldcg_s(g.dots + i + tid);
+        scs[tid] = g.cs[tid];
+        ssn[tid] = g.sn[tid];
+        const S* col = g.Hr + size_t(tid) * ld;
+        S* dst = shr + band_off(tid);
+#pragma unroll 8
+        for (int r = 0; r <= tid + 1; ++r) dst[r] = col[r];
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double nu = 1.0;  // V_0 = r / beta is final as written
+        if (i > 0) {
+            double nn = s_real(ldcg_s(g.dots + 2 * i));
+            for (int k = 0; k < i; ++k) nn -= abs2(sa[k]);
+            nu = nn > 0.0 ? sqrt(nn) : (nn == 0.0 || nn < 0.0 ? 0.0 : nn);  // NaN stays NaN
+        }
+        s_nu = nu;
+        s_go = !g.broken;
+    }
+    __syncthreads();
+    const double nu = s_nu;
+    if (s_go && i > 0) {
+        // complete column i-1 (its re-orthogonalisation) and take its Givens step
+        const double al = g.alpha;
+        S* hb = shr + band_off(i - 1);  // rows 0..i
+        if (tid < i) hb[tid] = s_fma(make_real<S>(al), sa[tid], hb[tid]);
+        if (tid == 0) hb[i] = make_real<S>(al * nu);
+        __syncthreads();
+        if (tid <= i) g.Hr[size_t(i - 1) * ld + tid] = hb[tid];
+        if (tid == 0) {
+            const int j = i - 1;
+            S x = hb[0];
+            for (int k = 0; k < j; ++k) {  // the earlier rotations, x carried down the column
+                S y = hb[k + 1];
+                giv_apply(x, y, scs[k], ssn[k]);
+                scol[k] = x;
+                x = y;
+            }
+            S y = hb[i];
+            S c, sn;
+            giv_make(x, y, c, sn);
+            giv_apply(x, y, c, sn);
+            scol[j] = x;
+            scol[i] = s_zero(S{});
+            g.cs[j] = c;
+            g.sn[j] = sn;
+            S s0 = g.s[j], s1 = g.s[j + 1];
+            giv_apply(s0, s1, c, sn);
+            g.s[j] = s0;
+            g.s[j + 1] = s1;
+            g.est = s_abs(s1);
+            g.nsteps = i;
+            if (!(nu > 0.0) || !isfinite(nu)) {
+                g.broken = 1;  // happy breakdown (u in the span of the basis) or overflow
+                s_go = 0;
+            }
+        }
+        __syncthreads();
+        if (tid <= i) g.H[size_t(i - 1) * ld + tid] = scol[tid];
+    }
+    if (!s_go || last) {
+        if (tid == 0) *ticket = 0;
+        return;
+    }
+    // column i: t = Q_{i+1}^H w, first projection (t - H a) / nu
+    if (tid < i) stt[tid] = sb[tid];
+    if (tid == 0) {
+        S c = ldcg_s(g.dots + 2 * i + 1);
+        for (int k = 0; k < i; ++k) c = s_sub(c, s_mul(conj_s(sa[k]), sb[k]));
+        stt[i] = s_mul(make_real<S>(1.0 / nu), c);
+    }
+    __syncthreads();
+    if (tid <= i) {
+        S h = stt[tid];
+        for (int k = tid > 0 ? tid - 1 : 0; k < i; ++k) h = s_sub(h, s_mul(shr[band_off(k) + tid], sa[k]));
+        g.Hr[size_t(i) * ld + tid] = s_mul(make_real<S>(1.0 / nu), h);
+        g.nt[tid] = s_neg(stt[tid]);
+        if (tid < i) g.na[tid] = s_neg(sa[tid]);
+    }
+    if (tid == 0) {
+        const double e = s_real(ldcg_s(g.dots + 2 * i + 2));
+        double tt = 0.0;
+        for (int k = 0; k <= i; ++k) tt += abs2(stt[k]);
+        const double a2 = (e - tt) / (nu * nu);
+        double al = a2 > 0.0 ? sqrt(a2) : 0.0;
+        if (!(al > 0.0) || !isfinite(al)) {
+            // cancellation left no usable estimate: any positive scale will
+            // do, a small one keeps the next vector near unit norm
+            const double r = sqrt(e) / nu * 1e-8;
+            al = (r > 0.0 && isfinite(r)) ? r : 1.0;
+        }
+        if (!isfinite(e) || !isfinite(tt)) g.broken = 1;  // non-finite product: columns 0..i-1 stand
+        g.inv_nu = 1.0 / nu;
+        g.f = 1.0 / (nu * al);
+        g.alpha = al;
+        *ticket = 0;
+    }
+}
+
+// V_i = (u - sum_k a_k V_k) / nu and V_{i+1} = (w - sum_k t_k V_k - t_i V_i)
+// / (nu alpha') in one pass (u = V_i on entry, K = i); each row accumulates
+// in the scalar type and rounds once.  At i = 0, V_0 stays.  After a
+// breakdown both slots are set to zero (the solution update reads every
+// slot with a zero coefficient past the breakdown).
+constexpr int kUpdBatch = 8;
+
+template <class E, int VW, bool VEC>
+__device__ __forceinline__ void update_body(int64_t n, int K, E* V, const E* __restrict__ w,
+                                            const typename scalar_of<E>::type* sna,
+                                            const typename scalar_of<E>::type* snt,
+                                            const GmState<typename scalar_of<E>::type>& g) {
+    using S = typename scalar_of<E>::type;
+    const int64_t nq = VEC ? n / VW : n;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    E* vi = V + size_t(K) * n;
+    E* vn = V + size_t(K + 1) * n;
+    if (g.broken) {
+        E z[VW];
+#pragma unroll
+        for (int j = 0; j < VW; ++j) z[j] = from_s<E>(s_zero(S{}));
+        for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq; q += stride) {
+            if (K > 0) st_pack<E, VW, VEC>(vi, q, z);
+            st_pack<E, VW, VEC>(vn, q, z);
+        }
+        return;
+    }
+    const S inv_nu = make_real<S>(g.inv_nu), f = make_real<S>(g.f), nti = snt[K];
+    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < nq; q += stride) {
+        E ue[VW], we[VW];
+        ld_pack<E, VW, VEC, false>(vi, q, ue);
+        ld_pack<E, VW, VEC, true>(w, q, we);
+        S qa[VW], wa[VW];
+#pragma unroll
+        for (int j = 0; j < VW; ++j) {
+            qa[j] = to_s(ue[j]);
+            wa[j] = to_s(we[j]);
+        }
+        // kUpdBatch basis packs in flight per thread, the FMAs in k order
+        int k = 0;
+        for (; k + kUpdBatch <= K; k += kUpdBatch) {
+            E vk[kUpdBatch][VW];
+#pragma unroll
+            for (int b = 0; b < kUpdBatch; ++b) ld_pack<E, VW, VEC, true>(V + size_t(k + b) * n, q, vk[b]);
+#pragma unroll
+            for (int b = 0; b < kUpdBatch; ++b) {
+                const S ak = sna[k + b], tk = snt[k + b];
+#pragma unroll
+                for (int j = 0; j < VW; ++j) {
+                    const S v = to_s(vk[b][j]);
+                    qa[j] = s_fma(ak, v, qa[j]);
+                    wa[j] = s_fma(tk, v, wa[j]);
+                }
+            }
+        }
+        for (; k < K; ++k) {
+            E vk[VW];
+            ld_pack<E, VW, VEC, true>(V + size_t(k) * n, q, vk);
+            const S ak = sna[k], tk = snt[k];
+#pragma unroll
+            for (int j = 0; j < VW; ++j) {
+                const S v = to_s(vk[j]);
+                qa[j] = s_fma(ak, v, qa[j]);
+                wa[j] = s_fma(tk, v, wa[j]);
+            }
+        }
+        E qe[VW], ne[VW];
+#pragma unroll
+        for (int j = 0; j < VW; ++j) {
+            qe[j] = K > 0 ? from_s<E>(s_mul(inv_nu, qa[j])) : ue[j];
+            ne[j] = from_s<E>(s_mul(f, s_fma(nti, to_s(qe[j]), wa[j])));
+        }
+        if (K > 0) st_pack<E, VW, VEC>(vi, q, qe);
+        st_pack<E, VW, VEC>(vn, q, ne);
+    }
+}
+
+template <class E>
+__global__ void __launch_bounds__(kGmThreads)
+k_dcgs_update(int64_t n, int K, int vec, E* V, const E* __restrict__ w,
+              const GmState<typename scalar_of<E>::type>* st) {
+    using S = typename scalar_of<E>::type;
+    __shared__ S sna[kGmMaxM], snt[kGmMaxM + 1];
+    for (int k = threadIdx.x; k <= K; k += blockDim.x) {
+        if (k < K) sna[k] = st->na[k];
+        snt[k] = st->nt[k];
+    }
+    __syncthreads();
+    if (vec)
+        update_body<E, pack_of<E>::value, true>(n, K, V, w, sna, snt, *st);
+    else
+        update_body<E, 1, false>(n, K, V, w, sna, snt, *st);
 }
 
 // ------------------------------------------------------------ updates
-// wout = win - sum_{k<K} coef[k] V_k ; if NORM: ||wout|| in Dot2 and the
-// Arnoldi column step (Hessenberg, Givens, residual estimate) in the last
-// block.  With step < 0 the epilogue only stores the norm.
-template <class E, bool NORM>
+// wout = win - sum_{k<K} coef[k] V_k (the solution update x += V y).
+template <class E>
 __global__ void __launch_bounds__(kGmThreads)
 k_gs_update(int64_t n, int K, const E* __restrict__ V, const E* win, E* wout,
-            const typename scalar_of<E>::type* __restrict__ coef, GmState<typename scalar_of<E>::type>* st, int m,
-            int step, typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket,
-            int* badflag) {
+            const typename scalar_of<E>::type* __restrict__ coef) {
     using S = typename scalar_of<E>::type;
-    using A = typename acc_of<S>::type;
     __shared__ S sc[kGmMaxM + 1];
     for (int k = threadIdx.x; k < K; k += blockDim.x) sc[k] = s_neg(coef[k]);
     __syncthreads();
-    typename pacc_of<E>::type pacc;
-    bool bad = false;
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     // binary32: four consecutive rows per thread with 16-byte loads and
     // stores (each row's FMA chain unchanged); win may equal wout, and each
@@ -242,16 +670,8 @@ k_gs_update(int64_t n, int K, const E* __restrict__ V, const E* win, E* wout,
                     v2 = s_fma(sc[k], to_s(vk.z), v2);
                     v3 = s_fma(sc[k], to_s(vk.w), v3);
                 }
-                const float4 v = make_float4(from_s<float>(v0), from_s<float>(v1), from_s<float>(v2),
-                                             from_s<float>(v3));
-                reinterpret_cast<float4*>(wout)[q] = v;
-                if (NORM) {
-                    pdot_add(pacc, v.x, v.x);
-                    pdot_add(pacc, v.y, v.y);
-                    pdot_add(pacc, v.z, v.z);
-                    pdot_add(pacc, v.w, v.w);
-                    bad |= !finite_e(v.x) || !finite_e(v.y) || !finite_e(v.z) || !finite_e(v.w);
-                }
+                reinterpret_cast<float4*>(wout)[q] = make_float4(from_s<float>(v0), from_s<float>(v1),
+                                                                 from_s<float>(v2), from_s<float>(v3));
             }
         }
     }
@@ -270,64 +690,14 @@ k_gs_update(int64_t n, int K, const E* __restrict__ V, const E* win, E* wout,
                     v1 = s_fma(sc[k], vk.y, v1);
                 }
                 reinterpret_cast<double2*>(wout)[q] = make_double2(v0, v1);
-                if (NORM) {
-                    pdot_add(pacc, v0, v0);
-                    pdot_add(pacc, v1, v1);
-                    bad |= !finite_e(v0) || !finite_e(v1);
-                }
             }
         }
     }
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; !vec4 && !vec2 && q < n; q += stride) {
         S v = to_s(ldE(win, q));
         for (int k = 0; k < K; ++k) v = s_fma(sc[k], to_s(ldE(V + size_t(k) * n, q)), v);
-        E ve = from_s<E>(v);
-        stE(wout, q, ve);
-        if (NORM) {
-            pdot_add(pacc, ve, ve);
-            bad |= !finite_e(ve);
-        }
+        stE(wout, q, from_s<E>(v));
     }
-    if (!NORM) return;
-    A acc[1] = {widen_acc(pacc)};
-    grid_finish<1>(acc, bad, partials, ticket, badflag, [&](const S* vals, bool anybad) {
-        GmState<S>& g = *st;
-        const double hn = norm_sqrt(s_real(vals[0]));
-        if (step < 0) {  // plain norm request
-            g.rnorm = hn;
-            g.nonfinite = anybad ? 1 : 0;
-            return;
-        }
-        const int i = step, ld = m + 1;
-        if (g.broken) return;
-        S* col = g.H + size_t(i) * ld;
-        for (int k = 0; k <= i; ++k) col[k] = s_add(g.h1[k], g.h2[k]);
-        col[i + 1] = make_real<S>(hn);
-        for (int k = 0; k < i; ++k) giv_apply(col[k], col[k + 1], g.cs[k], g.sn[k]);
-        giv_make(col[i], col[i + 1], g.cs[i], g.sn[i]);
-        giv_apply(col[i], col[i + 1], g.cs[i], g.sn[i]);
-        col[i + 1] = s_zero(S{});
-        giv_apply(g.s[i], g.s[i + 1], g.cs[i], g.sn[i]);
-        g.est = s_abs(g.s[i + 1]);
-        g.nsteps = i + 1;
-        if (hn == 0.0 || anybad) {
-            g.broken = 1;  // happy breakdown (or overflow): stop extending the basis
-            g.inv_h = 0.0;
-        } else {
-            g.inv_h = 1.0 / hn;
-        }
-    });
-}
-
-// y = x * st->inv_h
-template <class E>
-__global__ void __launch_bounds__(kGmThreads)
-k_gm_scale(int64_t n, const E* __restrict__ x, E* __restrict__ y, const GmState<typename scalar_of<E>::type>* st) {
-    using S = typename scalar_of<E>::type;
-    const S f = make_real<S>(st->inv_h);
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride)
-        stE(y, q, from_s<E>(s_mul(f, to_s(ldE(x, q)))));
 }
 
 // cycle start: V_0 = r / beta, s = (beta, 0, ...), reset the step state
@@ -347,6 +717,7 @@ k_gm_start(int64_t n, const E* __restrict__ r, E* __restrict__ v0, GmState<typen
         st->nsteps = 0;
         st->broken = beta > 0.0 ? 0 : 1;
         st->est = beta;
+        st->alpha = 1.0;
     }
 }
 
@@ -486,9 +857,8 @@ int gm_occupancy() {
         int o = 0;
         return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, kGmThreads, 0) == cudaSuccess && o > 0 ? o : 1;
     };
-    int o = occ(reinterpret_cast<const void*>(k_gs_update<E, false>));
-    o = std::min(o, occ(reinterpret_cast<const void*>(k_gs_update<E, true>)));
-    o = std::min(o, occ(reinterpret_cast<const void*>(k_gm_scale<E>)));
+    int o = occ(reinterpret_cast<const void*>(k_gs_update<E>));
+    o = std::min(o, occ(reinterpret_cast<const void*>(k_dcgs_update<E>)));
     o = std::min(o, occ(reinterpret_cast<const void*>(k_gm_jacobi<E>)));
     o = std::min(o, occ(reinterpret_cast<const void*>(k_gm_start<E>)));
     o = std::min(o, occ(reinterpret_cast<const void*>(k_gm_norm<E>)));
@@ -508,6 +878,8 @@ struct GmPlan<E>::Impl {
     const E* b = nullptr;
     E* x = nullptr;
     int g_ew = 1, g_md = 1, g_sp = 1, g_rc = 1, kernels = 0;
+    int vec = 0;  // the basis and w move as 16-byte packs
+    int g_f32 = 0, r_f32 = 0;  // grid and packs per thread of k_dcgs_dots_f32 (binary32 steps)
     SolverWorkspace ws;
     E *V = nullptr, *W = nullptr, *Z = nullptr, *R = nullptr, *diag = nullptr, *T = nullptr;
     GmState<S>* st = nullptr;
@@ -554,12 +926,14 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     const int64_t n = rows;
     const int g_ew = P.g_ew = int(
         std::max<int64_t>(1, std::min<int64_t>((n + kGmThreads - 1) / kGmThreads, int64_t(sms) * gm_occupancy<E>())));
-    int occ_md = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_md, reinterpret_cast<const void*>(k_multidot<E>), kGmThreads,
-                                                      0) != cudaSuccess || occ_md < 1)
-        occ_md = 1;
-    const int g_md = P.g_md = int(
-        std::max<int64_t>(1, std::min<int64_t>((n + kGmThreads - 1) / kGmThreads, int64_t(sms) * occ_md)));
+    // k_dcgs_dots: one pass over the vector, R packs (or elements) per
+    // thread; the partials are sized for elements, the grid is set once the
+    // basis is allocated and its alignment known
+    auto dots_grid = [&](int64_t items) {
+        constexpr int64_t per_block = int64_t(kGmThreads) * dots_shape<E>::R;
+        return int(std::max<int64_t>(1, (items + per_block - 1) / per_block));
+    };
+    const int g_md_max = dots_grid(n);
     const int g_sp = P.g_sp =
         int(std::max<int64_t>(1, std::min<int64_t>((int64_t(rows) + kGmThreads - 1) / kGmThreads, int64_t(sms) * 8)));
     // the compensated residual (k_resid_comp) takes one row per thread
@@ -580,7 +954,7 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     P.T = (M.kind == 3 && M.sweeps > 0) ? static_cast<E*>(ws.alloc(vb)) : nullptr;
     if (M.kind == 3 && M.sweeps > 0 && !P.T) return HPB_ERROR_OUT_OF_MEMORY;
     auto* st = P.st = static_cast<GmState<S>*>(ws.alloc(sizeof(GmState<S>)));
-    const size_t np = std::max<size_t>(size_t(m + 1) * g_md, std::max<size_t>(g_ew, std::max(g_sp, g_rc)));
+    const size_t np = std::max<size_t>(size_t(2 * m + 3) * g_md_max, std::max<size_t>(g_ew, std::max(g_sp, g_rc)));
     auto* partials = P.partials = static_cast<A*>(ws.alloc(np * sizeof(A)));
     auto* ticket = P.ticket = static_cast<unsigned int*>(ws.alloc(64));
     auto* badflag = P.badflag = static_cast<int*>(ws.alloc(64));
@@ -589,6 +963,24 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
         !P.dnorm)
         return HPB_ERROR_OUT_OF_MEMORY;
     auto* hv = P.hv = static_cast<GmHostView*>(ws.pinned);
+    const int vec = P.vec = (n % pack_of<E>::value == 0 &&
+                             ((reinterpret_cast<uintptr_t>(V) | reinterpret_cast<uintptr_t>(W)) & 15) == 0) ? 1 : 0;
+    const int g_md = P.g_md = dots_grid(vec ? n / pack_of<E>::value : n);
+    int g_f32 = 0, r_f32 = 0;
+    size_t smem_f32 = 0;
+    if constexpr (std::is_same<E, float>::value) {
+        if (vec) {
+            const int64_t packs = n / 4, wave = int64_t(kGmThreads) * sms * kF32BlocksPerSm;
+            r_f32 = int(std::min<int64_t>(kF32MaxR, std::max<int64_t>(1, (packs + wave - 1) / wave)));
+            g_f32 = int((packs + int64_t(kGmThreads) * r_f32 - 1) / (int64_t(kGmThreads) * r_f32));
+            smem_f32 = (size_t(2) * kF32T + size_t(2) * r_f32) * kGmThreads * sizeof(uint4);
+            if (cudaFuncSetAttribute(reinterpret_cast<const void*>(k_dcgs_dots_f32),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_f32)) != cudaSuccess)
+                return HPB_ERROR_CUDA;
+        }
+    }
+    P.g_f32 = g_f32;
+    P.r_f32 = r_f32;
     cudaMemsetAsync(ticket, 0, 64, s);
     cudaMemsetAsync(badflag, 0, 64, s);
     if (M.kind == 1) {
@@ -626,28 +1018,34 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
             kernels += 2 * (M.sweeps + 1);
         }
         k_gm_spmv<E><<<g_sp, kGmThreads, 0, s>>>(rows, rp, ci, val, src, W);
-        k_multidot<E><<<g_md, kGmThreads, 0, s>>>(n, i + 1, V, W, partials);
-        k_mdot_finish<S><<<i + 1, kGmThreads, 0, s>>>(g_md, partials, st->h1);
-        k_gs_update<E, false><<<g_ew, kGmThreads, 0, s>>>(n, i + 1, V, W, W, st->h1, st, m, i, partials, ticket,
-                                                           badflag);
-        k_multidot<E><<<g_md, kGmThreads, 0, s>>>(n, i + 1, V, W, partials);
-        k_mdot_finish<S><<<i + 1, kGmThreads, 0, s>>>(g_md, partials, st->h2);
-        k_gs_update<E, true><<<g_ew, kGmThreads, 0, s>>>(n, i + 1, V, W, W, st->h2, st, m, i, partials, ticket,
-                                                          badflag);
-        k_gm_scale<E><<<g_ew, kGmThreads, 0, s>>>(n, W, V + size_t(i + 1) * n, st);
-        kernels += 8;
+        int nb = g_md;
+        if constexpr (std::is_same<E, float>::value) {
+            if (g_f32 > 0) {
+                k_dcgs_dots_f32<<<g_f32, kGmThreads, smem_f32, s>>>(n, i, r_f32, V, W, partials);
+                nb = g_f32;
+            } else {
+                k_dcgs_dots<E, true><<<g_md, kGmThreads, 0, s>>>(n, i, vec, V, W, partials);
+            }
+        } else {
+            k_dcgs_dots<E, true><<<g_md, kGmThreads, 0, s>>>(n, i, vec, V, W, partials);
+        }
+        k_dcgs_finish<S><<<2 * i + 3, kGmThreads, 0, s>>>(nb, i, 0, partials, st, m, ticket);
+        k_dcgs_update<E><<<g_ew, kGmThreads, 0, s>>>(n, i, vec, V, W, st);
+        kernels += 4;
     }
+    // closing reduction: <V_k, V_m>, <V_m, V_m> complete column m-1
+    k_dcgs_dots<E, false><<<g_md, kGmThreads, 0, s>>>(n, m, vec, V, static_cast<const E*>(nullptr), partials);
+    k_dcgs_finish<S><<<m + 1, kGmThreads, 0, s>>>(g_md, m, 1, partials, st, m, ticket);
+    kernels += 2;
     k_gm_solve<S><<<1, 1, 0, s>>>(st, m);
     ++kernels;
     if (M.kind == 0) {
-        k_gs_update<E, false><<<g_ew, kGmThreads, 0, s>>>(n, m, V, x, x, st->neg_y, st, m, -1, partials, ticket,
-                                                           badflag);
+        k_gs_update<E><<<g_ew, kGmThreads, 0, s>>>(n, m, V, x, x, st->neg_y);
         ++kernels;
     } else {
         // t = V y, then x += M t
         cudaMemsetAsync(W, 0, vb, s);
-        k_gs_update<E, false><<<g_ew, kGmThreads, 0, s>>>(n, m, V, W, W, st->neg_y, st, m, -1, partials, ticket,
-                                                           badflag);
+        k_gs_update<E><<<g_ew, kGmThreads, 0, s>>>(n, m, V, W, W, st->neg_y);
         if (M.kind == 1) {
             k_gm_jacobi<E><<<g_ew, kGmThreads, 0, s>>>(n, W, diag, Z);
         } else if (M.kind == 2) {
