@@ -622,6 +622,92 @@ __device__ __forceinline__ void update_body(int64_t n, int K, E* V, const E* __r
     }
 }
 
+// The 16-byte-pack form with a per-thread two-stage cp.async ring: the
+// thread's work is a sequence of (row pack q, batch of kUpdRing basis
+// vectors) items, the first batch of a row also bringing u and w; the next
+// item's packs are in flight (across row boundaries) while the current one
+// is computed.  The same FMAs in the same k order as update_body.
+constexpr int kUpdRing = 6;                  // basis packs per item
+constexpr int kUpdSlot = kUpdRing + 2;       // + u and w
+template <class E, int VW>
+__device__ __forceinline__ void update_ring(int64_t n, int K, E* V, const E* __restrict__ w,
+                                            const typename scalar_of<E>::type* sna,
+                                            const typename scalar_of<E>::type* snt,
+                                            const GmState<typename scalar_of<E>::type>& g, uint4* ring) {
+    using S = typename scalar_of<E>::type;
+    const int64_t nq = n / VW;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const int nt = int(blockDim.x), tid = int(threadIdx.x);
+    const uint4* V4 = reinterpret_cast<const uint4*>(V);
+    const uint4* w4 = reinterpret_cast<const uint4*>(w);
+    E* vi = V + size_t(K) * n;
+    E* vn = V + size_t(K + 1) * n;
+    const S inv_nu = make_real<S>(g.inv_nu), f = make_real<S>(g.f), nti = snt[K];
+    auto issue = [&](int64_t q, int kb, int slot) {
+        if (q < nq) {
+            uint4* dst = ring + slot * kUpdSlot * nt + tid;
+            for (int b = 0; b < kUpdRing && kb + b < K; ++b)
+                cp_async16(dst + b * nt, V4 + size_t(kb + b) * size_t(nq) + q);
+            if (kb == 0) {
+                cp_async16(dst + kUpdRing * nt, V4 + size_t(K) * size_t(nq) + q);
+                cp_async16(dst + (kUpdRing + 1) * nt, w4 + q);
+            }
+        }
+        cp_async_commit();
+    };
+    int64_t q = int64_t(blockIdx.x) * nt + tid;
+    int kb = 0, slot = 0;
+    issue(q, 0, 0);
+    E ue[VW];
+    S qa[VW], wa[VW];
+    while (q < nq) {
+        cp_async_wait_none();
+        const int64_t nq2 = kb + kUpdRing < K ? q : q + stride;
+        const int nkb2 = kb + kUpdRing < K ? kb + kUpdRing : 0;
+        issue(nq2, nkb2, slot ^ 1);
+        const uint4* src = ring + slot * kUpdSlot * nt + tid;
+        if (kb == 0) {
+            const uint4 ua = src[kUpdRing * nt], wa4 = src[(kUpdRing + 1) * nt];
+            E we[VW];
+            memcpy(ue, &ua, 16);
+            memcpy(we, &wa4, 16);
+#pragma unroll
+            for (int j = 0; j < VW; ++j) {
+                qa[j] = to_s(ue[j]);
+                wa[j] = to_s(we[j]);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < kUpdRing; ++b) {
+            if (kb + b >= K) break;
+            const uint4 pk = src[b * nt];
+            E vk[VW];
+            memcpy(vk, &pk, 16);
+            const S ak = sna[kb + b], tk = snt[kb + b];
+#pragma unroll
+            for (int j = 0; j < VW; ++j) {
+                const S v = to_s(vk[j]);
+                qa[j] = s_fma(ak, v, qa[j]);
+                wa[j] = s_fma(tk, v, wa[j]);
+            }
+        }
+        if (kb + kUpdRing >= K) {  // the row is complete
+            E qe[VW], ne[VW];
+#pragma unroll
+            for (int j = 0; j < VW; ++j) {
+                qe[j] = from_s<E>(s_mul(inv_nu, qa[j]));
+                ne[j] = from_s<E>(s_mul(f, s_fma(nti, to_s(qe[j]), wa[j])));
+            }
+            st_pack<E, VW, true>(vi, q, qe);
+            st_pack<E, VW, true>(vn, q, ne);
+        }
+        q = nq2;
+        kb = nkb2;
+        slot ^= 1;
+    }
+    cp_async_wait_none();
+}
+
 template <class E>
 __global__ void __launch_bounds__(kGmThreads)
 k_dcgs_update(int64_t n, int K, int vec, E* V, const E* __restrict__ w,
@@ -633,10 +719,14 @@ k_dcgs_update(int64_t n, int K, int vec, E* V, const E* __restrict__ w,
         snt[k] = st->nt[k];
     }
     __syncthreads();
-    if (vec)
+    if (vec && K > 0 && !st->broken) {
+        extern __shared__ uint4 ring[];  // [2][kUpdSlot][blockDim.x]
+        update_ring<E, pack_of<E>::value>(n, K, V, w, sna, snt, *st, ring);
+    } else if (vec) {
         update_body<E, pack_of<E>::value, true>(n, K, V, w, sna, snt, *st);
-    else
+    } else {
         update_body<E, 1, false>(n, K, V, w, sna, snt, *st);
+    }
 }
 
 // ------------------------------------------------------------ updates
@@ -981,6 +1071,21 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     }
     P.g_f32 = g_f32;
     P.r_f32 = r_f32;
+    // k_dcgs_update: the 16-byte-pack form takes a two-stage ring of
+    // 2 x kUpdSlot packs per thread in dynamic shared memory; one resident wave
+    const size_t smem_up = vec ? size_t(2) * kUpdSlot * kGmThreads * sizeof(uint4) : 0;
+    int g_up = g_ew;
+    if (vec) {
+        if (cudaFuncSetAttribute(reinterpret_cast<const void*>(k_dcgs_update<E>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_up)) != cudaSuccess)
+            return HPB_ERROR_CUDA;
+        int occ_up = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_up, reinterpret_cast<const void*>(k_dcgs_update<E>),
+                                                          kGmThreads, smem_up) != cudaSuccess || occ_up < 1)
+            occ_up = 1;
+        g_up = int(std::max<int64_t>(1, std::min<int64_t>((n / pack_of<E>::value + kGmThreads - 1) / kGmThreads,
+                                                          int64_t(sms) * occ_up)));
+    }
     cudaMemsetAsync(ticket, 0, 64, s);
     cudaMemsetAsync(badflag, 0, 64, s);
     if (M.kind == 1) {
@@ -1030,7 +1135,7 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
             k_dcgs_dots<E, true><<<g_md, kGmThreads, 0, s>>>(n, i, vec, V, W, partials);
         }
         k_dcgs_finish<S><<<2 * i + 3, kGmThreads, 0, s>>>(nb, i, 0, partials, st, m, ticket);
-        k_dcgs_update<E><<<g_ew, kGmThreads, 0, s>>>(n, i, vec, V, W, st);
+        k_dcgs_update<E><<<g_up, kGmThreads, smem_up, s>>>(n, i, vec, V, W, st);
         kernels += 4;
     }
     // closing reduction: <V_k, V_m>, <V_m, V_m> complete column m-1
