@@ -435,6 +435,24 @@ def spmv_roofline(torch, L, ctx, A, reps=40):
                            "algorithmic_bytes_per_launch": alg_p, "avg_launch_us": us_p}}
 
 
+def gmres_cycle_bytes(n, nnz, m, elem=4, idx=4):
+    """Algorithmic HBM bytes of one fused, unpreconditioned GMRES(m) restart
+    cycle with DCGS2 (csrc/hpb_fused_gmres.cu): per Arnoldi step i (K = i
+    basis vectors) the product w = A u (values and column indices, row
+    pointers, u, w), the reduction (V_0..V_{K-1}, u, w) and the update (the
+    same K + 2 vectors read, q_i and the next vector written; at K = 0 only
+    u, w and the next vector); then the closing reduction (m + 1 vectors),
+    the solution update (m vectors, x read and written) and the compensated
+    residual (matrix, x, b, r)."""
+    vec = elem * n
+    spmv = (elem + idx) * nnz + 4 * (n + 1) + 2 * vec
+    total = 0
+    for k in range(m):
+        total += spmv + (k + 2) * vec + ((k + 4) if k > 0 else 3) * vec
+    total += (m + 1) * vec + (m + 2) * vec + spmv + 2 * vec
+    return total
+
+
 def bicgstabl_cycle_bytes(n, nnz, L, elem=8):
     """Algorithmic HBM bytes of one fused BiCGStab(L) cycle: 2L SpMVs (2L-1
     with the Dot2 against rt; the L products of r_j - beta u_j gather both
@@ -690,6 +708,15 @@ def bench_forms(torch, log=lambda *a: None):
                 "true_rel_residual": _rel(A, b, xir), "rel_err_vs_fp64_oracle": float(np.linalg.norm(xir - xo) / nx)},
             "fp64_oracle": {"tol": 1e-13, "status": sto, "iters": ro.iters},
             "speedup": t64 / tir if stir == 0 else None}
+        # byte-model roofline of the binary32 cycles (one GMRES(50) cycle per
+        # refinement; the refinement's own binary64 passes are not counted)
+        hbm, src = peaks()
+        cyc = gmres_cycle_bytes(A.n, A.nnz, 50)
+        ach = cyc * rir.refinements / tir / 1e9
+        out["precision_gmres50_poisson3d_aniso128"]["fp32_cycle_roofline"] = {
+            "bytes_per_cycle": cyc, "cycles": rir.refinements, "achieved": ach, "peak": hbm, "peak_source": src,
+            "unit": "GB/s", "frac": ach / hbm,
+            "note": "DCGS2 byte model of the binary32 inner cycles over the whole refinement solve"}
     except Exception as e:  # a failure here must not lose the headline line
         out["precision_gmres50_poisson3d_aniso128"] = {"error": repr(e)}
     # ---- config 4: complex form, BiCGStab(2), Helmholtz 2048^2
