@@ -202,3 +202,31 @@ def test_fused_gmres_ilu0_sweeps(gpu, t):
     pd = _lib.solver_params("gmres", basis=30, rel_tol=tol, max_iters=100, precond="ilu0", ilu_sweeps=2)
     st, _, _, _ = solve(torch, t, A, b, pd)
     assert st == -4
+
+
+def _diag(values):
+    n = len(values)
+    return problems.CSR(n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32), np.asarray(values))
+
+
+@pytest.mark.parametrize("t", ["f64", "c128", "f32"])
+def test_fused_gmres_invariant_krylov_space(gpu, t):
+    """Krylov spaces that stop growing: A = 2 I (dimension 1) and a diagonal
+    A with three distinct values (dimension 3).  Past that dimension the
+    delayed re-orthogonalisation meets vectors of rounding size (nu near
+    zero, the Pythagorean scale at its fallback, or an exact breakdown that
+    zeroes the remaining slots); the first restart cycle must still return
+    a finite solution that meets the tolerance."""
+    ctx, torch = gpu
+    n = 4000
+    cplx = t.startswith("c")
+    b = problems.rhs_uniform(n, 11, complex_=cplx)
+    tol = 1e-10 if t in ("f64", "c128") else 1e-6
+    for vals in (np.full(n, 2.0), np.array([1.0, 3.0, 7.0] * (n // 3) + [1.0] * (n % 3))):
+        A = _diag(vals.astype(np.complex128) if cplx else vals)
+        p = _lib.solver_params("gmres", basis=30, rel_tol=tol, max_iters=3000, fused=True)
+        st, rep, x, _ = solve(torch, t, A, b, p)
+        assert st == 0, (st, rep.iters)
+        assert np.isfinite(x).all()
+        assert true_rel(A, b, x) <= (1.05 if tol == 1e-10 else 20) * tol
+        assert rep.iters <= 30, rep.iters
