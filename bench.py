@@ -1114,10 +1114,23 @@ def cpu_baseline_dot2():
 
 def profile_solve(torch, max_iters, method="bicgstabl"):
     """One fused solve capped at max_iters iterations (a short, complete run
-    of the hot path for ncu): BiCGStab(4) on the config-2 system, or
-    GMRES(30) + Jacobi on the config-5 system."""
+    of the hot path for ncu): BiCGStab(4) on the config-2 system, GMRES(30)
+    + Jacobi on the config-5 system, or complex<binary64> BiCGStab(2) on the
+    config-4 system."""
     import ctypes as C
     from high_precision_blas1_b200 import _lib, spai, problems
+    if method == "complex":
+        A = problems.helmholtz2d(2048, ppw=10.0, damping=0.5)
+        b = problems.rhs_uniform(A.n, 404, complex_=True)
+        p = _lib.solver_params("bicgstabl", basis=2, rel_tol=SOLVER_TOL, max_iters=max_iters, fused=True)
+        d = [torch.from_numpy(np.ascontiguousarray(a)).cuda()
+             for a in (A.row_ptr, A.col_ind, A.val, b, np.zeros(A.n, dtype=np.complex128))]
+        rep = _lib.hpb_solver_report()
+        st = _lib.lib.hpb_csr_solve_c128(C.byref(p), A.n, A.nnz, *[a.data_ptr() for a in d], C.byref(rep), None, 0)
+        torch.cuda.synchronize()
+        print(f"profile solve: status {st}, iterations {rep.iters}, relative residual "
+              f"{rep.resid_norm / rep.rhs_norm:.3e}")
+        return
     if method == "gmres":
         A = spai.family(96, seed=424242)
         b = problems.rhs_uniform(A.n, 505)
@@ -1159,7 +1172,7 @@ def main():
     ap.add_argument("--profile-spai", type=int, default=0, metavar="K",
                     help="profiling aid: K learned-SPAI builds (features, MLP, assembly) on the config-5 96^3 "
                          "system, then exit")
-    ap.add_argument("--profile-method", choices=["bicgstabl", "gmres"], default="bicgstabl",
+    ap.add_argument("--profile-method", choices=["bicgstabl", "gmres", "complex"], default="bicgstabl",
                     help="with --profile-solve: BiCGStab(4) on the config-2 system, or GMRES(30) + Jacobi on the "
                          "config-5 lognormal 96^3 system")
     args = ap.parse_args()

@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <type_traits>
 
 #include "../../include/hpblas1.h"
 
@@ -125,6 +126,100 @@ __device__ __forceinline__ cf ldgE(const cf* p, int64_t i) {
 __device__ __forceinline__ cd ldgE(const cd* p, int64_t i) {
     const double* q = reinterpret_cast<const double*>(p) + 2 * i;
     return cd{__ldg(q), __ldg(q + 1)};
+}
+
+// Loads of a sparse product under a load mode LM chosen per launch:
+//   bit 0 (LM_ALIGNED): the values and x are aligned to the element size, so a
+//         complex element moves in one 8- or 16-byte access;
+//   bit 1 (LM_CACHED):  the values and column indices go through the
+//         read-only path with normal caching (__ldg) instead of evict-first
+//         (__ldcs).
+// Measured on B200 (5-point CSR products, two matrix copies alternating;
+// sizes are values + column indices): evict-first is faster while the
+// matrix is below L2's size (binary64 1024^2, 63 MB: 14.8 us against
+// 18.5 us; complex<double> 1024^2, 105 MB: 26.7 against 28.8 us) and much
+// slower well above it (complex<double> 2048^2, 419 MB: 217 us against
+// 92 us; binary64 and complex<float> 2048^2, 252 MB: 72 against 56 us and
+// 70 against 57 us; binary32 2048^2, 168 MB: equal), so the cached mode is
+// taken for matrices above 1.5x the L2 size.
+constexpr int LM_ALIGNED = 1, LM_CACHED = 2;
+template <int LM> __device__ __forceinline__ int32_t ld_idx(const int32_t* p, int64_t i) {
+    return (LM & LM_CACHED) ? __ldg(p + i) : __ldcs(p + i);
+}
+template <int LM> __device__ __forceinline__ float ld_val(const float* p, int64_t i) {
+    return (LM & LM_CACHED) ? __ldg(p + i) : __ldcs(p + i);
+}
+template <int LM> __device__ __forceinline__ double ld_val(const double* p, int64_t i) {
+    return (LM & LM_CACHED) ? __ldg(p + i) : __ldcs(p + i);
+}
+template <int LM> __device__ __forceinline__ cf ld_val(const cf* p, int64_t i) {
+    if (LM & LM_ALIGNED) {
+        const float2* q = reinterpret_cast<const float2*>(p) + i;
+        const float2 v = (LM & LM_CACHED) ? __ldg(q) : __ldcs(q);
+        return cf{v.x, v.y};
+    }
+    return (LM & LM_CACHED) ? ldgE(p, i) : ldcsE(p, i);
+}
+template <int LM> __device__ __forceinline__ cd ld_val(const cd* p, int64_t i) {
+    if (LM & LM_ALIGNED) {
+        const double2* q = reinterpret_cast<const double2*>(p) + i;
+        const double2 v = (LM & LM_CACHED) ? __ldg(q) : __ldcs(q);
+        return cd{v.x, v.y};
+    }
+    return (LM & LM_CACHED) ? ldgE(p, i) : ldcsE(p, i);
+}
+// the gathered vector: read-only path, one access per element when aligned
+template <int LM> __device__ __forceinline__ float ld_x(const float* p, int64_t i) { return __ldg(p + i); }
+template <int LM> __device__ __forceinline__ double ld_x(const double* p, int64_t i) { return __ldg(p + i); }
+template <int LM> __device__ __forceinline__ cf ld_x(const cf* p, int64_t i) {
+    if (LM & LM_ALIGNED) {
+        const float2 v = __ldg(reinterpret_cast<const float2*>(p) + i);
+        return cf{v.x, v.y};
+    }
+    return ldgE(p, i);
+}
+template <int LM> __device__ __forceinline__ cd ld_x(const cd* p, int64_t i) {
+    if (LM & LM_ALIGNED) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(p) + i);
+        return cd{v.x, v.y};
+    }
+    return ldgE(p, i);
+}
+// true when p is aligned to E's size (complex: 8 or 16 bytes)
+template <class E>
+inline bool elem_aligned(const void* p) { return (reinterpret_cast<uintptr_t>(p) % sizeof(E)) == 0; }
+// Calls f(std::integral_constant<int, LM>{}) for the load mode lm (complex
+// element types: the four modes; real types: evict-first or cached only,
+// the alignment bit changes nothing for them).
+template <class E, class F>
+inline void dispatch_lm(int lm, F&& f) {
+    if constexpr (sizeof(E) > 8 || std::is_same<E, cf>::value) {
+        switch (lm & 3) {
+            case 1: f(std::integral_constant<int, 1>{}); break;
+            case 2: f(std::integral_constant<int, 2>{}); break;
+            case 3: f(std::integral_constant<int, 3>{}); break;
+            default: f(std::integral_constant<int, 0>{}); break;
+        }
+    } else {
+        if (lm & LM_CACHED)
+            f(std::integral_constant<int, LM_CACHED>{});
+        else
+            f(std::integral_constant<int, 0>{});
+    }
+}
+// The load mode of a product over nnz entries of type E with values val and
+// gathered vector x, on the current device.
+template <class E>
+inline int load_mode(const void* val, const void* x, int64_t nnz) {
+    int lm = 0;
+    if (sizeof(E) > 8 || std::is_same<E, cf>::value) {  // complex element types
+        if (elem_aligned<E>(val) && (x == nullptr || elem_aligned<E>(x))) lm |= LM_ALIGNED;
+    }
+    int dev = 0, l2 = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev) == cudaSuccess &&
+        l2 > 0 && double(nnz) * double(sizeof(E) + sizeof(int32_t)) > 1.5 * double(l2))
+        lm |= LM_CACHED;
+    return lm;
 }
 
 template <class E>

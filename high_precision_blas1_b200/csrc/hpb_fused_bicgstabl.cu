@@ -140,7 +140,8 @@ __device__ void run_epi(const EpiArgs<S>& a, const S* v, bool bad) {
 // (the same FMA, so the same bits); the updated u_j itself is stored by the
 // next kernel (k_upd_urx), which reads both vectors anyway.  This removes the
 // separate pass that wrote u_j to HBM only for this product to read it back.
-template <class E, bool DOT, bool UPD = false>
+// LM: the load mode of the matrix and the gathered vectors (ld_val, ld_x).
+template <class E, bool DOT, bool UPD = false, int LM = 0>
 __global__ void __launch_bounds__(kThreads)
 k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const E* __restrict__ val,
            const E* __restrict__ diag, const E* __restrict__ x, E* __restrict__ y, const E* __restrict__ w,
@@ -162,13 +163,13 @@ k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
         const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
         S acc = s_zero(S{});
         for (int32_t k = b; k < e; ++k) {
-            const int32_t c = ldcsI(ci, k);
+            const int32_t c = ld_idx<LM>(ci, k);
             S xv;
             if (UPD)
-                xv = to_s(from_s<E>(s_fma(nb, to_s(ldgE(x, c)), to_s(ldgE(xr, c)))));
+                xv = to_s(from_s<E>(s_fma(nb, to_s(ld_x<LM>(x, c)), to_s(ld_x<LM>(xr, c)))));
             else
-                xv = to_s(ldgE(x, c));
-            acc = s_fma(to_s(ldcsE(val, k)), xv, acc);
+                xv = to_s(ld_x<LM>(x, c));
+            acc = s_fma(to_s(ld_val<LM>(val, k)), xv, acc);
         }
         if (diag) acc = s_div(acc, to_s(ldE(diag, r)));
         E out = from_s<E>(acc);
@@ -179,6 +180,19 @@ k_spmv_dot(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
         A dacc[1] = {widen_acc(pacc)};
         grid_finish<1>(dacc, false, partials, ticket, badflag, [&](const S* v, bool bad) { run_epi(ea, v, bad); });
     }
+}
+
+// k_spmv_dot under load mode lm
+template <class E, bool DOT, bool UPD>
+void launch_spmv_dot(int lm, int grid, cudaStream_t s, int32_t rows, const int32_t* rp, const int32_t* ci,
+                     const E* val, const E* diag, const E* x, E* y, const E* w,
+                     typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
+                     EpiArgs<typename scalar_of<E>::type> ea, const E* xr = nullptr) {
+    dispatch_lm<E>(lm, [&](auto mode) {
+        constexpr int M = decltype(mode)::value;
+        k_spmv_dot<E, DOT, UPD, M><<<grid, kThreads, 0, s>>>(rows, rp, ci, val, diag, x, y, w, partials, ticket,
+                                                             badflag, ea, xr);
+    });
 }
 
 // ------------------------------------------------------------ BiCG updates
@@ -564,6 +578,8 @@ struct BcgPlan<E>::Impl {
     const E* val = nullptr;
     E* x = nullptr;
     int g_ew = 1, g_red = 1, g_sp = 1, g_spd = 1, g_nrm = 1, kernels = 0;
+    int64_t nnz = 0;
+    int lm = 0;  // load mode of the cycle's products
     int g_upd[kMaxL] = {};
     SolverWorkspace ws;
     Vecs<E> V{};
@@ -636,7 +652,6 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
                      const E* val, E* x) {
     using S = typename Impl::S;
     using A = typename Impl::A;
-    (void)nnz;
     const int L = p->basis > 0 ? p->basis : 2;
     if (L > kMaxL) return HPB_ERROR_NOT_SUPPORTED;
     const bool jac = p->precond == HPB_PRECOND_JACOBI;
@@ -654,6 +669,7 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     P.jac = jac;
     P.rows = rows;
     P.n = rows;
+    P.nnz = nnz;
     P.rp = rp;
     P.ci = ci;
     P.val = val;
@@ -723,6 +739,9 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     E* diag = P.diag;
     E* rt = P.rt;
     EpiArgs<S> none{st, drep, EPI_NONE, 0, 0, L};
+    // the cycle's products gather workspace vectors (aligned); the matrix
+    // values are the caller's
+    const int lm = P.lm = load_mode<E>(val, nullptr, nnz);
     int kernels = 0;
     P.plain_graph = fused_plain_graph();
     // the loop graph: a WHILE node whose body is one cycle + the monitor
@@ -749,17 +768,15 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     }
     for (int j = 0; j < L; ++j) {
         // u_{j+1} = A (r_j - beta u_j) and alpha = rho / <rt, u_{j+1}>
-        k_spmv_dot<E, true, true><<<g_spd, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt,
-                                                             partials, ticket, badflag,
-                                                             EpiArgs<S>{st, drep, EPI_ALPHA, 0, j, L}, V.r[j]);
+        launch_spmv_dot<E, true, true>(lm, g_spd, s, rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt, partials,
+                                       ticket, badflag, EpiArgs<S>{st, drep, EPI_ALPHA, 0, j, L}, V.r[j]);
         launch_upd_urx<E>(j, P.g_upd[j], s, n, V, x, st);
         if (j + 1 < L)
-            k_spmv_dot<E, true><<<g_spd, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.r[j], V.r[j + 1], rt,
-                                                           partials, ticket, badflag,
-                                                           EpiArgs<S>{st, drep, EPI_BETA, 0, j, L});
+            launch_spmv_dot<E, true, false>(lm, g_spd, s, rows, rp, ci, val, diag, V.r[j], V.r[j + 1], rt, partials,
+                                            ticket, badflag, EpiArgs<S>{st, drep, EPI_BETA, 0, j, L});
         else
-            k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, rp, ci, val, diag, V.r[j], V.r[j + 1], nullptr,
-                                                           partials, ticket, badflag, none);
+            launch_spmv_dot<E, false, false>(lm, g_sp, s, rows, rp, ci, val, diag, V.r[j], V.r[j + 1], nullptr,
+                                             partials, ticket, badflag, none);
         kernels += 3;
     }
     for (int k = 1; k <= L; ++k) {
@@ -812,8 +829,8 @@ int BcgPlan<E>::run(const E* b, hpb_solver_report* rep, double* hist, int cap) {
     }
     k_norm<E><<<P.g_nrm, kThreads, 0, s>>>(n, pb, P.dnorm, P.partials, P.ticket, P.badflag);
     // r0 = P (b - A x), rt = r0 / ||r0||
-    k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, P.rp, P.ci, P.val, nullptr, x, P.tmp, nullptr, P.partials,
-                                                   P.ticket, P.badflag, none);
+    launch_spmv_dot<E, false, false>(load_mode<E>(P.val, x, P.nnz), g_sp, s, rows, P.rp, P.ci, P.val,
+                                     nullptr, x, P.tmp, nullptr, P.partials, P.ticket, P.badflag, none);
     k_residual_finish<E><<<g_ew, kThreads, 0, s>>>(n, b, P.tmp, P.diag, V.r[0]);
     k_norm<E><<<P.g_nrm, kThreads, 0, s>>>(n, V.r[0], P.dnorm + 1, P.partials, P.ticket, P.badflag);
     k_scale_by_inv_norm<E><<<g_ew, kThreads, 0, s>>>(n, V.r[0], P.dnorm + 1, P.rt);
@@ -897,8 +914,8 @@ int BcgPlan<E>::run(const E* b, hpb_solver_report* rep, double* hist, int cap) {
     auto t1 = std::chrono::steady_clock::now();
 
     // true residual ||b - A x|| and ||b|| (compensated)
-    k_spmv_dot<E, false><<<g_sp, kThreads, 0, s>>>(rows, P.rp, P.ci, P.val, nullptr, x, P.tmp, nullptr, P.partials,
-                                                   P.ticket, P.badflag, none);
+    launch_spmv_dot<E, false, false>(load_mode<E>(P.val, x, P.nnz), g_sp, s, rows, P.rp, P.ci, P.val,
+                                     nullptr, x, P.tmp, nullptr, P.partials, P.ticket, P.badflag, none);
     k_residual_finish<E><<<g_ew, kThreads, 0, s>>>(n, b, P.tmp, nullptr, V.r[1]);
     k_norm<E><<<P.g_nrm, kThreads, 0, s>>>(n, V.r[1], P.dnorm + 2, P.partials, P.ticket, P.badflag);
     k_norm<E><<<P.g_nrm, kThreads, 0, s>>>(n, b, P.dnorm + 3, P.partials, P.ticket, P.badflag);

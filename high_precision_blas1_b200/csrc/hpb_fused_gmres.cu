@@ -836,8 +836,9 @@ k_gm_jacobi(int64_t n, const E* __restrict__ x, const E* __restrict__ d, E* __re
         stE(y, q, from_s<E>(s_div(to_s(ldE(x, q)), to_s(ldE(d, q)))));
 }
 
-// plain CSR product y = A x (grid-stride rows; x gathered through L1/L2)
-template <class E>
+// plain CSR product y = A x (grid-stride rows; x gathered through L1/L2);
+// LM: the load mode (ld_val, ld_x)
+template <class E, int LM = 0>
 __global__ void __launch_bounds__(kGmThreads)
 k_gm_spmv(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const E* __restrict__ val,
           const E* __restrict__ x, E* __restrict__ y) {
@@ -847,15 +848,25 @@ k_gm_spmv(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restric
     for (int32_t r = blockIdx.x * kGmThreads + threadIdx.x; r < rows; r += stride) {
         const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
         S acc = s_zero(S{});
-        for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ldcsE(val, k)), to_s(ldgE(x, ldcsI(ci, k))), acc);
+        for (int32_t k = b; k < e; ++k) acc = s_fma(to_s(ld_val<LM>(val, k)), to_s(ld_x<LM>(x, ld_idx<LM>(ci, k))), acc);
         stE(y, r, from_s<E>(acc));
     }
+}
+
+// k_gm_spmv under the load mode of its matrix and x
+template <class E>
+void launch_gm_spmv(int grid, cudaStream_t s, int32_t rows, int64_t nnz, const int32_t* rp, const int32_t* ci,
+                    const E* val, const E* x, E* y) {
+    dispatch_lm<E>(load_mode<E>(val, x, nnz), [&](auto mode) {
+        constexpr int M = decltype(mode)::value;
+        k_gm_spmv<E, M><<<grid, kGmThreads, 0, s>>>(rows, rp, ci, val, x, y);
+    });
 }
 
 // r = b - A x with a compensated (Dot2) row sum, and ||r|| in Dot2 into
 // st->rnorm (finiteness of x into st->nonfinite).  The residual of the
 // iterative refinement and the monitor's true residual.
-template <class E, class R>
+template <class E, class R, int LM = 0>
 __global__ void __launch_bounds__(kGmThreads)
 k_resid_comp(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const E* __restrict__ val,
              const E* __restrict__ x, const E* __restrict__ b, R* __restrict__ r,
@@ -872,8 +883,8 @@ k_resid_comp(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __rest
         ra.s = bv;
         const int32_t kb = __ldg(rp + row), ke = __ldg(rp + row + 1);
         for (int32_t k = kb; k < ke; ++k) {
-            S a = to_s(ldcsE(val, k));
-            E xe = ldgE(x, ldcsI(ci, k));
+            S a = to_s(ld_val<LM>(val, k));
+            E xe = ld_x<LM>(x, ld_idx<LM>(ci, k));
             bad |= !finite_e(xe);
             dot_add(ra, s_neg(conj_s(a)), to_s(xe));  // conj(-conj(a)) * x = -a x
         }
@@ -970,6 +981,7 @@ struct GmPlan<E>::Impl {
     int g_ew = 1, g_md = 1, g_sp = 1, g_rc = 1, kernels = 0;
     int vec = 0;  // the basis and w move as 16-byte packs
     int g_f32 = 0, r_f32 = 0;  // grid and packs per thread of k_dcgs_dots_f32 (binary32 steps)
+    int lm_res = 0;            // load mode of the compensated residual
     SolverWorkspace ws;
     E *V = nullptr, *W = nullptr, *Z = nullptr, *R = nullptr, *diag = nullptr, *T = nullptr;
     GmState<S>* st = nullptr;
@@ -992,7 +1004,6 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
                     const E* val, const RightPrec<E>& M, const E* b, E* x, int max_cycles) {
     using S = typename Impl::S;
     using A = typename Impl::A;
-    (void)nnz;
     const int m = p->basis > 0 ? p->basis : 30;
     if (m > kGmMaxM) return HPB_ERROR_NOT_SUPPORTED;
     if (!p->high_precision) return HPB_ERROR_NOT_SUPPORTED;
@@ -1094,6 +1105,7 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
     }
     if (cudaStreamSynchronize(s) != cudaSuccess) return HPB_ERROR_CUDA;
 
+    const int lm_res = P.lm_res = load_mode<E>(val, x, nnz);
     // ---- one restart cycle as a CUDA graph
     int kernels = 0;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return HPB_ERROR_CUDA;
@@ -1108,7 +1120,7 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
             src = Z;
             ++kernels;
         } else if (M.kind == 2) {
-            k_gm_spmv<E><<<g_sp, kGmThreads, 0, s>>>(M.rows, M.rp, M.ci, M.val, vi, Z);
+            launch_gm_spmv<E>(g_sp, s, M.rows, M.nnz, M.rp, M.ci, M.val, vi, Z);
             src = Z;
             ++kernels;
         } else if (M.kind == 3 && M.sweeps == 0) {  // z = U^-1 L^-1 v_i (R is free inside the cycle)
@@ -1122,7 +1134,7 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
             src = Z;
             kernels += 2 * (M.sweeps + 1);
         }
-        k_gm_spmv<E><<<g_sp, kGmThreads, 0, s>>>(rows, rp, ci, val, src, W);
+        launch_gm_spmv<E>(g_sp, s, rows, nnz, rp, ci, val, src, W);
         int nb = g_md;
         if constexpr (std::is_same<E, float>::value) {
             if (g_f32 > 0) {
@@ -1154,7 +1166,7 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
         if (M.kind == 1) {
             k_gm_jacobi<E><<<g_ew, kGmThreads, 0, s>>>(n, W, diag, Z);
         } else if (M.kind == 2) {
-            k_gm_spmv<E><<<g_sp, kGmThreads, 0, s>>>(M.rows, M.rp, M.ci, M.val, W, Z);
+            launch_gm_spmv<E>(g_sp, s, M.rows, M.nnz, M.rp, M.ci, M.val, W, Z);
         } else if (M.sweeps == 0) {
             tri::launch_trsv<E>(M.lower->plan, 1, M.val, unit_of<E>(), W, R, s);
             tri::launch_trsv<E>(M.upper->plan, 0, M.val, unit_of<E>(), R, Z, s);
@@ -1167,7 +1179,10 @@ int GmPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, const
         k_gm_axpy<E><<<g_ew, kGmThreads, 0, s>>>(n, x, Z);
         kernels += 3;
     }
-    k_resid_comp<E, E><<<g_rc, kGmThreads, 0, s>>>(rows, rp, ci, val, x, b, R, st, partials, ticket, badflag);
+    dispatch_lm<E>(lm_res, [&](auto mode) {
+        constexpr int MD = decltype(mode)::value;
+        k_resid_comp<E, E, MD><<<g_rc, kGmThreads, 0, s>>>(rows, rp, ci, val, x, b, R, st, partials, ticket, badflag);
+    });
     ++kernels;
     cudaMemcpyAsync(&hv->rnorm, &st->rnorm, sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&hv->est, &st->est, sizeof(double), cudaMemcpyDeviceToHost, s);
@@ -1195,8 +1210,11 @@ int GmPlan<E>::run(hpb_solver_report* rep, double* hist, int cap) {
     auto t0 = std::chrono::steady_clock::now();
     cudaMemsetAsync(st, 0, sizeof(GmState<S>), s);
     k_gm_norm<E><<<P.g_ew, kGmThreads, 0, s>>>(P.n, P.b, P.dnorm, P.partials, P.ticket, P.badflag);
-    k_resid_comp<E, E><<<P.g_rc, kGmThreads, 0, s>>>(P.rows, P.rp, P.ci, P.val, P.x, P.b, P.R, st, P.partials,
-                                                     P.ticket, P.badflag);
+    dispatch_lm<E>(P.lm_res, [&](auto mode) {
+        constexpr int MD = decltype(mode)::value;
+        k_resid_comp<E, E, MD><<<P.g_rc, kGmThreads, 0, s>>>(P.rows, P.rp, P.ci, P.val, P.x, P.b, P.R, st,
+                                                            P.partials, P.ticket, P.badflag);
+    });
     cudaMemcpyAsync(&hv->rnorm, &st->rnorm, sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&hv->est, &st->est, sizeof(double), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(&hv->nsteps, &st->nsteps, sizeof(int), cudaMemcpyDeviceToHost, s);

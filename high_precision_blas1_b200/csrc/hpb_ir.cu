@@ -18,7 +18,8 @@
 namespace hpb {
 namespace fused {
 
-template <class E, class R>
+// LM: the load mode of the matrix and x (ld_val, ld_x)
+template <class E, int LM>
 __global__ void k_ir_resid(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                            const E* __restrict__ val, const E* __restrict__ x, const E* __restrict__ b,
                            E* __restrict__ r, double* out /* [0] ||r||, [1] nonfinite */,
@@ -34,9 +35,9 @@ __global__ void k_ir_resid(int32_t rows, const int32_t* __restrict__ rp, const i
         ra.s = to_s(ldE(b, row));
         const int32_t kb = __ldg(rp + row), ke = __ldg(rp + row + 1);
         for (int32_t k = kb; k < ke; ++k) {
-            E xe = ldgE(x, ldcsI(ci, k));
+            E xe = ld_x<LM>(x, ld_idx<LM>(ci, k));
             bad |= !finite_e(xe);
-            dot_add(ra, s_neg(conj_s(to_s(ldcsE(val, k)))), to_s(xe));
+            dot_add(ra, s_neg(conj_s(to_s(ld_val<LM>(val, k)))), to_s(xe));
         }
         S rv = acc_value(ra);
         stE(r, row, from_s<E>(rv));
@@ -196,11 +197,15 @@ int ir_solve(const hpb_ir_params* p, int32_t rows, int64_t nnz, const int32_t* r
         pst = bcg.init(&ip, rows, nnz, rp, ci, vlo, dlo);
     if (pst != HPB_SUCCESS) return pst;
 
+    const int lm = load_mode<E>(val, x, nnz);
     int refinements = 0, inner_iters = 0, hl = 0;
     bool conv = false, valid = true;
     double rn = 0.0;
     for (;;) {
-        k_ir_resid<E, E><<<g_row, 256>>>(rows, rp, ci, val, x, b, r, dn, partials, ticket, badflag);
+        dispatch_lm<E>(lm, [&](auto mode) {
+            constexpr int M = decltype(mode)::value;
+            k_ir_resid<E, M><<<g_row, 256>>>(rows, rp, ci, val, x, b, r, dn, partials, ticket, badflag);
+        });
         count_launch();
         if (cudaMemcpy(hn, dn, 2 * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return HPB_ERROR_CUDA;
         rn = hn[0];

@@ -32,7 +32,8 @@ __device__ __forceinline__ cd mul_s(cd a, cd b) { return cmul(a, b); }
 
 constexpr int kSpmvRows = 256;  // rows (threads) per block
 
-template <class E, bool BETA0>
+// LM: the load mode of the matrix and x (ld_val, ld_x)
+template <class E, bool BETA0, int LM>
 __global__ void __launch_bounds__(kSpmvRows)
 csr_row_kernel(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                const E* __restrict__ val, E alpha, const E* __restrict__ x, E beta, E* __restrict__ y) {
@@ -44,7 +45,7 @@ csr_row_kernel(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __re
     for (int32_t r = blockIdx.x * kSpmvRows + threadIdx.x; r < rows; r += stride) {
         const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
         E acc{};
-        for (int32_t k = b; k < e; ++k) acc = madd_s(ldcsE(val, k), ldgE(x, ldcsI(ci, k)), acc);
+        for (int32_t k = b; k < e; ++k) acc = madd_s(ld_val<LM>(val, k), ld_x<LM>(x, ld_idx<LM>(ci, k)), acc);
         E out = BETA0 ? mul_s(alpha, acc) : madd_s(alpha, acc, mul_s(beta, ldE(y, r)));
         stE(y, r, out);
     }
@@ -70,7 +71,7 @@ __device__ __forceinline__ void write_hi_lo(const fused::AccC& a, double* out) {
 // grid-stride loop (grid <= the context's partials capacity), y exactly as
 // csr_row_kernel with alpha = 1, beta = 0; the (s, c) pairs are merged by
 // the last block, which writes (hi, lo) like the Dot2 kernel.
-template <class E>
+template <class E, int LM>
 __global__ void __launch_bounds__(kSpmvRows)
 csr_row_dot_kernel(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
                    const E* __restrict__ val, const E* __restrict__ x, E* __restrict__ y, const E* __restrict__ w,
@@ -83,7 +84,7 @@ csr_row_dot_kernel(int32_t rows, const int32_t* __restrict__ rp, const int32_t* 
     for (int32_t r = blockIdx.x * kSpmvRows + threadIdx.x; r < rows; r += stride) {
         const int32_t b = __ldg(rp + r), e = __ldg(rp + r + 1);
         E acc{};
-        for (int32_t k = b; k < e; ++k) acc = madd_s(ldcsE(val, k), ldgE(x, ldcsI(ci, k)), acc);
+        for (int32_t k = b; k < e; ++k) acc = madd_s(ld_val<LM>(val, k), ld_x<LM>(x, ld_idx<LM>(ci, k)), acc);
         stE(y, r, acc);
         fused::dot_add(d[0], fused::to_s(ldE(w, r)), fused::to_s(acc));
     }
@@ -109,10 +110,13 @@ int spmv_impl(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz, const i
         (reinterpret_cast<uintptr_t>(rp) | reinterpret_cast<uintptr_t>(ci)) % 4)
         return set_error(ctx, HPB_ERROR_INVALID_VALUE, "%s: pointer not aligned to its element type", name);
     const int grid = grid_for(ctx, rows, kSpmvRows, 8);
-    if (is_zero(beta))
-        csr_row_kernel<E, true><<<grid, kSpmvRows, 0, ctx->stream>>>(rows, rp, ci, val, alpha, x, beta, y);
-    else
-        csr_row_kernel<E, false><<<grid, kSpmvRows, 0, ctx->stream>>>(rows, rp, ci, val, alpha, x, beta, y);
+    dispatch_lm<E>(load_mode<E>(val, x, nnz), [&](auto mode) {
+        constexpr int M = decltype(mode)::value;
+        if (is_zero(beta))
+            csr_row_kernel<E, true, M><<<grid, kSpmvRows, 0, ctx->stream>>>(rows, rp, ci, val, alpha, x, beta, y);
+        else
+            csr_row_kernel<E, false, M><<<grid, kSpmvRows, 0, ctx->stream>>>(rows, rp, ci, val, alpha, x, beta, y);
+    });
     count_launch();
     return check_launch(ctx, name);
 }
@@ -143,9 +147,12 @@ int spmv_dot2_impl(hpb_context* ctx, int32_t rows, int32_t cols, int64_t nnz, co
     if (grid < 1) grid = 1;
     // ticket[0]: the reductions' counter (same stream, so never concurrent);
     // ticket[1] serves as the (unused) non-finite flag and stays zero.
-    csr_row_dot_kernel<E><<<grid, kSpmvRows, 0, ctx->stream>>>(rows, rp, ci, val, x, y, w,
-                                                              static_cast<A*>(ctx->partials), ctx->ticket,
-                                                              reinterpret_cast<int*>(ctx->ticket + 1), out);
+    dispatch_lm<E>(load_mode<E>(val, x, nnz), [&](auto mode) {
+        constexpr int M = decltype(mode)::value;
+        csr_row_dot_kernel<E, M><<<grid, kSpmvRows, 0, ctx->stream>>>(rows, rp, ci, val, x, y, w,
+                                                                      static_cast<A*>(ctx->partials), ctx->ticket,
+                                                                      reinterpret_cast<int*>(ctx->ticket + 1), out);
+    });
     count_launch();
     return check_launch(ctx, name);
 }
