@@ -449,10 +449,13 @@ k_dcgs_finish(int nb, int K, int last, const typename acc_of<S>::type* __restric
         if (!last) sb[tid] = ldcg_s(g.dots + i + tid);
         scs[tid] = g.cs[tid];
         ssn[tid] = g.sn[tid];
-        const S* col = g.Hr + size_t(tid) * ld;
-        S* dst = shr + band_off(tid);
-#pragma unroll 8
-        for (int r = 0; r <= tid + 1; ++r) dst[r] = col[r];
+    }
+    // the band, entry f = band_off(k) + r of column k, spread over the block
+    for (int f = tid; f < band_off(i); f += blockDim.x) {
+        int k = int((sqrtf(9.f + 8.f * float(f)) - 3.f) * 0.5f);
+        while (k > 0 && band_off(k) > f) --k;
+        while (band_off(k + 1) <= f) ++k;
+        shr[f] = g.Hr[size_t(k) * ld + (f - band_off(k))];
     }
     __syncthreads();
     if (tid == 0) {
