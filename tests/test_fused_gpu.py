@@ -230,3 +230,44 @@ def test_fused_gmres_invariant_krylov_space(gpu, t):
         assert np.isfinite(x).all()
         assert true_rel(A, b, x) <= (1.05 if tol == 1e-10 else 20) * tol
         assert rep.iters <= 30, rep.iters
+
+
+@pytest.mark.parametrize("t", ["f32", "f64", "c64", "c128"])
+def test_fused_gmres_odd_sizes(gpu, t):
+    """Vector lengths that are not a multiple of the 16-byte pack (1089 =
+    33^2 rows, odd) take the element-wise forms of the DCGS2 reduction and
+    update; the solve converges on the true residual as the packed forms
+    do, for every storage type."""
+    ctx, torch = gpu
+    if t.startswith("c"):
+        A = problems.helmholtz2d(33)
+        b = problems.rhs_uniform(A.n, 5, complex_=True)
+    else:
+        A = problems.convdiff2d(33)
+        b = problems.rhs_uniform(A.n, 5)
+    assert A.n % 4 == 1
+    tol = 1e-10 if t in ("f64", "c128") else 1e-6
+    for precond in ("none", "jacobi"):
+        p = _lib.solver_params("gmres", basis=20, rel_tol=tol, max_iters=100000, precond=precond, fused=True)
+        st, rep, x, _ = solve(torch, t, A, b, p)
+        assert st == 0, (precond, st, rep.iters)
+        assert true_rel(A, b, x) <= (1.05 if tol == 1e-10 else 20) * tol
+
+
+@pytest.mark.parametrize("t,m", [("f64", 64), ("f32", 64), ("c128", 64), ("f64", 1), ("f64", 2)])
+def test_fused_gmres_basis_extremes(gpu, t, m):
+    """The largest basis the fused GMRES takes (m = 64: 131 inner products
+    per step, the whole Hessenberg band in shared memory) and the smallest
+    ones (m = 1, 2: the closing reduction right after the first steps)."""
+    ctx, torch = gpu
+    if t.startswith("c"):
+        A = problems.helmholtz2d(40)
+        b = problems.rhs_uniform(A.n, 9, complex_=True)
+    else:
+        A = problems.convdiff2d(40)
+        b = problems.rhs_uniform(A.n, 9)
+    tol = 1e-10 if t in ("f64", "c128") else 1e-6
+    p = _lib.solver_params("gmres", basis=m, rel_tol=tol, max_iters=200000, precond="jacobi", fused=True)
+    st, rep, x, _ = solve(torch, t, A, b, p)
+    assert st == 0, (st, rep.iters)
+    assert true_rel(A, b, x) <= (1.05 if tol == 1e-10 else 20) * tol
