@@ -501,14 +501,20 @@ def gmres_cycle_bytes(n, nnz, m, elem=4, idx=4):
 def bicgstabl_cycle_bytes(n, nnz, L, elem=8):
     """Algorithmic HBM bytes of one fused BiCGStab(L) cycle: 2L SpMVs (2L-1
     with the Dot2 against rt; the L products of r_j - beta u_j gather both
-    vectors), one update pass per BiCG step, the L modified Gram-Schmidt
-    sweeps and the closing update, each vector read or written once per
-    kernel."""
+    vectors, and so do the L products of r_j - alpha u_{j+1}), the BiCG
+    updates inside the second product of each step (r_j's own update
+    deferred to the next step, the last one to the first MGS sweep), the L
+    modified Gram-Schmidt sweeps and the closing update, each vector read or
+    written once per kernel."""
     mat = (elem + 4.0) * nnz + 4.0 * (n + 1)
     spmv = mat + 2.0 * elem * n
     vec = elem * float(n)
     passes = L                                             # r_j gathered beside u_j by A (r_j - beta u_j)
-    passes += sum(4 * j + 7 for j in range(L))             # u_i = r_i - beta u_i, r_i -= alpha u_{i+1}, x += alpha u_0
+    # step j's update + product beyond its SpMV (which gathers r_j and writes
+    # r_{j+1}): u_{j+1} gathered, r_0..r_{j-1}, u_0..u_j and x read, u_0..u_j,
+    # r_0..r_{j-1} and x written
+    passes += sum(4 * j + 5 for j in range(L))
+    passes += 2                                            # deferred r_{L-1} -= alpha u_L: u_L read, r_{L-1} written
     for k in range(1, L + 1):                              # right-looking MGS sweep k
         passes += (L + 1) if k == 1 else (L - k + 3) + (L - k + 1)
     passes += (2 + 2 * L + 2) + 3                          # closing update: reads, then x, r_0, u_0 written

@@ -45,6 +45,7 @@ constexpr int kThreads = 256;
 template <class S>
 struct BcgState {
     S rho, alpha, omega, beta;
+    S alpha_prev;  // alpha of the previous inner step (its deferred r update)
     S tau[kMaxL + 1][kMaxL + 1];
     S sigma[kMaxL + 1], gam[kMaxL + 1], gam1[kMaxL + 1], gam2[kMaxL + 1];
     S last[2];
@@ -90,6 +91,7 @@ __device__ void run_epi(const EpiArgs<S>& a, const S* v, bool bad) {
     BcgState<S>& st = *a.st;
     switch (a.kind) {
         case EPI_ALPHA:  // alpha = rho / <rt, u_{j+1}>
+            st.alpha_prev = st.alpha;
             st.alpha = s_div(st.rho, v[0]);
             break;
         case EPI_BETA:  // rho1 = <rt, r_j>; beta = alpha rho1 / rho; rho = rho1
@@ -138,7 +140,7 @@ __device__ void run_epi(const EpiArgs<S>& a, const S* v, bool bad) {
 // UPD: the operand is the BiCG update u_j = r_j - beta u_j, formed at every
 // gathered column from x = u_j and xr = r_j as the update kernel forms it
 // (the same FMA, so the same bits); the updated u_j itself is stored by the
-// next kernel (k_upd_urx), which reads both vectors anyway.  This removes the
+// next kernel (k_spmv_upd), which reads both vectors anyway.  This removes the
 // separate pass that wrote u_j to HBM only for this product to read it back.
 // LM: the load mode of the matrix and the gathered vectors (ld_val, ld_x).
 template <class E, bool DOT, bool UPD = false, int LM = 0>
@@ -195,77 +197,104 @@ void launch_spmv_dot(int lm, int grid, cudaStream_t s, int32_t rows, const int32
     });
 }
 
-// ------------------------------------------------------------ BiCG updates
-// One pass per inner step j, after u_{j+1} = A (r_j - beta u_j):
-//   u_i = r_i - beta u_i          (i = 0..j; u_j's value equals the one the
-//                                  product gathered)
-//   r_i = r_i - alpha u_{i+1}     (i = 0..j, with the updated u_{i+1})
-//   x   = x + alpha u_0
-// The same FMAs, in the same order per element, as separate u and r/x
-// passes, so the same bits; every vector is read and written once.  J = j is
-// a template parameter so the row's values stay in registers.
-template <class E, int J>
-__global__ void __launch_bounds__(kThreads) k_upd_urx(int64_t n, Vecs<E> V, E* __restrict__ x,
-                                                      const BcgState<typename scalar_of<E>::type>* st) {
+// ------------------------------------------------------------ BiCG update + product
+// One kernel per inner step j, after u_{j+1} = A (r_j - beta u_j) and alpha:
+//   r_{j-1} -= alpha_{j-1} u_j      (j >= 1: the previous step's r update,
+//                                    deferred to here, with u_j as that step
+//                                    left it)
+//   u_i = r_i - beta u_i            (i = 0..j)
+//   r_i = r_i - alpha u_{i+1}       (i = 0..j-1, with the updated u_{i+1})
+//   x  += alpha u_0
+//   r_{j+1} = D^-1 A r_j'           (r_j' = r_j - alpha u_{j+1}, formed at
+//                                    every gathered column as the update
+//                                    would store it: the same FMA, the same
+//                                    rounding)
+//   and, with dot, <rt, r_{j+1}> and the beta epilogue.
+// r_j' itself is stored by the next step's kernel, or after the last step
+// by the first MR sweep, so no block writes what another gathers.  Per
+// element these are the operations of a separate update pass followed by
+// the product, so the iterates are the same bits; the cycle saves the
+// update pass's launch.  J = j is a template parameter so the row's values
+// stay in registers.
+template <class E, int J, int LM>
+__global__ void __launch_bounds__(kThreads)
+k_spmv_upd(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const E* __restrict__ val,
+           const E* __restrict__ diag, Vecs<E> V, E* __restrict__ x, const E* __restrict__ w, int dot,
+           BcgState<typename scalar_of<E>::type>* st, typename acc_of<typename scalar_of<E>::type>::type* partials,
+           unsigned int* ticket, int* badflag, EpiArgs<typename scalar_of<E>::type> ea) {
     using S = typename scalar_of<E>::type;
-    const S nb = s_neg(st->beta), al = st->alpha, nal = s_neg(st->alpha);
-    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
-    if constexpr (std::is_same<E, double>::value) {
-        // binary64: two rows per thread with 16-byte loads and stores
-        bool vec = n % 2 == 0 && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(V.u[J + 1])) & 15) == 0;
-#pragma unroll
-        for (int i = 0; i <= J; ++i)
-            vec = vec && ((reinterpret_cast<uintptr_t>(V.u[i]) | reinterpret_cast<uintptr_t>(V.r[i])) & 15) == 0;
-        if (vec) {
-            for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n / 2; q += stride) {
-                double2 u[J + 2], r[J + 1];
-#pragma unroll
-                for (int i = 0; i <= J; ++i) {
-                    u[i] = reinterpret_cast<const double2*>(V.u[i])[q];
-                    r[i] = reinterpret_cast<const double2*>(V.r[i])[q];
-                }
-                u[J + 1] = reinterpret_cast<const double2*>(V.u[J + 1])[q];
-                const double2 xq = reinterpret_cast<const double2*>(x)[q];
-#pragma unroll
-                for (int i = 0; i <= J; ++i) {
-                    u[i] = make_double2(fma(nb, u[i].x, r[i].x), fma(nb, u[i].y, r[i].y));
-                    reinterpret_cast<double2*>(V.u[i])[q] = u[i];
-                }
-#pragma unroll
-                for (int i = 0; i <= J; ++i)
-                    reinterpret_cast<double2*>(V.r[i])[q] =
-                        make_double2(fma(nal, u[i + 1].x, r[i].x), fma(nal, u[i + 1].y, r[i].y));
-                reinterpret_cast<double2*>(x)[q] = make_double2(fma(al, u[0].x, xq.x), fma(al, u[0].y, xq.y));
-            }
-            return;
-        }
-    }
-    for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
-        E u[J + 2];
+    using A = typename acc_of<S>::type;
+    const S nb = s_neg(st->beta), al = st->alpha, nal = s_neg(st->alpha), nalp = s_neg(st->alpha_prev);
+    const E* rj = V.r[J];
+    const E* uj1 = V.u[J + 1];
+    E* y = V.r[J + 1];
+    typename pacc_of<E>::type pacc;
+    const int32_t stride = gridDim.x * kThreads;
+    for (int32_t q = blockIdx.x * kThreads + threadIdx.x; q < rows; q += stride) {
         S r[J + 1];
+        E u[J + 1];
+#pragma unroll
+        for (int i = 0; i <= J; ++i) r[i] = to_s(ldE(V.r[i], q));
+        if (J >= 1) {
+            const E ujold = ldE(V.u[J], q);
+            r[J - 1] = to_s(from_s<E>(s_fma(nalp, to_s(ujold), r[J - 1])));
+        }
 #pragma unroll
         for (int i = 0; i <= J; ++i) {
-            r[i] = to_s(ldE(V.r[i], q));
             u[i] = from_s<E>(s_fma(nb, to_s(ldE(V.u[i], q)), r[i]));
             stE(V.u[i], q, u[i]);
         }
-        u[J + 1] = ldE(V.u[J + 1], q);
 #pragma unroll
-        for (int i = 0; i <= J; ++i) stE(V.r[i], q, from_s<E>(s_fma(nal, to_s(u[i + 1]), r[i])));
+        for (int i = 0; i < J; ++i) stE(V.r[i], q, from_s<E>(s_fma(nal, to_s(u[i + 1]), r[i])));
         stE(x, q, from_s<E>(s_fma(al, to_s(u[0]), to_s(ldE(x, q)))));
+        // the product row q
+        const int32_t b = __ldg(rp + q), e = __ldg(rp + q + 1);
+        S acc = s_zero(S{});
+        for (int32_t k = b; k < e; ++k) {
+            const int32_t c = ld_idx<LM>(ci, k);
+            const S xv = to_s(from_s<E>(s_fma(nal, to_s(ld_x<LM>(uj1, c)), to_s(ld_x<LM>(rj, c)))));
+            acc = s_fma(to_s(ld_val<LM>(val, k)), xv, acc);
+        }
+        if (diag) acc = s_div(acc, to_s(ldE(diag, q)));
+        const E out = from_s<E>(acc);
+        stE(y, q, out);
+        if (dot) pdot_add(pacc, ldE(w, q), out);
+    }
+    if (dot) {
+        A dacc[1] = {widen_acc(pacc)};
+        grid_finish<1>(dacc, false, partials, ticket, badflag, [&](const S* v, bool bad) { run_epi(ea, v, bad); });
     }
 }
 
+template <class E, int J>
+void launch_spmv_upd_j(int lm, int grid, cudaStream_t s, int32_t rows, const int32_t* rp, const int32_t* ci,
+                       const E* val, const E* diag, const Vecs<E>& V, E* x, const E* w, int dot,
+                       BcgState<typename scalar_of<E>::type>* st,
+                       typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
+                       EpiArgs<typename scalar_of<E>::type> ea) {
+    dispatch_lm<E>(lm, [&](auto mode) {
+        constexpr int M = decltype(mode)::value;
+        k_spmv_upd<E, J, M><<<grid, kThreads, 0, s>>>(rows, rp, ci, val, diag, V, x, w, dot, st, partials, ticket,
+                                                       badflag, ea);
+    });
+}
+
 template <class E>
-void launch_upd_urx(int j, int grid, cudaStream_t s, int64_t n, const Vecs<E>& V, E* x,
-                    const BcgState<typename scalar_of<E>::type>* st) {
-#define HPB_URX(JJ) \
-    case JJ: k_upd_urx<E, JJ><<<grid, kThreads, 0, s>>>(n, V, x, st); break;
+void launch_spmv_upd(int j, int lm, int grid, cudaStream_t s, int32_t rows, const int32_t* rp, const int32_t* ci,
+                     const E* val, const E* diag, const Vecs<E>& V, E* x, const E* w, int dot,
+                     BcgState<typename scalar_of<E>::type>* st,
+                     typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
+                     EpiArgs<typename scalar_of<E>::type> ea) {
+#define HPB_SU(JJ)                                                                                          \
+    case JJ:                                                                                                \
+        launch_spmv_upd_j<E, JJ>(lm, grid, s, rows, rp, ci, val, diag, V, x, w, dot, st, partials, ticket, \
+                                 badflag, ea);                                                              \
+        break;
     switch (j) {
-        HPB_URX(0) HPB_URX(1) HPB_URX(2) HPB_URX(3) HPB_URX(4) HPB_URX(5) HPB_URX(6) HPB_URX(7)
+        HPB_SU(0) HPB_SU(1) HPB_SU(2) HPB_SU(3) HPB_SU(4) HPB_SU(5) HPB_SU(6) HPB_SU(7)
         default: break;
     }
-#undef HPB_URX
+#undef HPB_SU
 }
 
 // ------------------------------------------------------------ MR part
@@ -285,7 +314,7 @@ void launch_upd_urx(int j, int grid, cudaStream_t s, int64_t n, const Vecs<E>& V
 template <class E, int ND>  // ND = L - k + 2 inner products
 __global__ void __launch_bounds__(kThreads)
 k_mgs_step(int64_t n, int k, Vecs<E> V, const BcgState<typename scalar_of<E>::type>* st,
-           typename acc_of<typename scalar_of<E>::type>::type* partials) {
+           typename acc_of<typename scalar_of<E>::type>::type* partials, const E* __restrict__ pend_u) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
     constexpr int NV = ND - 1;  // r_k .. r_L
@@ -295,14 +324,27 @@ k_mgs_step(int64_t n, int k, Vecs<E> V, const BcgState<typename scalar_of<E>::ty
 #pragma unroll
     for (int i = 0; i < NV; ++i) ntau[i] = upd ? s_neg(st->tau[k - 1][k + i]) : s_zero(S{});
     const E* rprev = upd ? V.r[k - 1] : nullptr;
-    const E* r0 = V.r[0];
+    E* r0 = V.r[0];
+    const S nal = s_neg(st->alpha);
     typename pacc_of<E>::type pacc[ND];
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
     for (int64_t q = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < n; q += stride) {
         E ve[NV];
 #pragma unroll
         for (int i = 0; i < NV; ++i) ve[i] = ldE(V.r[k + i], q);
-        const E z = ldE(r0, q);
+        E z = ldE(r0, q);
+        if (pend_u) {
+            // k = 1, NV = L: the last BiCG step's r_{L-1} -= alpha u_L, with
+            // the FMA of the other r updates
+            const S uq = to_s(ldE(pend_u, q));
+            if constexpr (NV >= 2) {
+                ve[NV - 2] = from_s<E>(s_fma(nal, uq, to_s(ve[NV - 2])));
+                stE(V.r[k + NV - 2], q, ve[NV - 2]);
+            } else {
+                z = from_s<E>(s_fma(nal, uq, to_s(z)));
+                stE(r0, q, z);
+            }
+        }
         if (upd) {
             const S pv = to_s(ldE(rprev, q));
 #pragma unroll
@@ -409,6 +451,7 @@ template <class S>
 __global__ void k_init_state(BcgState<S>* st, Report* rep) {
     st->rho = s_one(S{});
     st->alpha = s_zero(S{});
+    st->alpha_prev = s_zero(S{});
     st->omega = s_one(S{});
     st->beta = s_zero(S{});
     rep->rnorm = 0.0;
@@ -493,18 +536,17 @@ inline int occupancy_of(const void* f) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, kThreads, 0) == cudaSuccess && o > 0 ? o : 1;
 }
 
-// blocks per SM of the BiCG update pass of step j (each step's own
-// occupancy: its register count grows with j)
+// blocks per SM of the update + product of step j (its registers grow with j)
 template <class E>
-int update_occupancy(int j) {
+int spmv_upd_occupancy(int j) {
     int occ = 1;
-#define HPB_OCC_U(JJ) \
-    case JJ: occ = occupancy_of(reinterpret_cast<const void*>(k_upd_urx<E, JJ>)); break;
+#define HPB_OCC_SU(JJ) \
+    case JJ: occ = occupancy_of(reinterpret_cast<const void*>(k_spmv_upd<E, JJ, 0>)); break;
     switch (j) {
-        HPB_OCC_U(0) HPB_OCC_U(1) HPB_OCC_U(2) HPB_OCC_U(3) HPB_OCC_U(4) HPB_OCC_U(5) HPB_OCC_U(6) HPB_OCC_U(7)
+        HPB_OCC_SU(0) HPB_OCC_SU(1) HPB_OCC_SU(2) HPB_OCC_SU(3) HPB_OCC_SU(4) HPB_OCC_SU(5) HPB_OCC_SU(6) HPB_OCC_SU(7)
         default: break;
     }
-#undef HPB_OCC_U
+#undef HPB_OCC_SU
     return occ;
 }
 
@@ -551,11 +593,11 @@ template <class E>
 void launch_mgs_step(int nd, int grid, cudaStream_t s, int64_t n, int k, const Vecs<E>& V,
                      const BcgState<typename scalar_of<E>::type>* st,
                      typename acc_of<typename scalar_of<E>::type>::type* partials,
-                     EpiArgs<typename scalar_of<E>::type> ea) {
+                     EpiArgs<typename scalar_of<E>::type> ea, const E* pend_u = nullptr) {
     using S = typename scalar_of<E>::type;
 #define HPB_STEP(ND)                                                                         \
     case ND:                                                                                 \
-        k_mgs_step<E, ND><<<grid, kThreads, 0, s>>>(n, k, V, st, partials);                  \
+        k_mgs_step<E, ND><<<grid, kThreads, 0, s>>>(n, k, V, st, partials, pend_u);          \
         k_mgs_finish<S, ND><<<1, kFinThreads, 0, s>>>(grid, partials, ea);                   \
         break;
     switch (nd) {
@@ -580,7 +622,7 @@ struct BcgPlan<E>::Impl {
     int g_ew = 1, g_red = 1, g_sp = 1, g_spd = 1, g_nrm = 1, kernels = 0;
     int64_t nnz = 0;
     int lm = 0;  // load mode of the cycle's products
-    int g_upd[kMaxL] = {};
+    int g_su[kMaxL] = {};  // grids of the update + product kernels
     SolverWorkspace ws;
     Vecs<E> V{};
     E *rt = nullptr, *tmp = nullptr, *diag = nullptr;
@@ -677,12 +719,15 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     const int64_t n = rows;
     const int64_t need = (n + kThreads - 1) / kThreads;
     P.g_ew = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * light_occupancy<E>())));
-    for (int j = 0; j < L; ++j)
-        P.g_upd[j] = int(std::max<int64_t>(1, std::min<int64_t>((n / 2 + kThreads - 1) / kThreads + 1,
-                                                                  int64_t(sms) * update_occupancy<E>(j))));
     P.g_red = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * reduction_occupancy<E>(L))));
     P.g_sp = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * 8)));  // grid-stride rows, 8 blocks per SM
     P.g_spd = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * 6)));
+    int g_su_max = 1;
+    for (int j = 0; j < L; ++j) {
+        const int cap = std::min(j + 1 < L ? 6 : 8, spmv_upd_occupancy<E>(j));
+        P.g_su[j] = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * cap)));
+        g_su_max = std::max(g_su_max, P.g_su[j]);
+    }
     P.g_nrm = int(std::max<int64_t>(
         1, std::min<int64_t>(need, int64_t(sms) * occupancy_of(reinterpret_cast<const void*>(k_norm<E>)))));
     const int g_ew = P.g_ew, g_red = P.g_red, g_sp = P.g_sp, g_spd = P.g_spd;
@@ -706,9 +751,12 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     P.st = static_cast<BcgState<S>*>(ws.alloc(sizeof(BcgState<S>)));
     P.drep = static_cast<Report*>(ws.alloc(sizeof(Report)));
     // block partials: ND dots x grid blocks for the largest producer -- the
-    // SpMV+Dot2 (1 x g_spd), the norms (1 x g_nrm), the closing update
-    // (2 x g_red) and the first MGS sweep (L + 1 x g_red)
-    const size_t npart = std::max<size_t>(std::max<size_t>(size_t(g_spd), size_t(P.g_nrm)), size_t(L + 1) * size_t(g_red));
+    // SpMV+Dot2 (1 x g_spd), the update + product (1 x g_su[j]), the norms
+    // (1 x g_nrm), the closing update (2 x g_red) and the first MGS sweep
+    // (L + 1 x g_red)
+    const size_t npart = std::max<size_t>(
+        std::max<size_t>(std::max<size_t>(size_t(g_spd), size_t(g_su_max)), size_t(P.g_nrm)),
+        size_t(L + 1) * size_t(g_red));
     P.partials = static_cast<A*>(ws.alloc(npart * sizeof(A)));
     P.ticket = static_cast<unsigned int*>(ws.alloc(64));
     P.badflag = static_cast<int*>(ws.alloc(64));
@@ -770,17 +818,17 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
         // u_{j+1} = A (r_j - beta u_j) and alpha = rho / <rt, u_{j+1}>
         launch_spmv_dot<E, true, true>(lm, g_spd, s, rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt, partials,
                                        ticket, badflag, EpiArgs<S>{st, drep, EPI_ALPHA, 0, j, L}, V.r[j]);
-        launch_upd_urx<E>(j, P.g_upd[j], s, n, V, x, st);
-        if (j + 1 < L)
-            launch_spmv_dot<E, true, false>(lm, g_spd, s, rows, rp, ci, val, diag, V.r[j], V.r[j + 1], rt, partials,
-                                            ticket, badflag, EpiArgs<S>{st, drep, EPI_BETA, 0, j, L});
-        else
-            launch_spmv_dot<E, false, false>(lm, g_sp, s, rows, rp, ci, val, diag, V.r[j], V.r[j + 1], nullptr,
-                                             partials, ticket, badflag, none);
-        kernels += 3;
+        // the BiCG updates of step j (r_j's deferred) and r_{j+1} = A r_j,
+        // with rho = <rt, r_{j+1}> and beta before the last step
+        const bool dot = j + 1 < L;
+        launch_spmv_upd<E>(j, lm, P.g_su[j], s, rows, rp, ci, val, diag, V, x, dot ? rt : nullptr, dot ? 1 : 0,
+                           st, partials, ticket, badflag, dot ? EpiArgs<S>{st, drep, EPI_BETA, 0, j, L} : none);
+        kernels += 2;
     }
     for (int k = 1; k <= L; ++k) {
-        launch_mgs_step<E>(L - k + 2, g_red, s, n, k, V, st, partials, EpiArgs<S>{st, drep, EPI_STEP, k, 0, L});
+        // the first sweep also applies the deferred r_{L-1} -= alpha u_L
+        launch_mgs_step<E>(L - k + 2, g_red, s, n, k, V, st, partials, EpiArgs<S>{st, drep, EPI_STEP, k, 0, L},
+                           k == 1 ? V.u[L] : nullptr);
         kernels += 2;
     }
     launch_final<E>(L, g_red, s, n, 1, V, x, rt, st, partials, ticket, badflag,
