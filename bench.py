@@ -505,7 +505,9 @@ def bicgstabl_cycle_bytes(n, nnz, L, elem=8):
     updates inside the second product of each step (r_j's own update
     deferred to the next step, the last one to the first MGS sweep), the L
     modified Gram-Schmidt sweeps and the closing update, each vector read or
-    written once per kernel."""
+    written once per kernel.  The first MGS sweep's inner products are formed
+    by the last step's kernel from the values it holds (no pass of their
+    own)."""
     mat = (elem + 4.0) * nnz + 4.0 * (n + 1)
     spmv = mat + 2.0 * elem * n
     vec = elem * float(n)
@@ -514,9 +516,12 @@ def bicgstabl_cycle_bytes(n, nnz, L, elem=8):
     # r_{j+1}): u_{j+1} gathered, r_0..r_{j-1}, u_0..u_j and x read, u_0..u_j,
     # r_0..r_{j-1} and x written
     passes += sum(4 * j + 5 for j in range(L))
-    passes += 2                                            # deferred r_{L-1} -= alpha u_L: u_L read, r_{L-1} written
-    for k in range(1, L + 1):                              # right-looking MGS sweep k
-        passes += (L + 1) if k == 1 else (L - k + 3) + (L - k + 1)
+    # deferred r_{L-1} -= alpha u_L in the second sweep: u_L read, and r_1
+    # written when L = 2 (the sweep writes r_2..r_L anyway; the closing
+    # update reads u_1 and writes r_0 anyway when L = 1)
+    passes += {1: 0, 2: 2}.get(L, 1)
+    for k in range(2, L + 1):                              # right-looking MGS sweep k
+        passes += (L - k + 3) + (L - k + 1)
     passes += (2 + 2 * L + 2) + 3                          # closing update: reads, then x, r_0, u_0 written
     return (2 * L) * spmv + (2 * L - 1) * vec + passes * vec
 

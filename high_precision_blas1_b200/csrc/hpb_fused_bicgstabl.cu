@@ -209,30 +209,36 @@ void launch_spmv_dot(int lm, int grid, cudaStream_t s, int32_t rows, const int32
 //                                    every gathered column as the update
 //                                    would store it: the same FMA, the same
 //                                    rounding)
-//   and, with dot, <rt, r_{j+1}> and the beta epilogue.
+// then, before the last step (MR = false), <rt, r_{j+1}> and the beta
+// epilogue; at the last step (MR = true, j = l - 1) the inner products of
+// the first MR sweep, <r_1, r_1>, <r_1, r_0>, <r_1, r_i> (i = 2..l), from
+// the row's values in registers, as block partials for k_mgs_finish.
 // r_j' itself is stored by the next step's kernel, or after the last step
-// by the first MR sweep, so no block writes what another gathers.  Per
-// element these are the operations of a separate update pass followed by
-// the product, so the iterates are the same bits; the cycle saves the
-// update pass's launch.  J = j is a template parameter so the row's values
-// stay in registers.
-template <class E, int J, int LM>
+// by the second MR sweep (the closing update when l = 1), so no block
+// writes what another gathers.  Per element these are the operations of a
+// separate update pass followed by the product, so the vectors are the
+// same bits; the cycle saves the update pass's launch and, at the last
+// step, the first sweep's pass over l + 1 vectors.  J = j is a template
+// parameter so the row's values stay in registers.
+template <class E, int J, int LM, bool MR>
 __global__ void __launch_bounds__(kThreads)
 k_spmv_upd(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci, const E* __restrict__ val,
-           const E* __restrict__ diag, Vecs<E> V, E* __restrict__ x, const E* __restrict__ w, int dot,
+           const E* __restrict__ diag, Vecs<E> V, E* __restrict__ x, const E* __restrict__ w,
            BcgState<typename scalar_of<E>::type>* st, typename acc_of<typename scalar_of<E>::type>::type* partials,
            unsigned int* ticket, int* badflag, EpiArgs<typename scalar_of<E>::type> ea) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
+    constexpr int ND = MR ? J + 2 : 1;  // inner products
     const S nb = s_neg(st->beta), al = st->alpha, nal = s_neg(st->alpha), nalp = s_neg(st->alpha_prev);
     const E* rj = V.r[J];
     const E* uj1 = V.u[J + 1];
     E* y = V.r[J + 1];
-    typename pacc_of<E>::type pacc;
+    typename pacc_of<E>::type pacc[ND];
     const int32_t stride = gridDim.x * kThreads;
     for (int32_t q = blockIdx.x * kThreads + threadIdx.x; q < rows; q += stride) {
         S r[J + 1];
         E u[J + 1];
+        E rv[J + 1];  // MR: r_0'..r_j' of this row
 #pragma unroll
         for (int i = 0; i <= J; ++i) r[i] = to_s(ldE(V.r[i], q));
         if (J >= 1) {
@@ -245,7 +251,11 @@ k_spmv_upd(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
             stE(V.u[i], q, u[i]);
         }
 #pragma unroll
-        for (int i = 0; i < J; ++i) stE(V.r[i], q, from_s<E>(s_fma(nal, to_s(u[i + 1]), r[i])));
+        for (int i = 0; i < J; ++i) {
+            rv[i] = from_s<E>(s_fma(nal, to_s(u[i + 1]), r[i]));
+            stE(V.r[i], q, rv[i]);
+        }
+        if (MR) rv[J] = from_s<E>(s_fma(nal, to_s(ldE(uj1, q)), r[J]));
         stE(x, q, from_s<E>(s_fma(al, to_s(u[0]), to_s(ldE(x, q)))));
         // the product row q
         const int32_t b = __ldg(rp + q), e = __ldg(rp + q + 1);
@@ -258,37 +268,60 @@ k_spmv_upd(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restri
         if (diag) acc = s_div(acc, to_s(ldE(diag, q)));
         const E out = from_s<E>(acc);
         stE(y, q, out);
-        if (dot) pdot_add(pacc, ldE(w, q), out);
+        if constexpr (MR) {
+            // r_1 is r_{j+1} itself when l = 1
+            const E r1 = J >= 1 ? rv[J >= 1 ? 1 : 0] : out;
+            pdot_add(pacc[0], r1, r1);
+            pdot_add(pacc[1], r1, rv[0]);
+#pragma unroll
+            for (int i = 2; i < ND; ++i) pdot_add(pacc[i], r1, i <= J ? rv[i <= J ? i : 0] : out);
+        } else {
+            pdot_add(pacc[0], ldE(w, q), out);
+        }
     }
-    if (dot) {
-        A dacc[1] = {widen_acc(pacc)};
+    A dacc[ND];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) dacc[d] = widen_acc(pacc[d]);
+    if constexpr (MR) {
+        __shared__ A sh[ND * 32];
+        block_merge<ND>(dacc, sh);
+        if (threadIdx.x == 0)
+#pragma unroll
+            for (int d = 0; d < ND; ++d) partials[size_t(d) * gridDim.x + blockIdx.x] = dacc[d];
+    } else {
         grid_finish<1>(dacc, false, partials, ticket, badflag, [&](const S* v, bool bad) { run_epi(ea, v, bad); });
     }
 }
 
-template <class E, int J>
+template <class E, int J, bool MR>
 void launch_spmv_upd_j(int lm, int grid, cudaStream_t s, int32_t rows, const int32_t* rp, const int32_t* ci,
-                       const E* val, const E* diag, const Vecs<E>& V, E* x, const E* w, int dot,
+                       const E* val, const E* diag, const Vecs<E>& V, E* x, const E* w,
                        BcgState<typename scalar_of<E>::type>* st,
                        typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
                        EpiArgs<typename scalar_of<E>::type> ea) {
     dispatch_lm<E>(lm, [&](auto mode) {
         constexpr int M = decltype(mode)::value;
-        k_spmv_upd<E, J, M><<<grid, kThreads, 0, s>>>(rows, rp, ci, val, diag, V, x, w, dot, st, partials, ticket,
-                                                       badflag, ea);
+        k_spmv_upd<E, J, M, MR><<<grid, kThreads, 0, s>>>(rows, rp, ci, val, diag, V, x, w, st, partials, ticket,
+                                                           badflag, ea);
     });
 }
 
+// step j of l: the rt inner product before the last step, the first MR
+// sweep's inner products at it
 template <class E>
-void launch_spmv_upd(int j, int lm, int grid, cudaStream_t s, int32_t rows, const int32_t* rp, const int32_t* ci,
-                     const E* val, const E* diag, const Vecs<E>& V, E* x, const E* w, int dot,
+void launch_spmv_upd(int j, int L, int lm, int grid, cudaStream_t s, int32_t rows, const int32_t* rp,
+                     const int32_t* ci, const E* val, const E* diag, const Vecs<E>& V, E* x, const E* w,
                      BcgState<typename scalar_of<E>::type>* st,
                      typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
                      EpiArgs<typename scalar_of<E>::type> ea) {
-#define HPB_SU(JJ)                                                                                          \
-    case JJ:                                                                                                \
-        launch_spmv_upd_j<E, JJ>(lm, grid, s, rows, rp, ci, val, diag, V, x, w, dot, st, partials, ticket, \
-                                 badflag, ea);                                                              \
+#define HPB_SU(JJ)                                                                                               \
+    case JJ:                                                                                                     \
+        if (JJ + 1 == L)                                                                                         \
+            launch_spmv_upd_j<E, JJ, true>(lm, grid, s, rows, rp, ci, val, diag, V, x, w, st, partials, ticket,  \
+                                           badflag, ea);                                                         \
+        else                                                                                                     \
+            launch_spmv_upd_j<E, JJ, false>(lm, grid, s, rows, rp, ci, val, diag, V, x, w, st, partials, ticket, \
+                                            badflag, ea);                                                        \
         break;
     switch (j) {
         HPB_SU(0) HPB_SU(1) HPB_SU(2) HPB_SU(3) HPB_SU(4) HPB_SU(5) HPB_SU(6) HPB_SU(7)
@@ -324,7 +357,7 @@ k_mgs_step(int64_t n, int k, Vecs<E> V, const BcgState<typename scalar_of<E>::ty
 #pragma unroll
     for (int i = 0; i < NV; ++i) ntau[i] = upd ? s_neg(st->tau[k - 1][k + i]) : s_zero(S{});
     const E* rprev = upd ? V.r[k - 1] : nullptr;
-    E* r0 = V.r[0];
+    const E* r0 = V.r[0];
     const S nal = s_neg(st->alpha);
     typename pacc_of<E>::type pacc[ND];
     const int64_t stride = int64_t(gridDim.x) * blockDim.x;
@@ -332,21 +365,22 @@ k_mgs_step(int64_t n, int k, Vecs<E> V, const BcgState<typename scalar_of<E>::ty
         E ve[NV];
 #pragma unroll
         for (int i = 0; i < NV; ++i) ve[i] = ldE(V.r[k + i], q);
-        E z = ldE(r0, q);
+        const E z = ldE(r0, q);
+        S pv = upd ? to_s(ldE(rprev, q)) : s_zero(S{});
         if (pend_u) {
-            // k = 1, NV = L: the last BiCG step's r_{L-1} -= alpha u_L, with
-            // the FMA of the other r updates
+            // k = 2, NV = L - 1: the last BiCG step's r_{L-1} -= alpha u_L,
+            // with the FMA of the other r updates (r_{L-1} = r_1 = rprev
+            // when L = 2)
             const S uq = to_s(ldE(pend_u, q));
             if constexpr (NV >= 2) {
                 ve[NV - 2] = from_s<E>(s_fma(nal, uq, to_s(ve[NV - 2])));
-                stE(V.r[k + NV - 2], q, ve[NV - 2]);
             } else {
-                z = from_s<E>(s_fma(nal, uq, to_s(z)));
-                stE(r0, q, z);
+                const E pe = from_s<E>(s_fma(nal, uq, pv));
+                stE(V.r[k - 1], q, pe);
+                pv = to_s(pe);
             }
         }
         if (upd) {
-            const S pv = to_s(ldE(rprev, q));
 #pragma unroll
             for (int i = 0; i < NV; ++i) {
                 ve[i] = from_s<E>(s_fma(ntau[i], pv, to_s(ve[i])));
@@ -396,7 +430,7 @@ template <class E, int L>
 __global__ void __launch_bounds__(kThreads)
 k_final(int64_t n, int update, Vecs<E> V, E* __restrict__ x, const E* __restrict__ rt,
         BcgState<typename scalar_of<E>::type>* st, typename acc_of<typename scalar_of<E>::type>::type* partials,
-        unsigned int* ticket, int* badflag, EpiArgs<typename scalar_of<E>::type> ea) {
+        unsigned int* ticket, int* badflag, EpiArgs<typename scalar_of<E>::type> ea, int pend) {
     using S = typename scalar_of<E>::type;
     using A = typename acc_of<S>::type;
     S g[L + 1], g1[L + 1], g2[L + 1];
@@ -421,6 +455,8 @@ k_final(int64_t n, int update, Vecs<E> V, E* __restrict__ x, const E* __restrict
                 ue[j] = ldE(V.u[j], q);
             }
             ue[0] = ldE(V.u[0], q);
+            // L = 1: the BiCG step's deferred r_0 -= alpha u_1
+            if (L == 1 && pend) r0e = from_s<E>(s_fma(s_neg(st->alpha), to_s(ue[L]), to_s(r0e)));
             S r0 = to_s(r0e);
             S xs = s_fma(gam_1, r0, to_s(xe));
             r0 = s_fma(g1[L], to_s(re[L]), r0);
@@ -536,12 +572,16 @@ inline int occupancy_of(const void* f) {
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, f, kThreads, 0) == cudaSuccess && o > 0 ? o : 1;
 }
 
-// blocks per SM of the update + product of step j (its registers grow with j)
+// blocks per SM of the update + product of step j of l (its registers grow
+// with j)
 template <class E>
-int spmv_upd_occupancy(int j) {
+int spmv_upd_occupancy(int j, int L) {
     int occ = 1;
-#define HPB_OCC_SU(JJ) \
-    case JJ: occ = occupancy_of(reinterpret_cast<const void*>(k_spmv_upd<E, JJ, 0>)); break;
+#define HPB_OCC_SU(JJ)                                                                                      \
+    case JJ:                                                                                                \
+        occ = JJ + 1 == L ? occupancy_of(reinterpret_cast<const void*>(k_spmv_upd<E, JJ, 0, true>))         \
+                          : occupancy_of(reinterpret_cast<const void*>(k_spmv_upd<E, JJ, 0, false>));       \
+        break;
     switch (j) {
         HPB_OCC_SU(0) HPB_OCC_SU(1) HPB_OCC_SU(2) HPB_OCC_SU(3) HPB_OCC_SU(4) HPB_OCC_SU(5) HPB_OCC_SU(6) HPB_OCC_SU(7)
         default: break;
@@ -579,9 +619,11 @@ template <class E>
 void launch_final(int L, int grid, cudaStream_t s, int64_t n, int update, const Vecs<E>& V, E* x, const E* rt,
                   BcgState<typename scalar_of<E>::type>* st,
                   typename acc_of<typename scalar_of<E>::type>::type* partials, unsigned int* ticket, int* badflag,
-                  EpiArgs<typename scalar_of<E>::type> ea) {
-#define HPB_FINAL(LL) \
-    case LL: k_final<E, LL><<<grid, kThreads, 0, s>>>(n, update, V, x, rt, st, partials, ticket, badflag, ea); break;
+                  EpiArgs<typename scalar_of<E>::type> ea, int pend = 0) {
+#define HPB_FINAL(LL)                                                                                           \
+    case LL:                                                                                                    \
+        k_final<E, LL><<<grid, kThreads, 0, s>>>(n, update, V, x, rt, st, partials, ticket, badflag, ea, pend); \
+        break;
     switch (L) {
         HPB_FINAL(1) HPB_FINAL(2) HPB_FINAL(3) HPB_FINAL(4) HPB_FINAL(5) HPB_FINAL(6) HPB_FINAL(7) HPB_FINAL(8)
         default: break;
@@ -605,6 +647,21 @@ void launch_mgs_step(int nd, int grid, cudaStream_t s, int64_t n, int k, const V
         default: break;
     }
 #undef HPB_STEP
+}
+
+// the combine of the first MR sweep, whose inner products the last BiCG
+// step's kernel formed (nb blocks)
+template <class E>
+void launch_mgs_finish(int nd, int nb, cudaStream_t s, const typename acc_of<typename scalar_of<E>::type>::type* partials,
+                       EpiArgs<typename scalar_of<E>::type> ea) {
+    using S = typename scalar_of<E>::type;
+#define HPB_FIN(ND) \
+    case ND: k_mgs_finish<S, ND><<<1, kFinThreads, 0, s>>>(nb, partials, ea); break;
+    switch (nd) {
+        HPB_FIN(2) HPB_FIN(3) HPB_FIN(4) HPB_FIN(5) HPB_FIN(6) HPB_FIN(7) HPB_FIN(8) HPB_FIN(9)
+        default: break;
+    }
+#undef HPB_FIN
 }
 
 template <class E>
@@ -724,7 +781,7 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     P.g_spd = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * 6)));
     int g_su_max = 1;
     for (int j = 0; j < L; ++j) {
-        const int cap = std::min(j + 1 < L ? 6 : 8, spmv_upd_occupancy<E>(j));
+        const int cap = std::min(6, spmv_upd_occupancy<E>(j, L));
         P.g_su[j] = int(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(sms) * cap)));
         g_su_max = std::max(g_su_max, P.g_su[j]);
     }
@@ -751,11 +808,11 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
     P.st = static_cast<BcgState<S>*>(ws.alloc(sizeof(BcgState<S>)));
     P.drep = static_cast<Report*>(ws.alloc(sizeof(Report)));
     // block partials: ND dots x grid blocks for the largest producer -- the
-    // SpMV+Dot2 (1 x g_spd), the update + product (1 x g_su[j]), the norms
-    // (1 x g_nrm), the closing update (2 x g_red) and the first MGS sweep
-    // (L + 1 x g_red)
+    // SpMV+Dot2 (1 x g_spd), the update + product (1 x g_su[j]; L + 1 x
+    // g_su[L - 1] at the last step), the norms (1 x g_nrm), the closing
+    // update (2 x g_red) and the MGS sweeps (at most L x g_red)
     const size_t npart = std::max<size_t>(
-        std::max<size_t>(std::max<size_t>(size_t(g_spd), size_t(g_su_max)), size_t(P.g_nrm)),
+        std::max<size_t>(std::max<size_t>(size_t(g_spd), size_t(L + 1) * size_t(g_su_max)), size_t(P.g_nrm)),
         size_t(L + 1) * size_t(g_red));
     P.partials = static_cast<A*>(ws.alloc(npart * sizeof(A)));
     P.ticket = static_cast<unsigned int*>(ws.alloc(64));
@@ -818,21 +875,26 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
         // u_{j+1} = A (r_j - beta u_j) and alpha = rho / <rt, u_{j+1}>
         launch_spmv_dot<E, true, true>(lm, g_spd, s, rows, rp, ci, val, diag, V.u[j], V.u[j + 1], rt, partials,
                                        ticket, badflag, EpiArgs<S>{st, drep, EPI_ALPHA, 0, j, L}, V.r[j]);
-        // the BiCG updates of step j (r_j's deferred) and r_{j+1} = A r_j,
-        // with rho = <rt, r_{j+1}> and beta before the last step
-        const bool dot = j + 1 < L;
-        launch_spmv_upd<E>(j, lm, P.g_su[j], s, rows, rp, ci, val, diag, V, x, dot ? rt : nullptr, dot ? 1 : 0,
-                           st, partials, ticket, badflag, dot ? EpiArgs<S>{st, drep, EPI_BETA, 0, j, L} : none);
+        // the BiCG updates of step j (r_j's deferred) and r_{j+1} = A r_j';
+        // before the last step rho = <rt, r_{j+1}> and beta, at it the first
+        // MR sweep's inner products
+        const bool last = j + 1 == L;
+        launch_spmv_upd<E>(j, L, lm, P.g_su[j], s, rows, rp, ci, val, diag, V, x, rt, st, partials, ticket,
+                           badflag, last ? none : EpiArgs<S>{st, drep, EPI_BETA, 0, j, L});
         kernels += 2;
     }
-    for (int k = 1; k <= L; ++k) {
-        // the first sweep also applies the deferred r_{L-1} -= alpha u_L
+    // MR part: the first sweep's combine, then sweeps 2..L; the second
+    // sweep (the closing update when L = 1) applies the deferred
+    // r_{L-1} -= alpha u_L
+    launch_mgs_finish<E>(L + 1, P.g_su[L - 1], s, partials, EpiArgs<S>{st, drep, EPI_STEP, 1, 0, L});
+    kernels += 1;
+    for (int k = 2; k <= L; ++k) {
         launch_mgs_step<E>(L - k + 2, g_red, s, n, k, V, st, partials, EpiArgs<S>{st, drep, EPI_STEP, k, 0, L},
-                           k == 1 ? V.u[L] : nullptr);
+                           k == 2 ? V.u[L] : nullptr);
         kernels += 2;
     }
     launch_final<E>(L, g_red, s, n, 1, V, x, rt, st, partials, ticket, badflag,
-                    EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L});
+                    EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L}, L == 1 ? 1 : 0);
     if (P.plain_graph) {
         kernels += 1;
         if (cudaStreamEndCapture(s, &ws.graph) != cudaSuccess) return HPB_ERROR_CUDA;
