@@ -220,6 +220,7 @@ _sig("hpb_spai_assemble", C.c_int, [P, C.POINTER(hpb_spai_system), P])
 _sig("hpb_spai_loss_grad", C.c_int, [P, C.POINTER(hpb_spai_system), C.c_float, C.c_float, P, P])
 _sig("hpb_spai_loss", C.c_int, [P, C.POINTER(hpb_spai_system), C.c_float, C.c_float, P])
 _sig("hpb_spai_adam", C.c_int, [P, C.c_float, C.c_float])
+_sig("hpb_spai_forward", C.c_int, [P, I32, P, P, C.c_int])
 
 
 def ir_params(inner="gmres", basis=50, inner_rel_tol=1e-5, inner_max_iters=5000, precond="none", rel_tol=1e-10,

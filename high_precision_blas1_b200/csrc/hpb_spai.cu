@@ -41,12 +41,12 @@
 
 #include "hpb_common.cuh"
 #include "hpb_fused.cuh"
+#include "hpb_spai.cuh"
 
 namespace hpb {
 namespace spai {
 
-constexpr int kF = 16, kH = 64, kO = 8, kMaxSlot = 8, kMaxSq = 64;
-constexpr int kNumParams = kF * kH + kH + kH * kH + kH + kH * kO + kO;  // 5768
+constexpr int kMaxSlot = 8, kMaxSq = 64;
 constexpr int kThreads = 256;
 
 struct Offsets {
@@ -60,10 +60,6 @@ struct Offsets {
     int dq[kMaxSlot][kMaxSlot];
     // slot of -off[s] (the transposed entry), -1 if absent
     int rev[kMaxSlot];
-};
-
-struct Params {  // offsets (in floats) of each tensor in the parameter vector
-    static constexpr int W1 = 0, B1 = W1 + kF * kH, W2 = B1 + kH, B2 = W2 + kH * kH, W3 = B2 + kH, B3 = W3 + kH * kO;
 };
 
 __device__ __forceinline__ int slot_of(const Offsets& o, int d) {
@@ -692,6 +688,8 @@ struct hpb_spai {
     float *ahat = nullptr, *rh = nullptr;
     double* lpart = nullptr;
     int part_blocks = 0;
+    int* tc_err = nullptr;       // mapped pinned word: a tensor-core wait ran out of time
+    int* tc_err_dev = nullptr;   // its device address
 };
 
 namespace {
@@ -778,6 +776,34 @@ int mean_log_diag(hpb_spai* net, int32_t n, const float* diag, double* scratch, 
     return st;
 }
 
+// The MLP on n rows of features: path 1 the tcgen05 kernel (hpb_spai_tc.cu),
+// path 0 the warp-level mma.sync kernel (k_forward).
+int mlp_forward(hpb_spai* net, int32_t n, const float* feat, float* out, float* h1, float* h2, int path) {
+    using namespace hpb::spai;
+    if (n <= 0) return HPB_SUCCESS;
+    if (path == 1) {
+        if (forward_tc(n, feat, net->wb, h1, h2, out, net->tc_err_dev, nullptr) != cudaSuccess) return HPB_ERROR_CUDA;
+    } else {
+        int occ = 1, dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_forward, kMmaWarps * 32, 0);
+        const int need = (n + 16 * kMmaWarps - 1) / (16 * kMmaWarps);
+        const int grid = std::max(1, std::min(need, sms * std::max(occ, 1)));
+        k_forward<<<grid, kMmaWarps * 32>>>(n, feat, net->wb, h1, h2, out);
+    }
+    hpb::count_launch();
+    return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
+}
+
+// after a synchronisation: HPB_ERROR_TIMEOUT if a tcgen05 forward gave up
+// waiting for its products since the last check (the word is cleared)
+int take_tc_status(hpb_spai* net) {
+    if (!net->tc_err || *reinterpret_cast<volatile int*>(net->tc_err) == 0) return HPB_SUCCESS;
+    *reinterpret_cast<volatile int*>(net->tc_err) = 0;
+    return HPB_ERROR_TIMEOUT;
+}
+
 // Features and the MLP forward pass of one system (binary32 CSR, device),
 // into feat / out; diag receives diag(A).  h1, h2 (post-ReLU) are kept for
 // the backward pass when not null.
@@ -792,17 +818,8 @@ int forward_rows(hpb_spai* net, const hpb_spai_system& sys, float* diag, float* 
     int st = mean_log_diag(net, n, diag, scratch, &ml);
     if (st) return st;
     k_features<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, diag, float(ml), net->off, feat);
-    {
-        int occ = 1, dev = 0, sms = 148;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_forward, kMmaWarps * 32, 0);
-        const int need = (n + 16 * kMmaWarps - 1) / (16 * kMmaWarps);
-        const int grid = std::max(1, std::min(need, sms * std::max(occ, 1)));
-        k_forward<<<grid, kMmaWarps * 32>>>(n, feat, net->wb, h1, h2, out);
-    }
-    hpb::count_launch(2);
-    return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
+    hpb::count_launch();
+    return mlp_forward(net, n, feat, out, h1, h2, 1);
 }
 
 // training: forward with h1/h2 kept, Mh (scaled) and Ah into the network's workspace
@@ -881,6 +898,16 @@ int hpb_spai_create(hpb_spai** out, int nslot, int dslot, const int* offsets, ui
         w[Params::B1 + i] = 0.01f;
         w[Params::B2 + i] = 0.01f;
     }
+    if (cudaHostAlloc(&net->tc_err, sizeof(int), cudaHostAllocMapped) != cudaSuccess) {
+        net->tc_err = nullptr;
+        hpb_spai_destroy(net);
+        return HPB_ERROR_OUT_OF_MEMORY;
+    }
+    *net->tc_err = 0;
+    if (cudaHostGetDevicePointer(reinterpret_cast<void**>(&net->tc_err_dev), net->tc_err, 0) != cudaSuccess) {
+        hpb_spai_destroy(net);
+        return HPB_ERROR_CUDA;
+    }
     if (cudaMalloc(&net->w, kNumParams * 4) || cudaMalloc(&net->wb, kNumParams * 2) ||
         cudaMalloc(&net->m1, kNumParams * 4) || cudaMalloc(&net->m2, kNumParams * 4) ||
         cudaMalloc(&net->grad, kNumParams * 4) || cudaMalloc(&net->gtmp, kNumParams * 4) ||
@@ -912,6 +939,7 @@ int hpb_spai_destroy(hpb_spai* net) {
                     net->out, net->dout, net->diag, net->mval, net->dm, net->G, net->y, net->z, net->g, net->lpart,
                     net->ahat, net->rh};
     for (void* p : ptrs) cudaFree(p);
+    if (net->tc_err) cudaFreeHost(net->tc_err);
     if (net->ctx) hpb_destroy(net->ctx);
     delete net;
     return HPB_SUCCESS;
@@ -960,7 +988,19 @@ int hpb_spai_assemble(hpb_spai* net, const hpb_spai_system* sys, float* m_val) {
                     static_cast<void*>(scratch)})
         pool_free(q, nullptr);
     if (cudaStreamSynchronize(nullptr) != cudaSuccess && st == HPB_SUCCESS) st = HPB_ERROR_CUDA;
-    return st;
+    const int tc = take_tc_status(net);
+    return st == HPB_SUCCESS ? tc : st;
+}
+
+// The MLP alone on rows x 16 features (device, binary32): out (device,
+// rows x 8); path 1 the tcgen05 kernel the build and training use, path 0
+// the warp-level mma.sync kernel.  Blocking.
+int hpb_spai_forward(hpb_spai* net, int32_t rows, const float* feat, float* out, int path) {
+    if (!net || rows < 0 || (rows > 0 && (!feat || !out)) || (path != 0 && path != 1)) return HPB_ERROR_INVALID_VALUE;
+    int st = mlp_forward(net, rows, feat, out, nullptr, nullptr, path);
+    if (cudaStreamSynchronize(nullptr) != cudaSuccess && st == HPB_SUCCESS) st = HPB_ERROR_CUDA;
+    const int tc = take_tc_status(net);
+    return st == HPB_SUCCESS ? tc : st;
 }
 
 // Loss of one system and its parameter gradient, added to the network's
@@ -1032,7 +1072,8 @@ int loss_impl(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_r
         loss[1] = lf;
         loss[2] = lr;
     }
-    return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
+    if (cudaStreamSynchronize(nullptr) != cudaSuccess || cudaGetLastError() != cudaSuccess) return HPB_ERROR_CUDA;
+    return take_tc_status(net);
 }
 
 }  // namespace

@@ -1,0 +1,369 @@
+// The learned SPAI's per-row MLP forward (16 -> 64 -> 64 -> 8, ReLU) on the
+// fifth-generation tensor cores.
+//
+// A block of four warps takes 128-row tiles in a grid-stride loop; the 128
+// rows are the M = 128 of every product and the 128 lanes of the block's
+// tensor-memory accumulators (warp w reads lanes 32w..32w+31: its rows).
+// Per tile:
+//   features (binary32, 64 B per row, loaded one tile ahead) -> bf16 hi/lo
+//   pairs in shared memory -> D1 = X W1 (two tcgen05.mma, hi and lo, K = 16)
+//   -> tcgen05.ld, + b1, ReLU -> bf16 hi/lo in shared memory -> D2 = H1 W2
+//   (eight tcgen05.mma, K = 4 x 16, hi and lo) -> + b2, ReLU -> hi/lo ->
+//   D3 = H2 W3 (N = 16: the 8 outputs padded) -> + b3 -> out.
+// Each binary32 activation x is carried as hi = bf16(x), lo = bf16(x - hi)
+// and multiplied as two bf16 products (about 16 bits of x kept) with bf16
+// weights and binary32 accumulation -- the arithmetic of the warp-level
+// kernel (hpb_spai.cu, k_forward) except for the order of the sums inside a
+// product.  One thread issues the products and commits them to an mbarrier
+// that the block waits on (bounded by %globaltimer; on expiry the block sets
+// *err, frees its tensor memory and returns).
+//
+// Operand images in shared memory are K-major without swizzle: 8-row x
+// 16-byte core matrices; element (r, k) of an R-row operand at byte
+//   (k / 8) * 16 R + (r / 8) * 128 + (r % 8) * 16 + (k % 8) * 2,
+// so the stride between 8-row groups (SBO) is 128 B and the stride between
+// the two 8-element K halves of one K = 16 product (LBO) is 16 R bytes.
+#include <algorithm>
+#include <cstring>
+
+#include "hpb_spai.cuh"
+
+namespace hpb {
+namespace spai {
+namespace {
+
+constexpr int kTile = 128;       // rows per tile (M of every product, TMEM lanes)
+constexpr int kTcThreads = 128;  // four warps
+constexpr int kN3 = 16;          // layer-3 N: the 8 outputs padded to the M = 128 minimum
+constexpr int kTmemCols = 128;   // D1 and D3 in columns 0..63, D2 in 64..127
+
+constexpr int kOffW1 = 0;                            // W1^T: 64 x 16
+constexpr int kOffW2 = kOffW1 + kH * kF * 2;         // W2^T: 64 x 64
+constexpr int kOffW3 = kOffW2 + kH * kH * 2;         // W3^T: 16 x 64 (rows 8..15 zero)
+constexpr int kOffA1h = kOffW3 + kN3 * kH * 2;       // features hi: 128 x 16
+constexpr int kOffA1l = kOffA1h + kTile * kF * 2;    // features lo
+constexpr int kOffA2h = kOffA1l + kTile * kF * 2;    // activations hi: 128 x 64
+constexpr int kOffA2l = kOffA2h + kTile * kH * 2;    // activations lo
+constexpr int kOffBias = kOffA2l + kTile * kH * 2;   // b1, b2, b3 (binary32)
+constexpr int kOffBar = kOffBias + (2 * kH + kO) * 4;
+constexpr int kOffTmem = kOffBar + 8;
+constexpr int kSmemUsed = kOffTmem + 4;
+// At least 46 KB per block keeps at most four blocks on an SM (228 KB), so
+// their tensor memory (4 x 128 columns) never exceeds the SM's 512 columns
+// and no allocation waits.
+constexpr int kSmemBytes = 56 * 1024;
+static_assert(kSmemUsed <= kSmemBytes, "shared-memory plan");
+static_assert(kOffBar % 8 == 0 && kOffA1h % 16 == 0 && kOffA2h % 16 == 0, "alignment");
+
+__host__ __device__ constexpr uint32_t kmaj(int r, int kc, int R) { return uint32_t(kc * 16 * R + (r >> 3) * 128 + (r & 7) * 16); }
+
+// instruction descriptor of kind::f16: binary32 accumulator, bf16 A and B,
+// both K-major, M x N
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
+}
+
+// shared-memory matrix descriptor: K-major, no swizzle, version 1
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t((lbo >> 4) & 0x3FFFu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3FFFu) << 32) | (uint64_t(1) << 46);
+}
+
+__device__ __forceinline__ void mma_f16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    const uint32_t z = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+        :
+        : "r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ uint64_t now_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// wait for phase `parity` of the mbarrier; false if 2 s pass first
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+    const uint64_t t0 = now_ns();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (now_ns() - t0 > 2000000000ull) return false;
+    }
+}
+
+// 64 consecutive binary32 accumulator columns of this thread's lane, with the
+// wait for the load inside the same statement (the values are final on exit)
+__device__ __forceinline__ void tmem_ld64(uint32_t addr, float (&v)[64]) {
+    uint32_t r[64];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%64];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, "
+        "[%65];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47}, "
+        "[%66];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, "
+        "[%67];\n\t"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(addr), "r"(addr + 16), "r"(addr + 32), "r"(addr + 48)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n\t"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(addr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t bf2(float a, float b) {  // a in the low half (the lower k)
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    uint32_t u;
+    memcpy(&u, &h, 4);
+    return u;
+}
+
+// eight consecutive activations of this row -> 16-byte hi and lo chunks
+__device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
+    float h[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) h[i] = __bfloat162float(__float2bfloat16_rn(x[i]));
+    hi = make_uint4(bf2(h[0], h[1]), bf2(h[2], h[3]), bf2(h[4], h[5]), bf2(h[6], h[7]));
+    lo = make_uint4(bf2(x[0] - h[0], x[1] - h[1]), bf2(x[2] - h[2], x[3] - h[3]), bf2(x[4] - h[4], x[5] - h[5]),
+                    bf2(x[6] - h[6], x[7] - h[7]));
+}
+
+__device__ __forceinline__ void load_feat(const float* __restrict__ feat, int32_t row, int32_t rows, float (&x)[kF]) {
+    if (row < rows) {
+        const float4* p = reinterpret_cast<const float4*>(feat + size_t(row) * kF);
+#pragma unroll
+        for (int i = 0; i < kF / 4; ++i) {
+            const float4 v = __ldcs(p + i);
+            x[4 * i] = v.x;
+            x[4 * i + 1] = v.y;
+            x[4 * i + 2] = v.z;
+            x[4 * i + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < kF; ++i) x[i] = 0.f;
+    }
+}
+
+__global__ void __launch_bounds__(kTcThreads)
+k_forward_tc(int32_t rows, const float* __restrict__ feat, const __nv_bfloat16* __restrict__ w, float* __restrict__ h1g,
+             float* __restrict__ h2g, float* __restrict__ out, int* err) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const int t = threadIdx.x, warp = t >> 5;
+    const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
+    const uint32_t bar = sbase + kOffBar;
+    float* sbias = reinterpret_cast<float*>(sm + kOffBias);
+
+    // ---- weights as the K-major B operands (W^T: rows n, K contiguous), biases
+    auto put = [&](int off, int R, int n, int k, __nv_bfloat16 v) {
+        *reinterpret_cast<__nv_bfloat16*>(sm + off + kmaj(n, k >> 3, R) + (k & 7) * 2) = v;
+    };
+    for (int i = t; i < kH * kF; i += kTcThreads) put(kOffW1, kH, i / kF, i % kF, w[Params::W1 + (i % kF) * kH + i / kF]);
+    for (int i = t; i < kH * kH; i += kTcThreads) put(kOffW2, kH, i / kH, i % kH, w[Params::W2 + (i % kH) * kH + i / kH]);
+    for (int i = t; i < kN3 * kH; i += kTcThreads) {
+        const int n = i / kH, k = i % kH;
+        put(kOffW3, kN3, n, k, n < kO ? w[Params::W3 + k * kO + n] : __float2bfloat16_rn(0.f));
+    }
+    for (int i = t; i < kH; i += kTcThreads) {
+        sbias[i] = __bfloat162float(w[Params::B1 + i]);
+        sbias[kH + i] = __bfloat162float(w[Params::B2 + i]);
+    }
+    if (t < kO) sbias[2 * kH + t] = __bfloat162float(w[Params::B3 + t]);
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kOffTmem),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();  // the weight images are read by the tensor cores
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kOffTmem);
+    const uint32_t lane_tmem = tmem + (uint32_t(32 * warp) << 16);  // this warp's lanes
+
+    constexpr uint32_t id64 = idesc_bf16(kTile, kH), id16 = idesc_bf16(kTile, kN3);
+    const uint32_t a1h = sbase + kOffA1h, a1l = sbase + kOffA1l, a2h = sbase + kOffA2h, a2l = sbase + kOffA2l;
+    const uint32_t w1 = sbase + kOffW1, w2 = sbase + kOffW2, w3 = sbase + kOffW3;
+    const uint32_t d1 = tmem, d2 = tmem + kH, d3 = tmem;
+
+    uint32_t phase = 0;
+    bool failed = false;
+    const int32_t ntiles = (rows + kTile - 1) / kTile;
+    float xf[kF];
+    if (int32_t(blockIdx.x) < ntiles) load_feat(feat, int32_t(blockIdx.x) * kTile + t, rows, xf);
+    for (int32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int32_t row = tile * kTile + t;
+        // ---- layer 1
+#pragma unroll
+        for (int kc = 0; kc < kF / 8; ++kc) {
+            uint4 hi, lo;
+            split8(xf + 8 * kc, hi, lo);
+            *reinterpret_cast<uint4*>(sm + kOffA1h + kmaj(t, kc, kTile)) = hi;
+            *reinterpret_cast<uint4*>(sm + kOffA1l + kmaj(t, kc, kTile)) = lo;
+        }
+        const int32_t next = tile + gridDim.x;
+        if (next < ntiles) load_feat(feat, next * kTile + t, rows, xf);  // in flight during this tile
+        fence_async_smem();
+        fence_before_sync();
+        __syncthreads();
+        if (t == 0) {
+            fence_after_sync();
+            mma_f16(d1, sdesc(a1h, 16 * kTile, 128), sdesc(w1, 16 * kH, 128), id64, 0u);
+            mma_f16(d1, sdesc(a1l, 16 * kTile, 128), sdesc(w1, 16 * kH, 128), id64, 1u);
+            mma_commit(bar);
+        }
+        failed = __syncthreads_or(!bar_wait(bar, phase));
+        phase ^= 1u;
+        if (failed) break;
+        fence_after_sync();
+        float v[kH];
+        tmem_ld64(lane_tmem + 0, v);
+#pragma unroll
+        for (int j = 0; j < kH; ++j) v[j] = fmaxf(v[j] + sbias[j], 0.f);
+        if (h1g && row < rows) {
+            float4* p = reinterpret_cast<float4*>(h1g + size_t(row) * kH);
+#pragma unroll
+            for (int j = 0; j < kH / 4; ++j) p[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+        }
+#pragma unroll
+        for (int kc = 0; kc < kH / 8; ++kc) {
+            uint4 hi, lo;
+            split8(v + 8 * kc, hi, lo);
+            *reinterpret_cast<uint4*>(sm + kOffA2h + kmaj(t, kc, kTile)) = hi;
+            *reinterpret_cast<uint4*>(sm + kOffA2l + kmaj(t, kc, kTile)) = lo;
+        }
+        // ---- layer 2
+        fence_async_smem();
+        fence_before_sync();
+        __syncthreads();
+        if (t == 0) {
+            fence_after_sync();
+#pragma unroll
+            for (int s = 0; s < kH / 16; ++s)
+                mma_f16(d2, sdesc(a2h + s * 2 * 16 * kTile, 16 * kTile, 128), sdesc(w2 + s * 2 * 16 * kH, 16 * kH, 128),
+                        id64, s > 0 ? 1u : 0u);
+#pragma unroll
+            for (int s = 0; s < kH / 16; ++s)
+                mma_f16(d2, sdesc(a2l + s * 2 * 16 * kTile, 16 * kTile, 128), sdesc(w2 + s * 2 * 16 * kH, 16 * kH, 128),
+                        id64, 1u);
+            mma_commit(bar);
+        }
+        failed = __syncthreads_or(!bar_wait(bar, phase));
+        phase ^= 1u;
+        if (failed) break;
+        fence_after_sync();
+        tmem_ld64(lane_tmem + kH, v);
+#pragma unroll
+        for (int j = 0; j < kH; ++j) v[j] = fmaxf(v[j] + sbias[kH + j], 0.f);
+        if (h2g && row < rows) {
+            float4* p = reinterpret_cast<float4*>(h2g + size_t(row) * kH);
+#pragma unroll
+            for (int j = 0; j < kH / 4; ++j) p[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+        }
+#pragma unroll
+        for (int kc = 0; kc < kH / 8; ++kc) {  // the layer-2 products are complete: reuse its operand
+            uint4 hi, lo;
+            split8(v + 8 * kc, hi, lo);
+            *reinterpret_cast<uint4*>(sm + kOffA2h + kmaj(t, kc, kTile)) = hi;
+            *reinterpret_cast<uint4*>(sm + kOffA2l + kmaj(t, kc, kTile)) = lo;
+        }
+        // ---- layer 3 (D1's columns were read above)
+        fence_async_smem();
+        fence_before_sync();
+        __syncthreads();
+        if (t == 0) {
+            fence_after_sync();
+#pragma unroll
+            for (int s = 0; s < kH / 16; ++s)
+                mma_f16(d3, sdesc(a2h + s * 2 * 16 * kTile, 16 * kTile, 128), sdesc(w3 + s * 2 * 16 * kN3, 16 * kN3, 128),
+                        id16, s > 0 ? 1u : 0u);
+#pragma unroll
+            for (int s = 0; s < kH / 16; ++s)
+                mma_f16(d3, sdesc(a2l + s * 2 * 16 * kTile, 16 * kTile, 128), sdesc(w3 + s * 2 * 16 * kN3, 16 * kN3, 128),
+                        id16, 1u);
+            mma_commit(bar);
+        }
+        failed = __syncthreads_or(!bar_wait(bar, phase));
+        phase ^= 1u;
+        if (failed) break;
+        fence_after_sync();
+        float o[kN3];
+        tmem_ld16(lane_tmem + 0, o);
+        if (row < rows) {
+            float4* p = reinterpret_cast<float4*>(out + size_t(row) * kO);
+            const float* b3 = sbias + 2 * kH;
+            p[0] = make_float4(o[0] + b3[0], o[1] + b3[1], o[2] + b3[2], o[3] + b3[3]);
+            p[1] = make_float4(o[4] + b3[4], o[5] + b3[5], o[6] + b3[6], o[7] + b3[7]);
+        }
+        fence_before_sync();  // the next tile's products overwrite columns read here
+    }
+    if (failed && t == 0) atomicExch(err, 1);
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after_sync();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+}  // namespace
+
+cudaError_t forward_tc(int32_t rows, const float* feat, const __nv_bfloat16* w, float* h1, float* h2, float* out,
+                       int* err, cudaStream_t stream) {
+    if (rows <= 0) return cudaSuccess;
+    int dev = 0, sms = 148, occ = 1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_forward_tc, kTcThreads, kSmemBytes);
+    if (e != cudaSuccess) return e;
+    occ = std::min(std::max(occ, 1), 512 / kTmemCols);
+    const int32_t ntiles = (rows + kTile - 1) / kTile;
+    const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sms) * occ)));
+    k_forward_tc<<<grid, kTcThreads, kSmemBytes, stream>>>(rows, feat, w, h1, h2, out, err);
+    return cudaGetLastError();
+}
+
+}  // namespace spai
+}  // namespace hpb

@@ -137,6 +137,14 @@ class SpaiNet:
         check(L.hpb_spai_assemble(self.h, C.byref(sysd), m.data_ptr()), "assemble")
         return m
 
+    def forward(self, torch, feat, path=1):
+        """The MLP alone on a (rows, 16) binary32 device tensor: (rows, 8)
+        outputs; path 1 the tcgen05 kernel, path 0 the warp-level mma.sync one."""
+        feat = feat.contiguous()
+        out = torch.empty((feat.shape[0], 8), dtype=torch.float32, device=feat.device)
+        check(L.hpb_spai_forward(self.h, feat.shape[0], feat.data_ptr(), out.data_ptr(), path), "forward")
+        return out
+
 
 def family(N: int, seed: int) -> problems.CSR:
     """The config-5 family: 3-D 7-point -div(kappa grad u), lognormal kappa,

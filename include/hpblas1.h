@@ -658,6 +658,12 @@ int hpb_spai_loss_grad(hpb_spai* net, const hpb_spai_system* sys, float w_frob, 
 int hpb_spai_loss(hpb_spai* net, const hpb_spai_system* sys, float w_frob, float w_resid, double* loss);
 /* Adam step on scale * accumulated gradient, then clears the accumulator. */
 int hpb_spai_adam(hpb_spai* net, float lr, float scale);
+/* The MLP alone: out (device, rows x 8) from feat (device, rows x 16),
+ * binary32.  path 1: the fifth-generation tensor-core kernel (tcgen05 with
+ * tensor-memory accumulators) that hpb_spai_assemble and training use;
+ * path 0: the warp-level mma.sync kernel, kept as a cross-check.  Blocking;
+ * HPB_ERROR_TIMEOUT if a bounded wait for the tensor cores gave up. */
+int hpb_spai_forward(hpb_spai* net, int32_t rows, const float* feat, float* out, int path);
 
 /* ---------------------------------------------------------------------- */
 /* Seeded input generators (host memory; no GPU needed)                    */

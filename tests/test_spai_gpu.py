@@ -52,6 +52,32 @@ def test_gradient_matches_cpu_oracle(gpu):
     net.close()
 
 
+@pytest.mark.parametrize("rows", [1, 127, 128, 129, 4999, 70001])
+def test_tcgen05_forward_matches_warp_kernel_and_oracle(gpu, rows):
+    """The tensor-memory MLP forward (128-row tiles, ragged last tile) against
+    the warp-level mma.sync kernel (the same bf16 hi/lo products in another
+    summation order: 2e-5 of the largest output) and the binary64 oracle
+    forward with the same bf16 weights (1e-4)."""
+    from oracle import spai_ref
+    ctx, torch = gpu
+    offs, dslot = spai.stencil7(8)
+    net = spai.SpaiNet(offs, dslot, seed=3)
+    rng = np.random.default_rng(rows)
+    w = (rng.standard_normal(spai.NUM_PARAMS) * 0.3).astype(np.float32)
+    net.set_weights(w)
+    X = rng.standard_normal((rows, 16)).astype(np.float32)
+    dX = dev(torch, X)
+    out_tc = host(net.forward(torch, dX, path=1)).astype(np.float64)
+    out_ws = host(net.forward(torch, dX, path=0)).astype(np.float64)
+    _, _, ref = spai_ref.forward(w, X.astype(np.float64))
+    scale = np.abs(ref).max()
+    assert np.abs(out_tc - ref).max() <= 1e-4 * scale
+    assert np.abs(out_tc - out_ws).max() <= 2e-5 * scale
+    # repeatable
+    assert np.array_equal(host(net.forward(torch, dX, path=1)).astype(np.float64), out_tc)
+    net.close()
+
+
 def test_untrained_network_is_jacobi(gpu):
     ctx, torch = gpu
     N = 8
