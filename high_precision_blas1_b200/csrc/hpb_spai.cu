@@ -688,6 +688,7 @@ struct hpb_spai {
     float *ahat = nullptr, *rh = nullptr;
     double* lpart = nullptr;
     int part_blocks = 0;
+    void* wimg = nullptr;        // the tcgen05 forward's weight image (rebuilt when wb changes)
     int* tc_err = nullptr;       // mapped pinned word: a tensor-core wait ran out of time
     int* tc_err_dev = nullptr;   // its device address
 };
@@ -782,7 +783,7 @@ int mlp_forward(hpb_spai* net, int32_t n, const float* feat, float* out, float* 
     using namespace hpb::spai;
     if (n <= 0) return HPB_SUCCESS;
     if (path == 1) {
-        if (forward_tc(n, feat, net->wb, h1, h2, out, net->tc_err_dev, nullptr) != cudaSuccess) return HPB_ERROR_CUDA;
+        if (forward_tc(n, feat, net->wimg, h1, h2, out, net->tc_err_dev, nullptr) != cudaSuccess) return HPB_ERROR_CUDA;
     } else {
         int occ = 1, dev = 0, sms = 148;
         cudaGetDevice(&dev);
@@ -911,7 +912,7 @@ int hpb_spai_create(hpb_spai** out, int nslot, int dslot, const int* offsets, ui
     if (cudaMalloc(&net->w, kNumParams * 4) || cudaMalloc(&net->wb, kNumParams * 2) ||
         cudaMalloc(&net->m1, kNumParams * 4) || cudaMalloc(&net->m2, kNumParams * 4) ||
         cudaMalloc(&net->grad, kNumParams * 4) || cudaMalloc(&net->gtmp, kNumParams * 4) ||
-        cudaMalloc(&net->part, size_t(kGridMlp) * kNumParams * 4)) {
+        cudaMalloc(&net->part, size_t(kGridMlp) * kNumParams * 4) || cudaMalloc(&net->wimg, kTcImageBytes)) {
         hpb_spai_destroy(net);
         return HPB_ERROR_OUT_OF_MEMORY;
     }
@@ -937,7 +938,7 @@ int hpb_spai_destroy(hpb_spai* net) {
     cudaDeviceSynchronize();
     void* ptrs[] = {net->w, net->wb, net->m1, net->m2, net->grad, net->gtmp, net->part, net->feat, net->h1, net->h2,
                     net->out, net->dout, net->diag, net->mval, net->dm, net->G, net->y, net->z, net->g, net->lpart,
-                    net->ahat, net->rh};
+                    net->ahat, net->rh, net->wimg};
     for (void* p : ptrs) cudaFree(p);
     if (net->tc_err) cudaFreeHost(net->tc_err);
     if (net->ctx) hpb_destroy(net->ctx);
@@ -952,8 +953,10 @@ int hpb_spai_set_weights(hpb_spai* net, const float* w_host) {
     std::vector<__nv_bfloat16> b(kNumParams);
     for (int i = 0; i < kNumParams; ++i) b[i] = __float2bfloat16(w_host[i]);
     if (cudaMemcpy(net->w, w_host, kNumParams * 4, cudaMemcpyHostToDevice) ||
-        cudaMemcpy(net->wb, b.data(), kNumParams * 2, cudaMemcpyHostToDevice))
+        cudaMemcpy(net->wb, b.data(), kNumParams * 2, cudaMemcpyHostToDevice) ||
+        hpb::spai::weight_image_tc(net->wb, net->wimg, nullptr) != cudaSuccess)
         return HPB_ERROR_CUDA;
+    hpb::count_launch();
     return HPB_SUCCESS;
 }
 
@@ -1096,8 +1099,10 @@ int hpb_spai_adam(hpb_spai* net, float lr, float scale) {
     ++net->step;
     k_adam<<<(kNumParams + 255) / 256, 256>>>(net->step, lr, scale, 0.9f, 0.999f, 1e-8f, net->w, net->m1, net->m2,
                                               net->grad, net->wb);
-    hpb::count_launch();
-    return cudaGetLastError() == cudaSuccess ? HPB_SUCCESS : HPB_ERROR_CUDA;
+    hpb::count_launch(2);
+    if (cudaGetLastError() != cudaSuccess || weight_image_tc(net->wb, net->wimg, nullptr) != cudaSuccess)
+        return HPB_ERROR_CUDA;
+    return HPB_SUCCESS;
 }
 
 }  // extern "C"

@@ -154,14 +154,20 @@ __device__ __forceinline__ uint32_t bf2(float a, float b) {  // a in the low hal
     return u;
 }
 
+// (a, b) -> hi = (bf16(a), bf16(b)), lo = (bf16(a - hi_a), bf16(b - hi_b)):
+// one paired conversion for the high parts, whose binary32 values are the
+// halves shifted into place
+__device__ __forceinline__ void split2(float a, float b, uint32_t& hi, uint32_t& lo) {
+    hi = bf2(a, b);
+    lo = bf2(a - __uint_as_float(hi << 16), b - __uint_as_float(hi & 0xFFFF0000u));
+}
+
 // eight consecutive activations of this row -> 16-byte hi and lo chunks
 __device__ __forceinline__ void split8(const float* x, uint4& hi, uint4& lo) {
-    float h[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) h[i] = __bfloat162float(__float2bfloat16_rn(x[i]));
-    hi = make_uint4(bf2(h[0], h[1]), bf2(h[2], h[3]), bf2(h[4], h[5]), bf2(h[6], h[7]));
-    lo = make_uint4(bf2(x[0] - h[0], x[1] - h[1]), bf2(x[2] - h[2], x[3] - h[3]), bf2(x[4] - h[4], x[5] - h[5]),
-                    bf2(x[6] - h[6], x[7] - h[7]));
+    split2(x[0], x[1], hi.x, lo.x);
+    split2(x[2], x[3], hi.y, lo.y);
+    split2(x[4], x[5], hi.z, lo.z);
+    split2(x[6], x[7], hi.w, lo.w);
 }
 
 __device__ __forceinline__ void load_feat(const float* __restrict__ feat, int32_t row, int32_t rows, float (&x)[kF]) {
@@ -181,30 +187,61 @@ __device__ __forceinline__ void load_feat(const float* __restrict__ feat, int32_
     }
 }
 
-__global__ void __launch_bounds__(kTcThreads)
-k_forward_tc(int32_t rows, const float* __restrict__ feat, const __nv_bfloat16* __restrict__ w, float* __restrict__ h1g,
-             float* __restrict__ h2g, float* __restrict__ out, int* err) {
+// The weights as the kernel's shared-memory image: the K-major B operands
+// (W^T: rows n, K contiguous; W3^T padded to 16 rows with zeros) in bytes
+// [0, kOffA1h) and the biases (binary32) after them; built once per weight
+// change, one element per thread.
+constexpr int kImgW = kOffA1h;                      // 12288 bytes of operands
+constexpr int kImgBias = (2 * kH + kO) * 4;         // 544 bytes
+static_assert(kImgW + kImgBias == kTcImageBytes && kImgW % 16 == 0 && kImgBias % 16 == 0, "image plan");
+constexpr int kImgElems = kH * kF + kH * kH + kN3 * kH + 2 * kH + kO;
+
+__global__ void k_weight_image(const __nv_bfloat16* __restrict__ w, unsigned char* __restrict__ img) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    auto put = [&](int off, int R, int n, int k, __nv_bfloat16 v) {
+        *reinterpret_cast<__nv_bfloat16*>(img + off + kmaj(n, k >> 3, R) + (k & 7) * 2) = v;
+    };
+    float* bias = reinterpret_cast<float*>(img + kImgW);
+    if (i < kH * kF) {
+        put(kOffW1, kH, i / kF, i % kF, w[Params::W1 + (i % kF) * kH + i / kF]);
+    } else if (i < kH * kF + kH * kH) {
+        const int j = i - kH * kF;
+        put(kOffW2, kH, j / kH, j % kH, w[Params::W2 + (j % kH) * kH + j / kH]);
+    } else if (i < kH * kF + kH * kH + kN3 * kH) {
+        const int j = i - kH * kF - kH * kH, n = j / kH, k = j % kH;
+        put(kOffW3, kN3, n, k, n < kO ? w[Params::W3 + k * kO + n] : __float2bfloat16_rn(0.f));
+    } else if (i < kImgElems) {
+        const int j = i - kH * kF - kH * kH - kN3 * kH;  // b1, b2, b3 in turn
+        bias[j] = __bfloat162float(w[Params::B1 + (j < kH ? j : j < 2 * kH ? kH * kH + j : kH * kH + kH * kO + j)]);
+    }
+}
+
+__global__ void __launch_bounds__(kTcThreads, 4)
+k_forward_tc(int32_t rows, const float* __restrict__ feat, const unsigned char* __restrict__ img,
+             float* __restrict__ h1g, float* __restrict__ h2g, float* __restrict__ out, int* err) {
     extern __shared__ __align__(1024) unsigned char sm[];
     const int t = threadIdx.x, warp = t >> 5;
     const uint32_t sbase = static_cast<uint32_t>(__cvta_generic_to_shared(sm));
     const uint32_t bar = sbase + kOffBar;
-    float* sbias = reinterpret_cast<float*>(sm + kOffBias);
+    const float* sbias = reinterpret_cast<const float*>(sm + kOffBias);
 
-    // ---- weights as the K-major B operands (W^T: rows n, K contiguous), biases
-    auto put = [&](int off, int R, int n, int k, __nv_bfloat16 v) {
-        *reinterpret_cast<__nv_bfloat16*>(sm + off + kmaj(n, k >> 3, R) + (k & 7) * 2) = v;
-    };
-    for (int i = t; i < kH * kF; i += kTcThreads) put(kOffW1, kH, i / kF, i % kF, w[Params::W1 + (i % kF) * kH + i / kF]);
-    for (int i = t; i < kH * kH; i += kTcThreads) put(kOffW2, kH, i / kH, i % kH, w[Params::W2 + (i % kH) * kH + i / kH]);
-    for (int i = t; i < kN3 * kH; i += kTcThreads) {
-        const int n = i / kH, k = i % kH;
-        put(kOffW3, kN3, n, k, n < kO ? w[Params::W3 + k * kO + n] : __float2bfloat16_rn(0.f));
+    // ---- the weight image: 16-byte loads, all issued before the stores
+    {
+        constexpr int NW = kImgW / 16, NB = kImgBias / 16, PER = (NW + NB + kTcThreads - 1) / kTcThreads;
+        const uint4* src = reinterpret_cast<const uint4*>(img);
+        uint4 v[PER];
+#pragma unroll
+        for (int r = 0; r < PER; ++r) {
+            const int q = t + r * kTcThreads;
+            if (q < NW + NB) v[r] = __ldg(src + q);
+        }
+#pragma unroll
+        for (int r = 0; r < PER; ++r) {
+            const int q = t + r * kTcThreads;
+            if (q < NW) *reinterpret_cast<uint4*>(sm + 16 * q) = v[r];
+            else if (q < NW + NB) *reinterpret_cast<uint4*>(sm + kOffBias + 16 * (q - NW)) = v[r];
+        }
     }
-    for (int i = t; i < kH; i += kTcThreads) {
-        sbias[i] = __bfloat162float(w[Params::B1 + i]);
-        sbias[kH + i] = __bfloat162float(w[Params::B2 + i]);
-    }
-    if (t < kO) sbias[2 * kH + t] = __bfloat162float(w[Params::B3 + t]);
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -349,19 +386,33 @@ k_forward_tc(int32_t rows, const float* __restrict__ feat, const __nv_bfloat16* 
 
 }  // namespace
 
-cudaError_t forward_tc(int32_t rows, const float* feat, const __nv_bfloat16* w, float* h1, float* h2, float* out,
-                       int* err, cudaStream_t stream) {
+cudaError_t weight_image_tc(const __nv_bfloat16* w, void* img, cudaStream_t stream) {
+    k_weight_image<<<(kImgElems + 255) / 256, 256, 0, stream>>>(w, static_cast<unsigned char*>(img));
+    return cudaGetLastError();
+}
+
+cudaError_t forward_tc(int32_t rows, const float* feat, const void* img, float* h1, float* h2, float* out, int* err,
+                       cudaStream_t stream) {
     if (rows <= 0) return cudaSuccess;
     int dev = 0, sms = 148, occ = 1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_forward_tc, kTcThreads, kSmemBytes);
+    // the whole unified L1 as shared memory: four blocks per SM (with the
+    // default split the occupancy query, and the launch, gave one)
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_forward_tc, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 int(cudaSharedmemCarveoutMaxShared));
     if (e != cudaSuccess) return e;
-    occ = std::min(std::max(occ, 1), 512 / kTmemCols);
+    // four blocks per SM: shared memory bounds residency to four, whose 4 x
+    // 128 tensor-memory columns fill the SM's 512 (the occupancy query
+    // reports one block for this kernel, which left three quarters of the
+    // SM idle)
+    occ = 512 / kTmemCols;
     const int32_t ntiles = (rows + kTile - 1) / kTile;
     const int grid = int(std::max<int64_t>(1, std::min<int64_t>(ntiles, int64_t(sms) * occ)));
-    k_forward_tc<<<grid, kTcThreads, kSmemBytes, stream>>>(rows, feat, w, h1, h2, out, err);
+    k_forward_tc<<<grid, kTcThreads, kSmemBytes, stream>>>(rows, feat, static_cast<const unsigned char*>(img), h1, h2,
+                                                           out, err);
     return cudaGetLastError();
 }
 
