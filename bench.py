@@ -835,6 +835,7 @@ def bench_forms(torch, log=lambda *a: None):
             net.assemble(torch, D5)  # warm-up (module load, workspace)
             tb, M = _timed(torch, lambda: net.assemble(torch, D5))
             res["spai_build"] = spai_build_roofline(A, tb)
+            res["spai_build"]["mlp_forward"] = mlp_probe(torch, net, A.n)
             t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond="matrix", M=M, inner_tol=0.0, max_iters=0,
                                    max_refinements=1000)
             res["fp32_dot2_gmres30_refined_learned_spai"] = {
@@ -911,6 +912,32 @@ def spai_build_roofline(A, t):
     alg = 3 * a_pass + 2 * 64.0 * A.n + 2 * 32.0 * A.n + 4.0 * A.nnz
     return {"s": t, "algorithmic_bytes": alg, "achieved_GBs": alg / t / 1e9, "frac_of_hbm": alg / t / 1e9 / hbm,
             "mlp_gflop": 2.0 * A.n * (16 * 64 + 64 * 64 + 64 * 8) / 1e9}
+
+
+def mlp_probe(torch, net, rows, reps=20):
+    """The learned SPAI's MLP alone (hpb_spai_forward) on `rows` rows of
+    seeded features: the tcgen05 kernel the build uses against the warp-level
+    mma.sync kernel, device time per launch from CUDA events over `reps`
+    back-to-back calls (each call synchronises on return, so the figure
+    includes one launch gap per call); the products' flops over the time of
+    the tcgen05 kernel against the measured dense bf16 peak (the activations
+    go through the tensor cores as bf16 hi/lo pairs: two products per
+    layer)."""
+    feat = torch.from_numpy(np.random.default_rng(5).standard_normal((rows, 16)).astype(np.float32)).cuda()
+    out = {"rows": rows}
+    for path, name in ((1, "tcgen05"), (0, "mma_sync")):
+        for _ in range(3):
+            net.forward(torch, feat, path)
+        us = _events_us(torch, lambda i: net.forward(torch, feat, path), reps, rounds=1)
+        out[f"{name}_us"] = us
+    try:
+        bf16_peak = float(json.loads(PEAKS_FILE.read_text())["bf16_tflops"])  # burst: a kernel timed alone
+    except Exception:
+        bf16_peak = None
+    flop = 2.0 * 2.0 * rows * (16 * 64 + 64 * 64 + 64 * 16)  # hi and lo products, layer 3 padded to N = 16
+    out["tcgen05_tensor_TFLOPs"] = flop / (out["tcgen05_us"] * 1e-6) / 1e12
+    out["tcgen05_frac_of_bf16_peak"] = out["tcgen05_tensor_TFLOPs"] / bf16_peak if bf16_peak else None
+    return out
 
 
 def ilu0_probe(torch, A, reps=10):
@@ -1231,6 +1258,9 @@ def main():
     ap.add_argument("--profile-spai", type=int, default=0, metavar="K",
                     help="profiling aid: K learned-SPAI builds (features, MLP, assembly) on the config-5 96^3 "
                          "system, then exit")
+    ap.add_argument("--profile-mlp", type=int, default=0, metavar="K",
+                    help="profiling aid: K launches each of the learned SPAI's MLP forward (tcgen05 and mma.sync "
+                         "kernels) on 884,736 rows of seeded features (the config-5 row count), then exit")
     ap.add_argument("--profile-method", choices=["bicgstabl", "gmres", "complex"], default="bicgstabl",
                     help="with --profile-solve: BiCGStab(4) on the config-2 system, or GMRES(30) + Jacobi on the "
                          "config-5 lognormal 96^3 system")
@@ -1290,6 +1320,15 @@ def main():
         net.close()
         r = spai_build_roofline(A, t / args.profile_spai)
         print(f"profile spai: {r['s'] * 1e3:.3f} ms per build, {r['achieved_GBs']:.0f} GB/s algorithmic")
+        return
+    if args.profile_mlp > 0:
+        from high_precision_blas1_b200 import spai
+        offs, dslot = spai.stencil7(96)
+        net = spai.SpaiNet(offs, dslot)
+        net.set_weights(np.load(spai.WEIGHTS_FILE))
+        r = mlp_probe(torch, net, 96 ** 3, reps=args.profile_mlp)
+        net.close()
+        print(f"profile mlp: tcgen05 {r['tcgen05_us']:.1f} us, mma.sync {r['mma_sync_us']:.1f} us per call")
         return
     if args.profile_spmv_dot2 > 0:
         from high_precision_blas1_b200 import Context, _lib
