@@ -72,10 +72,12 @@ __device__ __forceinline__ int slot_of(const Offsets& o, int d) {
 __device__ __forceinline__ float inv_sqrt_dd(float di, float dj) { return 1.f / sqrtf(fabsf(di * dj)); }
 
 __global__ void k_features(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                           const float* __restrict__ val, const float* __restrict__ diag, float mean_log_diag,
-                           Offsets o, float* __restrict__ feat) {
+                           const float* __restrict__ val, const float* __restrict__ diag,
+                           const double* __restrict__ lsum, Offsets o, float* __restrict__ feat) {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
+    // mean log|a_ii| from the device-side Sum2 of the logs (lsum[0])
+    const float mean_log_diag = float(lsum[0] / double(rows > 1 ? rows : 1));
     float f[kF];
 #pragma unroll
     for (int k = 0; k < kF; ++k) f[k] = 0.f;
@@ -728,14 +730,16 @@ int grow(hpb_spai* net, int32_t rows, int64_t nnz) {
 
 
 // diag of a binary32 CSR
+// diag(A) (binary32) and log|a_ii| (binary64, for the mean over the rows)
 __global__ void k_fdiag(int32_t rows, const int32_t* __restrict__ rp, const int32_t* __restrict__ ci,
-                        const float* __restrict__ val, float* __restrict__ d) {
+                        const float* __restrict__ val, float* __restrict__ d, double* __restrict__ logs) {
     const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
     float v = 0.f;
     for (int32_t k = rp[r]; k < rp[r + 1]; ++k)
         if (ci[k] == r) v = val[k];
     d[r] = v;
+    logs[r] = log(fabs(double(v)));
 }
 __global__ void k_sub(int32_t n, float* __restrict__ z, const float* __restrict__ r) {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -762,20 +766,7 @@ double host_sum(const double* dpart, int nb) {
     return s;
 }
 
-__global__ void k_logabs(int32_t n, const float* __restrict__ d, double* __restrict__ out) {
-    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = log(fabs(double(d[i])));
-}
 
-// mean log|diag| over the rows: binary64 logs summed with Sum2 (deterministic)
-int mean_log_diag(hpb_spai* net, int32_t n, const float* diag, double* scratch, double* mean) {
-    k_logabs<<<(n + 255) / 256, 256>>>(n, diag, scratch);
-    hpb::count_launch();
-    double r[2] = {0.0, 0.0};
-    const int st = hpb_sum2_f64_host(net->ctx, n, scratch, r);
-    *mean = r[0] / std::max(1, n);
-    return st;
-}
 
 // The MLP on n rows of features: path 1 the tcgen05 kernel (hpb_spai_tc.cu),
 // path 0 the warp-level mma.sync kernel (k_forward).
@@ -807,18 +798,20 @@ int take_tc_status(hpb_spai* net) {
 
 // Features and the MLP forward pass of one system (binary32 CSR, device),
 // into feat / out; diag receives diag(A).  h1, h2 (post-ReLU) are kept for
-// the backward pass when not null.
+// the backward pass when not null.  scratch: n + 2 doubles (device).
 int forward_rows(hpb_spai* net, const hpb_spai_system& sys, float* diag, float* feat, float* out, float* h1, float* h2,
                  double* scratch) {
     using namespace hpb::spai;
     const int32_t n = sys.rows;
     const int gb = (n + 255) / 256;
-    k_fdiag<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, diag);
+    // diag(A) and log|a_ii|; their sum by Sum2 (deterministic) stays on the
+    // device in lsum[0..1] (hi, lo) for k_features: no host round trip
+    k_fdiag<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, diag, scratch);
     hpb::count_launch();
-    double ml = 0.0;
-    int st = mean_log_diag(net, n, diag, scratch, &ml);
+    double* lsum = scratch + n;
+    int st = hpb_sum2_f64(net->ctx, n, scratch, lsum);
     if (st) return st;
-    k_features<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, diag, float(ml), net->off, feat);
+    k_features<<<gb, 256>>>(n, sys.row_ptr, sys.col_ind, sys.val, diag, lsum, net->off, feat);
     hpb::count_launch();
     return mlp_forward(net, n, feat, out, h1, h2, 1);
 }
@@ -829,7 +822,7 @@ int forward_system(hpb_spai* net, const hpb_spai_system& sys) {
     const int32_t n = sys.rows;
     int st = grow(net, n, sys.nnz);
     if (st) return st;
-    double* scratch = static_cast<double*>(hpb::fused::pool_alloc(size_t(n ? n : 1) * sizeof(double), nullptr));
+    double* scratch = static_cast<double*>(hpb::fused::pool_alloc((size_t(n) + 2) * sizeof(double), nullptr));
     if (!scratch) return HPB_ERROR_OUT_OF_MEMORY;
     st = forward_rows(net, sys, net->diag, net->feat, net->out, net->h1, net->h2, scratch);
     hpb::fused::pool_free(scratch, nullptr);
@@ -979,7 +972,7 @@ int hpb_spai_assemble(hpb_spai* net, const hpb_spai_system* sys, float* m_val) {
     float* diag = static_cast<float*>(pool_alloc(R * 4, nullptr));
     float* feat = static_cast<float*>(pool_alloc(R * kF * 4, nullptr));
     float* out = static_cast<float*>(pool_alloc(R * kO * 4, nullptr));
-    double* scratch = static_cast<double*>(pool_alloc(R * 8, nullptr));
+    double* scratch = static_cast<double*>(pool_alloc((R + 2) * 8, nullptr));
     int st = (diag && feat && out && scratch) ? HPB_SUCCESS : HPB_ERROR_OUT_OF_MEMORY;
     if (st == HPB_SUCCESS) st = forward_rows(net, *sys, diag, feat, out, nullptr, nullptr, scratch);
     if (st == HPB_SUCCESS) {
