@@ -833,8 +833,10 @@ def bench_forms(torch, log=lambda *a: None):
             net.set_weights(np.load(wfile))
             D5 = spai.DeviceCSR(torch, A)  # the matrix on the device before the timed build
             net.assemble(torch, D5)  # warm-up (module load, workspace)
-            tb, M = _timed(torch, lambda: net.assemble(torch, D5))
+            builds = [_timed(torch, lambda: net.assemble(torch, D5)) for _ in range(5)]
+            tb, M = float(np.median([t for t, _ in builds])), builds[-1][1]
             res["spai_build"] = spai_build_roofline(A, tb)
+            res["spai_build"]["builds_s"] = [t for t, _ in builds]
             res["spai_build"]["mlp_forward"] = mlp_probe(torch, net, A.n)
             t, st, r, x = ir_solve(torch, A, b, "gmres", 30, precond="matrix", M=M, inner_tol=0.0, max_iters=0,
                                    max_refinements=1000)
