@@ -375,7 +375,7 @@ k_forward_tc(int32_t rows, const float* __restrict__ feat, const unsigned char* 
         }
         fence_before_sync();  // the next tile's products overwrite columns read here
     }
-    if (failed && t == 0) atomicExch(err, 1);
+    if (failed && t == 0) *reinterpret_cast<volatile int*>(err) = 1;  // a plain store: err may be mapped host memory
     fence_before_sync();
     __syncthreads();
     if (warp == 0) {
