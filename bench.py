@@ -216,7 +216,9 @@ def ref_solver(args, cores):
     A, b = solver_problem(0)
     iters = ref_full_iters()
     per_step_cycles = 4
-    ref_cpu_cycles_sample(A, b, 1)  # warm-up
+    warm = max(3, args.warmup)
+    for _ in range(warm):  # warm-up samples of one cycle each
+        ref_cpu_cycles_sample(A, b, 1)
     t = []
     for _ in range(args.steps):
         sec_per_cycle, _ = ref_cpu_cycles_sample(A, b, per_step_cycles)
@@ -226,7 +228,7 @@ def ref_solver(args, cores):
     value = sec_per_cycle * (full / SOLVER_L) if full else None
     return {
         "impl": "reference", "metric": "time_to_1e-10_residual", "value": value, "unit": "s",
-        "higher_is_better": False, "n_gpus": 0, "steps": args.steps, "warmup": 1,
+        "higher_is_better": False, "n_gpus": 0, "steps": args.steps, "warmup": warm,
         "ms_per_step": sec_per_cycle * per_step_cycles * 1e3, "dtype": "f64", "data": "synthetic",
         "config": solver_config(),
         "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "reference",
