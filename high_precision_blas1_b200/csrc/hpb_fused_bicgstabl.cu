@@ -84,7 +84,44 @@ struct EpiArgs {
     BcgState<S>* st;
     Report* rep;
     int kind, k, j, L;
+    // EPI_FINAL inside the loop graph: the monitor's test and the loop's
+    // condition (monitor_step) after the cycle's report is complete
+    MonState* mon = nullptr;
+    double* hist = nullptr;
+    cudaGraphConditionalHandle cond = 0;
 };
+
+// End of a cycle inside the loop graph: the host loop's test, then the
+// loop's condition.  Every path reaches the one cudaGraphSetConditional
+// call, and the loop stops after chunk_left cycles whatever the test says,
+// so one launch of the graph always ends.
+__device__ inline void monitor_step(MonState* M, const Report* rep, double* hist, int L, cudaGraphConditionalHandle h) {
+    const int it = M->iters + L;
+    M->iters = it;
+    int fin;
+    if (rep->breakdown) {
+        M->breakdown = 1;
+        fin = 1;
+    } else {
+        const double rn = rep->rnorm;
+        const int valid = !rep->nonfinite && isfinite(rn);
+        const int conv = valid && rn <= M->tol;
+        M->rn = rn;
+        M->valid = valid;
+        M->conv = conv;
+        const int k = M->hl;
+        if (k < kLoopChunk) {
+            hist[2 * k] = double(it);
+            hist[2 * k + 1] = rn;
+            M->hl = k + 1;
+        }
+        fin = !valid || conv || it >= M->max_iters;
+    }
+    M->finished = fin;
+    const int left = M->chunk_left - 1;
+    M->chunk_left = left;
+    cudaGraphSetConditional(h, (fin || left <= 0) ? 0u : 1u);
+}
 
 template <class S>
 __device__ void run_epi(const EpiArgs<S>& a, const S* v, bool bad) {
@@ -127,6 +164,7 @@ __device__ void run_epi(const EpiArgs<S>& a, const S* v, bool bad) {
             if (s_is_zero(st.rho)) a.rep->breakdown = 1;
             st.beta = s_div(s_mul(st.alpha, v[0]), st.rho);
             st.rho = v[0];
+            if (a.mon) monitor_step(a.mon, a.rep, a.hist, a.L, a.cond);
             break;
         }
         default:
@@ -707,38 +745,6 @@ inline bool fused_plain_graph() {
     return v != nullptr && v[0] == '1';
 }
 
-// End of a cycle inside the loop graph: the host loop's test, then the
-// loop's condition.  Every path reaches the one cudaGraphSetConditional
-// call, and the loop stops after chunk_left cycles whatever the test says,
-// so one launch of the graph always ends.
-__global__ void k_monitor(MonState* M, const Report* rep, double* hist, int L, cudaGraphConditionalHandle h) {
-    const int it = M->iters + L;
-    M->iters = it;
-    int fin;
-    if (rep->breakdown) {
-        M->breakdown = 1;
-        fin = 1;
-    } else {
-        const double rn = rep->rnorm;
-        const int valid = !rep->nonfinite && isfinite(rn);
-        const int conv = valid && rn <= M->tol;
-        M->rn = rn;
-        M->valid = valid;
-        M->conv = conv;
-        const int k = M->hl;
-        if (k < kLoopChunk) {
-            hist[2 * k] = double(it);
-            hist[2 * k + 1] = rn;
-            M->hl = k + 1;
-        }
-        fin = !valid || conv || it >= M->max_iters;
-    }
-    M->finished = fin;
-    const int left = M->chunk_left - 1;
-    M->chunk_left = left;
-    cudaGraphSetConditional(h, (fin || left <= 0) ? 0u : 1u);
-}
-
 template <class E>
 BcgPlan<E>::BcgPlan() = default;
 template <class E>
@@ -893,16 +899,17 @@ int BcgPlan<E>::init(const hpb_solver_params* p, int32_t rows, int64_t nnz, cons
                            k == 2 ? V.u[L] : nullptr);
         kernels += 2;
     }
-    launch_final<E>(L, g_red, s, n, 1, V, x, rt, st, partials, ticket, badflag,
-                    EpiArgs<S>{st, drep, EPI_FINAL, 0, 0, L}, L == 1 ? 1 : 0);
-    if (P.plain_graph) {
-        kernels += 1;
-        if (cudaStreamEndCapture(s, &ws.graph) != cudaSuccess) return HPB_ERROR_CUDA;
-    } else {
-        k_monitor<<<1, 1, 0, s>>>(P.mon, drep, P.dhist, L, cond);
-        kernels += 2;
-        if (cudaStreamEndCapture(s, &body) != cudaSuccess) return HPB_ERROR_CUDA;
+    // the closing update; in the loop graph its last block also runs the
+    // monitor's test and sets the loop's condition
+    EpiArgs<S> fin{st, drep, EPI_FINAL, 0, 0, L};
+    if (!P.plain_graph) {
+        fin.mon = P.mon;
+        fin.hist = P.dhist;
+        fin.cond = cond;
     }
+    launch_final<E>(L, g_red, s, n, 1, V, x, rt, st, partials, ticket, badflag, fin, L == 1 ? 1 : 0);
+    kernels += 1;
+    if (cudaStreamEndCapture(s, P.plain_graph ? &ws.graph : &body) != cudaSuccess) return HPB_ERROR_CUDA;
     if (cudaGraphInstantiate(&ws.exec, ws.graph, 0) != cudaSuccess) return HPB_ERROR_CUDA;
     P.kernels = kernels;
     return HPB_SUCCESS;
