@@ -99,6 +99,43 @@ def test_fused_other_types(gpu, t):
     assert true_rel(A, b, x) <= (1.05 if t == "c128" else 20) * tol
 
 
+@pytest.mark.parametrize("t,L,precond", [("c128", 1, "none"), ("c128", 3, "jacobi"), ("f32", 1, "jacobi"),
+                                          ("c64", 5, "none"), ("f64", 3, "jacobi"), ("f64", 7, "none")])
+def test_fused_deferred_updates_match_dropin(gpu, t, L, precond):
+    """The cycle's deferred r updates (each BiCG step's r_j applied by the
+    next step's kernel, the last step's by the second MR sweep or, for
+    l = 1, by the closing update) and the first MR sweep's sums formed in
+    the last step's kernel, across element types, basis sizes and the
+    Jacobi scaling: the fused solve against the drop-in path.  The
+    residual histories agree while far from the rounding floor; the
+    iteration counts within two cycles or 3 % (with l = 1 the indefinite
+    complex Helmholtz operator, and binary32 storage near its rounding
+    floor, drift by two iterations between reduction orders)."""
+    ctx, torch = gpu
+    if t.startswith("c"):
+        A = problems.helmholtz2d(40)
+        b = problems.rhs_uniform(A.n, 21, complex_=True)
+    else:
+        A = problems.convdiff2d(40)
+        b = problems.rhs_uniform(A.n, 21)
+    tol = 1e-6 if t in ("f32", "c64") else 1e-10
+    pf = _lib.solver_params("bicgstabl", basis=L, rel_tol=tol, max_iters=50000, precond=precond, fused=True)
+    pp = _lib.solver_params("bicgstabl", basis=L, rel_tol=tol, max_iters=50000, precond=precond)
+    st1, r1, x1, h1 = solve(torch, t, A, b, pf, hist_cap=10000)
+    st2, r2, x2, h2 = solve(torch, t, A, b, pp, hist_cap=10000)
+    assert st1 == 0 and st2 == 0, (st1, st2, r1.iters, r2.iters)
+    k = min(h1.shape[0], h2.shape[0], 4)
+    assert np.allclose(h1[:k, 1], h2[:k, 1], rtol=1e-3 if t in ("f32", "c64") else 1e-6), (h1[:k], h2[:k])
+    assert abs(r1.iters - r2.iters) <= max(2 * L, 0.03 * r2.iters), (r1.iters, r2.iters)
+    # binary64: the tolerance on the true residual; binary32 storage: no
+    # further from it than the drop-in solve (whose recursive residual drifts
+    # from the true one the same way at large l)
+    if t in ("f32", "c64"):
+        assert true_rel(A, b, x1) <= max(20 * tol, 2 * true_rel(A, b, x2))
+    else:
+        assert true_rel(A, b, x1) <= 1.05 * tol
+
+
 def test_fused_not_converged_and_unsupported(gpu):
     ctx, torch = gpu
     A = problems.convdiff2d(32)
